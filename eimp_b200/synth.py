@@ -1,0 +1,215 @@
+"""Seeded synthetic reference panels and targets (Li-Stephens mosaics).
+
+The reference's headline configurations are quoted on real panels that are not
+available here, so every run uses seeded synthetic data of the same shape:
+
+* ``F`` founder haplotypes; per-site founder allele frequency ``f`` drawn from a
+  1/x site-frequency spectrum on ``[maf_min, 0.5]`` (inverse CDF
+  ``f = maf_min * (0.5/maf_min)**u``), a random half of the sites flipped to the
+  alternative-major side; founder alleles ~ Bernoulli(f).
+* site positions uniform-sorted over the segment, a linear genetic map of
+  ``cm_per_mb`` cM/Mb.
+* every reference and target haplotype is a mosaic of founders: it switches to a
+  uniformly drawn founder with probability ``1 - exp(-lambda * d_cM)`` between
+  consecutive sites (lambda = 1/``mean_segment_cm``), and each copied allele is
+  flipped with the copying error probability.
+* targets are held-out mosaics given as unphased genotypes 0/1/2 at a random
+  subset of the panel sites ("typed" sites) with a per-target missing rate
+  (genotype code 3).
+
+The data of one configuration is cached as ``.npz`` under ``$EIMP_CACHE``
+(default ``/tmp/eimp_cache``) keyed by all generator parameters.
+"""
+from __future__ import annotations
+
+import dataclasses
+import hashlib
+import json
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .bits import W, pack_rows
+
+
+@dataclass(frozen=True)
+class TargetGroup:
+    ntargets: int
+    typed_frac: float          # fraction of panel sites typed in this group
+    miss_lo: float             # per-target missing rate drawn from U(miss_lo, miss_hi)
+    miss_hi: float
+
+
+@dataclass(frozen=True)
+class SynthConfig:
+    name: str
+    nhaps: int                 # reference haplotypes (even: diploid samples)
+    nsites: int                # reference sites (Mref)
+    segment_mb: float
+    founders: int
+    groups: tuple = ()
+    K: int = 1024
+    beam: int = 64
+    maf_min: float = 5e-4
+    cm_per_mb: float = 1.0
+    mean_segment_cm: float = 1.0
+    copy_err: float = 1e-3
+    seed: int = 1
+
+    def key(self) -> str:
+        d = dataclasses.asdict(self)
+        return hashlib.sha1(json.dumps(d, sort_keys=True, default=str).encode()).hexdigest()[:16]
+
+
+CONFIGS = {
+    # unit-test sized
+    "tiny": SynthConfig("tiny", nhaps=200, nsites=3000, segment_mb=1.0, founders=20,
+                        groups=(TargetGroup(6, 0.2, 0.01, 0.01),), K=64, beam=16, seed=7),
+    "small-test": SynthConfig("small-test", nhaps=600, nsites=8000, segment_mb=2.0, founders=40,
+                              groups=(TargetGroup(8, 0.1, 0.01, 0.01),), K=200, beam=32, seed=11),
+    # configs of the reference's headline workloads
+    "cfg1": SynthConfig("cfg1", nhaps=5000, nsites=20000, segment_mb=5.0, founders=200,
+                        groups=(TargetGroup(100, 0.10, 0.01, 0.01),), K=1024, beam=64, seed=1001),
+    "cfg2": SynthConfig("cfg2", nhaps=10000, nsites=100000, segment_mb=20.0, founders=500,
+                        groups=(TargetGroup(1000, 0.05, 0.02, 0.02),), K=4096, beam=128, seed=1002),
+    "cfg3": SynthConfig("cfg3", nhaps=20000, nsites=400000, segment_mb=40.0, founders=1000,
+                        groups=(TargetGroup(3334, 0.01, 0.0, 0.05), TargetGroup(3333, 0.03, 0.0, 0.05),
+                                TargetGroup(3333, 0.08, 0.0, 0.05)), K=4096, beam=128, seed=1003),
+}
+
+
+@dataclass
+class Panel:
+    """A reference panel in the reference's in-memory layouts."""
+    nhaps: int
+    nsites: int
+    pos: np.ndarray            # int64 (Mref,) 0-based bp positions
+    cm: np.ndarray             # float64 (Mref,) genetic positions
+    af: np.ndarray             # float32 (Mref,) alt allele frequency in the panel
+    hapmajor: np.ndarray       # uint64 (nhaps, W(Mref))  one row per haplotype
+    sitemajor: np.ndarray      # uint64 (Mref, W(nhaps))  one row per site (referenceFullT)
+
+
+@dataclass
+class Targets:
+    """One group of targets sharing a typed-site set."""
+    typed: np.ndarray          # int64 (M,) indices into the panel sites, ascending
+    gt: np.ndarray             # uint8 (ntargets, M) 0/1/2, 3 = missing
+    truth: np.ndarray          # uint8 (2*ntargets, M) true haplotypes at typed sites
+
+
+def _mosaic_block(rng, founders_T, cm, nhap, mean_seg, copy_err):
+    """Return (nhap, nsites) uint8 mosaics of the founder matrix (nsites, F)."""
+    nsites, F = founders_T.shape
+    glen = float(cm[-1] - cm[0])
+    out = np.empty((nhap, nsites), dtype=np.uint8)
+    cols = np.arange(nsites)
+    for h in range(nhap):
+        nsw = rng.poisson(glen / mean_seg)
+        x = np.sort(rng.uniform(cm[0], cm[-1], nsw))
+        brk = np.searchsorted(cm, x, side="left")
+        brk = np.concatenate(([0], brk, [nsites]))
+        lens = np.diff(brk)
+        fid = rng.integers(0, F, len(lens))
+        fidx = np.repeat(fid, lens)
+        row = founders_T[cols, fidx]
+        nerr = rng.binomial(nsites, copy_err)
+        if nerr:
+            e = rng.integers(0, nsites, nerr)
+            row[e] ^= 1
+        out[h] = row
+    return out
+
+
+def _cache_dir() -> str:
+    d = os.environ.get("EIMP_CACHE", "/tmp/eimp_cache")
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def generate(cfg: SynthConfig | str, cache: bool = True):
+    """Generate (or load from cache) ``(panel, [targets per group])``."""
+    if isinstance(cfg, str):
+        cfg = CONFIGS[cfg]
+    path = os.path.join(_cache_dir(), f"{cfg.name}-{cfg.key()}.npz")
+    if cache and os.path.exists(path):
+        z = np.load(path)
+        panel = Panel(cfg.nhaps, cfg.nsites, z["pos"], z["cm"], z["af"], z["hapmajor"], z["sitemajor"])
+        groups = [Targets(z[f"typed{g}"], z[f"gt{g}"], z[f"truth{g}"]) for g in range(len(cfg.groups))]
+        return panel, groups
+
+    rng = np.random.default_rng(cfg.seed)
+    n = cfg.nsites
+    L = int(cfg.segment_mb * 1e6)
+    pos = np.sort(rng.integers(0, L - n, n)) + np.arange(n)
+    cm = pos.astype(np.float64) * (cfg.cm_per_mb / 1e6)
+    u = rng.uniform(0.0, 1.0, n)
+    f = cfg.maf_min * (0.5 / cfg.maf_min) ** u
+    flip = rng.uniform(0.0, 1.0, n) < 0.5
+    f = np.where(flip, 1.0 - f, f)
+    founders_T = (rng.uniform(0.0, 1.0, (n, cfg.founders)) < f[:, None]).astype(np.uint8)
+
+    # reference haplotypes, generated in blocks of 512 (a multiple of 64 so that
+    # the site-major words of a block are whole words)
+    nh = cfg.nhaps
+    hap_w = W(n)
+    site_w = W(nh)
+    hapmajor = np.zeros((nh, hap_w), dtype=np.uint64)
+    sitemajor = np.zeros((n, site_w), dtype=np.uint64)
+    ac = np.zeros(n, dtype=np.int64)
+    blk = 512
+    for b0 in range(0, nh, blk):
+        b1 = min(nh, b0 + blk)
+        block = _mosaic_block(rng, founders_T, cm, b1 - b0, cfg.mean_segment_cm, cfg.copy_err)
+        ac += block.sum(axis=0, dtype=np.int64)
+        hapmajor[b0:b1] = pack_rows(block, hap_w)
+        sm = np.packbits(np.ascontiguousarray(block.T), axis=1, bitorder="little")
+        nbytes = sm.shape[1]
+        sm_pad = np.zeros((n, ((nbytes + 7) // 8) * 8), dtype=np.uint8)
+        sm_pad[:, :nbytes] = sm
+        words = sm_pad.view("<u8")
+        sitemajor[:, b0 // 64: b0 // 64 + words.shape[1]] = words
+    af = (ac / float(nh)).astype(np.float32)
+    panel = Panel(nh, n, pos.astype(np.int64), cm, af, hapmajor, sitemajor)
+
+    groups = []
+    for g in cfg.groups:
+        m = max(2, int(round(g.typed_frac * n)))
+        typed = np.sort(rng.choice(n, m, replace=False)).astype(np.int64)
+        haps = _mosaic_block(rng, founders_T, cm, 2 * g.ntargets, cfg.mean_segment_cm, cfg.copy_err)
+        th = haps[:, typed]
+        gt = (th[0::2].astype(np.uint8) + th[1::2]).astype(np.uint8)
+        for t in range(g.ntargets):
+            rate = rng.uniform(g.miss_lo, g.miss_hi) if g.miss_hi > g.miss_lo else g.miss_lo
+            nmiss = int(round(rate * m))
+            if nmiss:
+                gt[t, rng.choice(m, nmiss, replace=False)] = 3
+        groups.append(Targets(typed, gt, th))
+
+    if cache:
+        kw = dict(pos=panel.pos, cm=panel.cm, af=panel.af, hapmajor=panel.hapmajor, sitemajor=panel.sitemajor)
+        for i, t in enumerate(groups):
+            kw[f"typed{i}"] = t.typed
+            kw[f"gt{i}"] = t.gt
+            kw[f"truth{i}"] = t.truth
+        tmp = path + ".tmp.npz"
+        np.savez(tmp, **kw)
+        os.replace(tmp, path)
+    return panel, groups
+
+
+def typed_views(panel: Panel, typed: np.ndarray):
+    """Typed-site views of a panel, as the reference's VCFData keeps them.
+
+    Returns ``(ref_hapmajor_typed (nhaps, W(M)), ref_sitemajor_typed (M, W(nhaps)),
+    cm_typed float32 (M,))`` -- ``reference``, ``referenceT`` and ``cMs``
+    (VCFData.h:199-205, 227).
+    """
+    from .bits import unpack_rows
+    M = len(typed)
+    sitemajor_typed = np.ascontiguousarray(panel.sitemajor[typed])
+    dense = unpack_rows(sitemajor_typed, panel.nhaps)       # (M, nhaps)
+    hapmajor_typed = pack_rows(np.ascontiguousarray(dense.T), W(M))
+    cm_typed = panel.cm[typed].astype(np.float32)
+    return hapmajor_typed, sitemajor_typed, cm_typed

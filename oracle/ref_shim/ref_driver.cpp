@@ -1,0 +1,319 @@
+/*
+ * Test-oracle driver: a C ABI over the reference's OWN hot-path classes
+ * (Target, PBWT, Beam, TargetImp, PBWTImputer), compiled from the read-only
+ * reference sources by oracle/Makefile into oracle/_ref/libeimp_refcore.so.
+ *
+ * This file is test infrastructure written for this project.  It is used by
+ * tests/ (to pin the oracle restatement and to make golden fixtures) and by
+ * bench.py's CPU-baseline leg; the product never links it.
+ *
+ * The reference keeps intermediate results in private members; the driver
+ * reads them by compiling the reference headers with private/protected
+ * mapped to public (only inside this translation unit).
+ */
+#include <cstdint>
+#include <cstring>
+#include <cstdlib>
+#include <cmath>
+#include <cassert>
+#include <string>
+#include <vector>
+#include <list>
+#include <map>
+#include <unordered_map>
+#include <array>
+#include <utility>
+#include <memory>
+#include <atomic>
+#include <mutex>
+#include <functional>
+#include <algorithm>
+#include <stdexcept>
+#include <iostream>
+#include <iomanip>
+#include <sstream>
+#include <fstream>
+#include <omp.h>
+#include <sys/resource.h>
+#include <sys/time.h>
+
+#define private public
+#define protected public
+#include "VCFData.h"
+#include "Target.h"
+#include "PBWT.h"
+#include "PBWTImputer.h"
+#include "TargetImp.h"
+#undef private
+#undef protected
+
+#include "StatusFile.h"
+#include "MyMalloc.h"
+
+StatusFile StatusFile::instance;
+MyMalloc MyMalloc::mm;
+
+namespace {
+
+size_t capBytes(size_t nbits) { return roundToMultiple(nbits, UNITWORDS * sizeof(uint64_t) * 8) / 8; }
+
+struct Handle {
+    VCFData vd;
+    std::vector<uint64_t*> bufs;
+    ~Handle() { for (auto p : bufs) free(p); }
+    uint64_t *alloc(size_t bytes) {
+        void *p = aligned_alloc(64, bytes ? bytes : 64);
+        memset(p, 0, bytes);
+        bufs.push_back((uint64_t*)p);
+        return (uint64_t*)p;
+    }
+};
+
+struct ImpHandle {
+    Handle *h;
+    std::string statfile;
+    PBWTImputer *imp = nullptr;
+    std::vector<BooleanVector> phased;
+    uint64_t *pdata = nullptr;
+    ~ImpHandle() { delete imp; free(pdata); }
+};
+
+void setParams(int hsize, int beamwidth, int delta, float cMmaxsplit,
+               int hsize_fast, int beamwidth_fast, int delta_fast) {
+    Target::cMmaxSplit = cMmaxsplit;
+    Target::HistorySize = hsize;
+    Target::BeamWidth = beamwidth;
+    Target::Delta = delta;
+    Target::HistorySizeFast = hsize_fast;
+    Target::BeamWidthFast = beamwidth_fast;
+    Target::DeltaFast = delta_fast;
+    Target::minFixSize = 0.5;
+    Target::maxFixSize = 0.9;
+    Target::minFixThresh = 0.99;
+    Target::maxFixThresh = 1.0;
+}
+
+} // namespace
+
+extern "C" {
+
+/* Panel + targets.  Bit matrices are given in the reference's layouts with
+ * 512-bit padded rows: hapmajor_typed (nhaps x W(M)), sitemajor_typed
+ * (M x W(nhaps)), sitemajor_full (Mref x W(nhaps)); gt is ntarget x M with
+ * 0/1/2 and 3 = missing. */
+void *refo_create(size_t nhaps, size_t M, size_t Mref,
+                  const uint64_t *hapmajor_typed, const uint64_t *sitemajor_typed,
+                  const uint64_t *sitemajor_full, const int64_t *typed_idx,
+                  const float *cm_typed, const float *af_full, const float *af_common,
+                  size_t ntarget, const uint8_t *gt) {
+    Handle *h = new Handle();
+    VCFData &v = h->vd;
+    v.Nrefhaps = nhaps; v.M = M; v.Mref = Mref; v.Ntarget = ntarget;
+    size_t capM = capBytes(M), capN = capBytes(nhaps);
+    v.reference.resize(nhaps);
+    uint64_t *rd = h->alloc(nhaps * capM);
+    memcpy(rd, hapmajor_typed, nhaps * capM);
+    for (size_t i = 0; i < nhaps; i++) v.reference[i].setData(rd + i * capM / 8, capM, M);
+    v.referenceT.reset(M, M);
+    uint64_t *rt = h->alloc(M * capN);
+    memcpy(rt, sitemajor_typed, M * capN);
+    for (size_t m = 0; m < M; m++) v.referenceT[m].setData(rt + m * capN / 8, capN, nhaps);
+    v.referenceFullT.resize(Mref);
+    uint64_t *rf = h->alloc(Mref * capN);
+    memcpy(rf, sitemajor_full, Mref * capN);
+    for (size_t m = 0; m < Mref; m++) v.referenceFullT[m].setData(rf + m * capN / 8, capN, nhaps);
+    v.cMs.reset(M, M);
+    for (size_t m = 0; m < M; m++) v.cMs[m] = cm_typed[m];
+    v.indexToRefFull.assign(typed_idx, typed_idx + M);
+    v.alleleFreqsFullRefRegion.assign(af_full, af_full + Mref);
+    v.alleleFreqsCommon.assign(af_common, af_common + M);
+    v.haploidsRef.assign(nhaps / 2, false);
+    v.haploidsTgt.assign(ntarget, false);
+    v.haploidsRefMap.resize(nhaps);
+    for (size_t i = 0; i < nhaps; i++) v.haploidsRefMap[i] = i;
+    v.haploidsTgtMap.resize(2 * ntarget);
+    for (size_t i = 0; i < 2 * ntarget; i++) v.haploidsTgtMap[i] = i;
+    v.chunkStartPhase.assign(ntarget, false);
+    v.targets.resize(ntarget);
+    v.tgtmiss.resize(ntarget);
+    v.tgtinphase.resize(ntarget);
+    for (size_t t = 0; t < ntarget; t++) {
+        v.targets[t].reserve(M);
+        v.tgtmiss[t].reset(16, 0);
+        v.targetIDs.push_back("t" + std::to_string(t));
+        for (size_t m = 0; m < M; m++) {
+            uint8_t g = gt[t * M + m];
+            v.targets[t].push_back((Genotype)g);
+            if (g == 3) v.tgtmiss[t].push_back(m);
+        }
+    }
+    return h;
+}
+
+void refo_destroy(void *hp) { delete (Handle*)hp; }
+
+void refo_set_params(int hsize, int beamwidth, int delta, float cMmaxsplit,
+                     int hsize_fast, int beamwidth_fast, int delta_fast) {
+    setParams(hsize, beamwidth, delta, cMmaxsplit, hsize_fast, beamwidth_fast, delta_fast);
+}
+
+/* Target::prepPhase (Target.cpp:95-163): best haps, monos, split/call sites.
+ * Buffers: besthaps K; monos W(M) words; splits/calls/cmdiffs capacity M+1.
+ * Returns the number of split sites S (ncalls via *ncalls). */
+long refo_prep(void *hp, size_t t, size_t K,
+               int64_t *besthaps, uint64_t *monos, int64_t *splitsites,
+               int64_t *calllocs, size_t *ncalls, float *cmsplitdiffs) {
+    Handle *h = (Handle*)hp;
+    VCFData &v = h->vd;
+    BooleanVector pm, pp; std::vector<float> dm, dp;
+    Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, v.Nrefhaps, K,
+              2.0f, 1.0f, 0.003f, 0.003f, false, true, true, false, false, false);
+    tg.prepPhase();
+    for (size_t k = 0; k < K; k++) besthaps[k] = tg.bestHaps[k];
+    memcpy(monos, tg.monos.getData(), capBytes(v.M));
+    size_t S = tg.splitsites.size();
+    for (size_t s = 0; s < S; s++) splitsites[s] = tg.splitsites[s];
+    for (size_t c = 0; c < tg.callLocs.size(); c++) calllocs[c] = tg.callLocs[c];
+    *ncalls = tg.callLocs.size();
+    for (size_t i = 0; i < tg.cMsplitDiffs.size(); i++) cmsplitdiffs[i] = tg.cMsplitDiffs[i];
+    return (long)S;
+}
+
+/* Condensed reference + compressed PBWT of one target, CPU path
+ * (Target.cpp:248-282, PBWT.cpp:33-70,207-285).
+ * cref: (2S+1) x W(K) words; count0: 2S+1; pbwt: 2*(2S+1) rows x 2*ceil(K/32) u32. */
+long refo_cref_pbwt(void *hp, size_t t, size_t K, uint64_t *cref, int *count0, uint32_t *pbwt) {
+    Handle *h = (Handle*)hp;
+    VCFData &v = h->vd;
+    BooleanVector pm, pp; std::vector<float> dm, dp;
+    Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, v.Nrefhaps, K,
+              2.0f, 1.0f, 0.003f, 0.003f, false, true, true, false, false, false);
+    tg.prepPhase();
+    size_t Mp = 2 * tg.splitsites.size() + 1;
+    size_t capacity = capBytes(K);
+    uint64_t *refincdata = (uint64_t*)MyMalloc::calloc(Mp * capacity, 1, "refo_refinc");
+    RingBuffer<BooleanVector> refincT(Mp, Mp);
+    uint64_t *cur = refincdata;
+    for (auto &r : refincT) { r.setData(cur, capacity, K); cur += capacity / 8; }
+    std::vector<int> *c0 = new std::vector<int>(Mp);
+    tg.condensedReferenceT(refincT, c0);
+    if (cref) memcpy(cref, refincdata, Mp * capacity);
+    if (count0) for (size_t i = 0; i < Mp; i++) count0[i] = (*c0)[i];
+    {
+        PBWT pb(&refincT, c0, t);   // takes ownership of c0
+        if (pbwt) memcpy(pbwt, pb.comprPBWT, 2 * Mp * pb.Kwords * sizeof(uint32_t));
+    }
+    MyMalloc::free(refincdata);
+    return (long)Mp;
+}
+
+/* Full phasing of one target: Target::phase() (Target.cpp:166-289).
+ * mat/pat: W(M) words each; dos_mat/dos_pat: M floats. */
+int refo_phase(void *hp, size_t t, size_t K, float expectIBDcM, float hist, float pErr, float pLimit,
+               int doPrePhasing, int doRevPhasing,
+               uint64_t *mat, uint64_t *pat, float *dos_mat, float *dos_pat,
+               float *totalconf, size_t *ncallsites) {
+    Handle *h = (Handle*)hp;
+    VCFData &v = h->vd;
+    size_t cap = capBytes(v.M);
+    uint64_t *md = (uint64_t*)aligned_alloc(64, cap), *pd = (uint64_t*)aligned_alloc(64, cap);
+    memset(md, 0, cap); memset(pd, 0, cap);
+    BooleanVector pm(md, cap, 0), pp(pd, cap, 0);
+    std::vector<float> dm, dp;
+    {
+        Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, v.Nrefhaps, K,
+                  expectIBDcM, hist, pErr, pLimit, doPrePhasing, doRevPhasing, true, false, false, false);
+        tg.phase();
+        *totalconf = tg.getTotalConfidence();
+        *ncallsites = tg.getNCallSites();
+    }
+    memcpy(mat, md, cap); memcpy(pat, pd, cap);
+    memcpy(dos_mat, dm.data(), v.M * sizeof(float));
+    memcpy(dos_pat, dp.data(), v.M * sizeof(float));
+    free(md); free(pd);
+    return 0;
+}
+
+/* The reference's CPU phasing loop (PBWTPhaser.cpp:695-723): OpenMP
+ * dynamic,1 over targets [t0, t1).  Outputs are indexed by t - t0. */
+int refo_phase_range(void *hp, size_t t0, size_t t1, int nthreads, size_t K, float expectIBDcM,
+                     float hist, float pErr, float pLimit, int doPrePhasing, int doRevPhasing,
+                     uint64_t *mats, uint64_t *pats, float *dos_mats, float *dos_pats) {
+    Handle *h = (Handle*)hp;
+    size_t wM = capBytes(h->vd.M) / 8;
+    omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (size_t t = t0; t < t1; t++) {
+        float tc; size_t nc;
+        refo_phase(hp, t, K, expectIBDcM, hist, pErr, pLimit, doPrePhasing, doRevPhasing,
+                   mats + (t - t0) * wM, pats + (t - t0) * wM,
+                   dos_mats + (t - t0) * h->vd.M, dos_pats + (t - t0) * h->vd.M, &tc, &nc);
+    }
+    return 0;
+}
+
+/* PBWTImputer::prepareImputation (PBWTImputer.cpp:63-185) over phased target
+ * haplotypes (2*ntarget x W(M) words, mat then pat per target). */
+void *refo_imp_create(void *hp, const uint64_t *phased, unsigned nthreads, int setmaxerrors, int imputeCalls) {
+    Handle *h = (Handle*)hp;
+    VCFData &v = h->vd;
+    ImpHandle *ih = new ImpHandle();
+    ih->h = h;
+    ih->statfile = "";
+    size_t cap = capBytes(v.M);
+    size_t nh = 2 * v.Ntarget;
+    ih->pdata = (uint64_t*)aligned_alloc(64, nh * cap);
+    memcpy(ih->pdata, phased, nh * cap);
+    ih->phased.resize(nh);
+    for (size_t i = 0; i < nh; i++) ih->phased[i].setData(ih->pdata + i * cap / 8, cap, v.M);
+    ih->imp = new PBWTImputer(v, ih->statfile, nthreads, 1, setmaxerrors, imputeCalls != 0, false);
+    std::vector<size_t> nsites = {0, v.Mref, 0};
+    ih->imp->prepareImputation(ih->phased, nsites);
+    return ih;
+}
+
+void refo_imp_destroy(void *ip) { delete (ImpHandle*)ip; }
+
+size_t refo_imp_nmatches(void *ip, size_t hap) {
+    ImpHandle *ih = (ImpHandle*)ip;
+    return ih->imp->targets[hap].sm_matches.size();
+}
+
+/* set-maximal matches of one target haplotype as (start, end, refstart, refend) */
+void refo_imp_matches(void *ip, size_t hap, int64_t *out) {
+    ImpHandle *ih = (ImpHandle*)ip;
+    const auto &mm = ih->imp->targets[hap].sm_matches;
+    for (size_t i = 0; i < mm.size(); i++) {
+        out[4*i] = mm[i].start; out[4*i+1] = mm[i].end;
+        out[4*i+2] = mm[i].refstart; out[4*i+3] = mm[i].refend;
+    }
+}
+
+/* reference PBWT of the imputer: compressed rows (M x 2*ceil(K/32) u32) and
+ * the prefix arrays gAbsPerm ((M+1) x K int) */
+void refo_imp_refpbwt(void *ip, uint32_t *compr, int32_t *absperm) {
+    ImpHandle *ih = (ImpHandle*)ip;
+    PBWT *p = ih->imp->pbwt;
+    if (compr) memcpy(compr, p->comprPBWT, p->M * p->Kwords * sizeof(uint32_t));
+    if (absperm)
+        for (size_t m = 0; m <= p->M; m++)
+            memcpy(absperm + m * p->K, p->gAbsPerm[m].data(), p->K * sizeof(int32_t));
+}
+
+/* one call of PBWTImputer::imputeBunch (PBWTImputer.cpp:187-204) for block 0:
+ * bits: 2*ntarget x W(bsize) words (cleared here first); dos: 2*ntarget x bsize */
+void refo_imp_bunch(void *ip, size_t bsize, unsigned nthreads, uint64_t *bits, float *dos) {
+    ImpHandle *ih = (ImpHandle*)ip;
+    VCFData &v = ih->h->vd;
+    size_t nh = 2 * v.Ntarget;
+    size_t cap = capBytes(bsize);
+    memset(bits, 0, nh * cap);
+    std::vector<BooleanVector> it(nh);
+    for (size_t i = 0; i < nh; i++) it[i].setData(bits + i * cap / 8, cap, 0);
+    std::vector<std::vector<float>> id(nh, std::vector<float>(bsize, 0.0f));
+    ih->imp->setNumThreads(nthreads);
+    ih->imp->imputeBunch(0, bsize, it, id);
+    for (size_t i = 0; i < nh; i++) memcpy(dos + i * bsize, id[i].data(), bsize * sizeof(float));
+}
+
+} // extern "C"

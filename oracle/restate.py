@@ -1,0 +1,185 @@
+"""ctypes binding of the C restatement oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg use this module as the checker; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from eimp_b200.bits import W, pack_genotypes
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "liboracle.so")
+
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+
+
+class PhaseParamsC(C.Structure):
+    _fields_ = [("K", C.c_int), ("hsize", C.c_int), ("beamwidth", C.c_int), ("delta", C.c_int),
+                ("hsize_fast", C.c_int), ("beamwidth_fast", C.c_int), ("delta_fast", C.c_int),
+                ("cMmaxsplit", C.c_float), ("expectIBDcM", C.c_float), ("hist", C.c_float),
+                ("pErr", C.c_float), ("pLimit", C.c_float), ("minfixsize", C.c_float),
+                ("maxfixsize", C.c_float), ("minfixthr", C.c_float), ("maxfixthr", C.c_float),
+                ("doPrePhasing", C.c_int), ("doRevPhasing", C.c_int)]
+
+
+def params_c(K=10000, hsize=100, beamwidth=128, delta=24, hsize_fast=30, beamwidth_fast=64, delta_fast=10,
+             cMmaxsplit=0.125, expectIBDcM=2.0, hist=1.0, pErr=0.003, pLimit=None, doPrePhasing=False,
+             doRevPhasing=True) -> PhaseParamsC:
+    return PhaseParamsC(K, hsize, beamwidth, delta, hsize_fast, beamwidth_fast, delta_fast, cMmaxsplit,
+                        expectIBDcM, hist, pErr, pErr if pLimit is None else pLimit, 0.5, 0.9, 0.99, 1.0,
+                        int(doPrePhasing), int(doRevPhasing))
+
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIBPATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIBPATH)
+        L.eo_besthaps.argtypes = [_u64p, _u64p, C.c_size_t, C.c_size_t, C.c_size_t, _i64p, C.c_void_p]
+        L.eo_monos.argtypes = [_u64p, C.c_size_t, C.c_size_t, _i64p, C.c_size_t, _u64p]
+        L.eo_calllocs.restype = C.c_long
+        L.eo_calllocs.argtypes = [_u8p, _u64p, _f32p, C.c_size_t, C.c_float, _i64p, _i64p,
+                                  C.POINTER(C.c_size_t), _f32p]
+        L.eo_cref.argtypes = [_u8p, _u64p, C.c_size_t, C.c_size_t, _i64p, C.c_size_t, _i64p, C.c_size_t,
+                              _u64p, _i32p]
+        L.eo_pbwt.argtypes = [_u64p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_int, _u32p, C.c_void_p, C.c_void_p]
+        L.eo_rank.restype = C.c_int
+        L.eo_rank.argtypes = [_u32p, C.c_int, C.c_int]
+        L.eo_smmatches.restype = C.c_long
+        L.eo_smmatches.argtypes = [_u32p, _i32p, C.c_size_t, C.c_size_t, _u64p, _i64p, C.c_size_t, C.c_int,
+                                   _i64p, C.c_size_t]
+        L.eo_impute.argtypes = [_i64p, C.c_size_t, _i32p, C.c_size_t, _u64p, C.c_size_t, C.c_size_t, _i64p,
+                                C.c_size_t, _f32p, C.c_size_t, _i64p, C.c_size_t, C.c_int, _u64p, _u64p,
+                                _f32p, _u8p]
+        L.eo_phase.restype = C.c_int
+        L.eo_phase.argtypes = [_u8p, _u64p, _u64p, _f32p, C.c_size_t, C.c_size_t, C.POINTER(PhaseParamsC),
+                               _u64p, _u64p, _f32p, _f32p, C.POINTER(C.c_float), C.POINTER(C.c_size_t)]
+        L.eo_phase_many.restype = C.c_int
+        L.eo_phase_many.argtypes = [_u8p, C.c_size_t, _u64p, _u64p, _f32p, C.c_size_t, C.c_size_t,
+                                    C.POINTER(PhaseParamsC), C.c_int, _u64p, _u64p, _f32p, _f32p]
+        _lib = L
+    return _lib
+
+
+def besthaps(gt_row: np.ndarray, hapmajor: np.ndarray, K: int):
+    nh, wM = hapmajor.shape
+    gtw = np.ascontiguousarray(pack_genotypes(gt_row))
+    out = np.zeros(min(K, nh), np.int64)
+    nerr = np.zeros(nh, np.uint32)
+    lib().eo_besthaps(gtw, np.ascontiguousarray(hapmajor), nh, wM, K, out, nerr.ctypes.data)
+    return out, nerr
+
+
+def monos(hapmajor: np.ndarray, M: int, bh: np.ndarray):
+    nh, wM = hapmajor.shape
+    out = np.zeros(wM, np.uint64)
+    lib().eo_monos(np.ascontiguousarray(hapmajor), wM, M, np.ascontiguousarray(bh, np.int64), len(bh), out)
+    return out
+
+
+def calllocs(gt_row, monos_w, cm, cMmaxsplit=0.125):
+    M = len(gt_row)
+    splits = np.zeros(M + 1, np.int64)
+    calls = np.zeros(M + 1, np.int64)
+    diffs = np.zeros(M + 2, np.float32)
+    nc = C.c_size_t(0)
+    S = lib().eo_calllocs(np.ascontiguousarray(gt_row, np.uint8), monos_w, np.ascontiguousarray(cm, np.float32),
+                          M, cMmaxsplit, splits, calls, C.byref(nc), diffs)
+    return splits[:S].copy(), calls[:nc.value].copy() if S else calls[:0].copy(), diffs[:S + 1].copy() if S else diffs[:0].copy()
+
+
+def cref(gt_row, sitemajor, nhaps, bh, splits):
+    M = len(gt_row)
+    K = len(bh)
+    Mp = 2 * len(splits) + 1
+    out = np.zeros((Mp, W(K)), np.uint64)
+    c0 = np.zeros(Mp, np.int32)
+    lib().eo_cref(np.ascontiguousarray(gt_row, np.uint8), np.ascontiguousarray(sitemajor), M, nhaps,
+                  np.ascontiguousarray(bh, np.int64), K, np.ascontiguousarray(splits, np.int64), len(splits), out, c0)
+    return out, c0
+
+
+def pbwt(rows: np.ndarray, K: int, reverse: bool = False, absperm: bool = False):
+    Mp, rw = rows.shape
+    kw = 2 * ((K + 31) // 32)
+    out = np.zeros((Mp, kw), np.uint32)
+    ap = np.zeros((Mp + 1, K), np.int32) if absperm else None
+    c0 = np.zeros(Mp, np.int32)
+    lib().eo_pbwt(np.ascontiguousarray(rows), rw, Mp, K, int(reverse), out,
+                  ap.ctypes.data if ap is not None else None, c0.ctypes.data)
+    return out, c0, ap
+
+
+def smmatches(refpbwt, count0, M, K, hap_words, miss, setmaxerrors=0, maxmatches=None):
+    if maxmatches is None:
+        maxmatches = 4 * M + 64
+    out = np.zeros((maxmatches, 4), np.int64)
+    n = lib().eo_smmatches(np.ascontiguousarray(refpbwt), np.ascontiguousarray(count0, np.int32), M, K,
+                           np.ascontiguousarray(hap_words, np.uint64), np.ascontiguousarray(miss, np.int64),
+                           len(miss), setmaxerrors, out, maxmatches)
+    if n < 0:
+        raise RuntimeError("match buffer overflow")
+    return out[:n].copy()
+
+
+def impute(matches, absperm, sitemajor_full, typed, af_full, nrefhaps, miss, hap_words, imputeCalls=False):
+    Mref, wN = sitemajor_full.shape
+    K = absperm.shape[1]
+    bits = np.zeros(W(Mref), np.uint64)
+    dos = np.zeros(Mref, np.float32)
+    imp = np.zeros(Mref, np.uint8)
+    m = np.ascontiguousarray(matches, np.int64).reshape(-1, 4)
+    lib().eo_impute(m.reshape(-1) if len(m) else np.zeros(4, np.int64), len(m), np.ascontiguousarray(absperm, np.int32),
+                    K, np.ascontiguousarray(sitemajor_full), wN, Mref, np.ascontiguousarray(typed, np.int64),
+                    len(typed), np.ascontiguousarray(af_full, np.float32), nrefhaps,
+                    np.ascontiguousarray(miss, np.int64) if len(miss) else np.zeros(1, np.int64), len(miss),
+                    int(imputeCalls), np.ascontiguousarray(hap_words, np.uint64), bits, dos, imp)
+    return bits, dos, imp
+
+
+def phase(gt_row, hapmajor, sitemajor, cm, params: PhaseParamsC):
+    M = len(gt_row)
+    nh = hapmajor.shape[0]
+    mat = np.zeros(W(M), np.uint64)
+    pat = np.zeros(W(M), np.uint64)
+    dm = np.zeros(M, np.float32)
+    dp = np.zeros(M, np.float32)
+    tc = C.c_float(0)
+    nc = C.c_size_t(0)
+    rc = lib().eo_phase(np.ascontiguousarray(gt_row, np.uint8), np.ascontiguousarray(hapmajor),
+                        np.ascontiguousarray(sitemajor), np.ascontiguousarray(cm, np.float32), M, nh,
+                        C.byref(params), mat, pat, dm, dp, C.byref(tc), C.byref(nc))
+    if rc:
+        raise RuntimeError(f"oracle phasing failed ({rc})")
+    return mat, pat, dm, dp, tc.value, nc.value
+
+
+def phase_many(gt, hapmajor, sitemajor, cm, params: PhaseParamsC, nthreads=8):
+    n, M = gt.shape
+    nh = hapmajor.shape[0]
+    mats = np.zeros((n, W(M)), np.uint64)
+    pats = np.zeros((n, W(M)), np.uint64)
+    dm = np.zeros((n, M), np.float32)
+    dp = np.zeros((n, M), np.float32)
+    rc = lib().eo_phase_many(np.ascontiguousarray(gt, np.uint8), n, np.ascontiguousarray(hapmajor),
+                             np.ascontiguousarray(sitemajor), np.ascontiguousarray(cm, np.float32), M, nh,
+                             C.byref(params), nthreads, mats, pats, dm, dp)
+    if rc:
+        raise RuntimeError(f"oracle phasing failed ({rc})")
+    return mats, pats, dm, dp
