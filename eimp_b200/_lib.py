@@ -1,0 +1,95 @@
+"""ctypes binding of libeimp_b200.so (the C ABI in include/eimp_gpu.h).
+
+The library is the product: every call runs CUDA kernels on the device.  If it
+is missing or no GPU is present, the calls fail loudly -- there is no CPU
+fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libeimp_b200.so")
+
+EIMP_OK, EIMP_E_CUDA, EIMP_E_ARG, EIMP_E_CAPACITY, EIMP_E_BEAM_EMPTY, EIMP_E_NOMEM = range(6)
+
+_vp = C.c_void_p
+_sz = C.c_size_t
+_i32 = C.c_int
+
+
+class EimpPhaseParams(C.Structure):
+    """eimp_phase_params (include/eimp_gpu.h)"""
+    _fields_ = [("K", C.c_int), ("hsize", C.c_int), ("beamwidth", C.c_int), ("delta", C.c_int),
+                ("hsize_fast", C.c_int), ("beamwidth_fast", C.c_int), ("delta_fast", C.c_int),
+                ("cMmaxsplit", C.c_float), ("expectIBDcM", C.c_float), ("hist", C.c_float),
+                ("pErr", C.c_float), ("pLimit", C.c_float), ("minfixsize", C.c_float),
+                ("maxfixsize", C.c_float), ("minfixthr", C.c_float), ("maxfixthr", C.c_float),
+                ("doPrePhasing", C.c_int), ("doRevPhasing", C.c_int)]
+
+
+# (name, restype, argtypes) of every exported entry point
+_PROTOS = [
+    ("eimp_create", _i32, [_i32, C.POINTER(_vp)]),
+    ("eimp_destroy", None, [_vp]),
+    ("eimp_last_error", C.c_char_p, [_vp]),
+    ("eimp_synchronize", _i32, [_vp]),
+    ("eimp_kernel_launches", C.c_uint64, [_vp]),
+    ("eimp_stream", _vp, [_vp]),
+    ("eimp_gpu_initialize", _i32, [_vp, _sz, _sz, _sz, _sz, _sz, _sz, _vp]),
+    ("eimp_gpu_block_size", _sz, [_vp]),
+    ("eimp_gpu_run_cref_pbwt", _i32, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("eimp_phase_set_reference", _i32, [_vp, _sz, _sz, _vp, _vp, _vp]),
+    ("eimp_phase_prep", _i32, [_vp, C.POINTER(EimpPhaseParams), _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("eimp_phase_cref_pbwt", _i32, [_vp, C.POINTER(EimpPhaseParams), _sz, _vp, C.POINTER(_sz), _vp, _vp, _vp, _vp]),
+    ("eimp_phase_targets", _i32, [_vp, C.POINTER(EimpPhaseParams), _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("eimp_phase_targets_dev", _i32, [_vp, C.POINTER(EimpPhaseParams), _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("eimp_imp_set_reference", _i32, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
+    ("eimp_imp_set_reference_dev", _i32, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
+    ("eimp_imp_prepare", _i32, [_vp, _sz, _vp, _vp, _i32, _i32, _sz]),
+    ("eimp_imp_prepare_dev", _i32, [_vp, _sz, _vp, _vp, _i32, _i32, _sz]),
+    ("eimp_imp_bunch", _i32, [_vp, _sz, _sz, _vp, _vp]),
+    ("eimp_imp_bunch_dev", _i32, [_vp, _sz, _sz, _vp, _sz, _vp, _sz]),
+    ("eimp_imp_matches", _i32, [_vp, _sz, _vp, _sz, C.POINTER(_sz)]),
+    ("eimp_imp_refpbwt", _i32, [_vp, _vp, _vp]),
+]
+
+_lib = None
+
+
+class EimpError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"eimp error {code}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load libeimp_b200.so (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise RuntimeError(f"{LIBPATH} is not built: run `python -m eimp_b200.build` (nvcc, sm_100a)")
+    L = C.CDLL(LIBPATH)
+    for name, res, args in _PROTOS:
+        f = getattr(L, name, None)
+        if f is None:
+            continue
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def exported_names():
+    return [n for n, _, _ in _PROTOS]
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array / torch tensor buffer (None passes NULL)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data

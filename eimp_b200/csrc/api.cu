@@ -1,0 +1,528 @@
+// C ABI of libeimp_b200 (include/eimp_gpu.h): context, device buffers, and the
+// host-facing entry points that mirror the reference's GPUEngine,
+// Target::prepPhase/phase and PBWTImputer interfaces.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "../../include/eimp_gpu.h"
+
+using namespace eimp;
+
+namespace {
+
+// grow-only device buffer
+struct DBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    ~DBuf() { if (p) cudaFree(p); }
+    cudaError_t reserve(size_t bytes) {
+        if (bytes <= n) return cudaSuccess;
+        if (p) { cudaFree(p); p = nullptr; n = 0; }
+        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+        if (e == cudaSuccess) n = bytes;
+        return e;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+}  // namespace
+
+struct eimp_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+    DBuf status;
+
+    // GPUEngine drop-in
+    size_t g_K = 0, g_Kwords = 0, g_M = 0, g_Ncorr = 0, g_NAD = 0, g_refTcap = 0;
+    DBuf g_refT, g_gt, g_splits, g_nsplits, g_bh, g_rowoff, g_cref, g_count0, g_pbwt;
+
+    // phasing reference
+    size_t p_M = 0, p_nhaps = 0;
+    DBuf p_hapmajor, p_sitemajor, p_cm;
+    // phasing batch scratch
+    DBuf b_gt, b_nerr, b_bh, b_flags, b_monos, b_splits, b_calls, b_cmd, b_nsplits, b_ncalls, b_rowoff, b_cref,
+        b_count0, b_pbwt, b_arena, b_out_mat, b_out_pat, b_out_dm, b_out_dp, b_out_tc, b_out_nc;
+    size_t b_rows = 0;
+
+    // imputation reference
+    size_t i_Mref = 0, i_nhaps = 0, i_M = 0;
+    DBuf i_hapfull, i_sitefull_tmp, i_af, i_typed, i_segm, i_common, i_sitetyped_tmp, i_compr, i_absperm,
+        i_count0;
+    // prepared targets
+    size_t i_ntargets = 0;
+    int i_imputeCalls = 0;
+    size_t i_cap = 0;
+    DBuf i_phased, i_gt, i_matches, i_nmatch;
+    // host <-> device staging for bunches
+    DBuf i_bits, i_dos;
+};
+
+namespace {
+
+int fail(eimp_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? EIMP_E_NOMEM : EIMP_E_CUDA,         \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+    } while (0)
+
+#define LAUNCH(call)                                                                               \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        ctx->launches++;                                                                           \
+        if (e_ != cudaSuccess) return fail(ctx, EIMP_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int use_device(eimp_ctx *ctx) {
+    CK(cudaSetDevice(ctx->device));
+    return 0;
+}
+
+int check_status(eimp_ctx *ctx) {
+    uint32_t st = 0;
+    CK(cudaMemcpyAsync(&st, ctx->status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (st) {
+        CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(uint32_t), ctx->stream));
+        if (st & EIMP_ERR_BEAM_EMPTY) return fail(ctx, EIMP_E_BEAM_EMPTY, "Beam is empty. No paths left.");
+        char b[160];
+        snprintf(b, sizeof b, "device structure capacity exceeded (status 0x%x)", st);
+        return fail(ctx, EIMP_E_CAPACITY, b);
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int eimp_create(int device, eimp_ctx **out) {
+    if (!out) return EIMP_E_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return EIMP_E_CUDA;
+    if (device < 0 || device >= n) return EIMP_E_ARG;
+    eimp_ctx *ctx = new eimp_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        ctx->status.reserve(sizeof(uint32_t)) != cudaSuccess || cudaMemset(ctx->status.p, 0, sizeof(uint32_t)) != cudaSuccess) {
+        delete ctx;
+        return EIMP_E_CUDA;
+    }
+    *out = ctx;
+    return 0;
+}
+
+void eimp_destroy(eimp_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaStream_t s = ctx->stream;
+    delete ctx;
+    if (s) cudaStreamDestroy(s);
+}
+
+const char *eimp_last_error(const eimp_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int eimp_synchronize(eimp_ctx *ctx) {
+    if (!ctx) return EIMP_E_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+uint64_t eimp_kernel_launches(const eimp_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+void *eimp_stream(eimp_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+// ------------------------------------------------------------------ imputation
+
+int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint64_t *d_sitemajor_full,
+                               const float *d_af_full, size_t M, const int64_t *d_typed,
+                               const uint64_t *d_sitemajor_typed) {
+    if (!ctx || !Mref || !nhaps || !M || M > Mref) return fail(ctx, EIMP_E_ARG, "eimp_imp_set_reference: bad sizes");
+    if (int r = use_device(ctx)) return r;
+    cudaStream_t st = ctx->stream;
+    const size_t wN = eimp_W(nhaps), wMref = eimp_W(Mref), kw = eimp_kw(nhaps);
+    ctx->i_Mref = Mref; ctx->i_nhaps = nhaps; ctx->i_M = M;
+    CK(ctx->i_hapfull.reserve(nhaps * wMref * 8));
+    CK(ctx->i_af.reserve(Mref * 4));
+    CK(ctx->i_typed.reserve(M * 8));
+    CK(ctx->i_segm.reserve(Mref * 4));
+    CK(ctx->i_common.reserve(Mref));
+    CK(ctx->i_compr.reserve(M * kw * 4));
+    CK(ctx->i_absperm.reserve((M + 1) * nhaps * 4));
+    CK(ctx->i_count0.reserve(M * 4));
+    CK(cudaMemcpyAsync(ctx->i_af.p, d_af_full, Mref * 4, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(ctx->i_typed.p, d_typed, M * 8, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(ctx->i_hapfull.p, 0, nhaps * wMref * 8, st));
+    LAUNCH(launch_transpose(d_sitemajor_full, Mref, wN, ctx->i_hapfull.as<uint64_t>(), nhaps, wMref, st));
+    LAUNCH(launch_segmap(ctx->i_typed.as<int64_t>(), (int)M, (int)Mref, ctx->i_segm.as<int32_t>(),
+                         ctx->i_common.as<uint8_t>(), st));
+    LAUNCH(launch_refpbwt(d_sitemajor_typed, (int)M, (int)nhaps, (int)wN, ctx->i_compr.as<uint32_t>(),
+                          ctx->i_absperm.as<int32_t>(), ctx->i_count0.as<int32_t>(), st));
+    return 0;
+}
+
+int eimp_imp_set_reference(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint64_t *sitemajor_full,
+                           const float *af_full, size_t M, const int64_t *typed, const uint64_t *sitemajor_typed) {
+    if (!ctx || !sitemajor_full || !af_full || !typed || !sitemajor_typed)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_set_reference: NULL argument");
+    if (int r = use_device(ctx)) return r;
+    const size_t wN = eimp_W(nhaps);
+    DBuf full, af, ty, st;
+    CK(full.reserve(Mref * wN * 8));
+    CK(af.reserve(Mref * 4));
+    CK(ty.reserve(M * 8));
+    CK(st.reserve(M * wN * 8));
+    CK(cudaMemcpyAsync(full.p, sitemajor_full, Mref * wN * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(af.p, af_full, Mref * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ty.p, typed, M * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(st.p, sitemajor_typed, M * wN * 8, cudaMemcpyHostToDevice, ctx->stream));
+    int r = eimp_imp_set_reference_dev(ctx, Mref, nhaps, full.as<uint64_t>(), af.as<float>(), M, ty.as<int64_t>(),
+                                       st.as<uint64_t>());
+    if (r) return r;
+    CK(cudaStreamSynchronize(ctx->stream));   // temporaries are freed on return
+    return 0;
+}
+
+int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phased, const uint8_t *d_gt,
+                         int setmaxerrors, int imputeCalls, size_t match_cap) {
+    if (!ctx || !ctx->i_Mref) return fail(ctx, EIMP_E_ARG, "eimp_imp_prepare: no reference set");
+    if (!ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_prepare: no targets");
+    if (int r = use_device(ctx)) return r;
+    const size_t M = ctx->i_M, wM = eimp_W(M), nh = 2 * ntargets;
+    size_t cap = match_cap ? match_cap : M / 4 + 64;
+    ctx->i_ntargets = ntargets;
+    ctx->i_imputeCalls = imputeCalls;
+    ctx->i_cap = cap;
+    CK(ctx->i_phased.reserve(nh * wM * 8));
+    CK(ctx->i_gt.reserve(ntargets * M));
+    CK(ctx->i_matches.reserve(nh * cap * sizeof(int4)));
+    CK(ctx->i_nmatch.reserve(nh * sizeof(int)));
+    if (d_phased != ctx->i_phased.as<uint64_t>())
+        CK(cudaMemcpyAsync(ctx->i_phased.p, d_phased, nh * wM * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (d_gt != ctx->i_gt.as<uint8_t>())
+        CK(cudaMemcpyAsync(ctx->i_gt.p, d_gt, ntargets * M, cudaMemcpyDeviceToDevice, ctx->stream));
+    LAUNCH(launch_smm(ctx->i_compr.as<uint32_t>(), ctx->i_count0.as<int32_t>(), (int)M, (int)ctx->i_nhaps,
+                      ctx->i_phased.as<uint64_t>(), (int)wM, ctx->i_gt.as<uint8_t>(), (int)nh, setmaxerrors,
+                      ctx->i_matches.as<int4>(), (int)cap, ctx->i_nmatch.as<int>(), ctx->status.as<uint32_t>(),
+                      ctx->stream));
+    return 0;
+}
+
+int eimp_imp_prepare(eimp_ctx *ctx, size_t ntargets, const uint64_t *phased, const uint8_t *gt, int setmaxerrors,
+                     int imputeCalls, size_t match_cap) {
+    if (!ctx || !ctx->i_Mref) return fail(ctx, EIMP_E_ARG, "eimp_imp_prepare: no reference set");
+    if (!phased || !gt) return fail(ctx, EIMP_E_ARG, "eimp_imp_prepare: NULL argument");
+    if (int r = use_device(ctx)) return r;
+    const size_t M = ctx->i_M, wM = eimp_W(M), nh = 2 * ntargets;
+    CK(ctx->i_phased.reserve(nh * wM * 8));
+    CK(ctx->i_gt.reserve(ntargets * M));
+    CK(cudaMemcpyAsync(ctx->i_phased.p, phased, nh * wM * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->i_gt.p, gt, ntargets * M, cudaMemcpyHostToDevice, ctx->stream));
+    int r = eimp_imp_prepare_dev(ctx, ntargets, ctx->i_phased.as<uint64_t>(), ctx->i_gt.as<uint8_t>(), setmaxerrors,
+                                 imputeCalls, match_cap);
+    if (r) return r;
+    return check_status(ctx);
+}
+
+int eimp_imp_bunch_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t *d_bits, size_t ldb_words,
+                       float *d_dos, size_t ldd) {
+    if (!ctx || !ctx->i_ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch: imputation not prepared");
+    if (mref_begin + nsites > ctx->i_Mref || !nsites) return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch: window out of range");
+    if (ldb_words < (nsites + 63) / 64 || ldd < nsites) return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch: leading dimension too small");
+    if (int r = use_device(ctx)) return r;
+    const size_t M = ctx->i_M;
+    LAUNCH(launch_dosage(ctx->i_matches.as<int4>(), (int)ctx->i_cap, ctx->i_nmatch.as<int>(),
+                         ctx->i_absperm.as<int32_t>(), (int)ctx->i_nhaps, ctx->i_hapfull.as<uint64_t>(),
+                         (int)eimp_W(ctx->i_Mref), ctx->i_segm.as<int32_t>(), ctx->i_common.as<uint8_t>(),
+                         ctx->i_af.as<float>(), (int)ctx->i_nhaps, ctx->i_phased.as<uint64_t>(), (int)eimp_W(M),
+                         ctx->i_gt.as<uint8_t>(), (int)M, (int)(2 * ctx->i_ntargets), (int)mref_begin, (int)nsites,
+                         ctx->i_imputeCalls, d_dos, (int)ldd, d_bits, (int)ldb_words, ctx->stream));
+    return 0;
+}
+
+int eimp_imp_bunch(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t *bits, float *dos) {
+    if (!ctx || !bits || !dos) return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch: NULL argument");
+    if (!ctx->i_ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch: imputation not prepared");
+    if (int r = use_device(ctx)) return r;
+    const size_t nh = 2 * ctx->i_ntargets, wb = eimp_W(nsites);
+    CK(ctx->i_bits.reserve(nh * wb * 8));
+    CK(ctx->i_dos.reserve(nh * nsites * 4));
+    CK(cudaMemsetAsync(ctx->i_bits.p, 0, nh * wb * 8, ctx->stream));
+    int r = eimp_imp_bunch_dev(ctx, mref_begin, nsites, ctx->i_bits.as<uint64_t>(), wb, ctx->i_dos.as<float>(), nsites);
+    if (r) return r;
+    CK(cudaMemcpyAsync(bits, ctx->i_bits.p, nh * wb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(dos, ctx->i_dos.p, nh * nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int eimp_imp_matches(eimp_ctx *ctx, size_t hap, int32_t *out, size_t cap, size_t *n) {
+    if (!ctx || !n || hap >= 2 * ctx->i_ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_matches: bad haplotype");
+    if (int r = use_device(ctx)) return r;
+    int cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, ctx->i_nmatch.as<int>() + hap, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (cnt < 0) return fail(ctx, EIMP_E_CAPACITY, "eimp_imp_matches: match search overflowed for this haplotype");
+    *n = (size_t)cnt;
+    if (out && cnt) {
+        size_t k = (size_t)cnt < cap ? (size_t)cnt : cap;
+        CK(cudaMemcpyAsync(out, ctx->i_matches.as<int4>() + hap * ctx->i_cap, k * sizeof(int4), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return 0;
+}
+
+int eimp_imp_refpbwt(eimp_ctx *ctx, uint32_t *compr, int32_t *absperm) {
+    if (!ctx || !ctx->i_Mref) return fail(ctx, EIMP_E_ARG, "eimp_imp_refpbwt: no reference set");
+    if (int r = use_device(ctx)) return r;
+    const size_t M = ctx->i_M, K = ctx->i_nhaps;
+    if (compr) CK(cudaMemcpyAsync(compr, ctx->i_compr.p, M * eimp_kw(K) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (absperm) CK(cudaMemcpyAsync(absperm, ctx->i_absperm.p, (M + 1) * K * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+// --------------------------------------------------------------------- phasing
+
+int eimp_phase_set_reference(eimp_ctx *ctx, size_t M, size_t nhaps, const uint64_t *hapmajor,
+                             const uint64_t *sitemajor, const float *cM) {
+    if (!ctx || !M || !nhaps || !hapmajor || !sitemajor || !cM)
+        return fail(ctx, EIMP_E_ARG, "eimp_phase_set_reference: bad argument");
+    if (int r = use_device(ctx)) return r;
+    const size_t wM = eimp_W(M), wN = eimp_W(nhaps);
+    ctx->p_M = M; ctx->p_nhaps = nhaps;
+    CK(ctx->p_hapmajor.reserve(nhaps * wM * 8));
+    CK(ctx->p_sitemajor.reserve(M * wN * 8));
+    CK(ctx->p_cm.reserve(M * 4));
+    CK(cudaMemcpyAsync(ctx->p_hapmajor.p, hapmajor, nhaps * wM * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->p_sitemajor.p, sitemajor, M * wN * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->p_cm.p, cM, M * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+namespace {
+
+// device-side prepPhase for ntgt targets whose genotypes are at d_gt
+int run_prep(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt) {
+    const size_t M = ctx->p_M, nh = ctx->p_nhaps, wM = eimp_W(M), wN = eimp_W(nh);
+    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    cudaStream_t st = ctx->stream;
+    CK(ctx->b_nerr.reserve(ntgt * nh * 4));
+    CK(ctx->b_bh.reserve(ntgt * K * 4));
+    CK(ctx->b_flags.reserve(ntgt * wN * 8));
+    CK(ctx->b_monos.reserve(ntgt * wM * 8));
+    CK(ctx->b_splits.reserve(ntgt * M * 4));
+    CK(ctx->b_calls.reserve(ntgt * M * 4));
+    CK(ctx->b_cmd.reserve(ntgt * (M + 1) * 4));
+    CK(ctx->b_nsplits.reserve(ntgt * 4));
+    CK(ctx->b_ncalls.reserve(ntgt * 4));
+    LAUNCH(launch_besthaps(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)nh, (int)wM, (int)K,
+                           ctx->b_nerr.as<uint32_t>(), ctx->b_bh.as<int32_t>(), ctx->b_flags.as<uint64_t>(), (int)wN,
+                           st));
+    LAUNCH(launch_monos_calls(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)wM,
+                              ctx->b_bh.as<int32_t>(), (int)K, ctx->p_cm.as<float>(), p->cMmaxsplit,
+                              ctx->b_monos.as<uint64_t>(), ctx->b_splits.as<int32_t>(), ctx->b_calls.as<int32_t>(),
+                              ctx->b_cmd.as<float>(), ctx->b_nsplits.as<int32_t>(), ctx->b_ncalls.as<int32_t>(), st));
+    return 0;
+}
+
+// condensed reference + PBWT for the prepared batch; fills ctx->b_rows and the
+// host copy of the row offsets
+int run_cref_pbwt(eimp_ctx *ctx, size_t K, size_t ntgt, const uint8_t *d_gt, std::vector<int64_t> &rowoff) {
+    const size_t M = ctx->p_M, nh = ctx->p_nhaps, wN = eimp_W(nh), wK = eimp_W(K), kw = eimp_kw(K);
+    cudaStream_t st = ctx->stream;
+    std::vector<int32_t> ns(ntgt);
+    CK(cudaMemcpyAsync(ns.data(), ctx->b_nsplits.p, ntgt * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    rowoff.assign(ntgt + 1, 0);
+    for (size_t t = 0; t < ntgt; t++) rowoff[t + 1] = rowoff[t] + 2 * (int64_t)ns[t] + 1;
+    const size_t rows = (size_t)rowoff[ntgt];
+    ctx->b_rows = rows;
+    CK(ctx->b_rowoff.reserve((ntgt + 1) * 8));
+    CK(ctx->b_cref.reserve(rows * wK * 8));
+    CK(ctx->b_count0.reserve(rows * 4));
+    CK(ctx->b_pbwt.reserve(2 * rows * kw * 4));
+    CK(cudaMemcpyAsync(ctx->b_rowoff.p, rowoff.data(), (ntgt + 1) * 8, cudaMemcpyHostToDevice, st));
+    LAUNCH(launch_cref(d_gt, (int)ntgt, (int)M, ctx->p_sitemajor.as<uint64_t>(), (int)nh, (int)wN,
+                       ctx->b_bh.as<int32_t>(), (int)K, ctx->b_splits.as<int32_t>(), ctx->b_nsplits.as<int32_t>(),
+                       ctx->b_rowoff.as<int64_t>(), ctx->b_cref.as<uint64_t>(), ctx->b_count0.as<int32_t>(), st));
+    LAUNCH(launch_pbwt(ctx->b_cref.as<uint64_t>(), ctx->b_count0.as<int32_t>(), ctx->b_rowoff.as<int64_t>(),
+                       (int)ntgt, (int)K, ctx->b_pbwt.as<uint32_t>(), kw, 0, st));
+    return 0;
+}
+
+int check_phase_args(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt) {
+    if (!ctx) return EIMP_E_ARG;
+    if (!ctx->p_M) return fail(ctx, EIMP_E_ARG, "phasing reference not set");
+    if (!p || p->K <= 0 || !ntgt) return fail(ctx, EIMP_E_ARG, "bad phasing parameters or empty batch");
+    if (p->hsize <= 0 || p->hsize > 128 || p->hsize_fast <= 0 || p->hsize_fast > 128)
+        return fail(ctx, EIMP_E_ARG, "hsize must be in 1..128 (BooleanHistory holds 128 sites)");
+    return 0;
+}
+
+}  // namespace
+
+int eimp_phase_prep(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *gt, int32_t *besthaps,
+                    uint64_t *flags, uint64_t *monos, int32_t *splits, int32_t *calls, float *cmdiffs,
+                    int32_t *nsplits, int32_t *ncalls) {
+    if (int r = check_phase_args(ctx, p, ntgt)) return r;
+    if (!gt) return fail(ctx, EIMP_E_ARG, "eimp_phase_prep: NULL genotypes");
+    if (int r = use_device(ctx)) return r;
+    const size_t M = ctx->p_M, nh = ctx->p_nhaps, wM = eimp_W(M), wN = eimp_W(nh);
+    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    cudaStream_t st = ctx->stream;
+    CK(ctx->b_gt.reserve(ntgt * M));
+    CK(cudaMemcpyAsync(ctx->b_gt.p, gt, ntgt * M, cudaMemcpyHostToDevice, st));
+    if (int r = run_prep(ctx, p, ntgt, ctx->b_gt.as<uint8_t>())) return r;
+    if (besthaps) CK(cudaMemcpyAsync(besthaps, ctx->b_bh.p, ntgt * K * 4, cudaMemcpyDeviceToHost, st));
+    if (flags) CK(cudaMemcpyAsync(flags, ctx->b_flags.p, ntgt * wN * 8, cudaMemcpyDeviceToHost, st));
+    if (monos) CK(cudaMemcpyAsync(monos, ctx->b_monos.p, ntgt * wM * 8, cudaMemcpyDeviceToHost, st));
+    if (splits) CK(cudaMemcpyAsync(splits, ctx->b_splits.p, ntgt * M * 4, cudaMemcpyDeviceToHost, st));
+    if (calls) CK(cudaMemcpyAsync(calls, ctx->b_calls.p, ntgt * M * 4, cudaMemcpyDeviceToHost, st));
+    if (cmdiffs) CK(cudaMemcpyAsync(cmdiffs, ctx->b_cmd.p, ntgt * (M + 1) * 4, cudaMemcpyDeviceToHost, st));
+    if (nsplits) CK(cudaMemcpyAsync(nsplits, ctx->b_nsplits.p, ntgt * 4, cudaMemcpyDeviceToHost, st));
+    if (ncalls) CK(cudaMemcpyAsync(ncalls, ctx->b_ncalls.p, ntgt * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int eimp_phase_cref_pbwt(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *gt,
+                         size_t *rows_out, int64_t *rowoff, uint64_t *cref, int32_t *count0, uint32_t *pbwt) {
+    if (int r = check_phase_args(ctx, p, ntgt)) return r;
+    if (!gt || !rows_out) return fail(ctx, EIMP_E_ARG, "eimp_phase_cref_pbwt: NULL argument");
+    if (int r = use_device(ctx)) return r;
+    const size_t M = ctx->p_M, nh = ctx->p_nhaps;
+    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    cudaStream_t st = ctx->stream;
+    CK(ctx->b_gt.reserve(ntgt * M));
+    CK(cudaMemcpyAsync(ctx->b_gt.p, gt, ntgt * M, cudaMemcpyHostToDevice, st));
+    if (int r = run_prep(ctx, p, ntgt, ctx->b_gt.as<uint8_t>())) return r;
+    std::vector<int64_t> ro;
+    if (int r = run_cref_pbwt(ctx, K, ntgt, ctx->b_gt.as<uint8_t>(), ro)) return r;
+    *rows_out = ctx->b_rows;
+    if (rowoff) memcpy(rowoff, ro.data(), (ntgt + 1) * 8);
+    if (cref) CK(cudaMemcpyAsync(cref, ctx->b_cref.p, ctx->b_rows * eimp_W(K) * 8, cudaMemcpyDeviceToHost, st));
+    if (count0) CK(cudaMemcpyAsync(count0, ctx->b_count0.p, ctx->b_rows * 4, cudaMemcpyDeviceToHost, st));
+    if (pbwt) CK(cudaMemcpyAsync(pbwt, ctx->b_pbwt.p, 2 * ctx->b_rows * eimp_kw(K) * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+// ------------------------------------------------------------ GPUEngine drop-in
+
+int eimp_gpu_initialize(eimp_ctx *ctx, size_t K, size_t Kwords, size_t M, size_t Nrefhapscorr, size_t NrefhapsAD,
+                        size_t refTCapacity, const uint64_t *refTData) {
+    if (!ctx || !refTData || !K || !M || !NrefhapsAD || K > NrefhapsAD || Kwords != eimp_W(K) ||
+        refTCapacity < eimp_W(NrefhapsAD) * 8 || refTCapacity % 64)
+        return fail(ctx, EIMP_E_ARG, "eimp_gpu_initialize: inconsistent sizes");
+    if (int r = use_device(ctx)) return r;
+    ctx->g_K = K; ctx->g_Kwords = Kwords; ctx->g_M = M; ctx->g_Ncorr = Nrefhapscorr; ctx->g_NAD = NrefhapsAD;
+    ctx->g_refTcap = refTCapacity;
+    CK(ctx->g_refT.reserve(M * refTCapacity));
+    CK(cudaMemcpyAsync(ctx->g_refT.p, refTData, M * refTCapacity, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+size_t eimp_gpu_block_size(const eimp_ctx *ctx) { (void)ctx; return 1024; }
+
+}  // extern "C"
+
+namespace eimp {
+// unpack the reference GPU path's per-target inputs into genotype bytes,
+// split lists and best-haplotype lists (one CTA per target)
+__global__ void unpack_gpu_inputs(const uint64_t *__restrict__ gtw, const uint64_t *__restrict__ splitw,
+                                  const uint64_t *__restrict__ flagw, int M, int wM, int nhaps, int wN, int K,
+                                  uint8_t *__restrict__ gt, int32_t *__restrict__ splits, int32_t *__restrict__ nsplits,
+                                  int32_t *__restrict__ bh) {
+    const int t = blockIdx.x;
+    const uint64_t *g = gtw + (size_t)t * 2 * wM;
+    const uint64_t *s = splitw + (size_t)t * wM;
+    const uint64_t *f = flagw + (size_t)t * wN;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        int a = (g[2 * (m >> 6)] >> (m & 63)) & 1, b = (g[2 * (m >> 6) + 1] >> (m & 63)) & 1;
+        gt[(size_t)t * M + m] = (uint8_t)(a && b ? 3 : (a ? 0 : (b ? 2 : 1)));
+    }
+    if (threadIdx.x == 0) {
+        int n = 0;
+        for (int m = 0; m < M; m++) if ((s[m >> 6] >> (m & 63)) & 1) splits[(size_t)t * M + n++] = m;
+        nsplits[t] = n;
+        int k = 0;
+        if (K == nhaps) for (int h = 0; h < nhaps; h++) bh[(size_t)t * K + h] = h;
+        else for (int h = 0; h < nhaps && k < K; h++) if ((f[h >> 6] >> (h & 63)) & 1) bh[(size_t)t * K + k++] = h;
+    }
+}
+}  // namespace eimp
+
+extern "C" int eimp_gpu_run_cref_pbwt(eimp_ctx *ctx, size_t ntgt, const uint64_t *const *tgtData,
+                                      const uint64_t *const *splitData, const uint64_t *const *besthapData,
+                                      const uint32_t *crefTOffsets, uint32_t *const *cPBWT, int *const *count0s) {
+    if (!ctx || !ctx->g_M) return fail(ctx, EIMP_E_ARG, "eimp_gpu_run_cref_pbwt: engine not initialized");
+    if (!ntgt || ntgt > eimp_gpu_block_size(ctx) || !tgtData || !splitData || !besthapData || !crefTOffsets || !cPBWT ||
+        !count0s)
+        return fail(ctx, EIMP_E_ARG, "eimp_gpu_run_cref_pbwt: bad arguments");
+    if (int r = use_device(ctx)) return r;
+    // rows of the uploaded reference and the best-haplotype flags are
+    // refTCapacity bytes long (GPUEngine.cu:78)
+    const size_t M = ctx->g_M, K = ctx->g_K, nh = ctx->g_NAD, wM = eimp_W(M), wN = ctx->g_refTcap / 8;
+    const size_t wK = ctx->g_Kwords, stride = 4 * ctx->g_Kwords;
+    const size_t gtbytes = eimp_W(2 * M) * 8;   // tgtGTSize (GPUEngine.cu:76)
+    cudaStream_t st = ctx->stream;
+    DBuf hgt, hsp, hfl;
+    CK(hgt.reserve(ntgt * 2 * wM * 8));
+    CK(hsp.reserve(ntgt * wM * 8));
+    CK(hfl.reserve(ntgt * wN * 8));
+    CK(cudaMemsetAsync(hgt.p, 0, ntgt * 2 * wM * 8, st));
+    for (size_t t = 0; t < ntgt; t++) {
+        CK(cudaMemcpyAsync(hgt.as<uint64_t>() + t * 2 * wM, tgtData[t], gtbytes, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(hsp.as<uint64_t>() + t * wM, splitData[t], wM * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(hfl.as<uint64_t>() + t * wN, besthapData[t], wN * 8, cudaMemcpyHostToDevice, st));
+    }
+    CK(ctx->g_gt.reserve(ntgt * M));
+    CK(ctx->g_splits.reserve(ntgt * M * 4));
+    CK(ctx->g_nsplits.reserve(ntgt * 4));
+    CK(ctx->g_bh.reserve(ntgt * K * 4));
+    eimp::unpack_gpu_inputs<<<(unsigned)ntgt, 256, 0, st>>>(hgt.as<uint64_t>(), hsp.as<uint64_t>(), hfl.as<uint64_t>(),
+                                                             (int)M, (int)wM, (int)nh, (int)wN, (int)K,
+                                                             ctx->g_gt.as<uint8_t>(), ctx->g_splits.as<int32_t>(),
+                                                             ctx->g_nsplits.as<int32_t>(), ctx->g_bh.as<int32_t>());
+    ctx->launches++;
+    CK(cudaGetLastError());
+    std::vector<int64_t> ro(ntgt + 1);
+    for (size_t t = 0; t <= ntgt; t++) ro[t] = crefTOffsets[t];
+    const size_t rows = (size_t)ro[ntgt];
+    CK(ctx->g_rowoff.reserve((ntgt + 1) * 8));
+    CK(ctx->g_cref.reserve(rows * wK * 8));
+    CK(ctx->g_count0.reserve(rows * 4));
+    CK(ctx->g_pbwt.reserve(2 * rows * stride * 4));
+    CK(cudaMemcpyAsync(ctx->g_rowoff.p, ro.data(), (ntgt + 1) * 8, cudaMemcpyHostToDevice, st));
+    LAUNCH(launch_cref(ctx->g_gt.as<uint8_t>(), (int)ntgt, (int)M, ctx->g_refT.as<uint64_t>(), (int)nh, (int)wN,
+                       ctx->g_bh.as<int32_t>(), (int)K, ctx->g_splits.as<int32_t>(), ctx->g_nsplits.as<int32_t>(),
+                       ctx->g_rowoff.as<int64_t>(), ctx->g_cref.as<uint64_t>(), ctx->g_count0.as<int32_t>(), st));
+    LAUNCH(launch_pbwt(ctx->g_cref.as<uint64_t>(), ctx->g_count0.as<int32_t>(), ctx->g_rowoff.as<int64_t>(), (int)ntgt,
+                       (int)K, ctx->g_pbwt.as<uint32_t>(), stride, 1, st));
+    for (size_t t = 0; t < ntgt; t++) {
+        size_t nr = (size_t)(ro[t + 1] - ro[t]);
+        CK(cudaMemcpyAsync(cPBWT[t], ctx->g_pbwt.as<uint32_t>() + 2 * (size_t)ro[t] * stride, 2 * nr * stride * 4,
+                           cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(count0s[t], ctx->g_count0.as<int32_t>() + ro[t], nr * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}

@@ -1,0 +1,65 @@
+// Kernel launchers shared between the translation units of libeimp_b200.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+// set-maximal match search: warps (target haplotypes) per CTA, tree node
+// pool per warp (shared memory) and traversal stack depth
+#define SMM_WARPS 4
+#define SMM_NODES 512
+#define SMM_STACK 512
+
+namespace eimp {
+
+// ---- imputation (imp_kernels.cu)
+size_t refpbwt_smem(int K, int wN);
+cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint32_t *compr, int32_t *absperm,
+                           int32_t *count0, cudaStream_t st);
+cudaError_t launch_transpose(const uint64_t *src, size_t rows, size_t srcw, uint64_t *dst, size_t cols, size_t dstw,
+                             cudaStream_t st);
+cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
+                       const uint8_t *gt, int nhaps, int setmaxerrors, int4 *matches, int cap, int *nmatch,
+                       uint32_t *status, cudaStream_t st);
+cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,
+                          const uint64_t *hapmajor_full, int wMref, const int32_t *segm, const uint8_t *common,
+                          const float *af, int nrefhaps_total, const uint64_t *phased, int wM, const uint8_t *gt,
+                          int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *dos, int ldd,
+                          uint64_t *bits, int ldb, cudaStream_t st);
+cudaError_t launch_segmap(const int64_t *typed, int M, int Mref, int32_t *segm, uint8_t *common, cudaStream_t st);
+
+// ---- phasing preparation, condensed reference, PBWT (phase_prep.cu)
+cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int nhaps, int wM, int K,
+                            uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, cudaStream_t st);
+cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM,
+                               const int32_t *besthaps, int K, const float *cm, float cMmaxsplit, uint64_t *monos,
+                               int32_t *splits, int32_t *calls, float *cmdiffs, int32_t *nsplits, int32_t *ncalls,
+                               cudaStream_t st);
+cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *sitemajor, int nhaps, int wN,
+                        const int32_t *besthaps, int K, const int32_t *splits, const int32_t *nsplits,
+                        const int64_t *rowoff, uint64_t *cref, int32_t *count0, cudaStream_t st);
+cudaError_t launch_pbwt(const uint64_t *cref, const int32_t *count0, const int64_t *rowoff, int ntgt, int K,
+                        uint32_t *pbwt, size_t rowstride, int emit_padded, cudaStream_t st);
+
+// ---- beam phasing (beam.cu)
+struct BeamParams {
+    int K;
+    int H, P, Delta;
+    int Hf, Pf, Deltaf;
+    float expectIBDcM, pErr, pLimit;
+    float minfixsize, maxfixsize, minfixthr, maxfixthr;
+    int doPrePhasing, doRevPhasing;
+};
+struct BeamBuffers {
+    void *arena;          // per-target scratch arena
+    size_t arena_bytes;   // per target
+};
+size_t beam_arena_bytes(const BeamParams &p, int S_max);
+cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt, const uint64_t *monos,
+                        const int32_t *splits, const int32_t *nsplits, const int32_t *calls, const int32_t *ncalls,
+                        const float *cmdiffs, const uint32_t *pbwt, const int32_t *count0, const int64_t *rowoff,
+                        void *arena, size_t arena_bytes, uint64_t *mats, uint64_t *pats, float *dmat, float *dpat,
+                        float *totalconf, int32_t *ncallsites, uint32_t *status, cudaStream_t st);
+
+}  // namespace eimp

@@ -1,0 +1,266 @@
+"""Host-side mirror of the reference's GPU and imputation interfaces.
+
+* :class:`GPUEngine` -- GPUEngine (GPUEngine.h:41-99): initialize /
+  getBlockSize / runCrefPBWTKernel / free, same argument meaning.
+* :class:`Phaser` -- Target::prepPhase / Target::phase (Target.h:30-72) for a
+  batch of targets on the device.
+* :class:`PBWTImputer` -- PBWTImputer (PBWTImputer.h:30-64): prepareImputation /
+  imputeBunch.
+
+All work runs in libeimp_b200.so (CUDA, sm_100a); numpy arrays are host
+buffers, torch CUDA tensors can be passed to the ``*_dev`` methods.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _lib
+from ._lib import EimpError, EimpPhaseParams, ptr
+from .bits import W
+
+
+class Context:
+    """One eimp_ctx: a CUDA device, a stream and the device-resident state."""
+
+    def __init__(self, device: int = 0):
+        self.L = _lib.load()
+        h = C.c_void_p()
+        rc = self.L.eimp_create(device, C.byref(h))
+        if rc != 0:
+            raise EimpError(rc, f"eimp_create(device={device}) failed (no CUDA device?)")
+        self.h = h.value
+        self.device = device
+
+    def check(self, rc: int):
+        if rc != 0:
+            raise EimpError(rc, self.L.eimp_last_error(self.h).decode())
+
+    def synchronize(self):
+        self.check(self.L.eimp_synchronize(self.h))
+
+    @property
+    def launches(self) -> int:
+        return int(self.L.eimp_kernel_launches(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(self.L.eimp_stream(self.h) or 0)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.eimp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class PhaseParams:
+    """Phasing parameters with the reference defaults (Args.cpp:274-299)."""
+    K: int = 10000
+    hsize: int = 100
+    beamwidth: int = 128
+    delta: int = 24
+    hsize_fast: int = 30
+    beamwidth_fast: int = 64
+    delta_fast: int = 10
+    cMmaxsplit: float = 0.125
+    expectIBDcM: float = 2.0
+    hist: float = 1.0
+    pErr: float = 0.003
+    pLimit: float | None = None
+    minfixsize: float = 0.5
+    maxfixsize: float = 0.9
+    minfixthr: float = 0.99
+    maxfixthr: float = 1.0
+    doPrePhasing: bool = False
+    doRevPhasing: bool = True
+
+    def c(self) -> EimpPhaseParams:
+        d = {f.name: getattr(self, f.name) for f in fields(self)}
+        if d["pLimit"] is None:
+            d["pLimit"] = d["pErr"]
+        d["doPrePhasing"] = int(d["doPrePhasing"])
+        d["doRevPhasing"] = int(d["doRevPhasing"])
+        return EimpPhaseParams(**d)
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class GPUEngine:
+    """GPUEngine (GPUEngine.h:41-99) over libeimp_b200."""
+
+    def __init__(self, index: int = 0, ctx: Context | None = None):
+        self.ctx = ctx or Context(index)
+        self.index = index
+
+    def initialize(self, K, Kwords, M, Nrefhapscorr, NrefhapsAD, refTCapacity, refTData: np.ndarray):
+        self._refT = _c(refTData, np.uint64)
+        self.K, self.Kwords, self.M = K, Kwords, M
+        self.ctx.check(self.ctx.L.eimp_gpu_initialize(self.ctx.h, K, Kwords, M, Nrefhapscorr, NrefhapsAD,
+                                                      refTCapacity, ptr(self._refT)))
+
+    def getBlockSize(self) -> int:
+        return int(self.ctx.L.eimp_gpu_block_size(self.ctx.h))
+
+    def runCrefPBWTKernel(self, tgtData, splitdata, besthapdata, crefTOffsets, cPBWT, count0s):
+        n = len(tgtData)
+        keep = [_c(a, np.uint64) for a in tgtData] + [_c(a, np.uint64) for a in splitdata] + \
+               [_c(a, np.uint64) for a in besthapdata]
+        P = C.c_void_p * n
+        tg = P(*[ptr(a) for a in keep[:n]])
+        sp = P(*[ptr(a) for a in keep[n:2 * n]])
+        bh = P(*[ptr(a) for a in keep[2 * n:]])
+        off = _c(crefTOffsets, np.uint32)
+        for a in list(cPBWT) + list(count0s):
+            if not a.flags["C_CONTIGUOUS"]:
+                raise ValueError("output buffers must be contiguous")
+        outp = P(*[ptr(a) for a in cPBWT])
+        c0p = P(*[ptr(a) for a in count0s])
+        self.ctx.check(self.ctx.L.eimp_gpu_run_cref_pbwt(self.ctx.h, n, tg, sp, bh, ptr(off), outp, c0p))
+
+    def free(self):
+        self.ctx.close()
+
+
+class Phaser:
+    """Target::prepPhase / Target::phase for batches of targets on the device."""
+
+    def __init__(self, ctx: Context, hapmajor: np.ndarray, sitemajor: np.ndarray, cm: np.ndarray):
+        self.ctx = ctx
+        self.nhaps, self.wM = hapmajor.shape
+        self.M = sitemajor.shape[0]
+        ctx.check(ctx.L.eimp_phase_set_reference(ctx.h, self.M, self.nhaps, ptr(_c(hapmajor, np.uint64)),
+                                                 ptr(_c(sitemajor, np.uint64)), ptr(_c(cm, np.float32))))
+
+    def prep(self, params: PhaseParams, gt: np.ndarray):
+        gt = _c(gt, np.uint8)
+        n, M = gt.shape
+        K = min(params.K, self.nhaps)
+        out = dict(besthaps=np.zeros((n, K), np.int32), flags=np.zeros((n, W(self.nhaps)), np.uint64),
+                   monos=np.zeros((n, W(M)), np.uint64), splits=np.zeros((n, M), np.int32),
+                   calls=np.zeros((n, M), np.int32), cmdiffs=np.zeros((n, M + 1), np.float32),
+                   nsplits=np.zeros(n, np.int32), ncalls=np.zeros(n, np.int32))
+        p = params.c()
+        self.ctx.check(self.ctx.L.eimp_phase_prep(self.ctx.h, C.byref(p), n, ptr(gt), *[ptr(out[k]) for k in (
+            "besthaps", "flags", "monos", "splits", "calls", "cmdiffs", "nsplits", "ncalls")]))
+        return out
+
+    def cref_pbwt(self, params: PhaseParams, gt: np.ndarray):
+        gt = _c(gt, np.uint8)
+        n = gt.shape[0]
+        K = min(params.K, self.nhaps)
+        p = params.c()
+        rows = C.c_size_t(0)
+        self.ctx.check(self.ctx.L.eimp_phase_cref_pbwt(self.ctx.h, C.byref(p), n, ptr(gt), C.byref(rows),
+                                                       None, None, None, None))
+        R = rows.value
+        rowoff = np.zeros(n + 1, np.int64)
+        cref = np.zeros((R, W(K)), np.uint64)
+        c0 = np.zeros(R, np.int32)
+        pb = np.zeros((2 * R, 2 * ((K + 31) // 32)), np.uint32)
+        self.ctx.check(self.ctx.L.eimp_phase_cref_pbwt(self.ctx.h, C.byref(p), n, ptr(gt), C.byref(rows),
+                                                       ptr(rowoff), ptr(cref), ptr(c0), ptr(pb)))
+        return rowoff, cref, c0, pb
+
+    def phase(self, params: PhaseParams, gt: np.ndarray):
+        gt = _c(gt, np.uint8)
+        n, M = gt.shape
+        mats = np.zeros((n, W(M)), np.uint64)
+        pats = np.zeros((n, W(M)), np.uint64)
+        dm = np.zeros((n, M), np.float32)
+        dp = np.zeros((n, M), np.float32)
+        tc = np.zeros(n, np.float32)
+        nc = np.zeros(n, np.int32)
+        p = params.c()
+        self.ctx.check(self.ctx.L.eimp_phase_targets(self.ctx.h, C.byref(p), n, ptr(gt), ptr(mats), ptr(pats),
+                                                     ptr(dm), ptr(dp), ptr(tc), ptr(nc)))
+        return mats, pats, dm, dp, tc, nc
+
+    def phase_dev(self, params: PhaseParams, d_gt, d_mats, d_pats, d_dm, d_dp, d_tc, d_nc):
+        p = params.c()
+        n = d_gt.shape[0]
+        self.ctx.check(self.ctx.L.eimp_phase_targets_dev(self.ctx.h, C.byref(p), n, ptr(d_gt), ptr(d_mats),
+                                                         ptr(d_pats), ptr(d_dm), ptr(d_dp), ptr(d_tc), ptr(d_nc)))
+
+
+class PBWTImputer:
+    """PBWTImputer (PBWTImputer.h:30-64) over libeimp_b200.
+
+    The reference's per-block state machine (prepareBlocks / forwardBlock,
+    TargetImp.cpp:250-304, 437-471) becomes a stateless site window: block b
+    imputes ``[block_start[b], block_start[b] + bsize)`` per call and advances.
+    """
+
+    def __init__(self, ctx: Context, sitemajor_full: np.ndarray, af_full: np.ndarray, typed: np.ndarray,
+                 sitemajor_typed: np.ndarray, nhaps: int, setmaxerrors: int = 0, imputeCalls: bool = False):
+        self.ctx = ctx
+        self.Mref = sitemajor_full.shape[0]
+        self.M = len(typed)
+        self.nhaps = nhaps
+        self.setmaxerrors = setmaxerrors
+        self.imputeCalls = imputeCalls
+        ctx.check(ctx.L.eimp_imp_set_reference(ctx.h, self.Mref, nhaps, ptr(_c(sitemajor_full, np.uint64)),
+                                               ptr(_c(af_full, np.float32)), self.M, ptr(_c(typed, np.int64)),
+                                               ptr(_c(sitemajor_typed, np.uint64))))
+        self.ntargets = 0
+        self.block_pos = {}
+
+    def prepareImputation(self, phasedTargets: np.ndarray, gt: np.ndarray, num_sites_per_block=None,
+                          match_cap: int = 0):
+        phased = _c(phasedTargets, np.uint64)
+        gt = _c(gt, np.uint8)
+        self.ntargets = gt.shape[0]
+        assert phased.shape == (2 * self.ntargets, W(self.M))
+        self.ctx.check(self.ctx.L.eimp_imp_prepare(self.ctx.h, self.ntargets, ptr(phased), ptr(gt),
+                                                   self.setmaxerrors, int(self.imputeCalls), match_cap))
+        self.block_pos = {}
+        if num_sites_per_block is not None:
+            # first entry: sites of the left overlap to skip; block b starts
+            # after the sites of the blocks before it (TargetImp.cpp:250-272)
+            start = int(num_sites_per_block[0])
+            for b in range(1, len(num_sites_per_block) - 1):
+                self.block_pos[b - 1] = start
+                start += int(num_sites_per_block[b])
+        else:
+            self.block_pos[0] = 0
+
+    def imputeBunch(self, block: int, bsize: int):
+        """Next ``bsize`` sites of ``block``: (bits 2N x W(bsize), dosages 2N x bsize)."""
+        b0 = self.block_pos.get(block, 0)
+        n = max(0, min(bsize, self.Mref - b0))
+        bits, dos = self.impute_window(b0, n) if n else (np.zeros((2 * self.ntargets, W(bsize)), np.uint64),
+                                                         np.zeros((2 * self.ntargets, bsize), np.float32))
+        self.block_pos[block] = b0 + n
+        return bits, dos
+
+    def impute_window(self, mref_begin: int, nsites: int):
+        nh = 2 * self.ntargets
+        bits = np.zeros((nh, W(nsites)), np.uint64)
+        dos = np.zeros((nh, nsites), np.float32)
+        self.ctx.check(self.ctx.L.eimp_imp_bunch(self.ctx.h, mref_begin, nsites, ptr(bits), ptr(dos)))
+        return bits, dos
+
+    def matches(self, hap: int) -> np.ndarray:
+        n = C.c_size_t(0)
+        self.ctx.check(self.ctx.L.eimp_imp_matches(self.ctx.h, hap, None, 0, C.byref(n)))
+        out = np.zeros((n.value, 4), np.int32)
+        if n.value:
+            self.ctx.check(self.ctx.L.eimp_imp_matches(self.ctx.h, hap, ptr(out), n.value, C.byref(n)))
+        return out
+
+    def refpbwt(self):
+        kw = 2 * ((self.nhaps + 31) // 32)
+        compr = np.zeros((self.M, kw), np.uint32)
+        ap = np.zeros((self.M + 1, self.nhaps), np.int32)
+        self.ctx.check(self.ctx.L.eimp_imp_refpbwt(self.ctx.h, ptr(compr), ptr(ap)))
+        return compr, ap

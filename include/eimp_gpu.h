@@ -1,0 +1,189 @@
+/*
+ * eimp_gpu.h -- C ABI of the B200 (sm_100a) implementation of EagleImp's
+ * data-parallel hot path: condensed-reference build, PBWT + beam phasing and
+ * PBWT imputation.
+ *
+ * Conventions (same as the reference):
+ *  - bit vectors are uint64 words, least significant bit first, each row padded
+ *    to whole 512-bit units: W(n) = ceil(n/512)*8 words (Datatypes.h:70);
+ *  - genotypes are one byte per site: 0 hom-ref, 1 het, 2 hom-alt, 3 missing
+ *    (Datatypes.h:81-86);
+ *  - all functions return 0 on success and a non-zero EIMP_E_* code otherwise;
+ *    eimp_last_error() then describes the failure (the reference throws
+ *    thrust::system_error from checkCUDAError, GPUKernels.h:29-38, or calls
+ *    StatusFile::addError + exit; callers map a non-zero return to that);
+ *  - a context is bound to one CUDA device and one stream; calls on one context
+ *    must not overlap (one context per host thread, as the reference keeps one
+ *    GPUEngine per preprocessing thread, PBWTPhaser.cpp:484-488).
+ * There is no CPU fallback: every entry point runs CUDA kernels and fails when
+ * no device is present.
+ */
+#ifndef EIMP_GPU_H_
+#define EIMP_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    EIMP_OK = 0,
+    EIMP_E_CUDA = 1,        /* a CUDA runtime call failed */
+    EIMP_E_ARG = 2,         /* invalid argument or call order */
+    EIMP_E_CAPACITY = 3,    /* a fixed-capacity device structure overflowed */
+    EIMP_E_BEAM_EMPTY = 4,  /* "Beam is empty. No paths left." (Beam.cpp:466-470) */
+    EIMP_E_NOMEM = 5        /* device allocation failed */
+};
+
+typedef struct eimp_ctx eimp_ctx;
+
+/* Phasing parameters; defaults of the reference in brackets (Args.cpp:274-299,
+ * main.cpp:207-237, 305-306, 326). */
+typedef struct {
+    int K;              /* conditioning haplotypes [10000], clamped to Nrefhaps */
+    int hsize;          /* history size H [100] */
+    int beamwidth;      /* beam width P [128] */
+    int delta;          /* call delay Delta [24] */
+    int hsize_fast;     /* pre-phasing history [30] */
+    int beamwidth_fast; /* pre-phasing beam width [64] */
+    int delta_fast;     /* pre-phasing delta [10] */
+    float cMmaxsplit;   /* [0.125] */
+    float expectIBDcM;  /* [2.0] */
+    float hist;         /* history factor [1.0] */
+    float pErr;         /* genotype error probability [0.003] */
+    float pLimit;       /* beam probability limit [= pErr] */
+    float minfixsize, maxfixsize, minfixthr, maxfixthr;   /* [0.5, 0.9, 0.99, 1.0] */
+    int doPrePhasing;   /* [0] */
+    int doRevPhasing;   /* [1] */
+} eimp_phase_params;
+
+/* ---------------------------------------------------------------- context */
+
+/* Opens a context on CUDA device `device` (replaces GPUEngine::GPUEngine(int),
+ * GPUEngine.h:45). */
+int eimp_create(int device, eimp_ctx **out);
+/* Frees all device memory of the context (GPUEngine::free, GPUEngine.h:64). */
+void eimp_destroy(eimp_ctx *ctx);
+/* Human-readable description of the last failure on this context. */
+const char *eimp_last_error(const eimp_ctx *ctx);
+/* Blocks until all work on the context's stream is done. */
+int eimp_synchronize(eimp_ctx *ctx);
+/* Number of kernels this context has launched so far. */
+uint64_t eimp_kernel_launches(const eimp_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * work with it. */
+void *eimp_stream(eimp_ctx *ctx);
+
+/* ------------------------------------------ GPUEngine drop-in (cref + PBWT) */
+
+/* GPUEngine::initialize (GPUEngine.h:50, GPUEngine.cu:44-96): uploads the typed
+ * reference in site-major layout (M rows of refTCapacity bytes, haplotype bits
+ * of NrefhapsAD haplotypes).  Kwords = W(K). */
+int eimp_gpu_initialize(eimp_ctx *ctx, size_t K, size_t Kwords, size_t M, size_t Nrefhapscorr,
+                        size_t NrefhapsAD, size_t refTCapacity, const uint64_t *refTData);
+/* GPUEngine::getBlockSize (GPUEngine.h:53): targets per runCrefPBWT call. */
+size_t eimp_gpu_block_size(const eimp_ctx *ctx);
+/* GPUEngine::runCrefPBWTKernel (GPUEngine.h:55-61, GPUEngine.cu:98-217) for
+ * ntgt <= block size targets.  Per target t: tgtData[t] = GenotypeVector data
+ * (interleaved is0/is2 words), splitData[t] = split-site flags (W(M) words),
+ * besthapData[t] = best-haplotype flags (W(NrefhapsAD) words);
+ * crefTOffsets = exclusive prefix of (2*S_t+1), ntgt+1 entries.  Output:
+ * cPBWT[t] = forward rows then backward rows (sweep order), 4*Kwords uint32
+ * per row ([data, cumulative zeros] pairs, 1-padded tail word, zero padding
+ * words); count0s[t] = zeros per condensed row (2*S_t+1 ints). */
+int eimp_gpu_run_cref_pbwt(eimp_ctx *ctx, size_t ntgt, const uint64_t *const *tgtData,
+                           const uint64_t *const *splitData, const uint64_t *const *besthapData,
+                           const uint32_t *crefTOffsets, uint32_t *const *cPBWT, int *const *count0s);
+
+/* ------------------------------------------------------------- phasing */
+
+/* Uploads the typed reference for phasing: hapmajor (nhaps x W(M) words,
+ * VCFData::reference, VCFData.h:199), sitemajor (M x W(nhaps) words,
+ * VCFData::referenceT, VCFData.h:201) and the genetic positions of the typed
+ * sites in cM (VCFData::cMs, VCFData.h:227). */
+int eimp_phase_set_reference(eimp_ctx *ctx, size_t M, size_t nhaps, const uint64_t *hapmajor,
+                             const uint64_t *sitemajor, const float *cM);
+
+/* Target::prepPhase (Target.cpp:95-163) for a batch of targets, on the device:
+ * best haplotypes (K ascending indices per target), best-haplotype flags
+ * (W(nhaps) words), monomorphic sites (W(M) words), split sites and call
+ * locations (capacity M each, counts in nsplits / ncalls) and the split-site cM
+ * differences (capacity M+1).  gt: ntgt x M genotype bytes.  Any output pointer
+ * may be NULL. */
+int eimp_phase_prep(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *gt,
+                    int32_t *besthaps, uint64_t *flags, uint64_t *monos, int32_t *splits, int32_t *calls,
+                    float *cmdiffs, int32_t *nsplits, int32_t *ncalls);
+
+/* Target::condensedReferenceT + PBWT construction (Target.cpp:250-282,
+ * PBWT.cpp:33-70) for a batch: returns in *rows_out the total number of
+ * condensed rows sum_t (2*S_t+1); with cref/count0/pbwt non-NULL also copies
+ * the condensed reference (rows x W(K) words), count0 (rows) and the
+ * compressed PBWT (2*rows x 2*ceil(K/32) uint32: per target the forward rows
+ * then the backward rows in sweep order) -- call once with NULL buffers to size
+ * them. */
+int eimp_phase_cref_pbwt(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *gt,
+                         size_t *rows_out, int64_t *rowoff, uint64_t *cref, int32_t *count0, uint32_t *pbwt);
+
+/* Target::phase (Target.cpp:166-289) for a batch of diploid targets: mats/pats
+ * ntgt x W(M) words, dos_mats/dos_pats ntgt x M floats, totalconf and
+ * ncallsites per target (Target.h:73-74). */
+int eimp_phase_targets(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *gt,
+                       uint64_t *mats, uint64_t *pats, float *dos_mats, float *dos_pats, float *totalconf,
+                       int32_t *ncallsites);
+
+/* ----------------------------------------------------------- imputation */
+
+/* Reference for PBWTImputer (PBWTImputer.cpp:31-185): the full reference in
+ * site-major layout (Mref x W(nhaps) words, VCFData::referenceFullT,
+ * VCFData.h:211), its allele frequencies (Mref floats), the typed sites (M
+ * ascending indices into the full reference, VCFData::indexToRefFull) and the
+ * typed reference in site-major layout (M x W(nhaps) words).  Builds the
+ * reference PBWT with its prefix arrays on the device. */
+int eimp_imp_set_reference(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint64_t *sitemajor_full,
+                           const float *af_full, size_t M, const int64_t *typed, const uint64_t *sitemajor_typed);
+
+/* PBWTImputer::prepareImputation (PBWTImputer.cpp:63-185): set-maximal matches
+ * of ntargets diploid targets.  phased: 2*ntargets x W(M) words (mat, pat per
+ * target, as phasedTargets); gt: ntargets x M genotype bytes (missing = 3,
+ * VCFData::tgtmiss).  match_cap = matches stored per haplotype (0: M/4+64). */
+int eimp_imp_prepare(eimp_ctx *ctx, size_t ntargets, const uint64_t *phased, const uint8_t *gt,
+                     int setmaxerrors, int imputeCalls, size_t match_cap);
+
+/* PBWTImputer::imputeBunch (PBWTImputer.cpp:187-204) for the window of nsites
+ * reference sites starting at mref_begin: bits 2*ntargets x W(nsites) words,
+ * dos 2*ntargets x nsites floats.  Sites the reference imputes get the
+ * imputed allele and dosage (uncovered sites: dosage -1, DOSAGE_CONFLICT,
+ * TargetImp.cpp:26); typed non-missing sites, which the reference leaves
+ * unwritten, get the phased allele as bit and 0.0/1.0 dosage. */
+int eimp_imp_bunch(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t *bits, float *dos);
+
+/* Set-maximal matches found for one target haplotype: returns their number in
+ * *n; with out non-NULL copies up to cap matches as int32 quadruples (start,
+ * end, refstart, refend) -- TargetImp::Match, TargetImp.h:64-75. */
+int eimp_imp_matches(eimp_ctx *ctx, size_t hap, int32_t *out, size_t cap, size_t *n);
+
+/* Reference PBWT of the imputer: compressed rows (M x 2*ceil(nhaps/32) uint32)
+ * and prefix arrays ((M+1) x nhaps int32, PBWT::getSortOrder, PBWT.h:67). */
+int eimp_imp_refpbwt(eimp_ctx *ctx, uint32_t *compr, int32_t *absperm);
+
+/* ------------------------------------------- device-resident variants ----
+ * Same operations on device pointers (inputs already in HBM; outputs written to
+ * device memory; no host<->device copies, no synchronisation). */
+int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phased, const uint8_t *d_gt,
+                         int setmaxerrors, int imputeCalls, size_t match_cap);
+int eimp_imp_bunch_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t *d_bits, size_t ldb_words,
+                       float *d_dos, size_t ldd);
+int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint64_t *d_sitemajor_full,
+                               const float *d_af_full, size_t M, const int64_t *d_typed,
+                               const uint64_t *d_sitemajor_typed);
+int eimp_phase_targets_dev(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt,
+                           uint64_t *d_mats, uint64_t *d_pats, float *d_dos_mats, float *d_dos_pats,
+                           float *d_totalconf, int32_t *d_ncallsites);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EIMP_GPU_H_ */

@@ -226,6 +226,9 @@ typedef struct {
     int nfree, cap, used;
 } eo_pool;
 
+static int eo_peak_nodes = 0;
+int eo_smm_peak_nodes(void) { return eo_peak_nodes; }
+
 static int pool_new(eo_pool *p, int l, int r, long depth, int errors) {
     int i;
     if (p->nfree) i = p->freelist[--p->nfree];
@@ -237,6 +240,7 @@ static int pool_new(eo_pool *p, int l, int r, long depth, int errors) {
         }
         i = p->used++;
     }
+    if (p->used - p->nfree > eo_peak_nodes) eo_peak_nodes = p->used - p->nfree;
     eo_node *n = &p->nodes[i];
     n->left = n->right = -1; n->l = l; n->r = r; n->depth = depth; n->errors = errors;
     return i;

@@ -67,6 +67,9 @@ long eo_smmatches(const uint32_t *refpbwt, const int32_t *count0, size_t M, size
                   const uint64_t *hap, const int64_t *miss, size_t nmiss, int setmaxerrors,
                   int64_t *out, size_t maxmatches);
 
+/* largest number of live match-tree nodes seen by eo_smmatches in this process */
+int eo_smm_peak_nodes(void);
+
 /* a9: TargetImp::imputeBunch (TargetImp.cpp:474-558) over all Mref sites of
  * one target haplotype, block 0, no forwarding.  bits: W(Mref) words
  * (cleared here); dos: Mref floats; imputed (optional): 1 where the
