@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark of the EagleImp hot path on B200: phasing + PBWT imputation.
+
+Default workload: the full phase+impute configuration -- 10,000 reference
+haplotypes x 100,000 sites over 20 Mb (500 founders), 1,000 targets typed at
+5 % of the sites with 2 % missing, K=4096, beam width 128, 95,000 imputed
+sites.  Synthetic seeded data of that shape (the reference's panels are not
+available here).
+
+One step = one pass of the hot path over the batch of targets:
+  phasing (stage "phase", when built): best haplotypes, condensed reference,
+    PBWT, beam phasing of every target;
+  imputation: reference PBWT + prefix arrays of the typed sites, set-maximal
+    matches of every target haplotype, dosages of every reference site.
+The panel itself stays resident in HBM (as the reference keeps it in memory).
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the reference's own
+CPU implementation (compiled from its sources under oracle/_ref) on the host
+cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from eimp_b200 import synth  # noqa: E402
+from eimp_b200.bits import W, pack_rows  # noqa: E402
+
+CONFIG = "cfg2"
+METRIC = "imputed hap x site dosages/sec"
+UNIT = "dosages/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default=CONFIG)
+    ap.add_argument("--stages", default="impute", help="comma list of: phase, impute")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-targets", type=int, default=200)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thr = threading.Thread(target=self._read, daemon=True)
+            self.thr.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- workload
+def load_workload(cfgname):
+    cfg = synth.CONFIGS[cfgname]
+    panel, groups = synth.generate(cfg)
+    tg = groups[0]
+    hm, sm, cm = synth.typed_views(panel, tg.typed)
+    return cfg, panel, tg, hm, sm, cm
+
+
+def imputed_count(tg, Mref):
+    M = len(tg.typed)
+    miss = (tg.gt == 3).sum(axis=1)
+    return int(2 * ((Mref - M) * tg.gt.shape[0] + miss.sum()))
+
+
+# ---------------------------------------------------------------- reference arm / CPU baseline
+def cpu_reference_sample(cfg, panel, tg, ntgt, nthreads, stages):
+    """The reference's own CPU path (oracle/_ref) on a bounded target sample:
+    phasing (PBWTPhaser::phaseCPU loop) and/or PBWTImputer prepare + bunch."""
+    from oracle import refcore
+    sub = synth.Targets(tg.typed, np.ascontiguousarray(tg.gt[:ntgt]), np.ascontiguousarray(tg.truth[:2 * ntgt]))
+    rc = refcore.RefCore(panel, sub)
+    rc.set_params(refcore.PhaseParams(K=cfg.K, beamwidth=cfg.beam))
+    M = len(tg.typed)
+    t0 = time.perf_counter()
+    if "phase" in stages:
+        mats, pats, _, _ = rc.phase_range(0, ntgt, nthreads)
+        phased = np.zeros((2 * ntgt, W(M)), np.uint64)
+        phased[0::2] = mats
+        phased[1::2] = pats
+    else:
+        phased = pack_rows(sub.truth, W(M))
+    t1 = time.perf_counter()
+    dt_imp = 0.0
+    if "impute" in stages:
+        imp = rc.imputer(phased, nthreads)
+        imp.bunch(panel.nsites, nthreads)
+        imp.close()
+        dt_imp = time.perf_counter() - t1
+    dt = time.perf_counter() - t0
+    rc.close()
+    return dt, t1 - t0, dt_imp
+
+
+def cpu_port_sample(cfg, panel, tg, ntgt, nthreads, stages):
+    """The oracle restatement (when the reference build is absent)."""
+    from oracle import restate as R
+    M = len(tg.typed)
+    hm, sm, cm = synth.typed_views(panel, tg.typed)
+    t0 = time.perf_counter()
+    if "phase" in stages:
+        P = R.params_c(K=cfg.K, beamwidth=cfg.beam)
+        mats, pats, _, _ = R.phase_many(tg.gt[:ntgt], hm, sm, cm, P, nthreads)
+        phased = np.zeros((2 * ntgt, W(M)), np.uint64)
+        phased[0::2] = mats
+        phased[1::2] = pats
+    else:
+        phased = pack_rows(tg.truth[:2 * ntgt], W(M))
+    t1 = time.perf_counter()
+    if "impute" in stages:
+        compr, c0, ap = R.pbwt(sm, panel.nhaps, absperm=True)
+        for h in range(2 * ntgt):
+            miss = np.where(tg.gt[h // 2] == 3)[0].astype(np.int64)
+            m = R.smmatches(compr, c0, M, panel.nhaps, phased[h], miss)
+            R.impute(m, ap, panel.sitemajor, tg.typed, panel.af, panel.nhaps, miss, phased[h])
+    t2 = time.perf_counter()
+    return t2 - t0, t1 - t0, t2 - t1
+
+
+def cpu_baseline(cfg, panel, tg, ntgt, stages):
+    nthreads = os.cpu_count() or 1
+    from oracle import refcore
+    kind = "reference" if refcore.available() else "port"
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    os.dup2(devnull, 1)   # the reference prints progress to stdout
+    try:
+        if kind == "reference":
+            dt, dtp, dti = cpu_reference_sample(cfg, panel, tg, ntgt, nthreads, stages)
+        else:
+            dt, dtp, dti = cpu_port_sample(cfg, panel, tg, ntgt, nthreads if "phase" in stages else 1, stages)
+    finally:
+        os.dup2(saved, 1)
+        os.close(devnull)
+        os.close(saved)
+    sub = synth.Targets(tg.typed, tg.gt[:ntgt], tg.truth[:2 * ntgt])
+    dos = imputed_count(sub, panel.nsites)
+    out = {"value": dos / dt if "impute" in stages else None, "unit": UNIT, "cores": nthreads, "kind": kind,
+           "sample": f"{ntgt} of {tg.gt.shape[0]} targets ({2 * ntgt} haplotypes) x all {panel.nsites} sites, "
+                     f"stages {','.join(stages)}, {dt:.2f} s wall"}
+    if "phase" in stages:
+        out["phased_samples_per_sec"] = ntgt / dtp
+    return out, dt
+
+
+def run_reference_arm(args, rank):
+    stages = args.stages.split(",")
+    if rank != 0:
+        return
+    cfg, panel, tg, hm, sm, cm = load_workload(args.config)
+    ntgt = args.cpu_sample_targets
+    times = []
+    res = None
+    for i in range(args.warmup + args.steps):
+        res, dt = cpu_baseline(cfg, panel, tg, ntgt, stages)
+        if i >= args.warmup:
+            times.append(dt)
+    sub = synth.Targets(tg.typed, tg.gt[:ntgt], tg.truth[:2 * ntgt])
+    dos = imputed_count(sub, panel.nsites)
+    tot = float(np.sum(times))
+    value = dos * len(times) / tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64/f32",
+            "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
+            "config": config_block(cfg, panel, tg, stages),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
+                             "sample": res["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if "phased_samples_per_sec" in res:
+        line["phased_samples_per_sec"] = res["phased_samples_per_sec"]
+    print(json.dumps(line), flush=True)
+
+
+def config_block(cfg, panel, tg, stages):
+    return {"workload": f"{cfg.name}: {panel.nhaps} ref haps x {panel.nsites} sites, {tg.gt.shape[0]} targets "
+                        f"typed at {len(tg.typed)} sites, K={cfg.K}, beam={cfg.beam}",
+            "stages": stages, "ref_haps": panel.nhaps, "sites": panel.nsites, "typed_sites": len(tg.typed),
+            "targets": int(tg.gt.shape[0]), "K": cfg.K, "beam": cfg.beam,
+            "l2": "flushed between timed steps (256 MiB write) and outputs > L2"}
+
+
+# ---------------------------------------------------------------- our arm
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from eimp_b200.engine import Context
+    stages = args.stages.split(",")
+    cfg, panel, tg, hm, sm, cm = load_workload(args.config)
+    nt = tg.gt.shape[0]
+    M, Mref, nh_ref = len(tg.typed), panel.nsites, panel.nhaps
+    ctx = Context(local)
+    L, h = ctx.L, ctx.h
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+    def todev(a):
+        a = np.ascontiguousarray(a)
+        if a.dtype == np.uint64:
+            a = a.view(np.int64)
+        return torch.from_numpy(a).to(dev)
+
+    # resident panel + per-batch inputs
+    d_full = todev(panel.sitemajor)
+    d_af = todev(panel.af.astype(np.float32))
+    d_typed = todev(tg.typed.astype(np.int64))
+    d_sitetyped = todev(sm)
+    d_gt = todev(tg.gt.astype(np.uint8))
+    phased_h = pack_rows(tg.truth, W(M))
+    d_phased = todev(phased_h)
+    ldb = (Mref + 63) // 64
+    d_dos = torch.empty((2 * nt, Mref), dtype=torch.float32, device=dev)
+    d_bits = torch.empty((2 * nt, ldb), dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step_imp():
+        ctx.check(L.eimp_imp_set_reference_dev(h, Mref, nh_ref, d_full.data_ptr(), d_af.data_ptr(), M,
+                                               d_typed.data_ptr(), d_sitetyped.data_ptr()))
+        ctx.check(L.eimp_imp_prepare_dev(h, nt, d_phased.data_ptr(), d_gt.data_ptr(), 0, 0, 0))
+        ctx.check(L.eimp_imp_bunch_dev(h, 0, Mref, d_bits.data_ptr(), ldb, d_dos.data_ptr(), Mref))
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    kern = {"refpbwt": [], "smm": [], "dosage": []}
+
+    def step_timed():
+        e = [ev() for _ in range(4)]
+        e[0].record(stream)
+        ctx.check(L.eimp_imp_set_reference_dev(h, Mref, nh_ref, d_full.data_ptr(), d_af.data_ptr(), M,
+                                               d_typed.data_ptr(), d_sitetyped.data_ptr()))
+        e[1].record(stream)
+        ctx.check(L.eimp_imp_prepare_dev(h, nt, d_phased.data_ptr(), d_gt.data_ptr(), 0, 0, 0))
+        e[2].record(stream)
+        ctx.check(L.eimp_imp_bunch_dev(h, 0, Mref, d_bits.data_ptr(), ldb, d_dos.data_ptr(), Mref))
+        e[3].record(stream)
+        return e
+
+    for _ in range(args.warmup):
+        step_imp()
+    ctx.synchronize()
+    # status check once (capacity errors would surface here)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = ctx.launches
+    evs = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        evs.append(step_timed())
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    launches = ctx.launches - launches0
+    clocks = sampler.stop()
+    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
+    for e in evs:
+        kern["refpbwt"].append(e[0].elapsed_time(e[1]))
+        kern["smm"].append(e[1].elapsed_time(e[2]))
+        kern["dosage"].append(e[2].elapsed_time(e[3]))
+    tot_ms = float(np.sum(step_ms))
+    if world > 1:
+        t = torch.tensor([tot_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+        dist.barrier()
+    dos_per_step = imputed_count(tg, Mref)
+    value = world * dos_per_step * args.steps / (tot_ms / 1e3)
+
+    # roofline of the dominant kernel (dosages): algorithmic bytes per launch =
+    # dosage + bit outputs of every (haplotype, site) + one read of the
+    # haplotype-major panel
+    dos_ms = float(np.mean(kern["dosage"]))
+    bytes_dos = 2 * nt * Mref * 4 + 2 * nt * ldb * 8 + nh_ref * W(Mref) * 8
+    peak, peak_kind = measured_peak_hbm()
+    achieved = bytes_dos / (dos_ms / 1e3) / 1e9
+    roofline = {"kernel": "dosage_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": bytes_dos, "avg_launch_ms": dos_ms,
+                "stage_ms": {k: float(np.mean(v)) for k, v in kern.items()}}
+
+    # end to end through the public API: host (pinned) targets in, host dosages out
+    e2e = None
+    if rank == 0 or world > 1:
+        ph_pin = torch.from_numpy(phased_h.view(np.int64)).pin_memory()
+        gt_pin = torch.from_numpy(tg.gt.astype(np.uint8)).pin_memory()
+        dos_pin = torch.empty((2 * nt, Mref), dtype=torch.float32).pin_memory()
+        bits_pin = torch.empty((2 * nt, W(Mref)), dtype=torch.int64).pin_memory()
+        h2d = ph_pin.numel() * 8 + gt_pin.numel()
+        d2h = dos_pin.numel() * 4 + bits_pin.numel() * 8
+
+        def e2e_step():
+            ctx.check(L.eimp_imp_set_reference_dev(h, Mref, nh_ref, d_full.data_ptr(), d_af.data_ptr(), M,
+                                                   d_typed.data_ptr(), d_sitetyped.data_ptr()))
+            ctx.check(L.eimp_imp_prepare(h, nt, ph_pin.data_ptr(), gt_pin.data_ptr(), 0, 0, 0))
+            ctx.check(L.eimp_imp_bunch(h, 0, Mref, bits_pin.data_ptr(), dos_pin.data_ptr()))
+        e2e_step()
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        n_e2e = max(1, min(args.steps, 3))
+        for _ in range(n_e2e):
+            e2e_step()
+        ctx.synchronize()
+        dt = (time.perf_counter() - t0) / n_e2e
+        e2e = {"value": world * dos_per_step / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        cpu, _ = cpu_baseline(cfg, panel, tg, args.cpu_sample_targets, stages)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64/f32",
+                "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
+                "config": config_block(cfg, panel, tg, stages), "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches)}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

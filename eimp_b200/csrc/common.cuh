@@ -22,8 +22,9 @@ EIMP_D int bit_at(const uint64_t *v, size_t i) { return (int)((v[i >> 6] >> (i &
 // PBWT::decodeRelPerm (PBWT.cpp:367-382): position of element 'from' after
 // the stable 0/1 partition of this row
 EIMP_D int pbwt_rank(const uint32_t *row, int cnt0, int from) {
-    uint32_t off = row[2 * (from >> 5) + 1];
-    uint32_t field = row[2 * (from >> 5)];
+    const uint2 pr = reinterpret_cast<const uint2 *>(row)[from >> 5];   // [data, zeros] pair
+    uint32_t off = pr.y;
+    uint32_t field = pr.x;
     uint32_t mask = 1u << (from & 31);
     uint32_t bit = field & mask;
     field |= mask - 1u;

@@ -137,13 +137,23 @@ __global__ void transpose_kernel(const uint64_t *__restrict__ src, size_t rows, 
 
 // ---------------------------------------------------------------------------
 // set-maximal matches
+//
+// The history tree of TargetImp::processHistorySubTree lives in shared memory,
+// one pool per warp.  Per site: lane 0 lists the live nodes in pre-order, all
+// lanes map their intervals through the site's PBWT row in parallel (the
+// mapping of a node depends only on its own interval, and a node's interval is
+// not changed before the recursion reaches it), then lane 0 replays the
+// recursion iteratively with the precomputed mappings.
 // ---------------------------------------------------------------------------
-struct SmmNode { int left, right, l, r, depth, errors; };
-
+struct SmmNode {
+    int l, r;
+    int de;              // depth | errors << 24
+    short left, right;   // node indices, -1 = none
+};
 struct SmmFrame {
-    int lt, rt;          // slots (see slot encoding below)
-    int ldepth, rdepth;
-    uint8_t perase, e0, e1, stage, cerase;
+    short lt, rt;        // slots (see slot encoding)
+    int cdepth;          // max depth returned by the children
+    unsigned char st;    // bits: 0-1 stage, 2 perase, 3 extend0, 4 extend1
 };
 
 // slot encoding: s >= 0 -> node (s>>1).left (s&1==0) or .right (s&1==1);
@@ -152,15 +162,18 @@ struct SmmFrame {
 
 struct SmmWarpSmem {
     SmmNode node[SMM_NODES];
-    short freel[SMM_NODES];
-    short order[SMM_NODES];
     int4 map[SMM_NODES];
+    SmmFrame stack[SMM_NODES];
+    short order[SMM_NODES];
+    short freel[SMM_NODES];
 };
 
-__device__ __forceinline__ int &slot_ref(SmmWarpSmem &S, int &rootvar, int s) {
+__device__ __forceinline__ short &slot_ref(SmmWarpSmem &S, short &rootvar, int s) {
     if (s == SLOT_ROOT) return rootvar;
     return (s & 1) ? S.node[s >> 1].right : S.node[s >> 1].left;
 }
+__device__ __forceinline__ int de_depth(int de) { return de & 0xffffff; }
+__device__ __forceinline__ int de_err(int de) { return (int)((unsigned)de >> 24); }
 
 __global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
     const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
@@ -183,128 +196,127 @@ __global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
     for (int o = 16; o; o >>= 1) nmiss += __shfl_xor_sync(0xffffffffu, nmiss, o);
     if (nmiss > M / 2) { if (lane == 0) nmatch[hap] = 0; return; }
 
-    // pool
     int nfree = 0, used = 0;
-    int root = -1, nres = 0, treedepth = 0;
+    short root = -1;
+    int nres = 0, treedepth = 0;
     uint32_t err = 0;
-    SmmFrame stack[SMM_STACK];
 
-    auto pool_new = [&](int l, int r, int depth, int errors) -> int {
+    auto pool_new = [&](int l, int r, int de) -> int {
         int i;
         if (nfree) i = S.freel[--nfree];
         else if (used < SMM_NODES) i = used++;
         else { err |= EIMP_ERR_NODE_OVERFLOW; return -1; }
         SmmNode &n = S.node[i];
-        n.left = -1; n.right = -1; n.l = l; n.r = r; n.depth = depth; n.errors = errors;
+        n.left = -1; n.right = -1; n.l = l; n.r = r; n.de = de;
         return i;
     };
     auto pool_del = [&](int i) { S.freel[nfree++] = (short)i; };
+    auto merge_single = [&](short &slot) {
+        // TargetImp.cpp:405-415: a node with one child of equal mapping is
+        // replaced by that child
+        SmmNode &N = S.node[slot];
+        if (N.left >= 0 && N.right < 0) {
+            const SmmNode &C = S.node[N.left];
+            if (C.l == N.l && C.r == N.r && de_err(C.de) == de_err(N.de)) { int t = slot; slot = N.left; pool_del(t); }
+        } else if (N.left < 0 && N.right >= 0) {
+            const SmmNode &C = S.node[N.right];
+            if (C.l == N.l && C.r == N.r && de_err(C.de) == de_err(N.de)) { int t = slot; slot = N.right; pool_del(t); }
+        }
+    };
 
-    // one site (m < M: map + update; m == M: final erase pass)
-    // Processing of TargetImp.cpp:346-435 with an explicit stack; node
-    // mappings come precomputed in S.map (indexed by node).
+    // TargetImp.cpp:346-435 as an explicit-stack traversal (lane 0)
     auto process = [&](int lt0, int rt0, bool perase0, int m, int curr, int missing, int &newcount) -> int {
         int sp = 0;
-        stack[0].lt = lt0; stack[0].rt = rt0; stack[0].perase = perase0; stack[0].stage = 0;
-        stack[0].ldepth = 0; stack[0].rdepth = 0;
+        S.stack[0].lt = (short)lt0; S.stack[0].rt = (short)rt0; S.stack[0].cdepth = 0;
+        S.stack[0].st = perase0 ? 4 : 0;
         int ret = 0;
         while (sp >= 0) {
-            SmmFrame &f = stack[sp];
-            if (f.stage == 0) {
+            SmmFrame &f = S.stack[sp];
+            int stage = f.st & 3;
+            if (stage == 0) {
                 int L = slot_ref(S, root, f.lt);
-                int4 mp = f.perase ? make_int4(0, -1, 0, -1) : S.map[L];
-                bool empty0 = mp.x > mp.y, empty1 = mp.z > mp.w;
+                bool perase = f.st & 4;
+                int4 mp = perase ? make_int4(0, -1, 0, -1) : S.map[L];
                 SmmNode &N = S.node[L];
-                bool e0 = !empty0 && (missing || !curr || N.errors < setmaxerrors);
-                bool e1 = !empty1 && (missing || curr || N.errors < setmaxerrors);
+                int ne = de_err(N.de);
+                bool e0 = mp.x <= mp.y && (missing || !curr || ne < setmaxerrors);
+                bool e1 = mp.z <= mp.w && (missing || curr || ne < setmaxerrors);
                 if (e1) {
-                    int ni = pool_new(mp.z, mp.w, N.depth + 1, (curr || missing) ? N.errors : N.errors + 1);
+                    int ni = pool_new(mp.z, mp.w, (de_depth(N.de) + 1) | (((curr || missing) ? ne : ne + 1) << 24));
                     if (ni < 0) return -1;
-                    slot_ref(S, root, f.rt) = ni;
+                    slot_ref(S, root, f.rt) = (short)ni;
                 }
                 if (e0) {
-                    N.l = mp.x; N.r = mp.y; N.depth++;
-                    if (curr && !missing) N.errors++;
+                    N.l = mp.x; N.r = mp.y;
+                    N.de = (de_depth(N.de) + 1) | (((curr && !missing) ? ne + 1 : ne) << 24);
                 }
                 if (!e0 && !e1) {
-                    if (N.depth == treedepth && treedepth > 0) {
-                        if (nres + newcount < cap)
-                            out[nres + newcount] = make_int4(m - N.depth, m, N.l, N.r);
-                        else
-                            err |= EIMP_ERR_MATCH_OVERFLOW;
+                    int d = de_depth(N.de);
+                    if (d == treedepth && treedepth > 0) {
+                        if (nres + newcount < cap) out[nres + newcount] = make_int4(m - d, m, N.l, N.r);
+                        else err |= EIMP_ERR_MATCH_OVERFLOW;
                         newcount++;
                     }
                 }
-                f.e0 = e0; f.e1 = e1; f.cerase = !e0 && !e1;
-                f.stage = 1;
+                unsigned char st = (unsigned char)(1 | (perase ? 4 : 0) | (e0 ? 8 : 0) | (e1 ? 16 : 0));
+                f.st = st;
                 if (N.left >= 0) {
-                    if (sp + 1 >= SMM_STACK) { err |= EIMP_ERR_STACK_OVERFLOW; return -1; }
+                    if (sp + 1 >= SMM_NODES) { err |= EIMP_ERR_STACK_OVERFLOW; return -1; }
                     int R = slot_ref(S, root, f.rt);
-                    SmmFrame &c = stack[++sp];
-                    c.lt = 2 * L; c.rt = (R >= 0) ? 2 * R : f.rt;
-                    c.perase = f.cerase; c.stage = 0; c.ldepth = 0; c.rdepth = 0;
+                    SmmFrame &c = S.stack[++sp];
+                    c.lt = (short)(2 * L); c.rt = (short)((R >= 0) ? 2 * R : f.rt);
+                    c.cdepth = 0; c.st = (!e0 && !e1) ? 4 : 0;
                     continue;
                 }
+                stage = 1;
             }
-            if (f.stage == 1) {
-                f.stage = 2;
+            if (stage == 1) {
+                f.st = (f.st & ~3) | 2;
                 int L = slot_ref(S, root, f.lt);
                 if (S.node[L].right >= 0) {
-                    if (sp + 1 >= SMM_STACK) { err |= EIMP_ERR_STACK_OVERFLOW; return -1; }
+                    if (sp + 1 >= SMM_NODES) { err |= EIMP_ERR_STACK_OVERFLOW; return -1; }
                     int R = slot_ref(S, root, f.rt);
-                    SmmFrame &c = stack[++sp];
-                    c.lt = 2 * L + 1; c.rt = (R >= 0) ? 2 * R + 1 : f.rt;
-                    c.perase = f.cerase; c.stage = 0; c.ldepth = 0; c.rdepth = 0;
+                    bool ce = !(f.st & 8) && !(f.st & 16);
+                    SmmFrame &c = S.stack[++sp];
+                    c.lt = (short)(2 * L + 1); c.rt = (short)((R >= 0) ? 2 * R + 1 : f.rt);
+                    c.cdepth = 0; c.st = ce ? 4 : 0;
                     continue;
                 }
             }
-            // stage 2: post-processing
-            int depth = f.ldepth > f.rdepth ? f.ldepth : f.rdepth;
-            int &Ls = slot_ref(S, root, f.lt);
-            if (f.e0) {
-                SmmNode &N = S.node[Ls];
-                if (N.depth > depth) depth = N.depth;
-                if (N.left >= 0 && N.right < 0 && S.node[N.left].l == N.l && S.node[N.left].r == N.r &&
-                    S.node[N.left].errors == N.errors) {
-                    int t = Ls; Ls = N.left; pool_del(t);
-                } else if (N.left < 0 && N.right >= 0 && S.node[N.right].l == N.l && S.node[N.right].r == N.r &&
-                           S.node[N.right].errors == N.errors) {
-                    int t = Ls; Ls = N.right; pool_del(t);
-                }
+            // post-processing (TargetImp.cpp:392-432)
+            int depth = f.cdepth;
+            short &Ls = slot_ref(S, root, f.lt);
+            if (f.st & 8) {
+                int d = de_depth(S.node[Ls].de);
+                if (d > depth) depth = d;
+                merge_single(Ls);
             } else {
                 pool_del(Ls);
                 Ls = -1;
             }
-            if (f.e1) {
-                int &Rs = slot_ref(S, root, f.rt);
-                SmmNode &R = S.node[Rs];
-                if (R.depth > depth) depth = R.depth;
-                if (R.left >= 0 && R.right < 0 && S.node[R.left].l == R.l && S.node[R.left].r == R.r &&
-                    S.node[R.left].errors == R.errors) {
-                    int t = Rs; Rs = R.left; pool_del(t);
-                } else if (R.left < 0 && R.right >= 0 && S.node[R.right].l == R.l && S.node[R.right].r == R.r &&
-                           S.node[R.right].errors == R.errors) {
-                    int t = Rs; Rs = R.right; pool_del(t);
-                }
+            if (f.st & 16) {
+                short &Rs = slot_ref(S, root, f.rt);
+                int d = de_depth(S.node[Rs].de);
+                if (d > depth) depth = d;
+                merge_single(Rs);
             }
             sp--;
-            if (sp >= 0) {
-                if (stack[sp].stage == 1) stack[sp].ldepth = depth;
-                else stack[sp].rdepth = depth;
-            } else ret = depth;
+            if (sp >= 0) { if (depth > S.stack[sp].cdepth) S.stack[sp].cdepth = depth; }
+            else ret = depth;
         }
         return ret;
     };
 
-    if (lane == 0) root = pool_new(0, K - 1, 0, 0);
+    if (lane == 0) root = (short)pool_new(0, K - 1, 0);
     bool failed = false;
     for (int m = 0; m < M && !failed; m++) {
-        int curr = bit_at(hw, m);
-        int missing = g[m] == 3;
-        // pre-order of the tree below the (old) root, then map all nodes
+        const int curr = bit_at(hw, m);
+        const int missing = g[m] == 3;
+        // pre-order of the tree below the (old) root; S.stack doubles as the
+        // traversal stack (it is free between sites)
         int n = 0;
         if (lane == 0) {
-            int st[SMM_NODES];
+            short *st = reinterpret_cast<short *>(S.stack);
             int sp = 0;
             st[sp++] = root;
             while (sp) {
@@ -326,17 +338,18 @@ __global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
         }
         __syncwarp();
         if (lane == 0) {
-            int nr = pool_new(0, K - 1, 0, 0);
+            int nr = pool_new(0, K - 1, 0);
             if (nr < 0) failed = true;
             else {
                 S.node[nr].left = root;
-                root = nr;
+                root = (short)nr;
                 int newcount = 0;
                 int td = process(2 * root, 2 * root + 1, false, m, curr, missing, newcount);
                 if (td < 0) failed = true;
                 else {
                     // TargetImp.cpp:132-136: report only if no longer path is alive
-                    if (newcount && out[nres].y - out[nres].x >= td && nres + newcount <= cap) nres += newcount;
+                    if (newcount && nres < cap && out[nres].y - out[nres].x >= td && nres + newcount <= cap)
+                        nres += newcount;
                     treedepth = td;
                 }
             }
@@ -348,9 +361,7 @@ __global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
         if (!failed) {
             int newcount = 0;
             int td = process(SLOT_ROOT, SLOT_ROOT, true, M, 0, 0, newcount);
-            if (td >= 0) {
-                if (nres + newcount <= cap) nres += newcount;
-            }
+            if (td >= 0 && nres + newcount <= cap) nres += newcount;
         }
         nmatch[hap] = err ? -1 : nres;
         if (err) atomicOr(status, err);

@@ -5,11 +5,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-// set-maximal match search: warps (target haplotypes) per CTA, tree node
-// pool per warp (shared memory) and traversal stack depth
+// set-maximal match search: warps (target haplotypes) per CTA and the size of
+// the per-warp match-tree node pool in shared memory
 #define SMM_WARPS 4
 #define SMM_NODES 512
-#define SMM_STACK 512
 
 namespace eimp {
 
