@@ -21,6 +21,7 @@ cores instead.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import subprocess
@@ -48,7 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", default=CONFIG)
-    ap.add_argument("--stages", default="impute", help="comma list of: phase, impute")
+    ap.add_argument("--stages", default="phase,impute", help="comma list of: phase, impute")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-targets", type=int, default=200)
     return ap.parse_args()
@@ -281,30 +282,49 @@ def main():
     phased_h = pack_rows(tg.truth, W(M))
     d_phased = todev(phased_h)
     ldb = (Mref + 63) // 64
+    wM = W(M)
+    do_phase = "phase" in stages
+    from eimp_b200.engine import PhaseParams
+    pparams = PhaseParams(K=cfg.K, beamwidth=cfg.beam).c()
+    d_ph3 = torch.empty((nt, 2, wM), dtype=torch.int64, device=dev)     # phased haps, mat/pat interleaved
+    d_mats = torch.empty((nt, wM), dtype=torch.int64, device=dev)
+    d_pats = torch.empty((nt, wM), dtype=torch.int64, device=dev)
+    d_pdm = torch.empty((nt, M), dtype=torch.float32, device=dev)
+    d_pdp = torch.empty((nt, M), dtype=torch.float32, device=dev)
+    d_tc = torch.empty(nt, dtype=torch.float32, device=dev)
+    d_nc = torch.empty(nt, dtype=torch.int32, device=dev)
     d_dos = torch.empty((2 * nt, Mref), dtype=torch.float32, device=dev)
     d_bits = torch.empty((2 * nt, ldb), dtype=torch.int64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    def step_imp():
-        ctx.check(L.eimp_imp_set_reference_dev(h, Mref, nh_ref, d_full.data_ptr(), d_af.data_ptr(), M,
-                                               d_typed.data_ptr(), d_sitetyped.data_ptr()))
-        ctx.check(L.eimp_imp_prepare_dev(h, nt, d_phased.data_ptr(), d_gt.data_ptr(), 0, 0, 0))
-        ctx.check(L.eimp_imp_bunch_dev(h, 0, Mref, d_bits.data_ptr(), ldb, d_dos.data_ptr(), Mref))
-
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-    kern = {"refpbwt": [], "smm": [], "dosage": []}
+    kern = {"phase": [], "refpbwt": [], "smm": [], "dosage": []}
 
     def step_timed():
-        e = [ev() for _ in range(4)]
+        e = [ev() for _ in range(5)]
         e[0].record(stream)
+        if do_phase:
+            ctx.check(L.eimp_phase_targets_dev(h, C.byref(pparams), nt, d_gt.data_ptr(), d_mats.data_ptr(),
+                                               d_pats.data_ptr(), d_pdm.data_ptr(), d_pdp.data_ptr(),
+                                               d_tc.data_ptr(), d_nc.data_ptr()))
+            with torch.cuda.stream(stream):
+                d_ph3[:, 0].copy_(d_mats)
+                d_ph3[:, 1].copy_(d_pats)
+            src = d_ph3
+        else:
+            src = d_phased
+        e[1].record(stream)
         ctx.check(L.eimp_imp_set_reference_dev(h, Mref, nh_ref, d_full.data_ptr(), d_af.data_ptr(), M,
                                                d_typed.data_ptr(), d_sitetyped.data_ptr()))
-        e[1].record(stream)
-        ctx.check(L.eimp_imp_prepare_dev(h, nt, d_phased.data_ptr(), d_gt.data_ptr(), 0, 0, 0))
         e[2].record(stream)
-        ctx.check(L.eimp_imp_bunch_dev(h, 0, Mref, d_bits.data_ptr(), ldb, d_dos.data_ptr(), Mref))
+        ctx.check(L.eimp_imp_prepare_dev(h, nt, src.data_ptr(), d_gt.data_ptr(), 0, 0, 0))
         e[3].record(stream)
+        ctx.check(L.eimp_imp_bunch_dev(h, 0, Mref, d_bits.data_ptr(), ldb, d_dos.data_ptr(), Mref))
+        e[4].record(stream)
         return e
+
+    def step_imp():
+        step_timed()
 
     for _ in range(args.warmup):
         step_imp()
@@ -326,11 +346,12 @@ def main():
     torch.cuda.synchronize()
     launches = ctx.launches - launches0
     clocks = sampler.stop()
-    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
+    step_ms = [e[0].elapsed_time(e[4]) for e in evs]
     for e in evs:
-        kern["refpbwt"].append(e[0].elapsed_time(e[1]))
-        kern["smm"].append(e[1].elapsed_time(e[2]))
-        kern["dosage"].append(e[2].elapsed_time(e[3]))
+        kern["phase"].append(e[0].elapsed_time(e[1]))
+        kern["refpbwt"].append(e[1].elapsed_time(e[2]))
+        kern["smm"].append(e[2].elapsed_time(e[3]))
+        kern["dosage"].append(e[3].elapsed_time(e[4]))
     tot_ms = float(np.sum(step_ms))
     if world > 1:
         t = torch.tensor([tot_ms], device=dev)
@@ -362,7 +383,25 @@ def main():
         h2d = ph_pin.numel() * 8 + gt_pin.numel()
         d2h = dos_pin.numel() * 4 + bits_pin.numel() * 8
 
+        mats_pin = torch.empty((nt, wM), dtype=torch.int64).pin_memory()
+        pats_pin = torch.empty((nt, wM), dtype=torch.int64).pin_memory()
+        pdm_pin = torch.empty((nt, M), dtype=torch.float32).pin_memory()
+        pdp_pin = torch.empty((nt, M), dtype=torch.float32).pin_memory()
+        tc_pin = torch.empty(nt, dtype=torch.float32).pin_memory()
+        nc_pin = torch.empty(nt, dtype=torch.int32).pin_memory()
+        if do_phase:
+            h2d = 2 * gt_pin.numel() + ph_pin.numel() * 8   # genotypes (phasing + imputation) and phased haplotypes
+            d2h += (mats_pin.numel() + pats_pin.numel()) * 8 + (pdm_pin.numel() + pdp_pin.numel()) * 4 + nt * 8
+
         def e2e_step():
+            if do_phase:
+                # phasing through the host API (genotypes in, phased haplotypes and dosages out)
+                ctx.check(L.eimp_phase_targets(h, C.byref(pparams), nt, gt_pin.data_ptr(), mats_pin.data_ptr(),
+                                               pats_pin.data_ptr(), pdm_pin.data_ptr(), pdp_pin.data_ptr(),
+                                               tc_pin.data_ptr(), nc_pin.data_ptr()))
+                phv = ph_pin.view(nt, 2, wM)
+                phv[:, 0].copy_(mats_pin)
+                phv[:, 1].copy_(pats_pin)
             ctx.check(L.eimp_imp_set_reference_dev(h, Mref, nh_ref, d_full.data_ptr(), d_af.data_ptr(), M,
                                                    d_typed.data_ptr(), d_sitetyped.data_ptr()))
             ctx.check(L.eimp_imp_prepare(h, nt, ph_pin.data_ptr(), gt_pin.data_ptr(), 0, 0, 0))
@@ -389,6 +428,9 @@ def main():
                 "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
                 "config": config_block(cfg, panel, tg, stages), "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches)}
+        if do_phase:
+            line["phased_samples_per_sec"] = world * nt * args.steps / (tot_ms / 1e3)
+            line["phase_ms_per_step"] = float(np.mean(kern["phase"]))
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -424,6 +424,89 @@ int eimp_phase_cref_pbwt(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt,
     return 0;
 }
 
+namespace {
+
+size_t hist_len(int hsize, float hist) {
+    // Target.cpp:326,466: static_cast<size_t>((HistorySize * hist) + 0.5)
+    return (size_t)((double)((float)hsize * hist) + 0.5);
+}
+
+int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt, uint64_t *d_mats,
+              uint64_t *d_pats, float *d_dm, float *d_dp, float *d_tc, int32_t *d_nc) {
+    const size_t M = ctx->p_M, nh = ctx->p_nhaps;
+    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    BeamParams bp;
+    bp.K = (int)K;
+    bp.H = (int)hist_len(p->hsize, p->hist);
+    bp.Hf = (int)hist_len(p->hsize_fast, p->hist);
+    if (bp.H < 1 || bp.H > 128 || bp.Hf < 1 || bp.Hf > 128)
+        return fail(ctx, EIMP_E_ARG, "history length hsize*hist must be in 1..128 (BooleanHistory.cpp:31-37)");
+    if (p->beamwidth < 1 || p->beamwidth > 128 || p->beamwidth_fast < 1 || p->beamwidth_fast > 128)
+        return fail(ctx, EIMP_E_ARG, "beam width must be in 1..128");
+    bp.P = p->beamwidth; bp.Pf = p->beamwidth_fast;
+    bp.Delta = p->delta; bp.Deltaf = p->delta_fast;
+    bp.expectIBDcM = p->expectIBDcM; bp.pErr = p->pErr; bp.pLimit = p->pLimit;
+    bp.minfixsize = p->minfixsize; bp.maxfixsize = p->maxfixsize;
+    bp.minfixthr = p->minfixthr; bp.maxfixthr = p->maxfixthr;
+    bp.doPrePhasing = p->doPrePhasing; bp.doRevPhasing = p->doRevPhasing;
+    if (int r = run_prep(ctx, p, ntgt, d_gt)) return r;
+    std::vector<int64_t> ro;
+    if (int r = run_cref_pbwt(ctx, K, ntgt, d_gt, ro)) return r;
+    const size_t ab = beam_arena_bytes(bp, (int)M);
+    CK(ctx->b_arena.reserve(ntgt * ab));
+    LAUNCH(launch_beam(bp, (int)ntgt, (int)M, d_gt, ctx->b_monos.as<uint64_t>(), ctx->b_splits.as<int32_t>(),
+                       ctx->b_nsplits.as<int32_t>(), ctx->b_calls.as<int32_t>(), ctx->b_ncalls.as<int32_t>(),
+                       ctx->b_cmd.as<float>(), ctx->b_pbwt.as<uint32_t>(), ctx->b_count0.as<int32_t>(),
+                       ctx->b_rowoff.as<int64_t>(), ctx->b_arena.p, ab, d_mats, d_pats, d_dm, d_dp, d_tc, d_nc,
+                       ctx->status.as<uint32_t>(), ctx->stream));
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int eimp_phase_targets_dev(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt,
+                           uint64_t *d_mats, uint64_t *d_pats, float *d_dos_mats, float *d_dos_pats,
+                           float *d_totalconf, int32_t *d_ncallsites) {
+    if (int r = check_phase_args(ctx, p, ntgt)) return r;
+    if (!d_gt || !d_mats || !d_pats || !d_dos_mats || !d_dos_pats || !d_totalconf || !d_ncallsites)
+        return fail(ctx, EIMP_E_ARG, "eimp_phase_targets: NULL argument");
+    if (int r = use_device(ctx)) return r;
+    return run_phase(ctx, p, ntgt, d_gt, d_mats, d_pats, d_dos_mats, d_dos_pats, d_totalconf, d_ncallsites);
+}
+
+int eimp_phase_targets(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *gt, uint64_t *mats,
+                       uint64_t *pats, float *dos_mats, float *dos_pats, float *totalconf, int32_t *ncallsites) {
+    if (int r = check_phase_args(ctx, p, ntgt)) return r;
+    if (!gt || !mats || !pats || !dos_mats || !dos_pats || !totalconf || !ncallsites)
+        return fail(ctx, EIMP_E_ARG, "eimp_phase_targets: NULL argument");
+    if (int r = use_device(ctx)) return r;
+    const size_t M = ctx->p_M, wM = eimp_W(M);
+    cudaStream_t st = ctx->stream;
+    CK(ctx->b_gt.reserve(ntgt * M));
+    CK(ctx->b_out_mat.reserve(ntgt * wM * 8));
+    CK(ctx->b_out_pat.reserve(ntgt * wM * 8));
+    CK(ctx->b_out_dm.reserve(ntgt * M * 4));
+    CK(ctx->b_out_dp.reserve(ntgt * M * 4));
+    CK(ctx->b_out_tc.reserve(ntgt * 4));
+    CK(ctx->b_out_nc.reserve(ntgt * 4));
+    CK(cudaMemcpyAsync(ctx->b_gt.p, gt, ntgt * M, cudaMemcpyHostToDevice, st));
+    int r = run_phase(ctx, p, ntgt, ctx->b_gt.as<uint8_t>(), ctx->b_out_mat.as<uint64_t>(),
+                      ctx->b_out_pat.as<uint64_t>(), ctx->b_out_dm.as<float>(), ctx->b_out_dp.as<float>(),
+                      ctx->b_out_tc.as<float>(), ctx->b_out_nc.as<int32_t>());
+    if (r) return r;
+    CK(cudaMemcpyAsync(mats, ctx->b_out_mat.p, ntgt * wM * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(pats, ctx->b_out_pat.p, ntgt * wM * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(dos_mats, ctx->b_out_dm.p, ntgt * M * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(dos_pats, ctx->b_out_dp.p, ntgt * M * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(totalconf, ctx->b_out_tc.p, ntgt * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ncallsites, ctx->b_out_nc.p, ntgt * 4, cudaMemcpyDeviceToHost, st));
+    return check_status(ctx);
+}
+
+}  // extern "C"
+
 // ------------------------------------------------------------ GPUEngine drop-in
 
 int eimp_gpu_initialize(eimp_ctx *ctx, size_t K, size_t Kwords, size_t M, size_t Nrefhapscorr, size_t NrefhapsAD,

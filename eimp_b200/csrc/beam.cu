@@ -1,0 +1,1107 @@
+// Eagle2-style beam phasing over the condensed PBWT, one warp per target.
+//
+// Device restatement of Target::phaseExtPBWT (Target.cpp:291-777) with Beam
+// (Beam.cpp:41-837), BeamPath (BeamPath.cpp:29-291), HaplotypePath
+// (HaplotypePath.cpp:36-483), BooleanHistory (BooleanHistory.cpp:31-113),
+// History (History.h:29-81) and MinMaxHeap (MinMaxHeap.h:29-214).
+//
+// Work split inside the warp:
+//  * haplotype-path extensions (the PBWT interval mappings over the history,
+//    the bulk of the work) run one path per lane.  Each path's probabilities
+//    are accumulated in its own lane in the reference's order.  The reference
+//    copies intervals from the previously extended path (HaplotypePath.cpp:
+//    330-390); they are recomputed here, which gives the same intervals: an
+//    interval depends only on the recent history the two paths share;
+//  * beam-path extensions run one path per lane (per-path products; the
+//    maximum and the reference counts do not depend on the order);
+//  * pruning (min-max heap), merging, list order and the keep/switch sums
+//    follow the reference's sequential order on lane 0.
+// Floating point follows the reference operation by operation: float
+// arithmetic with explicit double where the reference promotes (pow(), double
+// literals, std::ilogb), explicit round-to-nearest intrinsics (no FMA).
+//
+// Storage per target lives in an arena in global memory: haplotype-path
+// records, their probability rings, a pool of interval buffers (a path owns
+// three: its intervals and its two extensions; copying a path hands over a
+// buffer instead of copying it), the beam in list order (two buffers), and
+// the constraint and probability vectors of the target.
+#include <climits>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace eimp {
+
+namespace {
+
+enum { C_HOMREF = 0, C_HETKEEP = 1, C_HETSWITCH = 2, C_HOMALT = 3, C_NONE = 4 };
+
+struct Cons { int type, refidx; };
+
+constexpr int PHMAX = 128;   // History<fp_type> ring (power of two >= H, H <= 128)
+constexpr int HT = 1024;     // merge hash table entries
+
+struct HPh {   // HaplotypePath
+    unsigned long long d0, d1;   // BooleanHistory data (fill mask applied)
+    int last;
+    float p;
+    int scaleexp;
+    int niv, next0, next1;       // lengths of pbwtInt and of the two extension vectors
+    float extp0, extp1;
+    int extscaleexp;
+    int refcnt0, refcnt1;
+    int phstart;
+    int biv, bext0, bext1;       // interval buffer ids
+    unsigned char active0, active1, toext0, toext1;
+};
+
+struct BPh {   // BeamPath
+    int mat, pat;
+    float prob, weight;
+    int nErr;
+    float pErrPath, pErrPathp1;
+    float extp[4];
+    unsigned char active[4];
+    int actidx;
+    int extgeno;
+};
+
+struct Hel { float key; int a; int b; };
+
+struct WS {   // per-warp shared state
+    float prec[PHMAX];
+    Hel heap[PHMAX + 2];
+    int2 ht[HT];
+    int cursor, curridx, refidx, reverse;
+    int nbp, bpsel, nhap, nfree, nivfree, err;
+    int H, P, Delta, phsize;
+    unsigned long long fill0, fill1;
+    int histlast;
+    int ires, ires2;
+    int wse, delerr;   // weightScaleExp and deleteErr of the last prune (Beam.cpp:673-678)
+    float fres;
+    const Cons *constr;
+};
+
+struct Ctx {
+    // arena
+    HPh *hp;
+    float *ph;
+    int2 *ivpool;
+    int *ivfree;
+    BPh *bpbuf[2];
+    int *happ, *happ_old;
+    int2 *hapmap;
+    int *fstack;
+    int *copies;
+    int NH, BPC, HMAX;
+    // pbwt of this target
+    const uint32_t *rows;
+    const int32_t *count0;
+    int Mp, K, kw;
+    float Kinv;
+    // condensed target
+    const float *cmd;
+    int S;
+    const int32_t *calls;
+    int ncalls;
+    const uint8_t *tg;
+    float pErr, pLimit, expectIBDcM;
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// std::ilogb(float) as glibc defines it: the unbiased exponent (subnormals
+// included), INT_MIN for zero and NaN, INT_MAX for infinity
+__device__ __forceinline__ int ilogb_exact(float x) {
+    const unsigned u = __float_as_uint(x) & 0x7fffffffu;
+    if (u == 0) return INT_MIN;
+    if (u >= 0x7f800000u) return u == 0x7f800000u ? INT_MAX : INT_MIN;
+    const int e = (int)(u >> 23);
+    if (e == 0) return (31 - __clz(u)) - 149;
+    return e - 127;
+}
+// pow(2, n) for an integer n, exact
+__device__ __forceinline__ double pow2i(int n) { return ldexp(1.0, n); }
+
+// ------------------------------------------------------------------ histories
+__device__ __forceinline__ void bh_push(HPh &h, int b, const WS &w) {   // BooleanHistory.cpp:55-70
+    unsigned long long c0 = h.d0 >> 63;
+    h.d0 = (h.d0 << 1) | (unsigned long long)(b ? 1 : 0);
+    h.d1 = (h.d1 << 1) | c0;
+    if (h.last != w.histlast) h.last++;
+    h.d0 |= w.fill0;
+    h.d1 |= w.fill1;
+}
+__device__ __forceinline__ int bh_at(const HPh &h, int pos) {
+    return (int)(((pos < 64 ? h.d0 : h.d1) >> (pos & 63)) & 1ull);
+}
+__device__ __forceinline__ int bh_equal(const HPh &a, const HPh &b) {
+    // BooleanHistory.cpp:91-97 compares a third 8-byte slot after the data
+    // words, i.e. the members 'last' and 'histlast'
+    return a.d0 == b.d0 && a.d1 == b.d1 && a.last == b.last;
+}
+
+__device__ __forceinline__ float *ph_ptr(const Ctx &c, int slot) { return c.ph + (size_t)slot * PHMAX; }
+__device__ __forceinline__ int2 *iv_buf(const Ctx &c, int b) { return c.ivpool + (size_t)b * c.HMAX; }
+
+// ------------------------------------------------------------------ pbwt
+__device__ __forceinline__ void pv_map(const Ctx &c, int reverse, int m, int l, int r, int &l0, int &r0, int &l1,
+                                       int &r1) {
+    const uint32_t *row = c.rows + (size_t)(reverse ? (2 * c.Mp - 1 - m) : m) * c.kw;
+    pbwt_map(row, c.count0[m], l, r, l0, r0, l1, r1);
+}
+
+// ------------------------------------------------------------------ min-max heap (MinMaxHeap.h)
+__device__ __forceinline__ int hlt(const Hel &x, const Hel &y) { return x.key < y.key; }
+__device__ __forceinline__ void hswap(Hel *h, int i, int j) { Hel t = h[i]; h[i] = h[j]; h[j] = t; }
+__device__ __forceinline__ int hminlevel(int i) { return ((31 - __clz(i + 1)) % 2) == 0; }
+__device__ __forceinline__ int hpar(int i) { return (i - 1) / 2; }
+
+__device__ void heap_bubble_helper(Hel *h, int i, int ismax) {
+    while (i != 0) {
+        int p = hpar(i);
+        if (p == 0) return;
+        int g = hpar(p);
+        if (hlt(h[i], h[g]) ^ ismax) { hswap(h, g, i); i = g; }
+        else return;
+    }
+}
+__device__ void heap_push(Hel *h, int &n, float key, int a, int b) {
+    h[n].key = key; h[n].a = a; h[n].b = b;
+    int i = n++;
+    if (i == 0) return;
+    int p = hpar(i);
+    if (hminlevel(i)) {
+        if (hlt(h[p], h[i])) { hswap(h, p, i); heap_bubble_helper(h, p, 1); }
+        else heap_bubble_helper(h, i, 0);
+    } else {
+        if (hlt(h[i], h[p])) { hswap(h, p, i); heap_bubble_helper(h, p, 0); }
+        else heap_bubble_helper(h, i, 1);
+    }
+}
+__device__ void heap_trickle(Hel *h, int n, int i) {
+    const int ismax = hminlevel(i) ? 0 : 1;
+    while (true) {
+        int ext = i, lc = 2 * i + 1;
+        if (lc < n && (hlt(h[lc], h[ext]) ^ ismax)) ext = lc;
+        if (lc + 1 < n && (hlt(h[lc + 1], h[ext]) ^ ismax)) ext = lc + 1;
+        int lg = 2 * lc + 1;
+        for (int k = 0; k < 4 && lg + k < n; ++k)
+            if (hlt(h[lg + k], h[ext]) ^ ismax) ext = lg + k;
+        if (i == ext) return;
+        hswap(h, i, ext);
+        if (ext - lc > 1) {
+            if (hlt(h[hpar(ext)], h[ext]) ^ ismax) hswap(h, hpar(ext), ext);
+            i = ext;
+        } else return;
+    }
+}
+__device__ Hel heap_popmin(Hel *h, int &n) {
+    Hel e = h[0];
+    if (n == 1) { n = 0; return e; }
+    hswap(h, 0, n - 1);
+    n--;
+    heap_trickle(h, n, 0);
+    return e;
+}
+__device__ __forceinline__ int heap_maxidx(const Hel *h, int n) {
+    if (n == 1) return 0;
+    if (n == 2) return 1;
+    return hlt(h[1], h[2]) ? 2 : 1;
+}
+
+// ------------------------------------------------------------------ haplotype paths
+__device__ int ivbuf_alloc(const Ctx &c, WS &w) {
+    if (w.nivfree == 0) { w.err |= EIMP_ERR_BEAM_CAPACITY; return 0; }
+    return c.ivfree[--w.nivfree];
+}
+__device__ __forceinline__ void ivbuf_free(const Ctx &c, WS &w, int b) { c.ivfree[w.nivfree++] = b; }
+
+__device__ void hp_new(const Ctx &c, WS &w, int slot, int alt) {   // HaplotypePath.cpp:36-53 (lane 0)
+    HPh &h = c.hp[slot];
+    h.d0 = w.fill0; h.d1 = w.fill1; h.last = -1;
+    bh_push(h, alt, w);
+    h.p = 1.0f; h.scaleexp = 0;
+    float *ph = ph_ptr(c, slot);
+    for (int i = 0; i < w.phsize; i++) ph[i] = 0.0f;
+    h.phstart = w.phsize - 1;
+    ph[h.phstart] = 1.0f;
+    h.niv = 0; h.next0 = 0; h.next1 = 0;
+    h.extp0 = 0.0f; h.extp1 = 0.0f; h.extscaleexp = 0;
+    h.refcnt0 = 0; h.refcnt1 = 0;
+    h.active0 = h.active1 = h.toext0 = h.toext1 = 0;
+    h.biv = ivbuf_alloc(c, w); h.bext0 = ivbuf_alloc(c, w); h.bext1 = ivbuf_alloc(c, w);
+}
+
+__device__ __forceinline__ void hp_mark_deleted(HPh &h, int e) {   // HaplotypePath.cpp:105-109
+    if (e == 0) { h.refcnt0--; if (h.refcnt0 == 0) h.active0 = 0; }
+    else { h.refcnt1--; if (h.refcnt1 == 0) h.active1 = 0; }
+}
+
+__device__ __forceinline__ void hp_mark_required(HPh &h, const Cons &cn) {   // HaplotypePath.cpp:139-158
+    if (cn.type == C_NONE) { h.toext0 = 1; h.toext1 = 1; return; }
+    int hb = bh_at(h, cn.refidx);
+    if ((cn.type == C_HETKEEP && hb == 0) || (cn.type == C_HETSWITCH && hb == 1) || cn.type == C_HOMREF)
+        h.toext0 = 1;
+    else if ((cn.type == C_HETKEEP && hb == 1) || (cn.type == C_HETSWITCH && hb == 0) || cn.type == C_HOMALT)
+        h.toext1 = 1;
+}
+
+// HaplotypePath::extend with updateScaling and calculateHaplotypeProbabilities
+// (HaplotypePath.cpp:162-479); returns extscaleexp
+__device__ int hp_extend(const Ctx &c, const WS &w, int slot, int cursor) {
+    HPh &h = c.hp[slot];
+    float *ph = ph_ptr(c, slot);
+    const int pm = w.phsize - 1;
+    {   // updateScaling (:224-258)
+        int e = ilogb_exact(h.p);
+        int ns = h.scaleexp;
+        if (abs(e) >= 20) {
+            ns += e;
+            double f = pow2i(-e);
+            for (int i = 0; i <= h.niv; i++) {
+                float *x = &ph[(i + h.phstart) & pm];
+                *x = (float)((double)*x * f);
+            }
+        }
+        h.extscaleexp = ns;
+    }
+    const int calc0 = h.toext0, calc1 = h.toext1;
+    const int2 *iv = iv_buf(c, h.biv);
+    int2 *e0 = iv_buf(c, h.bext0);
+    int2 *e1 = iv_buf(c, h.bext1);
+    const int lim = w.H < h.niv + 1 ? w.H : h.niv + 1;
+    float p0 = 0.0f, p1 = 0.0f;
+    int n0 = 0, n1 = 0;
+    const int cnt0 = c.count0[2 * cursor + 1];
+    const float t0 = __fmul_rn(ph[h.phstart & pm], w.prec[0]);
+    if (cnt0 > 0) {
+        if (calc0) p0 = __fmul_rn((float)cnt0, t0);
+        e0[n0++] = make_int2(0, cnt0 - 1);
+    }
+    if (cnt0 < c.K) {
+        if (calc1) p1 = __fmul_rn((float)(c.K - cnt0), t0);
+        e1[n1++] = make_int2(cnt0, c.K - 1);
+    }
+    const int rev = w.reverse;
+    const int incrow = rev ? 2 * (cursor + 1) : 2 * cursor;
+    int2 prevfrom = make_int2(0, -1);
+    for (int i = 1; i < lim; i++) {
+        const int2 from = iv[i - 1];
+        int a0 = 0, b0 = -1, a1 = 0, b1 = -1;
+        if (i > 1 && prevfrom.x == from.x && prevfrom.y == from.y) {   // :395-399
+            if (n0 == i) { a0 = e0[n0 - 1].x; b0 = e0[n0 - 1].y; }
+            if (n1 == i) { a1 = e1[n1 - 1].x; b1 = e1[n1 - 1].y; }
+        } else {
+            int cl, cr, il, ir;
+            pv_map(c, rev, incrow, from.x, from.y, cl, cr, il, ir);
+            pv_map(c, rev, 2 * cursor + 1, cl, cr, a0, b0, a1, b1);
+        }
+        prevfrom = from;
+        const float ti = __fmul_rn(ph[(i + h.phstart) & pm], w.prec[i]);
+        bool any = false;
+        if (a0 <= b0) {
+            if (calc0) p0 = __fadd_rn(p0, __fmul_rn((float)(b0 - a0 + 1), ti));
+            e0[n0++] = make_int2(a0, b0);
+            any = true;
+        }
+        if (a1 <= b1) {
+            if (calc1) p1 = __fadd_rn(p1, __fmul_rn((float)(b1 - a1 + 1), ti));
+            e1[n1++] = make_int2(a1, b1);
+            any = true;
+        }
+        if (!any) break;
+    }
+    h.next0 = n0; h.next1 = n1;
+    h.extp0 = p0; h.extp1 = p1;
+    h.active0 = h.toext0; h.active1 = h.toext1;
+    return h.extscaleexp;
+}
+
+// HaplotypePath::applyExtension (HaplotypePath.cpp:77-103)
+__device__ void hp_apply(const Ctx &c, const WS &w, int slot, int e) {
+    HPh &h = c.hp[slot];
+    bh_push(h, e, w);
+    h.p = e ? h.extp1 : h.extp0;
+    h.scaleexp = h.extscaleexp;
+    float *ph = ph_ptr(c, slot);
+    h.phstart = (h.phstart - 1) & (w.phsize - 1);
+    ph[h.phstart] = h.p;
+    int t = h.biv;
+    if (e) { h.biv = h.bext1; h.bext1 = t; h.niv = h.next1; }
+    else { h.biv = h.bext0; h.bext0 = t; h.niv = h.next0; }
+    h.next0 = 0; h.next1 = 0;
+    h.extp0 = 0.0f; h.extp1 = 0.0f; h.extscaleexp = 0;
+    h.active0 = h.active1 = h.toext0 = h.toext1 = 0;
+    h.refcnt0 = 0; h.refcnt1 = 0;
+}
+
+// ------------------------------------------------------------------ beam paths
+__device__ __forceinline__ int incon_(int ext, int g) {   // BeamPath.cpp:246-274
+    switch (g) {
+    case 1: return ext == 0 || ext == 3;
+    case 0: return ext > 0;
+    case 2: return ext < 3;
+    default: return 1;
+    }
+}
+__device__ __forceinline__ void bp_update_errors(BPh &b, int ext, int delerr, float pErr) {   // BeamPath.cpp:209-228
+    int add = (incon_(ext, b.extgeno) ? 1 : 0) - (delerr ? 1 : 0);
+    b.nErr += add;
+    if (add < 0) { b.pErrPathp1 = b.pErrPath; b.pErrPath = __fdiv_rn(b.pErrPath, pErr); }
+    else for (int a = 0; a < add; a++) { b.pErrPath = b.pErrPathp1; b.pErrPathp1 = __fmul_rn(b.pErrPathp1, pErr); }
+}
+__device__ __forceinline__ void bp_update_actidx(BPh &b) {
+    b.actidx = -1;
+    for (int i = 3; i >= 0; i--) if (b.active[i]) { b.actidx = i; break; }
+}
+__device__ __forceinline__ int bp_next_active(const BPh &b, int x) {
+    for (int i = x - 1; i >= 0; i--) if (b.active[i]) return i;
+    return -1;
+}
+__device__ __forceinline__ void bp_single(BPh &b, int id, float p1, float p2, float scale, int incon, float &maxP) {
+    float x = __fmul_rn(__fmul_rn(p1, p2), scale);
+    x = __fmul_rn(x, incon ? b.pErrPathp1 : b.pErrPath);
+    b.extp[id] = x;
+    if (maxP < x) maxP = x;
+    b.active[id] = 1;
+    b.actidx = id;
+}
+
+// BeamPath::extend (BeamPath.cpp:121-197); reference counts by atomics
+__device__ float bp_extend(const Ctx &c, BPh &b, int g, const Cons &cn, int bpscaleexp) {
+    b.extgeno = g;
+    HPh &pm = c.hp[c.happ[b.mat]];
+    HPh &pp = c.hp[c.happ[b.pat]];
+    const float pm0 = pm.extp0, pm1 = pm.extp1, pp0 = pp.extp0, pp1 = pp.extp1;
+    const int c0 = pm.active0, c1 = pm.active1, d0 = pp.active0, d1 = pp.active1;
+    const float scale = (float)pow2i(pm.extscaleexp + pp.extscaleexp + bpscaleexp);
+    float maxP = 0.0f;
+    const int t = cn.type;
+    const int hb = (t == C_HETKEEP || t == C_HETSWITCH) ? bh_at(pm, cn.refidx) : 0;
+    if (t == C_NONE || t == C_HOMREF) {
+        if (c0 && d0) { bp_single(b, 0, pm0, pp0, scale, incon_(0, g), maxP); atomicAdd(&pm.refcnt0, 1); atomicAdd(&pp.refcnt0, 1); }
+    }
+    if (t == C_NONE || (t == C_HETKEEP && hb == 0) || (t == C_HETSWITCH && hb == 1)) {
+        if (c0 && d1) { bp_single(b, 1, pm0, pp1, scale, incon_(1, g), maxP); atomicAdd(&pm.refcnt0, 1); atomicAdd(&pp.refcnt1, 1); }
+    }
+    if (t == C_NONE || (t == C_HETKEEP && hb == 1) || (t == C_HETSWITCH && hb == 0)) {
+        if (c1 && d0) { bp_single(b, 2, pm1, pp0, scale, incon_(2, g), maxP); atomicAdd(&pm.refcnt1, 1); atomicAdd(&pp.refcnt0, 1); }
+    }
+    if (t == C_NONE || t == C_HOMALT) {
+        if (c1 && d1) { bp_single(b, 3, pm1, pp1, scale, incon_(3, g), maxP); atomicAdd(&pm.refcnt1, 1); atomicAdd(&pp.refcnt1, 1); }
+    }
+    return maxP;
+}
+
+__device__ __forceinline__ void bp_mark_deleted(const Ctx &c, BPh &b, int ext) {   // BeamPath.cpp:101-112
+    b.active[ext] = 0;
+    hp_mark_deleted(c.hp[c.happ[b.mat]], ext / 2);
+    hp_mark_deleted(c.hp[c.happ[b.pat]], ext % 2);
+    bp_update_actidx(b);
+}
+
+// ------------------------------------------------------------------ beam
+__device__ void beam_calc_rec(const Ctx &c, WS &w) {   // Beam.cpp:541-573 (lane 0)
+    const int cur = w.cursor;
+    int ci = w.reverse ? cur + 1 : cur;
+    const float cursordiff = w.reverse ? c.cmd[cur] : c.cmd[cur + 1];
+    float cd = 0.0f;
+    for (int i = 0; i < w.H; i++) {
+        float tmp1 = (float)(1.0 + (double)__fdiv_rn(cd, c.expectIBDcM));
+        float pr = (float)(1.0 / (double)__fmul_rn(tmp1, tmp1));
+        float tmp2 = (float)(1.0 + (double)__fdiv_rn(__fadd_rn(cd, cursordiff), c.expectIBDcM));
+        pr = (float)((double)pr - 1.0 / (double)__fmul_rn(tmp2, tmp2));
+        pr = fmaxf(fminf(pr, 1.0f), 0.000001f);
+        w.prec[i] = __fmul_rn(pr, c.Kinv);
+        cd = __fadd_rn(cd, c.cmd[ci]);
+        if (w.reverse) { ci++; if (ci >= c.S + 1) break; }
+        else { if (ci == 0) break; ci--; }
+    }
+}
+
+__device__ void beam_init(const Ctx &c, WS &w, const Cons *constr, int reverse, int H, int P, int Delta) {
+    if (lane_id() == 0) {   // Beam.cpp:41-92
+        w.H = H; w.P = P; w.Delta = Delta;
+        int l2 = 31 - __clz(H);
+        if ((1 << l2) != H) l2++;
+        w.phsize = 1 << l2;
+        w.histlast = H - 1;
+        int lw = (H - 1) / 64;
+        unsigned long long mlw = (H % 64 == 0) ? 0ull : ~((1ull << (H % 64)) - 1ull);
+        w.fill0 = 0 < lw ? 0ull : (0 == lw ? mlw : ~0ull);
+        w.fill1 = 1 < lw ? 0ull : (1 == lw ? mlw : ~0ull);
+        w.reverse = reverse;
+        w.constr = constr;
+        w.cursor = reverse ? c.S : -1;
+        w.curridx = -1; w.refidx = -1;
+        w.err = 0;
+        for (int i = 0; i < PHMAX; i++) w.prec[i] = 0.0f;
+        w.nfree = c.NH;
+        for (int i = 0; i < c.NH; i++) c.fstack[i] = c.NH - 1 - i;
+        w.nivfree = 3 * c.NH;
+        for (int i = 0; i < 3 * c.NH; i++) c.ivfree[i] = 3 * c.NH - 1 - i;
+        int mat = c.fstack[--w.nfree], pat = c.fstack[--w.nfree];
+        hp_new(c, w, mat, 0);
+        hp_new(c, w, pat, 1);
+        c.happ[0] = mat; c.happ[1] = pat;
+        w.nhap = 2;
+        w.bpsel = 0;
+        BPh &b = c.bpbuf[0][0];
+        b.mat = 0; b.pat = 1; b.weight = 1.0f;
+        b.nErr = 0; b.pErrPath = 1.0f; b.pErrPathp1 = __fmul_rn(1.0f, c.pErr);
+        b.prob = (float)(pow2i(0) * (double)c.hp[mat].p * (double)c.hp[pat].p * 1.0);
+        for (int i = 0; i < 4; i++) { b.extp[i] = 0.0f; b.active[i] = 0; }
+        b.actidx = -1; b.extgeno = 3;
+        w.nbp = 1;
+    }
+    __syncwarp();
+}
+
+// Beam::prunePaths (Beam.cpp:577-787) -- filter + heap part, lane 0.
+// Returns 0 when no extension survives (the beam would be empty).
+__device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn) {
+    const float limit = __fmul_rn(c.pLimit, maxP);
+    BPh *bp = c.bpbuf[w.bpsel];
+    Hel *hq = w.heap;
+    int n = 0;
+    for (int it = 0; it < w.nbp; it++) {
+        BPh &b = bp[it];
+        int ex = b.actidx;
+        while (ex >= 0) {
+            float p = b.extp[ex];
+            if (p >= limit) {
+                if (n < w.P || (n == w.P && p > hq[0].key)) {
+                    if (n == w.P) {
+                        Hel e = heap_popmin(hq, n);
+                        bp_mark_deleted(c, bp[e.a], e.b);
+                    }
+                    heap_push(hq, n, p, it, ex);
+                } else bp_mark_deleted(c, b, ex);
+            } else bp_mark_deleted(c, b, ex);
+            ex = cn.type == C_NONE ? ex - 1 : -1;
+        }
+    }
+    if (n == 0) return 0;
+    w.wse = -ilogb_exact(bp[hq[0].a].weight);                    // weightScaleExp
+    w.delerr = bp[hq[heap_maxidx(hq, n)].a].nErr > 0;            // deleteErr
+    return 1;
+}
+
+// apply the haplotype-path extensions (Beam.cpp:684-726).  Lane 0 plans the
+// new order; the warp copies the probability rings of duplicated paths; the
+// lanes then apply the extensions.
+__device__ void beam_apply_hap(const Ctx &c, WS &w) {
+    const int lane = lane_id();
+    if (lane == 0) {
+        const int nold = w.nhap;
+        for (int i = 0; i < nold; i++) c.happ_old[i] = c.happ[i];
+        int next0 = 0;
+        for (int i = 0; i < nold; i++) if (c.hp[c.happ_old[i]].active0) next0++;
+        int one = next0, zero = 0, ncopy = 0;
+        for (int i = 0; i < nold; i++) {
+            int id = c.happ_old[i];
+            HPh &h = c.hp[id];
+            c.hapmap[i] = make_int2(zero, one);
+            if (!(h.active0 || h.active1)) {
+                c.fstack[w.nfree++] = id;
+                ivbuf_free(c, w, h.biv); ivbuf_free(c, w, h.bext0); ivbuf_free(c, w, h.bext1);
+                continue;
+            }
+            if (h.active0 && h.active1) {
+                if (w.nfree == 0) { w.err |= EIMP_ERR_BEAM_CAPACITY; break; }
+                int cp = c.fstack[--w.nfree];
+                c.happ[one++] = cp;
+                c.happ[zero++] = id;
+                c.copies[2 * ncopy] = id;
+                c.copies[2 * ncopy + 1] = cp;
+                ncopy++;
+                continue;
+            }
+            if (h.active0) c.happ[zero++] = id;
+            else c.happ[one++] = id;
+        }
+        // the old list (for applying) after the copies
+        w.ires = ncopy;
+        w.ires2 = nold;
+        w.nhap = one;
+        // records of the copies (HaplotypePath.cpp:55-75): the copy takes the
+        // extension-1 intervals as its own; the source gets a fresh buffer
+        for (int k = 0; k < ncopy; k++) {
+            HPh &o = c.hp[c.copies[2 * k]];
+            HPh &n = c.hp[c.copies[2 * k + 1]];
+            n.d0 = o.d0; n.d1 = o.d1; n.last = o.last;
+            n.p = o.extp1; n.scaleexp = o.extscaleexp;
+            n.phstart = o.phstart;
+            n.biv = o.bext1; n.niv = o.next1;
+            n.bext0 = ivbuf_alloc(c, w); n.bext1 = ivbuf_alloc(c, w);
+            n.next0 = 0; n.next1 = 0;
+            n.active0 = n.active1 = n.toext0 = n.toext1 = 0;
+            n.refcnt0 = 0; n.refcnt1 = 0;
+            n.extp0 = 0.0f; n.extp1 = 0.0f; n.extscaleexp = 0;
+            o.bext1 = ivbuf_alloc(c, w);
+            o.next1 = 0;   // (the reference keeps a stale copy; it is rewritten before use)
+        }
+    }
+    __syncwarp();
+    const int ncopy = w.ires, nold = w.ires2;
+    // probability rings of the copies
+    const int phs = w.phsize;
+    for (int e = lane; e < ncopy * phs; e += 32) {
+        int k = e / phs, i = e % phs;
+        ph_ptr(c, c.copies[2 * k + 1])[i] = ph_ptr(c, c.copies[2 * k])[i];
+    }
+    __syncwarp();
+    // new paths: push bit 1 and the extension-1 probability
+    for (int k = lane; k < ncopy; k += 32) {
+        int slot = c.copies[2 * k + 1];
+        HPh &n = c.hp[slot];
+        bh_push(n, 1, w);
+        float *ph = ph_ptr(c, slot);
+        n.phstart = (n.phstart - 1) & (phs - 1);
+        ph[n.phstart] = n.p;
+    }
+    // old paths still alive: apply their (single or zero) extension
+    for (int i = lane; i < nold; i += 32) {
+        int id = c.happ_old[i];
+        HPh &h = c.hp[id];
+        if (!(h.active0 || h.active1)) continue;
+        hp_apply(c, w, id, h.active0 ? 0 : 1);
+    }
+    __syncwarp();
+}
+
+// apply the beam-path extensions (Beam.cpp:728-779), lane 0: survivors keep
+// their order, extra extensions of a path are appended in the reference's
+// order (descending extension index, the lowest is applied in place)
+__device__ void beam_apply_bp(const Ctx &c, WS &w) {
+    if (lane_id() == 0) {
+        const int wse = w.wse, delerr = w.delerr;
+        BPh *src = c.bpbuf[w.bpsel];
+        BPh *dst = c.bpbuf[w.bpsel ^ 1];
+        const double wsf = pow2i(wse);
+        int n = 0;
+        for (int it = 0; it < w.nbp; it++) {
+            if (src[it].actidx >= 0) n++;
+        }
+        int napp = n;
+        int k = 0;
+        for (int it = 0; it < w.nbp; it++) {
+            BPh &b = src[it];
+            int ex = b.actidx;
+            if (ex < 0) continue;
+            int2 mm = c.hapmap[b.mat], pm = c.hapmap[b.pat];
+            int mat[2] = {mm.x, mm.y}, pat[2] = {pm.x, pm.y};
+            int nx = bp_next_active(b, ex);
+            while (nx != -1) {
+                if (napp >= c.BPC) { w.err |= EIMP_ERR_BEAM_CAPACITY; return; }
+                BPh &o = dst[napp++];   // BeamPath.cpp:44-68
+                o.mat = mat[ex / 2]; o.pat = pat[ex % 2];
+                o.prob = b.extp[ex]; o.weight = b.weight;
+                o.nErr = b.nErr; o.pErrPath = b.pErrPath; o.pErrPathp1 = b.pErrPathp1;
+                o.extgeno = b.extgeno;
+                if (wse != 0) o.weight = (float)((double)o.weight * wsf);
+                bp_update_errors(o, ex, delerr, c.pErr);
+                for (int q = 0; q < 4; q++) { o.extp[q] = 0.0f; o.active[q] = 0; }
+                o.actidx = -1; o.extgeno = 3;
+                ex = nx;
+                nx = bp_next_active(b, nx);
+            }
+            BPh &o = dst[k++];   // BeamPath.cpp:70-96
+            o.mat = mat[ex / 2]; o.pat = pat[ex % 2];
+            o.prob = b.extp[ex]; o.weight = b.weight;
+            o.nErr = b.nErr; o.pErrPath = b.pErrPath; o.pErrPathp1 = b.pErrPathp1;
+            o.extgeno = b.extgeno;
+            if (wse != 0) o.weight = (float)((double)o.weight * wsf);
+            bp_update_errors(o, ex, delerr, c.pErr);
+            for (int q = 0; q < 4; q++) { o.extp[q] = 0.0f; o.active[q] = 0; }
+            o.actidx = -1; o.extgeno = 3;
+        }
+        w.nbp = napp;
+        w.bpsel ^= 1;
+    }
+    __syncwarp();
+}
+
+// Beam::mergePaths (Beam.cpp:790-837), lane 0
+__device__ void beam_merge(const Ctx &c, WS &w) {
+    if (lane_id() == 0) {
+        BPh *bp = c.bpbuf[w.bpsel];
+        for (int i = 0; i < HT; i++) w.ht[i].x = -1;
+        const int n = w.nbp;
+        int keep = 0;
+        // erased flags in extp[0] sign bit is not usable: keep a separate mark
+        for (int it = 0; it < n; it++) bp[it].actidx = 0;   // 0 = alive, -2 = erased (actidx is -1 anyway here)
+        for (int it = 0; it < n; it++) {
+            BPh &b = bp[it];
+            int mr = b.mat;
+            while (mr > 0 && bh_equal(c.hp[c.happ[mr]], c.hp[c.happ[mr - 1]])) mr--;
+            int pr = b.pat;
+            while (pr > 0 && bh_equal(c.hp[c.happ[pr]], c.hp[c.happ[pr - 1]])) pr--;
+            int k0 = mr < pr ? mr : pr, k1 = mr < pr ? pr : mr;
+            int key = (k0 << 16) | k1;
+            int hsh = (int)(((unsigned)key * 2654435761u) >> 22) & (HT - 1);
+            int found = -1, slot = hsh;
+            while (w.ht[slot].x != -1) {
+                if (w.ht[slot].x == key) { found = slot; break; }
+                slot = (slot + 1) & (HT - 1);
+            }
+            if (found >= 0) {
+                BPh &o = bp[w.ht[found].y];
+                if (o.prob > b.prob) {
+                    o.weight = __fadd_rn(o.weight, __fmul_rn(b.weight, __fdiv_rn(b.prob, o.prob)));
+                    b.actidx = -2;
+                } else {
+                    b.weight = __fadd_rn(b.weight, __fmul_rn(o.weight, __fdiv_rn(o.prob, b.prob)));
+                    o.actidx = -2;
+                    w.ht[found].y = it;
+                }
+            } else {
+                w.ht[slot] = make_int2(key, it);
+            }
+        }
+        for (int it = 0; it < n; it++) {
+            if (bp[it].actidx == -2) continue;
+            if (keep != it) bp[keep] = bp[it];
+            bp[keep].actidx = -1;
+            keep++;
+        }
+        w.nbp = keep;
+    }
+    __syncwarp();
+}
+
+// Beam::advanceBeamFront (Beam.cpp:263-539)
+__device__ int beam_advance(const Ctx &c, WS &w) {
+    const int lane = lane_id();
+    if (lane == 0) {
+        w.cursor += w.reverse ? -1 : 1;
+        beam_calc_rec(c, w);
+    }
+    __syncwarp();
+    const int cursor = w.cursor;
+    Cons cn = w.constr[cursor];
+    while (true) {
+        BPh *bp = c.bpbuf[w.bpsel];
+        const int nbp = w.nbp, nhap = w.nhap;
+        // markRequiredExtensions (only sets flags: order free)
+        for (int it = lane; it < nbp; it += 32) {
+            hp_mark_required(c.hp[c.happ[bp[it].mat]], cn);
+            hp_mark_required(c.hp[c.happ[bp[it].pat]], cn);
+        }
+        __syncwarp();
+        // happath extensions, one path per lane
+        int minse = 0, maxse = INT_MIN;
+        for (int i = lane; i < nhap; i += 32) {
+            int id = c.happ[i];
+            HPh &h = c.hp[id];
+            if (h.toext0 || h.toext1) {
+                int se = hp_extend(c, w, id, cursor);
+                if (se < minse) minse = se;
+                if (se > maxse) maxse = se;
+            }
+        }
+        for (int o = 16; o; o >>= 1) {
+            minse = min(minse, __shfl_xor_sync(0xffffffffu, minse, o));
+            maxse = max(maxse, __shfl_xor_sync(0xffffffffu, maxse, o));
+        }
+        const int bpscaleexp = -(maxse + minse);
+        __syncwarp();
+        // beam-path extensions
+        float maxP = 0.0f;
+        const int g = c.tg[cursor];
+        for (int it = lane; it < nbp; it += 32) {
+            float mp = bp_extend(c, bp[it], g, cn, bpscaleexp);
+            if (maxP < mp) maxP = mp;
+        }
+        for (int o = 16; o; o >>= 1) maxP = fmaxf(maxP, __shfl_xor_sync(0xffffffffu, maxP, o));
+        __syncwarp();
+        int ok = 0;
+        if (lane == 0) ok = beam_prune_select(c, w, maxP, cn);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        if (ok) break;
+        if (cn.type != C_NONE) { cn.type = C_NONE; continue; }
+        if (lane == 0) w.err |= EIMP_ERR_BEAM_EMPTY;
+        __syncwarp();
+        return -1;
+    }
+    beam_apply_hap(c, w);
+    if (w.err) return -1;
+    beam_apply_bp(c, w);
+    if (w.err) return -1;
+    beam_merge(c, w);
+    return 0;
+}
+
+// Beam::callKeepPhaseProb (Beam.cpp:95-185)
+__device__ float beam_call_keep(const Ctx &c, WS &w, int ci, int twoback) {
+    if (lane_id() == 0) {
+        int cl = c.calls[ci];
+        int front = w.reverse ? max(cl - w.Delta, 0) : min(cl + w.Delta, c.S - 1);
+        w.curridx = w.reverse ? cl - front : front - cl;
+        int r = w.reverse ? (twoback ? c.calls[ci + 2] : c.calls[ci + 1]) : (twoback ? c.calls[ci - 2] : c.calls[ci - 1]);
+        w.refidx = w.reverse ? r - front : front - r;
+        w.ires = front;
+    }
+    __syncwarp();
+    const int front = w.ires;
+    while ((w.reverse && w.cursor > front) || (!w.reverse && w.cursor < front))
+        if (beam_advance(c, w)) return -1.0f;
+    if (lane_id() == 0) {
+        float acckp = 0.0f, accsp = 0.0f;
+        const BPh *bp = c.bpbuf[w.bpsel];
+        for (int it = 0; it < w.nbp; it++) {
+            const BPh &b = bp[it];
+            const HPh &hm = c.hp[c.happ[b.mat]], &hq = c.hp[c.happ[b.pat]];
+            int cf = bh_at(hm, w.curridx), cs = bh_at(hq, w.curridx);
+            int rf = bh_at(hm, w.refidx), rs = bh_at(hq, w.refidx);
+            float p = __fmul_rn(b.weight, b.prob);
+            if (cf != cs && rf != rs) {
+                if (cf == rf) acckp = __fadd_rn(acckp, p); else accsp = __fadd_rn(accsp, p);
+            } else {
+                acckp = __fadd_rn(acckp, __fdiv_rn(p, 2.0f));
+                accsp = __fadd_rn(accsp, __fdiv_rn(p, 2.0f));
+            }
+        }
+        float ret = 0.5f;
+        if (__fadd_rn(acckp, accsp) > 0.0f) ret = __fdiv_rn(acckp, __fadd_rn(acckp, accsp));
+        w.fres = ret;
+    }
+    __syncwarp();
+    return w.fres;
+}
+
+// Beam::callDosage (Beam.cpp:187-261)
+__device__ float beam_call_dosage(const Ctx &c, WS &w, int si) {
+    if (lane_id() == 0) {
+        int front = w.reverse ? max(si - w.Delta, 0) : min(si + w.Delta, c.S - 1);
+        w.curridx = w.reverse ? si - front : front - si;
+        w.refidx = -1;
+        w.ires = front;
+    }
+    __syncwarp();
+    const int front = w.ires;
+    while ((w.reverse && w.cursor > front) || (!w.reverse && w.cursor < front))
+        if (beam_advance(c, w)) return -1.0f;
+    if (lane_id() == 0) {
+        float dos = 0.0f, ptot = 0.0f;
+        const BPh *bp = c.bpbuf[w.bpsel];
+        for (int it = 0; it < w.nbp; it++) {
+            const BPh &b = bp[it];
+            const HPh &hm = c.hp[c.happ[b.mat]], &hq = c.hp[c.happ[b.pat]];
+            int cf = bh_at(hm, w.curridx), cs = bh_at(hq, w.curridx);
+            float p = __fmul_rn(b.weight, b.prob);
+            ptot = __fadd_rn(ptot, p);
+            if (cf == cs) { if (cf == 1) dos = __fadd_rn(dos, __fmul_rn(2.0f, p)); }
+            else dos = __fadd_rn(dos, p);
+        }
+        float ret = 1.0f;
+        if (ptot > 0.0f) ret = __fdiv_rn(dos, ptot);
+        w.fres = ret;
+    }
+    __syncwarp();
+    return w.fres;
+}
+
+__host__ __device__ __forceinline__ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+// arena layout per target (bytes)
+struct ArenaLayout {
+    size_t hp, ph, ivpool, ivfree, bp0, bp1, happ, happ_old, hapmap, fstack, copies, cons, rcons, probs, confs, tg,
+        total;
+    int NH, BPC, HMAX;
+};
+
+static ArenaLayout arena_layout(const BeamParams &p, int M) {
+    ArenaLayout a;
+    int P = p.P > p.Pf ? p.P : p.Pf;
+    int H = p.H > p.Hf ? p.H : p.Hf;
+    a.NH = 4 * P + 8;
+    a.BPC = 4 * P + 8;
+    a.HMAX = H;
+    size_t o = 0;
+    a.hp = o; o = align256(o + sizeof(HPh) * a.NH);
+    a.ph = o; o = align256(o + sizeof(float) * PHMAX * a.NH);
+    a.ivpool = o; o = align256(o + sizeof(int2) * (size_t)H * 3 * a.NH);
+    a.ivfree = o; o = align256(o + sizeof(int) * 3 * a.NH);
+    a.bp0 = o; o = align256(o + sizeof(BPh) * a.BPC);
+    a.bp1 = o; o = align256(o + sizeof(BPh) * a.BPC);
+    a.happ = o; o = align256(o + sizeof(int) * a.NH);
+    a.happ_old = o; o = align256(o + sizeof(int) * a.NH);
+    a.hapmap = o; o = align256(o + sizeof(int2) * a.NH);
+    a.fstack = o; o = align256(o + sizeof(int) * a.NH);
+    a.copies = o; o = align256(o + sizeof(int) * 2 * a.NH);
+    a.cons = o; o = align256(o + sizeof(Cons) * (size_t)(M + 1));
+    a.rcons = o; o = align256(o + sizeof(Cons) * (size_t)(M + 1));
+    a.probs = o; o = align256(o + sizeof(float) * (size_t)(M + 1));
+    a.confs = o; o = align256(o + sizeof(float) * (size_t)(M + 1));
+    a.tg = o; o = align256(o + (size_t)(M + 1));
+    a.total = o;
+    return a;
+}
+
+size_t beam_arena_bytes(const BeamParams &p, int M) { return arena_layout(p, M).total; }
+
+__device__ __forceinline__ void setbit_(uint64_t *v, int i) { v[i >> 6] |= 1ull << (i & 63); }
+__device__ __forceinline__ void clrbit_(uint64_t *v, int i) { v[i >> 6] &= ~(1ull << (i & 63)); }
+
+// One warp per target: Target::phaseExtPBWT (Target.cpp:291-777)
+__global__ void __launch_bounds__(32 * BEAM_WARPS) beam_kernel(
+    BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
+    const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
+    const int32_t *__restrict__ ncalls, const float *__restrict__ cmdiffs, const uint32_t *__restrict__ pbwt,
+    const int32_t *__restrict__ count0, const int64_t *__restrict__ rowoff, uint8_t *__restrict__ arena,
+    size_t arena_bytes, uint64_t *__restrict__ mats, uint64_t *__restrict__ pats, float *__restrict__ dmat,
+    float *__restrict__ dpat, float *__restrict__ totalconf, int32_t *__restrict__ ncallsites,
+    uint32_t *__restrict__ status) {
+    extern __shared__ uint8_t smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int t = blockIdx.x * BEAM_WARPS + wid;
+    if (t >= ntgt) return;
+    WS &w = reinterpret_cast<WS *>(smem_raw)[wid];
+    const int wM = (int)eimp_W(M);
+    const uint8_t *g = gt + (size_t)t * M;
+    const uint64_t *mo = monos + (size_t)t * wM;
+    uint64_t *mat = mats + (size_t)t * wM;
+    uint64_t *pat = pats + (size_t)t * wM;
+    float *dm = dmat + (size_t)t * M;
+    float *dp = dpat + (size_t)t * M;
+    for (int i = lane; i < wM; i += 32) { mat[i] = 0ull; pat[i] = 0ull; }
+    for (int i = lane; i < M; i += 32) { dm[i] = 0.0f; dp[i] = 0.0f; }
+
+    const int S = nsplits[t];
+    const int C = ncalls[t];
+    const int K = p.K;
+    Ctx c;
+    uint8_t *ab = arena + (size_t)t * arena_bytes;
+    c.hp = reinterpret_cast<HPh *>(ab + al.hp);
+    c.ph = reinterpret_cast<float *>(ab + al.ph);
+    c.ivpool = reinterpret_cast<int2 *>(ab + al.ivpool);
+    c.ivfree = reinterpret_cast<int *>(ab + al.ivfree);
+    c.bpbuf[0] = reinterpret_cast<BPh *>(ab + al.bp0);
+    c.bpbuf[1] = reinterpret_cast<BPh *>(ab + al.bp1);
+    c.happ = reinterpret_cast<int *>(ab + al.happ);
+    c.happ_old = reinterpret_cast<int *>(ab + al.happ_old);
+    c.hapmap = reinterpret_cast<int2 *>(ab + al.hapmap);
+    c.fstack = reinterpret_cast<int *>(ab + al.fstack);
+    c.copies = reinterpret_cast<int *>(ab + al.copies);
+    c.NH = al.NH; c.BPC = al.BPC; c.HMAX = al.HMAX;
+    Cons *cons = reinterpret_cast<Cons *>(ab + al.cons);
+    Cons *rcons = reinterpret_cast<Cons *>(ab + al.rcons);
+    float *phaseProbs = reinterpret_cast<float *>(ab + al.probs);
+    float *callConfs = reinterpret_cast<float *>(ab + al.confs);
+    uint8_t *tg = ab + al.tg;
+    const int64_t r0 = rowoff[t];
+    const size_t kw = eimp_kw(K);
+    c.Mp = 2 * S + 1;
+    c.rows = pbwt + (size_t)2 * r0 * kw;
+    c.count0 = count0 + r0;
+    c.K = K; c.kw = (int)kw;
+    c.Kinv = (float)(1.0 / (double)(float)K);
+    c.cmd = cmdiffs + (size_t)t * (M + 1);
+    c.S = S;
+    c.calls = calls + (size_t)t * M;
+    c.ncalls = C;
+    c.tg = tg;
+    c.pErr = p.pErr; c.pLimit = p.pLimit; c.expectIBDcM = p.expectIBDcM;
+    const int32_t *sp = splits + (size_t)t * M;
+    for (int s = lane; s < S; s += 32) { tg[s] = g[sp[s]]; cons[s].type = C_NONE; cons[s].refidx = 0; }
+    __syncwarp();
+
+    int err = 0;
+    int cur = 0, lastph = 0;   // VCFData::getStartPhase: Ref
+    if (p.doPrePhasing) {   // Target.cpp:324-438
+        beam_init(c, w, cons, 0, p.Hf, p.Pf, p.Deltaf);
+        if (lane == 0 && S > 0) { cons[0].type = C_HETKEEP; cons[0].refidx = 0; }
+        __syncwarp();
+        int nci = 1;
+        for (int si = 1; si < S && !err; si++) {
+            if (si == c.calls[nci]) {
+                float pr = (float)((double)beam_call_keep(c, w, nci, 0) - 0.5);
+                if (w.err) { err = 1; break; }
+                int ref = cur;
+                int refidx = c.calls[nci] - c.calls[nci - 1] - 1;
+                if (nci > 1) {
+                    float p2 = (float)((double)beam_call_keep(c, w, nci, 1) - 0.5);
+                    if (w.err) { err = 1; break; }
+                    if (fabsf(p2) > fabsf(pr)) { pr = p2; ref = lastph; refidx = c.calls[nci] - c.calls[nci - 2] - 1; }
+                }
+                lastph = cur;
+                int type;
+                if (pr < 0.0f) { cur = !ref; type = C_HETSWITCH; } else { cur = ref; type = C_HETKEEP; }
+                if (lane == 0) { cons[si].type = type; cons[si].refidx = refidx; phaseProbs[si] = fabsf(pr); }
+                nci++;
+            } else {
+                float pr = beam_call_dosage(c, w, si);
+                if (w.err) { err = 1; break; }
+                if (lane == 0) {
+                    if (tg[si] == 0) { cons[si].type = C_HOMREF; cons[si].refidx = 0; pr = (float)(2.0 - (double)pr); }
+                    else { cons[si].type = C_HOMALT; cons[si].refidx = 0; }
+                    phaseProbs[si] = pr;
+                }
+            }
+            __syncwarp();
+        }
+        if (!err && lane == 0) {
+            // the constraint heaps (Target.cpp:402-436), filled in site order as
+            // the reference does; the interval pool of the finished fast beam
+            // serves as heap storage
+            Hel *hq = reinterpret_cast<Hel *>(c.ivpool);
+            for (int pass = 0; pass < 2; pass++) {   // 0: call sites, 1: homozygous split sites
+                int n = 0;
+                int nci2 = 1;
+                for (int si = 1; si < S; si++) {
+                    bool iscall = (si == c.calls[nci2]);
+                    if (iscall) nci2++;
+                    if ((pass == 0) == iscall) heap_push(hq, n, phaseProbs[si], si, 0);
+                }
+                const size_t total = (size_t)n;
+                const size_t smin = (size_t)__fmul_rn((float)total, p.minfixsize);
+                const size_t smax = (size_t)((double)total * (1.0 - (double)p.maxfixsize));
+                size_t si;
+                const double thrmax = pass == 0 ? (double)p.maxfixthr - 0.5 : (double)p.maxfixthr * 2.0;
+                const double thrmin = pass == 0 ? (double)p.minfixthr - 0.5 : (double)p.minfixthr * 2.0;
+                for (si = 0; si < smin; si++) {
+                    Hel cc = heap_popmin(hq, n);
+                    if ((double)cc.key >= thrmax || ((double)cc.key >= thrmin && si >= smax)) break;
+                    cons[cc.a].type = C_NONE;
+                }
+                if (pass == 0 && si == smin) {
+                    // (Target.cpp:416-425: compared against the shrinking heap)
+                    for (; si < (size_t)n; si++) {
+                        Hel cc = heap_popmin(hq, n);
+                        if (cc.key > 0.0f) break;
+                        cons[cc.a].type = C_NONE;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+
+    // fine phasing forward (Target.cpp:458-599)
+    cur = 0;
+    int nprobs = 0;
+    if (lane == 0) phaseProbs[0] = 0.0f;
+    nprobs = 1;
+    if (!err) {
+        beam_init(c, w, cons, 0, p.H, p.P, p.Delta);
+        int m = 0;
+        const int stop = S > 0 ? sp[c.calls[0]] : M;
+        if (lane == 0) {
+            for (; m < stop; m++) {
+                uint8_t gg = g[m];
+                if (gg == 2) { setbit_(mat, m); setbit_(pat, m); dm[m] = 1.0f; dp[m] = 1.0f; }
+                else if (gg == 1) { setbit_(pat, m); dm[m] = 0.5f; dp[m] = 0.5f; }
+            }
+            if (m < M) { if (cur) setbit_(mat, m); else setbit_(pat, m); }
+        }
+        m = stop;
+        if (m < M) m++;
+        int nci = 1;
+        for (; m < M && !err; m++) {
+            const uint8_t gg = g[m];
+            if (gg == 1) {
+                const bool mono = (mo[m >> 6] >> (m & 63)) & 1ull;
+                if (!mono) {
+                    float pr = (float)((double)beam_call_keep(c, w, nci, 0) - 0.5);
+                    if (w.err) { err = 1; break; }
+                    if (lane == 0) phaseProbs[nprobs] = pr;
+                    nprobs++;
+                    cur = pr < 0.0f ? !cur : cur;
+                    nci++;
+                } else if (lane == 0) { dm[m] = 0.5f; dp[m] = 0.5f; }
+                if (lane == 0) { if (cur) setbit_(mat, m); else setbit_(pat, m); }
+            } else if (gg == 2 && lane == 0) {
+                setbit_(mat, m); setbit_(pat, m); dm[m] = 1.0f; dp[m] = 1.0f;
+            }
+        }
+        __syncwarp();
+    }
+    if (!err && S > 0) {   // Target.cpp:601-619
+        if (lane == 0) {
+            for (int i = 0; i < C; i++) callConfs[i] = 0.0f;
+            if (p.doRevPhasing) callConfs[C - 1] = (float)((double)fabsf(phaseProbs[nprobs - 1]) + 0.5);
+            else for (int i = 0; i < nprobs && i < C; i++) callConfs[i] = (float)((double)fabsf(phaseProbs[i]) + 0.5);
+        }
+        __syncwarp();
+    }
+    if (!err && p.doRevPhasing && S > 0) {   // Target.cpp:620-758
+        if (lane == 0) {
+            for (int s = 0; s < S; s++) { rcons[s].type = C_NONE; rcons[s].refidx = 0; }
+            for (int ci = 1; ci < S; ci++) {
+                Cons cc = cons[ci];
+                if (cc.type == C_HETKEEP || cc.type == C_HETSWITCH) {
+                    Cons &r = rcons[ci - cc.refidx - 1];
+                    if (r.type != C_NONE) {
+                        int ridx = ci - cc.refidx + r.refidx;
+                        rcons[ridx].refidx = cc.refidx - r.refidx - 1;
+                        rcons[ridx].type = (cc.type != r.type) ? C_HETSWITCH : C_HETKEEP;
+                    } else { r.type = cc.type; r.refidx = cc.refidx; }
+                } else if (cc.type == C_HOMREF || cc.type == C_HOMALT) {
+                    rcons[ci].type = cc.type;
+                }
+            }
+            rcons[S - 1].type = C_HETKEEP; rcons[S - 1].refidx = 0;
+            float last = phaseProbs[nprobs - 1];
+            float dref = last < 0.0f ? (float)(0.5 + (double)last) : (float)(0.5 - (double)last);
+            float dalt = last < 0.0f ? (float)(0.5 - (double)last) : (float)(0.5 + (double)last);
+            int site = sp[c.calls[C - 1]];
+            dm[site] = cur == 0 ? dref : dalt;
+            dp[site] = cur == 0 ? dalt : dref;
+        }
+        __syncwarp();
+        beam_init(c, w, rcons, 1, p.H, p.P, p.Delta);
+        for (int rci = C - 2; rci >= 0 && !err; rci--) {
+            float pr = (float)((double)beam_call_keep(c, w, rci, 0) - 0.5);
+            if (w.err) { err = 1; break; }
+            float fw = phaseProbs[rci + 1];
+            if (fabsf(fw) > fabsf(pr)) pr = fw;
+            cur = pr < 0.0f ? !cur : cur;
+            if (lane == 0) {
+                int s2 = sp[c.calls[rci]];
+                if (cur) { setbit_(mat, s2); clrbit_(pat, s2); } else { clrbit_(mat, s2); setbit_(pat, s2); }
+                float dref = pr < 0.0f ? (float)(0.5 + (double)pr) : (float)(0.5 - (double)pr);
+                float dalt = pr < 0.0f ? (float)(0.5 - (double)pr) : (float)(0.5 + (double)pr);
+                dm[s2] = cur == 0 ? dref : dalt;
+                dp[s2] = cur == 0 ? dalt : dref;
+                callConfs[rci] = (float)((double)fabsf(pr) + 0.5);
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0) {
+        float tc = 0.0f;
+        int nc = 0;
+        if (!err && S > 0) {   // Target.cpp:761-772
+            for (int i = 0; i < C; i++) tc = __fadd_rn(tc, callConfs[i]);
+            nc = C;
+        }
+        totalconf[t] = tc;
+        ncallsites[t] = nc;
+        if (err) atomicOr(status, w.err ? w.err : (uint32_t)EIMP_ERR_BEAM_EMPTY);
+    }
+}
+
+cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt, const uint64_t *monos,
+                        const int32_t *splits, const int32_t *nsplits, const int32_t *calls, const int32_t *ncalls,
+                        const float *cmdiffs, const uint32_t *pbwt, const int32_t *count0, const int64_t *rowoff,
+                        void *arena, size_t arena_bytes, uint64_t *mats, uint64_t *pats, float *dmat, float *dpat,
+                        float *totalconf, int32_t *ncallsites, uint32_t *status, cudaStream_t st) {
+    ArenaLayout al = arena_layout(p, M);
+    if (arena_bytes < al.total) return cudaErrorInvalidValue;
+    size_t sm = sizeof(WS) * BEAM_WARPS;
+    cudaError_t e = cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int blocks = (ntgt + BEAM_WARPS - 1) / BEAM_WARPS;
+    beam_kernel<<<blocks, 32 * BEAM_WARPS, sm, st>>>(p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls,
+                                                     cmdiffs, pbwt, count0, rowoff, (uint8_t *)arena, arena_bytes,
+                                                     mats, pats, dmat, dpat, totalconf, ncallsites, status);
+    return cudaGetLastError();
+}
+
+}  // namespace eimp

@@ -9,6 +9,8 @@
 // the per-warp match-tree node pool in shared memory
 #define SMM_WARPS 4
 #define SMM_NODES 512
+// beam phasing: warps (targets) per CTA
+#define BEAM_WARPS 4
 
 namespace eimp {
 
@@ -44,15 +46,11 @@ cudaError_t launch_pbwt(const uint64_t *cref, const int32_t *count0, const int64
 // ---- beam phasing (beam.cu)
 struct BeamParams {
     int K;
-    int H, P, Delta;
-    int Hf, Pf, Deltaf;
+    int H, P, Delta;      // history length (hsize*hist rounded), beam width, call delay
+    int Hf, Pf, Deltaf;   // the same for the pre-phasing beam
     float expectIBDcM, pErr, pLimit;
     float minfixsize, maxfixsize, minfixthr, maxfixthr;
     int doPrePhasing, doRevPhasing;
-};
-struct BeamBuffers {
-    void *arena;          // per-target scratch arena
-    size_t arena_bytes;   // per target
 };
 size_t beam_arena_bytes(const BeamParams &p, int S_max);
 cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt, const uint64_t *monos,
