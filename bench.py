@@ -274,11 +274,14 @@ def main():
         return torch.from_numpy(a).to(dev)
 
     # resident panel + per-batch inputs
+    if "phase" in stages:
+        from eimp_b200.engine import Phaser
+        Phaser(ctx, hm, sm, cm)   # uploads the typed reference used by the phasing kernels
     d_full = todev(panel.sitemajor)
     d_af = todev(panel.af.astype(np.float32))
     d_typed = todev(tg.typed.astype(np.int64))
     d_sitetyped = todev(sm)
-    d_gt = todev(tg.gt.astype(np.uint8))
+    d_gt = todev(np.ascontiguousarray(tg.gt, dtype=np.uint8))
     phased_h = pack_rows(tg.truth, W(M))
     d_phased = todev(phased_h)
     ldb = (Mref + 63) // 64
@@ -376,8 +379,8 @@ def main():
     # end to end through the public API: host (pinned) targets in, host dosages out
     e2e = None
     if rank == 0 or world > 1:
-        ph_pin = torch.from_numpy(phased_h.view(np.int64)).pin_memory()
-        gt_pin = torch.from_numpy(tg.gt.astype(np.uint8)).pin_memory()
+        ph_pin = torch.from_numpy(np.ascontiguousarray(phased_h).view(np.int64)).pin_memory()
+        gt_pin = torch.from_numpy(np.ascontiguousarray(tg.gt, dtype=np.uint8)).pin_memory()
         dos_pin = torch.empty((2 * nt, Mref), dtype=torch.float32).pin_memory()
         bits_pin = torch.empty((2 * nt, W(Mref)), dtype=torch.int64).pin_memory()
         h2d = ph_pin.numel() * 8 + gt_pin.numel()

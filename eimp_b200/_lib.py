@@ -87,9 +87,16 @@ def exported_names():
 
 
 def ptr(a) -> int | None:
-    """Address of a numpy array / torch tensor buffer (None passes NULL)."""
+    """Address of a C-contiguous numpy array / torch tensor (None passes NULL).
+
+    The C ABI takes plain row-major buffers; a strided view would be read as
+    if it were row-major, so non-contiguous inputs are rejected."""
     if a is None:
         return None
     if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor passed to libeimp_b200 must be contiguous")
         return a.data_ptr()
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array passed to libeimp_b200 must be C-contiguous")
     return a.ctypes.data

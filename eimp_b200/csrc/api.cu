@@ -139,7 +139,7 @@ const char *eimp_last_error(const eimp_ctx *ctx) { return ctx ? ctx->err.c_str()
 int eimp_synchronize(eimp_ctx *ctx) {
     if (!ctx) return EIMP_E_ARG;
     CK(cudaStreamSynchronize(ctx->stream));
-    return 0;
+    return check_status(ctx);
 }
 
 uint64_t eimp_kernel_launches(const eimp_ctx *ctx) { return ctx ? ctx->launches : 0; }

@@ -136,7 +136,8 @@ def generate(cfg: SynthConfig | str, cache: bool = True):
     if cache and os.path.exists(path):
         z = np.load(path)
         panel = Panel(cfg.nhaps, cfg.nsites, z["pos"], z["cm"], z["af"], z["hapmajor"], z["sitemajor"])
-        groups = [Targets(z[f"typed{g}"], z[f"gt{g}"], z[f"truth{g}"]) for g in range(len(cfg.groups))]
+        groups = [Targets(z[f"typed{g}"], np.ascontiguousarray(z[f"gt{g}"]), np.ascontiguousarray(z[f"truth{g}"]))
+                  for g in range(len(cfg.groups))]
         return panel, groups
 
     rng = np.random.default_rng(cfg.seed)
@@ -185,7 +186,7 @@ def generate(cfg: SynthConfig | str, cache: bool = True):
             nmiss = int(round(rate * m))
             if nmiss:
                 gt[t, rng.choice(m, nmiss, replace=False)] = 3
-        groups.append(Targets(typed, gt, th))
+        groups.append(Targets(typed, np.ascontiguousarray(gt), np.ascontiguousarray(th)))
 
     if cache:
         kw = dict(pos=panel.pos, cm=panel.cm, af=panel.af, hapmajor=panel.hapmajor, sitemajor=panel.sitemajor)

@@ -68,7 +68,9 @@ int eimp_create(int device, eimp_ctx **out);
 void eimp_destroy(eimp_ctx *ctx);
 /* Human-readable description of the last failure on this context. */
 const char *eimp_last_error(const eimp_ctx *ctx);
-/* Blocks until all work on the context's stream is done. */
+/* Blocks until all work on the context's stream is done; returns
+ * EIMP_E_CAPACITY / EIMP_E_BEAM_EMPTY if a kernel launched since the last
+ * check reported one (the *_dev entry points do not synchronise). */
 int eimp_synchronize(eimp_ctx *ctx);
 /* Number of kernels this context has launched so far. */
 uint64_t eimp_kernel_launches(const eimp_ctx *ctx);
