@@ -53,6 +53,7 @@ _PROTOS = [
     ("eimp_imp_bunch_dev", _i32, [_vp, _sz, _sz, _vp, _sz, _vp, _sz]),
     ("eimp_imp_matches", _i32, [_vp, _sz, _vp, _sz, C.POINTER(_sz)]),
     ("eimp_imp_refpbwt", _i32, [_vp, _vp, _vp]),
+    ("eimp_besthaps_noalloc", _i32, [_vp, _sz, _sz, _vp, _vp, _sz, _sz, _vp, _vp]),
 ]
 
 _lib = None

@@ -184,6 +184,30 @@ int eimp_phase_targets_dev(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntg
                            uint64_t *d_mats, uint64_t *d_pats, float *d_dos_mats, float *d_dos_pats,
                            float *d_totalconf, int32_t *d_ncallsites);
 
+/* ------------------------------------------------ allocation-free variant ----
+ * No counterpart in the reference.  Best-haplotype selection (the Hamming
+ * counts and K-smallest choice of Target::findBestHaps) for callers that cannot
+ * let this library allocate device memory -- e.g. a host framework that owns
+ * the device budget through its own pool, or a serving loop that allows no
+ * allocation after start-up.  It needs no context and calls no
+ * cudaMalloc/cudaFree: the per-haplotype error counts live in a fixed device
+ * array of EIMP_BESTHAPS_NOALLOC_MAX uint32 (16 MiB), which every GPU that
+ * loads the library holds until the process exits.
+ *  - all pointers are device pointers on the current device; `stream` is a
+ *    cudaStream_t (NULL: the default stream); the call only enqueues work;
+ *  - inputs: d_gt ntgt x M genotype bytes, d_hapmajor nhaps x W(M) words;
+ *    outputs: d_besthaps ntgt x min(K, nhaps) ascending indices, d_flags
+ *    ntgt x W(nhaps) words -- the same values eimp_phase_prep returns;
+ *  - ntgt x nhaps must not exceed EIMP_BESTHAPS_NOALLOC_MAX, otherwise the call
+ *    returns EIMP_E_CAPACITY and does nothing (split the targets into batches);
+ *  - the first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress); make it before capturing a stream on that device;
+ *  - all calls on a device share the array: calls that overlap on the GPU
+ *    (different streams, unsynchronised) race and give wrong results. */
+#define EIMP_BESTHAPS_NOALLOC_MAX (4u << 20)
+int eimp_besthaps_noalloc(void *stream, size_t ntgt, size_t M, const uint8_t *d_gt, const uint64_t *d_hapmajor,
+                          size_t nhaps, size_t K, int32_t *d_besthaps, uint64_t *d_flags);
+
 #ifdef __cplusplus
 }
 #endif

@@ -51,3 +51,19 @@ def test_no_device_means_loud_failure():
     from eimp_b200.engine import Context
     with pytest.raises(Exception):
         Context(0)
+
+
+def test_besthaps_noalloc_rejects_oversized_batches():
+    """Batches beyond the fixed scratch array are refused on the host before
+    any device work (the pointers are never dereferenced)."""
+    from eimp_b200 import build
+    L = ctypes.CDLL(build.build())
+    f = L.eimp_besthaps_noalloc
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]
+    dummy = 0x1000
+    # 5 targets x 2^20 haplotypes > 4 Mi entries -> EIMP_E_CAPACITY (3)
+    assert f(None, 5, 10, dummy, dummy, 1 << 20, 4, dummy, dummy) == 3
+    # missing buffers -> EIMP_E_ARG (2)
+    assert f(None, 1, 10, None, dummy, 100, 4, dummy, dummy) == 2
