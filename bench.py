@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--stages", default="phase,impute", help="comma list of: phase, impute")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-targets", type=int, default=200)
+    ap.add_argument("--targets", type=int, default=0, help="use only the first N targets (small profiling case)")
     return ap.parse_args()
 
 
@@ -111,10 +112,13 @@ def measured_peak_hbm():
 
 
 # ---------------------------------------------------------------- workload
-def load_workload(cfgname):
+def load_workload(cfgname, ntargets=0):
     cfg = synth.CONFIGS[cfgname]
     panel, groups = synth.generate(cfg)
     tg = groups[0]
+    if ntargets:
+        tg = synth.Targets(tg.typed, np.ascontiguousarray(tg.gt[:ntargets]),
+                           np.ascontiguousarray(tg.truth[:2 * ntargets]))
     hm, sm, cm = synth.typed_views(panel, tg.typed)
     return cfg, panel, tg, hm, sm, cm
 
@@ -259,7 +263,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     from eimp_b200.engine import Context
     stages = args.stages.split(",")
-    cfg, panel, tg, hm, sm, cm = load_workload(args.config)
+    cfg, panel, tg, hm, sm, cm = load_workload(args.config, args.targets)
     nt = tg.gt.shape[0]
     M, Mref, nh_ref = len(tg.typed), panel.nsites, panel.nhaps
     ctx = Context(local)

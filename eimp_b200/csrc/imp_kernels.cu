@@ -138,42 +138,40 @@ __global__ void transpose_kernel(const uint64_t *__restrict__ src, size_t rows, 
 // ---------------------------------------------------------------------------
 // set-maximal matches
 //
-// The history tree of TargetImp::processHistorySubTree lives in shared memory,
-// one pool per warp.  Per site: lane 0 lists the live nodes in pre-order, all
-// lanes map their intervals through the site's PBWT row in parallel (the
-// mapping of a node depends only on its own interval, and a node's interval is
-// not changed before the recursion reaches it), then lane 0 replays the
-// recursion iteratively with the precomputed mappings.
+// TargetImp::calcSMMatches / processHistorySubTree (TargetImp.cpp:74-246,
+// 346-435) keep a tree of PBWT intervals.  Two facts make the per-site update
+// of that tree data-parallel:
+//  * a node's descendants hold sub-intervals of its interval and at least its
+//    number of errors, so a descendant can extend only if the node can;
+//  * the 1-extensions are built as a mirror of the tree (TargetImp.cpp:370-388).
+// Hence, with the tree stored in pre-order, one site turns the pre-order array
+// O into  [new root] ++ {v in O : v extends with 0} ++ {v in O : v extends
+// with 1}  (mapped intervals, depth + 1), each part keeping the relative order,
+// sides and parents of O; nodes that extend neither way are deleted and, when
+// at the maximum depth, report matches in pre-order; a node with exactly one
+// child of equal interval and errors is replaced by that child, which in
+// pre-order is the next entry.  One warp handles one target haplotype; the
+// filters, scans and parent remaps run across the lanes.
 // ---------------------------------------------------------------------------
-struct SmmNode {
+struct SNode {
     int l, r;
-    int de;              // depth | errors << 24
-    short left, right;   // node indices, -1 = none
+    int de;                 // depth | errors << 24
+    short parent;           // index in the array, -1 for the root
+    unsigned char side;     // 0: left child, 1: right child of the parent
+    unsigned char pad;
 };
-struct SmmFrame {
-    short lt, rt;        // slots (see slot encoding)
-    int cdepth;          // max depth returned by the children
-    unsigned char st;    // bits: 0-1 stage, 2 perase, 3 extend0, 4 extend1
-};
-
-// slot encoding: s >= 0 -> node (s>>1).left (s&1==0) or .right (s&1==1);
-// SLOT_ROOT -> the root variable
-#define SLOT_ROOT (-2)
 
 struct SmmWarpSmem {
-    SmmNode node[SMM_NODES];
-    int4 map[SMM_NODES];
-    SmmFrame stack[SMM_NODES];
-    short order[SMM_NODES];
-    short freel[SMM_NODES];
+    SNode A[SMM_NODES];     // tree in pre-order
+    SNode B[SMM_NODES];     // tree being built
+    int4 mp[SMM_NODES];     // mappings (to0, to1); reused by the merge pass
+    short idx0[SMM_NODES];  // position of a node's 0-extension in B (-1: none)
+    short idx1[SMM_NODES];  // position of a node's 1-extension in B (-1: none)
 };
 
-__device__ __forceinline__ short &slot_ref(SmmWarpSmem &S, short &rootvar, int s) {
-    if (s == SLOT_ROOT) return rootvar;
-    return (s & 1) ? S.node[s >> 1].right : S.node[s >> 1].left;
-}
 __device__ __forceinline__ int de_depth(int de) { return de & 0xffffff; }
 __device__ __forceinline__ int de_err(int de) { return (int)((unsigned)de >> 24); }
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
 
 __global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
     const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
@@ -189,180 +187,147 @@ __global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
     const uint64_t *hw = phased + (size_t)hap * wM;
     int4 *out = matches + (size_t)hap * cap;
     const size_t kw = eimp_kw(K);
+    const unsigned FULL = 0xffffffffu;
 
     // missingness > 50 %: no matches (TargetImp.cpp:79-80)
     int nmiss = 0;
     for (int m = lane; m < M; m += 32) nmiss += g[m] == 3;
-    for (int o = 16; o; o >>= 1) nmiss += __shfl_xor_sync(0xffffffffu, nmiss, o);
+    for (int o = 16; o; o >>= 1) nmiss += __shfl_xor_sync(FULL, nmiss, o);
     if (nmiss > M / 2) { if (lane == 0) nmatch[hap] = 0; return; }
 
-    int nfree = 0, used = 0;
-    short root = -1;
-    int nres = 0, treedepth = 0;
     uint32_t err = 0;
+    int n = 1, nres = 0, td = 0;
+    if (lane == 0) { S.A[0].l = 0; S.A[0].r = K - 1; S.A[0].de = 0; S.A[0].parent = -1; S.A[0].side = 0; }
+    __syncwarp();
 
-    auto pool_new = [&](int l, int r, int de) -> int {
-        int i;
-        if (nfree) i = S.freel[--nfree];
-        else if (used < SMM_NODES) i = used++;
-        else { err |= EIMP_ERR_NODE_OVERFLOW; return -1; }
-        SmmNode &n = S.node[i];
-        n.left = -1; n.right = -1; n.l = l; n.r = r; n.de = de;
-        return i;
-    };
-    auto pool_del = [&](int i) { S.freel[nfree++] = (short)i; };
-    auto merge_single = [&](short &slot) {
-        // TargetImp.cpp:405-415: a node with one child of equal mapping is
-        // replaced by that child
-        SmmNode &N = S.node[slot];
-        if (N.left >= 0 && N.right < 0) {
-            const SmmNode &C = S.node[N.left];
-            if (C.l == N.l && C.r == N.r && de_err(C.de) == de_err(N.de)) { int t = slot; slot = N.left; pool_del(t); }
-        } else if (N.left < 0 && N.right >= 0) {
-            const SmmNode &C = S.node[N.right];
-            if (C.l == N.l && C.r == N.r && de_err(C.de) == de_err(N.de)) { int t = slot; slot = N.right; pool_del(t); }
+    for (int m = 0; m <= M; m++) {
+        const bool final = (m == M);   // TargetImp.cpp:144: erase pass, every node reports
+        const int curr = final ? 0 : bit_at(hw, m);
+        const int missing = final ? 0 : (g[m] == 3);
+        const uint32_t *crow = compr + (size_t)(final ? 0 : m) * kw;
+        const int c0 = final ? 0 : count0[m];
+        // pass 1: mappings, extension flags, matches of nodes that end here
+        int cnt0 = 0, cnt1 = 0, newcount = 0;
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            bool e0 = false, e1 = false, dead = false;
+            if (i < n) {
+                const SNode v = S.A[i];
+                int l0 = 0, r0 = -1, l1 = 0, r1 = -1;
+                if (!final) pbwt_map(crow, c0, v.l, v.r, l0, r0, l1, r1);
+                const int ne = de_err(v.de);
+                e0 = l0 <= r0 && (missing || !curr || ne < setmaxerrors);
+                e1 = l1 <= r1 && (missing || curr || ne < setmaxerrors);
+                S.mp[i] = make_int4(l0, r0, l1, r1);
+                dead = !e0 && !e1 && de_depth(v.de) == td && td > 0;
+            }
+            const unsigned b0 = __ballot_sync(FULL, e0), b1 = __ballot_sync(FULL, e1), bd = __ballot_sync(FULL, dead);
+            if (i < n) {
+                S.idx0[i] = e0 ? (short)(1 + cnt0 + __popc(b0 & lanemask_lt())) : (short)-1;
+                S.idx1[i] = e1 ? (short)(cnt1 + __popc(b1 & lanemask_lt())) : (short)-1;   // offset added below
+            }
+            if (dead) {
+                const SNode v = S.A[i];
+                const int d = de_depth(v.de);
+                const int pos = nres + newcount + __popc(bd & lanemask_lt());
+                if (pos < cap) out[pos] = make_int4(m - d, m, v.l, v.r);
+                else err |= EIMP_ERR_MATCH_OVERFLOW;
+            }
+            cnt0 += __popc(b0); cnt1 += __popc(b1); newcount += __popc(bd);
         }
-    };
-
-    // TargetImp.cpp:346-435 as an explicit-stack traversal (lane 0)
-    auto process = [&](int lt0, int rt0, bool perase0, int m, int curr, int missing, int &newcount) -> int {
-        int sp = 0;
-        S.stack[0].lt = (short)lt0; S.stack[0].rt = (short)rt0; S.stack[0].cdepth = 0;
-        S.stack[0].st = perase0 ? 4 : 0;
-        int ret = 0;
-        while (sp >= 0) {
-            SmmFrame &f = S.stack[sp];
-            int stage = f.st & 3;
-            if (stage == 0) {
-                int L = slot_ref(S, root, f.lt);
-                bool perase = f.st & 4;
-                int4 mp = perase ? make_int4(0, -1, 0, -1) : S.map[L];
-                SmmNode &N = S.node[L];
-                int ne = de_err(N.de);
-                bool e0 = mp.x <= mp.y && (missing || !curr || ne < setmaxerrors);
-                bool e1 = mp.z <= mp.w && (missing || curr || ne < setmaxerrors);
-                if (e1) {
-                    int ni = pool_new(mp.z, mp.w, (de_depth(N.de) + 1) | (((curr || missing) ? ne : ne + 1) << 24));
-                    if (ni < 0) return -1;
-                    slot_ref(S, root, f.rt) = (short)ni;
-                }
-                if (e0) {
-                    N.l = mp.x; N.r = mp.y;
-                    N.de = (de_depth(N.de) + 1) | (((curr && !missing) ? ne + 1 : ne) << 24);
-                }
-                if (!e0 && !e1) {
-                    int d = de_depth(N.de);
-                    if (d == treedepth && treedepth > 0) {
-                        if (nres + newcount < cap) out[nres + newcount] = make_int4(m - d, m, N.l, N.r);
-                        else err |= EIMP_ERR_MATCH_OVERFLOW;
-                        newcount++;
-                    }
-                }
-                unsigned char st = (unsigned char)(1 | (perase ? 4 : 0) | (e0 ? 8 : 0) | (e1 ? 16 : 0));
-                f.st = st;
-                if (N.left >= 0) {
-                    if (sp + 1 >= SMM_NODES) { err |= EIMP_ERR_STACK_OVERFLOW; return -1; }
-                    int R = slot_ref(S, root, f.rt);
-                    SmmFrame &c = S.stack[++sp];
-                    c.lt = (short)(2 * L); c.rt = (short)((R >= 0) ? 2 * R : f.rt);
-                    c.cdepth = 0; c.st = (!e0 && !e1) ? 4 : 0;
-                    continue;
-                }
-                stage = 1;
-            }
-            if (stage == 1) {
-                f.st = (f.st & ~3) | 2;
-                int L = slot_ref(S, root, f.lt);
-                if (S.node[L].right >= 0) {
-                    if (sp + 1 >= SMM_NODES) { err |= EIMP_ERR_STACK_OVERFLOW; return -1; }
-                    int R = slot_ref(S, root, f.rt);
-                    bool ce = !(f.st & 8) && !(f.st & 16);
-                    SmmFrame &c = S.stack[++sp];
-                    c.lt = (short)(2 * L + 1); c.rt = (short)((R >= 0) ? 2 * R + 1 : f.rt);
-                    c.cdepth = 0; c.st = ce ? 4 : 0;
-                    continue;
-                }
-            }
-            // post-processing (TargetImp.cpp:392-432)
-            int depth = f.cdepth;
-            short &Ls = slot_ref(S, root, f.lt);
-            if (f.st & 8) {
-                int d = de_depth(S.node[Ls].de);
-                if (d > depth) depth = d;
-                merge_single(Ls);
-            } else {
-                pool_del(Ls);
-                Ls = -1;
-            }
-            if (f.st & 16) {
-                short &Rs = slot_ref(S, root, f.rt);
-                int d = de_depth(S.node[Rs].de);
-                if (d > depth) depth = d;
-                merge_single(Rs);
-            }
-            sp--;
-            if (sp >= 0) { if (depth > S.stack[sp].cdepth) S.stack[sp].cdepth = depth; }
-            else ret = depth;
-        }
-        return ret;
-    };
-
-    if (lane == 0) root = (short)pool_new(0, K - 1, 0);
-    bool failed = false;
-    for (int m = 0; m < M && !failed; m++) {
-        const int curr = bit_at(hw, m);
-        const int missing = g[m] == 3;
-        // pre-order of the tree below the (old) root; S.stack doubles as the
-        // traversal stack (it is free between sites)
-        int n = 0;
-        if (lane == 0) {
-            short *st = reinterpret_cast<short *>(S.stack);
-            int sp = 0;
-            st[sp++] = root;
-            while (sp) {
-                int x = st[--sp];
-                S.order[n++] = (short)x;
-                if (S.node[x].right >= 0) st[sp++] = S.node[x].right;
-                if (S.node[x].left >= 0) st[sp++] = S.node[x].left;
-            }
-        }
-        n = __shfl_sync(0xffffffffu, n, 0);
         __syncwarp();
-        const uint32_t *crow = compr + (size_t)m * kw;
-        const int c0 = count0[m];
+        if (final) {
+            if (nres + newcount <= cap) nres += newcount;
+            break;
+        }
+        const int nb = 1 + cnt0 + cnt1;
+        if (nb > SMM_NODES) { err |= EIMP_ERR_NODE_OVERFLOW; break; }
+        // pass 2: build B = [new root] ++ 0-tree ++ 1-tree
         for (int i = lane; i < n; i += 32) {
-            int x = S.order[i];
-            int l0, r0, l1, r1;
-            pbwt_map(crow, c0, S.node[x].l, S.node[x].r, l0, r0, l1, r1);
-            S.map[x] = make_int4(l0, r0, l1, r1);
-        }
-        __syncwarp();
-        if (lane == 0) {
-            int nr = pool_new(0, K - 1, 0);
-            if (nr < 0) failed = true;
-            else {
-                S.node[nr].left = root;
-                root = (short)nr;
-                int newcount = 0;
-                int td = process(2 * root, 2 * root + 1, false, m, curr, missing, newcount);
-                if (td < 0) failed = true;
-                else {
-                    // TargetImp.cpp:132-136: report only if no longer path is alive
-                    if (newcount && nres < cap && out[nres].y - out[nres].x >= td && nres + newcount <= cap)
-                        nres += newcount;
-                    treedepth = td;
-                }
+            const SNode v = S.A[i];
+            const int4 mp = S.mp[i];
+            const int d = de_depth(v.de) + 1, ne = de_err(v.de);
+            const int p0 = S.idx0[i], p1 = S.idx1[i];
+            if (p0 >= 0) {
+                SNode &o = S.B[p0];
+                o.l = mp.x; o.r = mp.y;
+                o.de = d | (((curr && !missing) ? ne + 1 : ne) << 24);
+                o.parent = i == 0 ? 0 : S.idx0[v.parent];
+                o.side = i == 0 ? 0 : v.side;
+            }
+            if (p1 >= 0) {
+                SNode &o = S.B[1 + cnt0 + p1];
+                o.l = mp.z; o.r = mp.w;
+                o.de = d | (((!curr && !missing) ? ne + 1 : ne) << 24);
+                o.parent = i == 0 ? 0 : (short)(1 + cnt0 + S.idx1[v.parent]);
+                o.side = i == 0 ? 1 : v.side;
             }
         }
-        failed = __shfl_sync(0xffffffffu, (int)failed, 0);
+        if (lane == 0) { S.B[0].l = 0; S.B[0].r = K - 1; S.B[0].de = 0; S.B[0].parent = -1; S.B[0].side = 0; }
         __syncwarp();
-    }
-    if (lane == 0) {
-        if (!failed) {
-            int newcount = 0;
-            int td = process(SLOT_ROOT, SLOT_ROOT, true, M, 0, 0, newcount);
-            if (td >= 0 && nres + newcount <= cap) nres += newcount;
+        // pass 3: merges (TargetImp.cpp:405-432).  Child flags first.
+        int *cflag = reinterpret_cast<int *>(S.mp);   // mp[i].x
+        for (int i = lane; i < nb; i += 32) S.mp[i].x = 0;
+        __syncwarp();
+        for (int u = 1 + lane; u < nb; u += 32) atomicOr(&S.mp[S.B[u].parent].x, 1 << S.B[u].side);
+        __syncwarp();
+        (void)cflag;
+        // removal flags, kept-position scan, start of each removed run
+        int kept = 0, laststart = -1;
+        for (int base = 0; base < nb; base += 32) {
+            const int v = base + lane;
+            bool rm = false, start = false;
+            if (v >= 1 && v < nb) {
+                const int cf = S.mp[v].x;
+                if (cf == 1 || cf == 2) {   // exactly one child: the next entry
+                    const SNode a = S.B[v], c = S.B[v + 1];
+                    rm = a.l == c.l && a.r == c.r && de_err(a.de) == de_err(c.de);
+                }
+            }
+            const unsigned brm = __ballot_sync(FULL, rm);
+            // a removed run starts where the previous entry is kept
+            const unsigned prevrm = (brm << 1) | (base > 0 ? (unsigned)((S.mp[base - 1].w >> 1) & 1) : 0u);
+            start = rm && !((prevrm >> lane) & 1);
+            const unsigned bst = __ballot_sync(FULL, start);
+            // last run start at or before this entry (inclusive prefix max)
+            const unsigned upto = bst & (lanemask_lt() | (1u << lane));
+            const int ls = upto ? base + (31 - __clz(upto)) : laststart;
+            const bool keep = v < nb && !rm;
+            const unsigned bk = __ballot_sync(FULL, keep);
+            if (v < nb) S.mp[v] = make_int4(S.mp[v].x, keep ? kept + __popc(bk & lanemask_lt()) : -1, ls,
+                                            rm ? 2 : 0);
+            kept += __popc(bk);
+            if (bst) laststart = base + (31 - __clz(bst));
+            __syncwarp();
         }
+        // compact into A with remapped parents
+        for (int u = lane; u < nb; u += 32) {
+            const int np = S.mp[u].y;
+            if (np < 0) continue;
+            SNode o = S.B[u];
+            if (u > 0) {
+                int p = o.parent;
+                if (S.mp[p].w & 2) {   // parent removed: take the place of its run's first node
+                    const int q = S.mp[p].z;
+                    p = S.B[q].parent;
+                    o.side = S.B[q].side;
+                }
+                o.parent = (short)S.mp[p].y;
+            }
+            S.A[np] = o;
+        }
+        __syncwarp();
+        n = kept;
+        int md = 0;
+        for (int i = lane; i < n; i += 32) md = max(md, de_depth(S.A[i].de));
+        for (int o = 16; o; o >>= 1) md = max(md, __shfl_xor_sync(FULL, md, o));
+        // TargetImp.cpp:132-136: the site's matches are set-maximal only if no
+        // longer path is still alive
+        if (newcount && td >= md && nres + newcount <= cap) nres += newcount;
+        td = md;
+    }
+    for (int o = 16; o; o >>= 1) err |= __shfl_xor_sync(FULL, err, o);
+    if (lane == 0) {
         nmatch[hap] = err ? -1 : nres;
         if (err) atomicOr(status, err);
     }
