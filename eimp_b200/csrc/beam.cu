@@ -7,24 +7,31 @@
 //
 // Work split inside the warp:
 //  * haplotype-path extensions (the PBWT interval mappings over the history,
-//    the bulk of the work) run one path per lane.  Each path's probabilities
-//    are accumulated in its own lane in the reference's order.  The reference
-//    copies intervals from the previously extended path (HaplotypePath.cpp:
-//    330-390); they are recomputed here, which gives the same intervals: an
-//    interval depends only on the recent history the two paths share;
+//    the bulk of the work) run one path per lane against the cursor's two
+//    PBWT rows, which the warp stages in shared memory at every advance.  Each
+//    path's probabilities are accumulated in its own lane in the reference's
+//    order.  The reference copies intervals from the previously extended path
+//    (HaplotypePath.cpp:330-390); they are recomputed here, which gives the
+//    same intervals: an interval depends only on the recent history the two
+//    paths share;
 //  * beam-path extensions run one path per lane (per-path products; the
 //    maximum and the reference counts do not depend on the order);
-//  * pruning (min-max heap), merging, list order and the keep/switch sums
-//    follow the reference's sequential order on lane 0.
+//  * the new list orders (haplotype paths after applying, beam paths after
+//    applying and merging) are computed with warp scans; the positions are
+//    the ones the reference's sequential loops produce;
+//  * what depends on the sequential order stays on lane 0: the min-max heap
+//    of the pruning, the merge of beam paths that share both histories (only
+//    the duplicates, in list order), and the float sums of the calls and of
+//    the recombination distances (over per-path terms the lanes prepare).
 // Floating point follows the reference operation by operation: float
 // arithmetic with explicit double where the reference promotes (pow(), double
 // literals, std::ilogb), explicit round-to-nearest intrinsics (no FMA).
 //
-// Storage per target lives in an arena in global memory: haplotype-path
-// records, their probability rings, a pool of interval buffers (a path owns
-// three: its intervals and its two extensions; copying a path hands over a
-// buffer instead of copying it), the beam in list order (two buffers), and
-// the constraint and probability vectors of the target.
+// The beam (two list buffers) and the per-warp scalars live in shared memory.
+// The haplotype-path records, their probability rings and a pool of interval
+// buffers (a path owns three: its intervals and its two extensions; copying a
+// path hands over a buffer instead of copying it), and the constraint and
+// probability vectors of the target live in an arena in global memory.
 #include <climits>
 
 #include "common.cuh"
@@ -39,7 +46,10 @@ enum { C_HOMREF = 0, C_HETKEEP = 1, C_HETSWITCH = 2, C_HOMALT = 3, C_NONE = 4 };
 struct Cons { int type, refidx; };
 
 constexpr int PHMAX = 128;   // History<fp_type> ring (power of two >= H, H <= 128)
-constexpr int HT = 1024;     // merge hash table entries
+constexpr int PMAX = 128;    // largest beam width
+constexpr int BPMAX = PMAX;  // beam paths held between two prunes (<= P)
+constexpr int HTS = 512;     // merge hash table entries (load <= 1/4)
+static_assert(BPMAX < HTS, "the merge table must never fill");
 
 struct HPh {   // HaplotypePath
     unsigned long long d0, d1;   // BooleanHistory data (fill mask applied)
@@ -68,10 +78,15 @@ struct BPh {   // BeamPath
 
 struct Hel { float key; int a; int b; };
 
-struct WS {   // per-warp shared state
+struct __align__(16) WS {   // per-warp state in shared memory
     float prec[PHMAX];
-    Hel heap[PHMAX + 2];
-    int2 ht[HT];
+    float cdv[PHMAX];
+    Hel heap[PMAX + 2];
+    int2 ht[HTS];                 // merge keys: (key, surviving beam path), x = -1 when free
+    BPh bp[2][BPMAX];             // the beam in list order (two buffers)
+    float acc0[BPMAX], acc1[BPMAX];
+    short slot[BPMAX];            // hash slot of each beam path during a merge
+    unsigned char delmask[BPMAX]; // extensions the pruning deleted, per beam path
     int cursor, curridx, refidx, reverse;
     int nbp, bpsel, nhap, nfree, nivfree, err;
     int H, P, Delta, phsize;
@@ -79,8 +94,11 @@ struct WS {   // per-warp shared state
     int histlast;
     int ires, ires2;
     int wse, delerr;   // weightScaleExp and deleteErr of the last prune (Beam.cpp:673-678)
+    int c0inc, c0ref;  // zero counts of the cursor's two PBWT rows
     float fres;
     const Cons *constr;
+    uint32_t *rowinc, *rowref;   // the cursor's PBWT rows (shared memory after the WS array)
+    short *canon;                // per list position: first position of its run of equal histories
 };
 
 struct Ctx {
@@ -89,12 +107,11 @@ struct Ctx {
     float *ph;
     int2 *ivpool;
     int *ivfree;
-    BPh *bpbuf[2];
     int *happ, *happ_old;
     int2 *hapmap;
     int *fstack;
     int *copies;
-    int NH, BPC, HMAX;
+    int NH, HMAX;
     // pbwt of this target
     const uint32_t *rows;
     const int32_t *count0;
@@ -110,6 +127,7 @@ struct Ctx {
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
 
 // std::ilogb(float) as glibc defines it: the unbiased exponent (subnormals
 // included), INT_MIN for zero and NaN, INT_MAX for infinity
@@ -144,13 +162,6 @@ __device__ __forceinline__ int bh_equal(const HPh &a, const HPh &b) {
 
 __device__ __forceinline__ float *ph_ptr(const Ctx &c, int slot) { return c.ph + (size_t)slot * PHMAX; }
 __device__ __forceinline__ int2 *iv_buf(const Ctx &c, int b) { return c.ivpool + (size_t)b * c.HMAX; }
-
-// ------------------------------------------------------------------ pbwt
-__device__ __forceinline__ void pv_map(const Ctx &c, int reverse, int m, int l, int r, int &l0, int &r0, int &l1,
-                                       int &r1) {
-    const uint32_t *row = c.rows + (size_t)(reverse ? (2 * c.Mp - 1 - m) : m) * c.kw;
-    pbwt_map(row, c.count0[m], l, r, l0, r0, l1, r1);
-}
 
 // ------------------------------------------------------------------ min-max heap (MinMaxHeap.h)
 __device__ __forceinline__ int hlt(const Hel &x, const Hel &y) { return x.key < y.key; }
@@ -216,7 +227,6 @@ __device__ int ivbuf_alloc(const Ctx &c, WS &w) {
     if (w.nivfree == 0) { w.err |= EIMP_ERR_BEAM_CAPACITY; return 0; }
     return c.ivfree[--w.nivfree];
 }
-__device__ __forceinline__ void ivbuf_free(const Ctx &c, WS &w, int b) { c.ivfree[w.nivfree++] = b; }
 
 __device__ void hp_new(const Ctx &c, WS &w, int slot, int alt) {   // HaplotypePath.cpp:36-53 (lane 0)
     HPh &h = c.hp[slot];
@@ -234,11 +244,6 @@ __device__ void hp_new(const Ctx &c, WS &w, int slot, int alt) {   // HaplotypeP
     h.biv = ivbuf_alloc(c, w); h.bext0 = ivbuf_alloc(c, w); h.bext1 = ivbuf_alloc(c, w);
 }
 
-__device__ __forceinline__ void hp_mark_deleted(HPh &h, int e) {   // HaplotypePath.cpp:105-109
-    if (e == 0) { h.refcnt0--; if (h.refcnt0 == 0) h.active0 = 0; }
-    else { h.refcnt1--; if (h.refcnt1 == 0) h.active1 = 0; }
-}
-
 __device__ __forceinline__ void hp_mark_required(HPh &h, const Cons &cn) {   // HaplotypePath.cpp:139-158
     if (cn.type == C_NONE) { h.toext0 = 1; h.toext1 = 1; return; }
     int hb = bh_at(h, cn.refidx);
@@ -249,8 +254,9 @@ __device__ __forceinline__ void hp_mark_required(HPh &h, const Cons &cn) {   // 
 }
 
 // HaplotypePath::extend with updateScaling and calculateHaplotypeProbabilities
-// (HaplotypePath.cpp:162-479); returns extscaleexp
-__device__ int hp_extend(const Ctx &c, const WS &w, int slot, int cursor) {
+// (HaplotypePath.cpp:162-479) against the cursor's two PBWT rows in shared
+// memory; returns extscaleexp
+__device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
     HPh &h = c.hp[slot];
     float *ph = ph_ptr(c, slot);
     const int pm = w.phsize - 1;
@@ -274,7 +280,7 @@ __device__ int hp_extend(const Ctx &c, const WS &w, int slot, int cursor) {
     const int lim = w.H < h.niv + 1 ? w.H : h.niv + 1;
     float p0 = 0.0f, p1 = 0.0f;
     int n0 = 0, n1 = 0;
-    const int cnt0 = c.count0[2 * cursor + 1];
+    const int cnt0 = w.c0ref;
     const float t0 = __fmul_rn(ph[h.phstart & pm], w.prec[0]);
     if (cnt0 > 0) {
         if (calc0) p0 = __fmul_rn((float)cnt0, t0);
@@ -284,22 +290,23 @@ __device__ int hp_extend(const Ctx &c, const WS &w, int slot, int cursor) {
         if (calc1) p1 = __fmul_rn((float)(c.K - cnt0), t0);
         e1[n1++] = make_int2(cnt0, c.K - 1);
     }
-    const int rev = w.reverse;
-    const int incrow = rev ? 2 * (cursor + 1) : 2 * cursor;
+    const uint32_t *rinc = w.rowinc, *rref = w.rowref;
+    const int cinc = w.c0inc;
     int2 prevfrom = make_int2(0, -1);
+    int2 from = lim > 1 ? iv[0] : make_int2(0, -1);
     for (int i = 1; i < lim; i++) {
-        const int2 from = iv[i - 1];
+        const int2 nextfrom = i + 1 < lim ? iv[i] : make_int2(0, -1);   // prefetch
+        const float ti = __fmul_rn(ph[(i + h.phstart) & pm], w.prec[i]);
         int a0 = 0, b0 = -1, a1 = 0, b1 = -1;
         if (i > 1 && prevfrom.x == from.x && prevfrom.y == from.y) {   // :395-399
             if (n0 == i) { a0 = e0[n0 - 1].x; b0 = e0[n0 - 1].y; }
             if (n1 == i) { a1 = e1[n1 - 1].x; b1 = e1[n1 - 1].y; }
         } else {
             int cl, cr, il, ir;
-            pv_map(c, rev, incrow, from.x, from.y, cl, cr, il, ir);
-            pv_map(c, rev, 2 * cursor + 1, cl, cr, a0, b0, a1, b1);
+            pbwt_map(rinc, cinc, from.x, from.y, cl, cr, il, ir);
+            pbwt_map(rref, cnt0, cl, cr, a0, b0, a1, b1);
         }
         prevfrom = from;
-        const float ti = __fmul_rn(ph[(i + h.phstart) & pm], w.prec[i]);
         bool any = false;
         if (a0 <= b0) {
             if (calc0) p0 = __fadd_rn(p0, __fmul_rn((float)(b0 - a0 + 1), ti));
@@ -312,12 +319,15 @@ __device__ int hp_extend(const Ctx &c, const WS &w, int slot, int cursor) {
             any = true;
         }
         if (!any) break;
+        from = nextfrom;
     }
     h.next0 = n0; h.next1 = n1;
     h.extp0 = p0; h.extp1 = p1;
     h.active0 = h.toext0; h.active1 = h.toext1;
     return h.extscaleexp;
 }
+
+
 
 // HaplotypePath::applyExtension (HaplotypePath.cpp:77-103)
 __device__ void hp_apply(const Ctx &c, const WS &w, int slot, int e) {
@@ -395,34 +405,80 @@ __device__ float bp_extend(const Ctx &c, BPh &b, int g, const Cons &cn, int bpsc
     return maxP;
 }
 
-__device__ __forceinline__ void bp_mark_deleted(const Ctx &c, BPh &b, int ext) {   // BeamPath.cpp:101-112
+__device__ __forceinline__ void hp_mark_deleted_atomic(HPh &h, int e) {   // HaplotypePath.cpp:105-109
+    // the decrements of one prune commute: the extension becomes inactive iff
+    // one of them brings its count to zero
+    if (e == 0) { if (atomicSub(&h.refcnt0, 1) == 1) h.active0 = 0; }
+    else { if (atomicSub(&h.refcnt1, 1) == 1) h.active1 = 0; }
+}
+
+// BeamPath::markExtensionDeleted (BeamPath.cpp:101-112) on the beam path; the
+// haplotype-path side is applied after the heap pass from delmask
+__device__ __forceinline__ void bp_mark_deleted_deferred(WS &w, BPh &b, int it, int ext) {
     b.active[ext] = 0;
-    hp_mark_deleted(c.hp[c.happ[b.mat]], ext / 2);
-    hp_mark_deleted(c.hp[c.happ[b.pat]], ext % 2);
     bp_update_actidx(b);
+    w.delmask[it] |= (unsigned char)(1u << ext);
 }
 
 // ------------------------------------------------------------------ beam
-__device__ void beam_calc_rec(const Ctx &c, WS &w) {   // Beam.cpp:541-573 (lane 0)
+// Beam::calculateRecProbs (Beam.cpp:541-573).  The distance to history entry
+// i is the float sum of the i preceding split-site distances (lane 0, in the
+// reference's order); the probabilities are per entry (lanes).
+__device__ void beam_calc_rec(const Ctx &c, WS &w) {
+    const int lane = lane_id();
     const int cur = w.cursor;
-    int ci = w.reverse ? cur + 1 : cur;
+    const int L = w.reverse ? min(w.H, c.S - cur) : min(w.H, cur + 1);
+    for (int i = lane; i < L; i += 32) w.cdv[i] = c.cmd[w.reverse ? cur + 1 + i : cur - i];
+    __syncwarp();
+    if (lane == 0) {
+        float cd = 0.0f;
+        int i = 0;
+        for (; i + 4 <= L; i += 4) {
+            const float4 x = *reinterpret_cast<const float4 *>(&w.cdv[i]);
+            w.cdv[i] = cd; cd = __fadd_rn(cd, x.x);
+            w.cdv[i + 1] = cd; cd = __fadd_rn(cd, x.y);
+            w.cdv[i + 2] = cd; cd = __fadd_rn(cd, x.z);
+            w.cdv[i + 3] = cd; cd = __fadd_rn(cd, x.w);
+        }
+        for (; i < L; i++) { const float x = w.cdv[i]; w.cdv[i] = cd; cd = __fadd_rn(cd, x); }
+    }
+    __syncwarp();
     const float cursordiff = w.reverse ? c.cmd[cur] : c.cmd[cur + 1];
-    float cd = 0.0f;
-    for (int i = 0; i < w.H; i++) {
+    for (int i = lane; i < L; i += 32) {
+        const float cd = w.cdv[i];
         float tmp1 = (float)(1.0 + (double)__fdiv_rn(cd, c.expectIBDcM));
         float pr = (float)(1.0 / (double)__fmul_rn(tmp1, tmp1));
         float tmp2 = (float)(1.0 + (double)__fdiv_rn(__fadd_rn(cd, cursordiff), c.expectIBDcM));
         pr = (float)((double)pr - 1.0 / (double)__fmul_rn(tmp2, tmp2));
         pr = fmaxf(fminf(pr, 1.0f), 0.000001f);
         w.prec[i] = __fmul_rn(pr, c.Kinv);
-        cd = __fadd_rn(cd, c.cmd[ci]);
-        if (w.reverse) { ci++; if (ci >= c.S + 1) break; }
-        else { if (ci == 0) break; ci--; }
     }
+    __syncwarp();
+}
+
+// the cursor's two PBWT rows (the incon row of the previous split site and
+// the ref row of this one) into shared memory
+__device__ void beam_load_rows(const Ctx &c, WS &w) {
+    const int cur = w.cursor;
+    const int mi = w.reverse ? 2 * (cur + 1) : 2 * cur, mr = 2 * cur + 1;
+    const int pi = w.reverse ? 2 * c.Mp - 1 - mi : mi, pr = w.reverse ? 2 * c.Mp - 1 - mr : mr;
+    const uint2 *si = reinterpret_cast<const uint2 *>(c.rows + (size_t)pi * c.kw);
+    const uint2 *sr = reinterpret_cast<const uint2 *>(c.rows + (size_t)pr * c.kw);
+    uint2 *di = reinterpret_cast<uint2 *>(w.rowinc), *dr = reinterpret_cast<uint2 *>(w.rowref);
+    const int n2 = c.kw / 2;
+    for (int i = lane_id(); i < n2; i += 32) { di[i] = si[i]; dr[i] = sr[i]; }
+    if (lane_id() == 0) { w.c0inc = c.count0[mi]; w.c0ref = c.count0[mr]; }
+    __syncwarp();
 }
 
 __device__ void beam_init(const Ctx &c, WS &w, const Cons *constr, int reverse, int H, int P, int Delta) {
-    if (lane_id() == 0) {   // Beam.cpp:41-92
+    const int lane = lane_id();
+    for (int i = lane; i < c.NH; i += 32) c.fstack[i] = c.NH - 1 - i;
+    for (int i = lane; i < 3 * c.NH; i += 32) c.ivfree[i] = 3 * c.NH - 1 - i;
+    for (int i = lane; i < HTS; i += 32) w.ht[i] = make_int2(-1, INT_MAX);
+    for (int i = lane; i < PHMAX; i += 32) w.prec[i] = 0.0f;
+    __syncwarp();
+    if (lane == 0) {   // Beam.cpp:41-92
         w.H = H; w.P = P; w.Delta = Delta;
         int l2 = 31 - __clz(H);
         if ((1 << l2) != H) l2++;
@@ -437,18 +493,15 @@ __device__ void beam_init(const Ctx &c, WS &w, const Cons *constr, int reverse, 
         w.cursor = reverse ? c.S : -1;
         w.curridx = -1; w.refidx = -1;
         w.err = 0;
-        for (int i = 0; i < PHMAX; i++) w.prec[i] = 0.0f;
         w.nfree = c.NH;
-        for (int i = 0; i < c.NH; i++) c.fstack[i] = c.NH - 1 - i;
         w.nivfree = 3 * c.NH;
-        for (int i = 0; i < 3 * c.NH; i++) c.ivfree[i] = 3 * c.NH - 1 - i;
         int mat = c.fstack[--w.nfree], pat = c.fstack[--w.nfree];
         hp_new(c, w, mat, 0);
         hp_new(c, w, pat, 1);
         c.happ[0] = mat; c.happ[1] = pat;
         w.nhap = 2;
         w.bpsel = 0;
-        BPh &b = c.bpbuf[0][0];
+        BPh &b = w.bp[0][0];
         b.mat = 0; b.pat = 1; b.weight = 1.0f;
         b.nErr = 0; b.pErrPath = 1.0f; b.pErrPathp1 = __fmul_rn(1.0f, c.pErr);
         b.prob = (float)(pow2i(0) * (double)c.hp[mat].p * (double)c.hp[pat].p * 1.0);
@@ -459,103 +512,149 @@ __device__ void beam_init(const Ctx &c, WS &w, const Cons *constr, int reverse, 
     __syncwarp();
 }
 
-// Beam::prunePaths (Beam.cpp:577-787) -- filter + heap part, lane 0.
-// Returns 0 when no extension survives (the beam would be empty).
+// Beam::prunePaths (Beam.cpp:577-787), the filter and the min-max heap: lane
+// 0 over the beam in shared memory.  The reference counts of the haplotype
+// paths are decremented afterwards by the lanes (nothing in the heap pass
+// reads them).  Returns 0 when no extension survives.
 __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn) {
-    const float limit = __fmul_rn(c.pLimit, maxP);
-    BPh *bp = c.bpbuf[w.bpsel];
-    Hel *hq = w.heap;
-    int n = 0;
-    for (int it = 0; it < w.nbp; it++) {
-        BPh &b = bp[it];
-        int ex = b.actidx;
-        while (ex >= 0) {
-            float p = b.extp[ex];
-            if (p >= limit) {
-                if (n < w.P || (n == w.P && p > hq[0].key)) {
-                    if (n == w.P) {
-                        Hel e = heap_popmin(hq, n);
-                        bp_mark_deleted(c, bp[e.a], e.b);
-                    }
-                    heap_push(hq, n, p, it, ex);
-                } else bp_mark_deleted(c, b, ex);
-            } else bp_mark_deleted(c, b, ex);
-            ex = cn.type == C_NONE ? ex - 1 : -1;
+    const int lane = lane_id();
+    BPh *bp = w.bp[w.bpsel];
+    for (int it = lane; it < w.nbp; it += 32) w.delmask[it] = 0;
+    __syncwarp();
+    if (lane == 0) {
+        const float limit = __fmul_rn(c.pLimit, maxP);
+        Hel *hq = w.heap;
+        const int P = w.P;
+        int n = 0;
+        for (int it = 0; it < w.nbp; it++) {
+            BPh &b = bp[it];
+            int ex = b.actidx;
+            while (ex >= 0) {
+                const float p = b.extp[ex];
+                if (p >= limit) {
+                    if (n < P || (n == P && p > hq[0].key)) {
+                        if (n == P) {
+                            Hel e = heap_popmin(hq, n);
+                            bp_mark_deleted_deferred(w, bp[e.a], e.a, e.b);
+                        }
+                        heap_push(hq, n, p, it, ex);
+                    } else bp_mark_deleted_deferred(w, b, it, ex);
+                } else bp_mark_deleted_deferred(w, b, it, ex);
+                ex = cn.type == C_NONE ? ex - 1 : -1;
+            }
+        }
+        w.ires = n;
+        if (n) {
+            w.wse = -ilogb_exact(bp[hq[0].a].weight);                    // weightScaleExp
+            w.delerr = bp[hq[heap_maxidx(hq, n)].a].nErr > 0;            // deleteErr
         }
     }
-    if (n == 0) return 0;
-    w.wse = -ilogb_exact(bp[hq[0].a].weight);                    // weightScaleExp
-    w.delerr = bp[hq[heap_maxidx(hq, n)].a].nErr > 0;            // deleteErr
-    return 1;
+    __syncwarp();
+    const int n = w.ires;
+    for (int it = lane; it < w.nbp; it += 32) {
+        const unsigned dm = w.delmask[it];
+        if (!dm) continue;
+        HPh &pm = c.hp[c.happ[bp[it].mat]];
+        HPh &pp = c.hp[c.happ[bp[it].pat]];
+        for (int ex = 0; ex < 4; ex++)
+            if (dm & (1u << ex)) { hp_mark_deleted_atomic(pm, ex >> 1); hp_mark_deleted_atomic(pp, ex & 1); }
+    }
+    __syncwarp();
+    return n > 0;
 }
 
-// apply the haplotype-path extensions (Beam.cpp:684-726).  Lane 0 plans the
-// new order; the warp copies the probability rings of duplicated paths; the
-// lanes then apply the extensions.
+// apply the haplotype-path extensions (Beam.cpp:684-726).  The new list holds
+// the paths extended with 0 in old order, then the paths extended with 1 in
+// old order; a path with both extensions stays among the first and its copy
+// (HaplotypePath.cpp:55-75), which takes the 1-extension, among the second.
+// Positions come from warp scans; released slots are pushed before the copies
+// take theirs (slot numbers are storage only and do not change results).
 __device__ void beam_apply_hap(const Ctx &c, WS &w) {
     const int lane = lane_id();
-    if (lane == 0) {
-        const int nold = w.nhap;
-        for (int i = 0; i < nold; i++) c.happ_old[i] = c.happ[i];
-        int next0 = 0;
-        for (int i = 0; i < nold; i++) if (c.hp[c.happ_old[i]].active0) next0++;
-        int one = next0, zero = 0, ncopy = 0;
-        for (int i = 0; i < nold; i++) {
-            int id = c.happ_old[i];
-            HPh &h = c.hp[id];
-            c.hapmap[i] = make_int2(zero, one);
-            if (!(h.active0 || h.active1)) {
-                c.fstack[w.nfree++] = id;
-                ivbuf_free(c, w, h.biv); ivbuf_free(c, w, h.bext0); ivbuf_free(c, w, h.bext1);
-                continue;
+    const unsigned FULL = 0xffffffffu;
+    const int nold = w.nhap;
+    for (int i = lane; i < nold; i += 32) c.happ_old[i] = c.happ[i];
+    __syncwarp();
+    int next0 = 0, nrel = 0, ncp = 0;
+    for (int base = 0; base < nold; base += 32) {
+        const int i = base + lane;
+        bool a0 = false, a1 = false;
+        if (i < nold) { const HPh &h = c.hp[c.happ_old[i]]; a0 = h.active0; a1 = h.active1; }
+        next0 += __popc(__ballot_sync(FULL, a0));
+        nrel += __popc(__ballot_sync(FULL, i < nold && !a0 && !a1));
+        ncp += __popc(__ballot_sync(FULL, a0 && a1));
+    }
+    const int nfree0 = w.nfree, nivfree0 = w.nivfree;
+    if (nfree0 + nrel < ncp || nivfree0 + 3 * nrel < 3 * ncp) {
+        if (lane == 0) w.err |= EIMP_ERR_BEAM_CAPACITY;
+        __syncwarp();
+        return;
+    }
+    int zero = 0, one = next0, rel = 0, cp = 0;
+    for (int base = 0; base < nold; base += 32) {
+        const int i = base + lane;
+        bool a0 = false, a1 = false;
+        int id = -1;
+        if (i < nold) { id = c.happ_old[i]; const HPh &h = c.hp[id]; a0 = h.active0; a1 = h.active1; }
+        const unsigned b0 = __ballot_sync(FULL, a0), b1 = __ballot_sync(FULL, a1);
+        const unsigned br = __ballot_sync(FULL, i < nold && !a0 && !a1), bc = __ballot_sync(FULL, a0 && a1);
+        const unsigned lt = lanemask_lt();
+        if (i < nold) {
+            const int z = zero + __popc(b0 & lt), o = one + __popc(b1 & lt);
+            c.hapmap[i] = make_int2(z, o);
+            if (a0) c.happ[z] = id;
+            else if (a1) c.happ[o] = id;
+            if (!a0 && !a1) {
+                const int r = rel + __popc(br & lt);
+                const HPh &h = c.hp[id];
+                c.fstack[nfree0 + r] = id;
+                c.ivfree[nivfree0 + 3 * r] = h.biv;
+                c.ivfree[nivfree0 + 3 * r + 1] = h.bext0;
+                c.ivfree[nivfree0 + 3 * r + 2] = h.bext1;
+            } else if (a0 && a1) {
+                const int k = cp + __popc(bc & lt);
+                c.copies[3 * k] = id;
+                c.copies[3 * k + 2] = o;
             }
-            if (h.active0 && h.active1) {
-                if (w.nfree == 0) { w.err |= EIMP_ERR_BEAM_CAPACITY; break; }
-                int cp = c.fstack[--w.nfree];
-                c.happ[one++] = cp;
-                c.happ[zero++] = id;
-                c.copies[2 * ncopy] = id;
-                c.copies[2 * ncopy + 1] = cp;
-                ncopy++;
-                continue;
-            }
-            if (h.active0) c.happ[zero++] = id;
-            else c.happ[one++] = id;
         }
-        // the old list (for applying) after the copies
-        w.ires = ncopy;
-        w.ires2 = nold;
-        w.nhap = one;
-        // records of the copies (HaplotypePath.cpp:55-75): the copy takes the
-        // extension-1 intervals as its own; the source gets a fresh buffer
-        for (int k = 0; k < ncopy; k++) {
-            HPh &o = c.hp[c.copies[2 * k]];
-            HPh &n = c.hp[c.copies[2 * k + 1]];
-            n.d0 = o.d0; n.d1 = o.d1; n.last = o.last;
-            n.p = o.extp1; n.scaleexp = o.extscaleexp;
-            n.phstart = o.phstart;
-            n.biv = o.bext1; n.niv = o.next1;
-            n.bext0 = ivbuf_alloc(c, w); n.bext1 = ivbuf_alloc(c, w);
-            n.next0 = 0; n.next1 = 0;
-            n.active0 = n.active1 = n.toext0 = n.toext1 = 0;
-            n.refcnt0 = 0; n.refcnt1 = 0;
-            n.extp0 = 0.0f; n.extp1 = 0.0f; n.extscaleexp = 0;
-            o.bext1 = ivbuf_alloc(c, w);
-            o.next1 = 0;   // (the reference keeps a stale copy; it is rewritten before use)
-        }
+        zero += __popc(b0); one += __popc(b1); rel += __popc(br); cp += __popc(bc);
     }
     __syncwarp();
-    const int ncopy = w.ires, nold = w.ires2;
+    const int nf = nfree0 + nrel, nvf = nivfree0 + 3 * nrel;
+    // records of the copies: the copy takes the extension-1 intervals as its
+    // own; the source gets a fresh buffer for them
+    for (int k = lane; k < ncp; k += 32) {
+        const int id = c.copies[3 * k];
+        const int slot = c.fstack[nf - 1 - k];
+        c.copies[3 * k + 1] = slot;
+        c.happ[c.copies[3 * k + 2]] = slot;
+        HPh &o = c.hp[id];
+        HPh &n = c.hp[slot];
+        n.d0 = o.d0; n.d1 = o.d1; n.last = o.last;
+        n.p = o.extp1; n.scaleexp = o.extscaleexp;
+        n.phstart = o.phstart;
+        n.biv = o.bext1; n.niv = o.next1;
+        n.bext0 = c.ivfree[nvf - 1 - 3 * k];
+        n.bext1 = c.ivfree[nvf - 2 - 3 * k];
+        n.next0 = 0; n.next1 = 0;
+        n.active0 = n.active1 = n.toext0 = n.toext1 = 0;
+        n.refcnt0 = 0; n.refcnt1 = 0;
+        n.extp0 = 0.0f; n.extp1 = 0.0f; n.extscaleexp = 0;
+        o.bext1 = c.ivfree[nvf - 3 - 3 * k];
+        o.next1 = 0;   // (the reference keeps a stale copy; it is rewritten before use)
+    }
+    if (lane == 0) { w.nfree = nf - ncp; w.nivfree = nvf - 3 * ncp; w.nhap = one; }
+    __syncwarp();
     // probability rings of the copies
     const int phs = w.phsize;
-    for (int e = lane; e < ncopy * phs; e += 32) {
-        int k = e / phs, i = e % phs;
-        ph_ptr(c, c.copies[2 * k + 1])[i] = ph_ptr(c, c.copies[2 * k])[i];
+    for (int e = lane; e < ncp * phs; e += 32) {
+        const int k = e / phs, i = e % phs;
+        ph_ptr(c, c.copies[3 * k + 1])[i] = ph_ptr(c, c.copies[3 * k])[i];
     }
     __syncwarp();
-    // new paths: push bit 1 and the extension-1 probability
-    for (int k = lane; k < ncopy; k += 32) {
-        int slot = c.copies[2 * k + 1];
+    // the copies: push bit 1 and the extension-1 probability
+    for (int k = lane; k < ncp; k += 32) {
+        const int slot = c.copies[3 * k + 1];
         HPh &n = c.hp[slot];
         bh_push(n, 1, w);
         float *ph = ph_ptr(c, slot);
@@ -564,7 +663,7 @@ __device__ void beam_apply_hap(const Ctx &c, WS &w) {
     }
     // old paths still alive: apply their (single or zero) extension
     for (int i = lane; i < nold; i += 32) {
-        int id = c.happ_old[i];
+        const int id = c.happ_old[i];
         HPh &h = c.hp[id];
         if (!(h.active0 || h.active1)) continue;
         hp_apply(c, w, id, h.active0 ? 0 : 1);
@@ -572,118 +671,174 @@ __device__ void beam_apply_hap(const Ctx &c, WS &w) {
     __syncwarp();
 }
 
-// apply the beam-path extensions (Beam.cpp:728-779), lane 0: survivors keep
-// their order, extra extensions of a path are appended in the reference's
-// order (descending extension index, the lowest is applied in place)
+__device__ __forceinline__ void bp_make(BPh &o, const BPh &b, int ex, int mat, int pat, int wse, double wsf,
+                                        int delerr, float pErr) {   // BeamPath.cpp:44-96
+    o.mat = mat; o.pat = pat;
+    o.prob = b.extp[ex]; o.weight = b.weight;
+    o.nErr = b.nErr; o.pErrPath = b.pErrPath; o.pErrPathp1 = b.pErrPathp1;
+    o.extgeno = b.extgeno;
+    if (wse != 0) o.weight = (float)((double)o.weight * wsf);
+    bp_update_errors(o, ex, delerr, pErr);
+    for (int q = 0; q < 4; q++) { o.extp[q] = 0.0f; o.active[q] = 0; }
+    o.actidx = -1; o.extgeno = 3;
+}
+
+// apply the beam-path extensions (Beam.cpp:728-779): each path with a
+// surviving extension keeps its position with its lowest extension; its other
+// extensions are appended in the reference's order (paths in list order,
+// extensions in descending index).  Positions come from warp scans.
 __device__ void beam_apply_bp(const Ctx &c, WS &w) {
-    if (lane_id() == 0) {
-        const int wse = w.wse, delerr = w.delerr;
-        BPh *src = c.bpbuf[w.bpsel];
-        BPh *dst = c.bpbuf[w.bpsel ^ 1];
-        const double wsf = pow2i(wse);
-        int n = 0;
-        for (int it = 0; it < w.nbp; it++) {
-            if (src[it].actidx >= 0) n++;
+    const int lane = lane_id();
+    const unsigned FULL = 0xffffffffu;
+    const int wse = w.wse, delerr = w.delerr;
+    const double wsf = pow2i(wse);
+    const BPh *src = w.bp[w.bpsel];
+    BPh *dst = w.bp[w.bpsel ^ 1];
+    const int nbp = w.nbp;
+    int nsurv = 0;
+    for (int base = 0; base < nbp; base += 32) {
+        const int it = base + lane;
+        nsurv += __popc(__ballot_sync(FULL, it < nbp && src[it].actidx >= 0));
+    }
+    int k = 0, app = nsurv;
+    for (int base = 0; base < nbp; base += 32) {
+        const int it = base + lane;
+        int nact = 0;
+        if (it < nbp) {
+            const BPh &b = src[it];
+            nact = (int)b.active[0] + (int)b.active[1] + (int)b.active[2] + (int)b.active[3];
         }
-        int napp = n;
-        int k = 0;
-        for (int it = 0; it < w.nbp; it++) {
-            BPh &b = src[it];
+        const unsigned bs = __ballot_sync(FULL, nact > 0);
+        const int extra = nact > 0 ? nact - 1 : 0;
+        int x = extra;   // inclusive scan of the extra extensions
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        const int tot = __shfl_sync(FULL, x, 31);
+        if (nact > 0) {
+            const BPh &b = src[it];
+            const int2 mm = c.hapmap[b.mat], pm = c.hapmap[b.pat];
+            const int mat[2] = {mm.x, mm.y}, pat[2] = {pm.x, pm.y};
+            int pos = app + x - extra;
             int ex = b.actidx;
-            if (ex < 0) continue;
-            int2 mm = c.hapmap[b.mat], pm = c.hapmap[b.pat];
-            int mat[2] = {mm.x, mm.y}, pat[2] = {pm.x, pm.y};
-            int nx = bp_next_active(b, ex);
-            while (nx != -1) {
-                if (napp >= c.BPC) { w.err |= EIMP_ERR_BEAM_CAPACITY; return; }
-                BPh &o = dst[napp++];   // BeamPath.cpp:44-68
-                o.mat = mat[ex / 2]; o.pat = pat[ex % 2];
-                o.prob = b.extp[ex]; o.weight = b.weight;
-                o.nErr = b.nErr; o.pErrPath = b.pErrPath; o.pErrPathp1 = b.pErrPathp1;
-                o.extgeno = b.extgeno;
-                if (wse != 0) o.weight = (float)((double)o.weight * wsf);
-                bp_update_errors(o, ex, delerr, c.pErr);
-                for (int q = 0; q < 4; q++) { o.extp[q] = 0.0f; o.active[q] = 0; }
-                o.actidx = -1; o.extgeno = 3;
-                ex = nx;
-                nx = bp_next_active(b, nx);
+            for (int r = 0; r < extra; r++) {
+                if (pos < BPMAX) bp_make(dst[pos], b, ex, mat[ex >> 1], pat[ex & 1], wse, wsf, delerr, c.pErr);
+                pos++;
+                ex = bp_next_active(b, ex);
             }
-            BPh &o = dst[k++];   // BeamPath.cpp:70-96
-            o.mat = mat[ex / 2]; o.pat = pat[ex % 2];
-            o.prob = b.extp[ex]; o.weight = b.weight;
-            o.nErr = b.nErr; o.pErrPath = b.pErrPath; o.pErrPathp1 = b.pErrPathp1;
-            o.extgeno = b.extgeno;
-            if (wse != 0) o.weight = (float)((double)o.weight * wsf);
-            bp_update_errors(o, ex, delerr, c.pErr);
-            for (int q = 0; q < 4; q++) { o.extp[q] = 0.0f; o.active[q] = 0; }
-            o.actidx = -1; o.extgeno = 3;
+            bp_make(dst[k + __popc(bs & lanemask_lt())], b, ex, mat[ex >> 1], pat[ex & 1], wse, wsf, delerr,
+                    c.pErr);
         }
-        w.nbp = napp;
+        k += __popc(bs);
+        app += tot;
+    }
+    if (lane == 0) {
+        if (app > BPMAX) w.err |= EIMP_ERR_BEAM_CAPACITY;
+        w.nbp = min(app, BPMAX);
         w.bpsel ^= 1;
     }
     __syncwarp();
 }
 
-// Beam::mergePaths (Beam.cpp:790-837), lane 0
+// Beam::mergePaths (Beam.cpp:790-837).  Each beam path's key is the pair of
+// first list positions of its two histories (runs of equal histories are
+// adjacent in the list).  The first path of each key survives unless a later
+// one with the same key is more probable; the duplicates are merged on lane
+// 0 in list order (the reference's sequential order within each key), then
+// the survivors are compacted into the other buffer.
 __device__ void beam_merge(const Ctx &c, WS &w) {
-    if (lane_id() == 0) {
-        BPh *bp = c.bpbuf[w.bpsel];
-        for (int i = 0; i < HT; i++) w.ht[i].x = -1;
-        const int n = w.nbp;
-        int keep = 0;
-        // erased flags in extp[0] sign bit is not usable: keep a separate mark
-        for (int it = 0; it < n; it++) bp[it].actidx = 0;   // 0 = alive, -2 = erased (actidx is -1 anyway here)
+    const int lane = lane_id();
+    const unsigned FULL = 0xffffffffu;
+    const int nhap = w.nhap;
+    int carry = 0;
+    for (int base = 0; base < nhap; base += 32) {
+        const int i = base + lane;
+        bool head = true;
+        if (i < nhap && i > 0) head = !bh_equal(c.hp[c.happ[i]], c.hp[c.happ[i - 1]]);
+        const unsigned hb = __ballot_sync(FULL, i < nhap && head);
+        const unsigned upto = hb & (lane == 31 ? FULL : ((2u << lane) - 1u));
+        const int cn = upto ? base + 31 - __clz(upto) : carry;
+        if (i < nhap) w.canon[i] = (short)cn;
+        carry = __shfl_sync(FULL, cn, 31);
+    }
+    __syncwarp();
+    BPh *bp = w.bp[w.bpsel];
+    const int n = w.nbp;
+    bool anydup = false;
+    for (int it = lane; it < n; it += 32) {
+        const int mr = w.canon[bp[it].mat], pr = w.canon[bp[it].pat];
+        const int k0 = mr < pr ? mr : pr, k1 = mr < pr ? pr : mr;
+        const int key = (k0 << 16) | k1;
+        int slot = (int)(((unsigned)key * 2654435761u) >> 23) & (HTS - 1);
+        // linear probing; the table holds at most BPMAX < HTS keys, so a
+        // free or matching slot exists within HTS probes
+        for (int probe = 0; probe < HTS; probe++) {
+            const int old = atomicCAS(&w.ht[slot].x, -1, key);
+            if (old == -1 || old == key) break;
+            slot = (slot + 1) & (HTS - 1);
+        }
+        atomicMin(&w.ht[slot].y, it);
+        w.slot[it] = (short)slot;
+    }
+    __syncwarp();
+    for (int it = lane; it < n; it += 32) {
+        const bool dup = w.ht[w.slot[it]].y != it;
+        bp[it].actidx = dup ? 1 : -1;   // marks: 1 = merge pending, -1 = alive, -2 = erased
+        anydup |= dup;
+    }
+    __syncwarp();
+    if (__any_sync(FULL, anydup) && lane == 0) {
         for (int it = 0; it < n; it++) {
             BPh &b = bp[it];
-            int mr = b.mat;
-            while (mr > 0 && bh_equal(c.hp[c.happ[mr]], c.hp[c.happ[mr - 1]])) mr--;
-            int pr = b.pat;
-            while (pr > 0 && bh_equal(c.hp[c.happ[pr]], c.hp[c.happ[pr - 1]])) pr--;
-            int k0 = mr < pr ? mr : pr, k1 = mr < pr ? pr : mr;
-            int key = (k0 << 16) | k1;
-            int hsh = (int)(((unsigned)key * 2654435761u) >> 22) & (HT - 1);
-            int found = -1, slot = hsh;
-            while (w.ht[slot].x != -1) {
-                if (w.ht[slot].x == key) { found = slot; break; }
-                slot = (slot + 1) & (HT - 1);
-            }
-            if (found >= 0) {
-                BPh &o = bp[w.ht[found].y];
-                if (o.prob > b.prob) {
-                    o.weight = __fadd_rn(o.weight, __fmul_rn(b.weight, __fdiv_rn(b.prob, o.prob)));
-                    b.actidx = -2;
-                } else {
-                    b.weight = __fadd_rn(b.weight, __fmul_rn(o.weight, __fdiv_rn(o.prob, b.prob)));
-                    o.actidx = -2;
-                    w.ht[found].y = it;
-                }
+            if (b.actidx != 1) continue;
+            int2 &hs = w.ht[w.slot[it]];
+            BPh &o = bp[hs.y];
+            if (o.prob > b.prob) {
+                o.weight = __fadd_rn(o.weight, __fmul_rn(b.weight, __fdiv_rn(b.prob, o.prob)));
+                b.actidx = -2;
             } else {
-                w.ht[slot] = make_int2(key, it);
+                b.weight = __fadd_rn(b.weight, __fmul_rn(o.weight, __fdiv_rn(o.prob, b.prob)));
+                o.actidx = -2;
+                b.actidx = -1;
+                hs.y = it;
             }
         }
-        for (int it = 0; it < n; it++) {
-            if (bp[it].actidx == -2) continue;
-            if (keep != it) bp[keep] = bp[it];
-            bp[keep].actidx = -1;
-            keep++;
-        }
-        w.nbp = keep;
     }
+    __syncwarp();
+    BPh *dst = w.bp[w.bpsel ^ 1];
+    int keep = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int it = base + lane;
+        const bool alive = it < n && bp[it].actidx != -2;
+        const unsigned ba = __ballot_sync(FULL, alive);
+        if (alive) {
+            BPh &o = dst[keep + __popc(ba & lanemask_lt())];
+            o = bp[it];
+            o.actidx = -1;
+        }
+        keep += __popc(ba);
+    }
+    for (int it = lane; it < n; it += 32) w.ht[w.slot[it]] = make_int2(-1, INT_MAX);
+    if (lane == 0) { w.nbp = keep; w.bpsel ^= 1; }
     __syncwarp();
 }
 
 // Beam::advanceBeamFront (Beam.cpp:263-539)
 __device__ int beam_advance(const Ctx &c, WS &w) {
     const int lane = lane_id();
-    if (lane == 0) {
-        w.cursor += w.reverse ? -1 : 1;
-        beam_calc_rec(c, w);
-    }
+    // every lane has read the cursor for its loop condition before lane 0
+    // moves it (otherwise lanes could leave the caller's loop at different
+    // iterations and meet different warp collectives)
     __syncwarp();
+    if (lane == 0) w.cursor += w.reverse ? -1 : 1;
+    __syncwarp();
+    beam_calc_rec(c, w);
+    beam_load_rows(c, w);
     const int cursor = w.cursor;
     Cons cn = w.constr[cursor];
     while (true) {
-        BPh *bp = c.bpbuf[w.bpsel];
+        BPh *bp = w.bp[w.bpsel];
         const int nbp = w.nbp, nhap = w.nhap;
         // markRequiredExtensions (only sets flags: order free)
         for (int it = lane; it < nbp; it += 32) {
@@ -694,10 +849,10 @@ __device__ int beam_advance(const Ctx &c, WS &w) {
         // happath extensions, one path per lane
         int minse = 0, maxse = INT_MIN;
         for (int i = lane; i < nhap; i += 32) {
-            int id = c.happ[i];
+            const int id = c.happ[i];
             HPh &h = c.hp[id];
             if (h.toext0 || h.toext1) {
-                int se = hp_extend(c, w, id, cursor);
+                const int se = hp_extend(c, w, id);
                 if (se < minse) minse = se;
                 if (se > maxse) maxse = se;
             }
@@ -712,16 +867,12 @@ __device__ int beam_advance(const Ctx &c, WS &w) {
         float maxP = 0.0f;
         const int g = c.tg[cursor];
         for (int it = lane; it < nbp; it += 32) {
-            float mp = bp_extend(c, bp[it], g, cn, bpscaleexp);
+            const float mp = bp_extend(c, bp[it], g, cn, bpscaleexp);
             if (maxP < mp) maxP = mp;
         }
         for (int o = 16; o; o >>= 1) maxP = fmaxf(maxP, __shfl_xor_sync(0xffffffffu, maxP, o));
         __syncwarp();
-        int ok = 0;
-        if (lane == 0) ok = beam_prune_select(c, w, maxP, cn);
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        __syncwarp();
-        if (ok) break;
+        if (beam_prune_select(c, w, maxP, cn)) break;
         if (cn.type != C_NONE) { cn.type = C_NONE; continue; }
         if (lane == 0) w.err |= EIMP_ERR_BEAM_EMPTY;
         __syncwarp();
@@ -735,13 +886,17 @@ __device__ int beam_advance(const Ctx &c, WS &w) {
     return 0;
 }
 
-// Beam::callKeepPhaseProb (Beam.cpp:95-185)
+// Beam::callKeepPhaseProb (Beam.cpp:95-185): the lanes classify the beam
+// paths and prepare each path's terms of the two sums (0 where a path adds
+// nothing, which leaves a float sum unchanged); lane 0 adds them in list order
 __device__ float beam_call_keep(const Ctx &c, WS &w, int ci, int twoback) {
-    if (lane_id() == 0) {
-        int cl = c.calls[ci];
-        int front = w.reverse ? max(cl - w.Delta, 0) : min(cl + w.Delta, c.S - 1);
+    const int lane = lane_id();
+    if (lane == 0) {
+        const int cl = c.calls[ci];
+        const int front = w.reverse ? max(cl - w.Delta, 0) : min(cl + w.Delta, c.S - 1);
         w.curridx = w.reverse ? cl - front : front - cl;
-        int r = w.reverse ? (twoback ? c.calls[ci + 2] : c.calls[ci + 1]) : (twoback ? c.calls[ci - 2] : c.calls[ci - 1]);
+        const int r = w.reverse ? (twoback ? c.calls[ci + 2] : c.calls[ci + 1])
+                                : (twoback ? c.calls[ci - 2] : c.calls[ci - 1]);
         w.refidx = w.reverse ? r - front : front - r;
         w.ires = front;
     }
@@ -749,22 +904,28 @@ __device__ float beam_call_keep(const Ctx &c, WS &w, int ci, int twoback) {
     const int front = w.ires;
     while ((w.reverse && w.cursor > front) || (!w.reverse && w.cursor < front))
         if (beam_advance(c, w)) return -1.0f;
-    if (lane_id() == 0) {
-        float acckp = 0.0f, accsp = 0.0f;
-        const BPh *bp = c.bpbuf[w.bpsel];
-        for (int it = 0; it < w.nbp; it++) {
-            const BPh &b = bp[it];
-            const HPh &hm = c.hp[c.happ[b.mat]], &hq = c.hp[c.happ[b.pat]];
-            int cf = bh_at(hm, w.curridx), cs = bh_at(hq, w.curridx);
-            int rf = bh_at(hm, w.refidx), rs = bh_at(hq, w.refidx);
-            float p = __fmul_rn(b.weight, b.prob);
-            if (cf != cs && rf != rs) {
-                if (cf == rf) acckp = __fadd_rn(acckp, p); else accsp = __fadd_rn(accsp, p);
-            } else {
-                acckp = __fadd_rn(acckp, __fdiv_rn(p, 2.0f));
-                accsp = __fadd_rn(accsp, __fdiv_rn(p, 2.0f));
-            }
+    const BPh *bp = w.bp[w.bpsel];
+    const int n = w.nbp, curridx = w.curridx, refidx = w.refidx;
+    for (int it = lane; it < n; it += 32) {
+        const BPh &b = bp[it];
+        const HPh &hm = c.hp[c.happ[b.mat]], &hq = c.hp[c.happ[b.pat]];
+        const int cf = bh_at(hm, curridx), cs = bh_at(hq, curridx);
+        const int rf = bh_at(hm, refidx), rs = bh_at(hq, refidx);
+        const float p = __fmul_rn(b.weight, b.prob);
+        float k, s;
+        if (cf != cs && rf != rs) {
+            k = cf == rf ? p : 0.0f;
+            s = cf == rf ? 0.0f : p;
+        } else {
+            k = __fdiv_rn(p, 2.0f);
+            s = k;
         }
+        w.acc0[it] = k; w.acc1[it] = s;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        float acckp = 0.0f, accsp = 0.0f;
+        for (int it = 0; it < n; it++) { acckp = __fadd_rn(acckp, w.acc0[it]); accsp = __fadd_rn(accsp, w.acc1[it]); }
         float ret = 0.5f;
         if (__fadd_rn(acckp, accsp) > 0.0f) ret = __fdiv_rn(acckp, __fadd_rn(acckp, accsp));
         w.fres = ret;
@@ -773,10 +934,11 @@ __device__ float beam_call_keep(const Ctx &c, WS &w, int ci, int twoback) {
     return w.fres;
 }
 
-// Beam::callDosage (Beam.cpp:187-261)
+// Beam::callDosage (Beam.cpp:187-261), split like beam_call_keep
 __device__ float beam_call_dosage(const Ctx &c, WS &w, int si) {
-    if (lane_id() == 0) {
-        int front = w.reverse ? max(si - w.Delta, 0) : min(si + w.Delta, c.S - 1);
+    const int lane = lane_id();
+    if (lane == 0) {
+        const int front = w.reverse ? max(si - w.Delta, 0) : min(si + w.Delta, c.S - 1);
         w.curridx = w.reverse ? si - front : front - si;
         w.refidx = -1;
         w.ires = front;
@@ -785,18 +947,20 @@ __device__ float beam_call_dosage(const Ctx &c, WS &w, int si) {
     const int front = w.ires;
     while ((w.reverse && w.cursor > front) || (!w.reverse && w.cursor < front))
         if (beam_advance(c, w)) return -1.0f;
-    if (lane_id() == 0) {
+    const BPh *bp = w.bp[w.bpsel];
+    const int n = w.nbp, curridx = w.curridx;
+    for (int it = lane; it < n; it += 32) {
+        const BPh &b = bp[it];
+        const HPh &hm = c.hp[c.happ[b.mat]], &hq = c.hp[c.happ[b.pat]];
+        const int cf = bh_at(hm, curridx), cs = bh_at(hq, curridx);
+        const float p = __fmul_rn(b.weight, b.prob);
+        w.acc0[it] = p;
+        w.acc1[it] = cf == cs ? (cf == 1 ? __fmul_rn(2.0f, p) : 0.0f) : p;
+    }
+    __syncwarp();
+    if (lane == 0) {
         float dos = 0.0f, ptot = 0.0f;
-        const BPh *bp = c.bpbuf[w.bpsel];
-        for (int it = 0; it < w.nbp; it++) {
-            const BPh &b = bp[it];
-            const HPh &hm = c.hp[c.happ[b.mat]], &hq = c.hp[c.happ[b.pat]];
-            int cf = bh_at(hm, w.curridx), cs = bh_at(hq, w.curridx);
-            float p = __fmul_rn(b.weight, b.prob);
-            ptot = __fadd_rn(ptot, p);
-            if (cf == cs) { if (cf == 1) dos = __fadd_rn(dos, __fmul_rn(2.0f, p)); }
-            else dos = __fadd_rn(dos, p);
-        }
+        for (int it = 0; it < n; it++) { ptot = __fadd_rn(ptot, w.acc0[it]); dos = __fadd_rn(dos, w.acc1[it]); }
         float ret = 1.0f;
         if (ptot > 0.0f) ret = __fdiv_rn(dos, ptot);
         w.fres = ret;
@@ -809,11 +973,11 @@ __host__ __device__ __forceinline__ size_t align256(size_t x) { return (x + 255)
 
 }  // namespace
 
+
 // arena layout per target (bytes)
 struct ArenaLayout {
-    size_t hp, ph, ivpool, ivfree, bp0, bp1, happ, happ_old, hapmap, fstack, copies, cons, rcons, probs, confs, tg,
-        total;
-    int NH, BPC, HMAX;
+    size_t hp, ph, ivpool, ivfree, happ, happ_old, hapmap, fstack, copies, cons, rcons, probs, confs, tg, total;
+    int NH, HMAX;
 };
 
 static ArenaLayout arena_layout(const BeamParams &p, int M) {
@@ -821,20 +985,20 @@ static ArenaLayout arena_layout(const BeamParams &p, int M) {
     int P = p.P > p.Pf ? p.P : p.Pf;
     int H = p.H > p.Hf ? p.H : p.Hf;
     a.NH = 4 * P + 8;
-    a.BPC = 4 * P + 8;
     a.HMAX = H;
     size_t o = 0;
     a.hp = o; o = align256(o + sizeof(HPh) * a.NH);
     a.ph = o; o = align256(o + sizeof(float) * PHMAX * a.NH);
-    a.ivpool = o; o = align256(o + sizeof(int2) * (size_t)H * 3 * a.NH);
+    // the interval pool doubles as the storage of the pre-phasing constraint
+    // heaps (one entry per split site) once the fast beam is done
+    const size_t ivb = sizeof(int2) * (size_t)H * 3 * a.NH, heapb = sizeof(Hel) * (size_t)(M + 1);
+    a.ivpool = o; o = align256(o + (ivb > heapb ? ivb : heapb));
     a.ivfree = o; o = align256(o + sizeof(int) * 3 * a.NH);
-    a.bp0 = o; o = align256(o + sizeof(BPh) * a.BPC);
-    a.bp1 = o; o = align256(o + sizeof(BPh) * a.BPC);
     a.happ = o; o = align256(o + sizeof(int) * a.NH);
     a.happ_old = o; o = align256(o + sizeof(int) * a.NH);
     a.hapmap = o; o = align256(o + sizeof(int2) * a.NH);
     a.fstack = o; o = align256(o + sizeof(int) * a.NH);
-    a.copies = o; o = align256(o + sizeof(int) * 2 * a.NH);
+    a.copies = o; o = align256(o + sizeof(int) * 3 * a.NH);
     a.cons = o; o = align256(o + sizeof(Cons) * (size_t)(M + 1));
     a.rcons = o; o = align256(o + sizeof(Cons) * (size_t)(M + 1));
     a.probs = o; o = align256(o + sizeof(float) * (size_t)(M + 1));
@@ -845,6 +1009,11 @@ static ArenaLayout arena_layout(const BeamParams &p, int M) {
 }
 
 size_t beam_arena_bytes(const BeamParams &p, int M) { return arena_layout(p, M).total; }
+
+// shared memory per warp besides its WS: the cursor's two PBWT rows and the
+// merge key of each haplotype path
+__host__ __device__ __forceinline__ size_t beam_rows_bytes(int K) { return ((2 * eimp_kw(K) * 4 + 15) / 16) * 16; }
+__host__ __device__ __forceinline__ size_t beam_canon_bytes(int NH) { return (((size_t)NH * 2 + 15) / 16) * 16; }
 
 __device__ __forceinline__ void setbit_(uint64_t *v, int i) { v[i >> 6] |= 1ull << (i & 63); }
 __device__ __forceinline__ void clrbit_(uint64_t *v, int i) { v[i >> 6] &= ~(1ull << (i & 63)); }
@@ -858,7 +1027,7 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS) beam_kernel(
     size_t arena_bytes, uint64_t *__restrict__ mats, uint64_t *__restrict__ pats, float *__restrict__ dmat,
     float *__restrict__ dpat, float *__restrict__ totalconf, int32_t *__restrict__ ncallsites,
     uint32_t *__restrict__ status) {
-    extern __shared__ uint8_t smem_raw[];
+    extern __shared__ __align__(16) uint8_t smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int t = blockIdx.x * BEAM_WARPS + wid;
     if (t >= ntgt) return;
@@ -876,27 +1045,32 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS) beam_kernel(
     const int S = nsplits[t];
     const int C = ncalls[t];
     const int K = p.K;
+    const size_t kw = eimp_kw(K);
+    if (lane == 0) {   // the warp's PBWT row pair and merge keys after the WS array
+        uint8_t *base = smem_raw + sizeof(WS) * BEAM_WARPS;
+        w.rowinc = reinterpret_cast<uint32_t *>(base + (size_t)wid * beam_rows_bytes(K));
+        w.rowref = w.rowinc + kw;
+        w.canon = reinterpret_cast<short *>(base + (size_t)BEAM_WARPS * beam_rows_bytes(K) +
+                                            (size_t)wid * beam_canon_bytes(al.NH));
+    }
     Ctx c;
     uint8_t *ab = arena + (size_t)t * arena_bytes;
     c.hp = reinterpret_cast<HPh *>(ab + al.hp);
     c.ph = reinterpret_cast<float *>(ab + al.ph);
     c.ivpool = reinterpret_cast<int2 *>(ab + al.ivpool);
     c.ivfree = reinterpret_cast<int *>(ab + al.ivfree);
-    c.bpbuf[0] = reinterpret_cast<BPh *>(ab + al.bp0);
-    c.bpbuf[1] = reinterpret_cast<BPh *>(ab + al.bp1);
     c.happ = reinterpret_cast<int *>(ab + al.happ);
     c.happ_old = reinterpret_cast<int *>(ab + al.happ_old);
     c.hapmap = reinterpret_cast<int2 *>(ab + al.hapmap);
     c.fstack = reinterpret_cast<int *>(ab + al.fstack);
     c.copies = reinterpret_cast<int *>(ab + al.copies);
-    c.NH = al.NH; c.BPC = al.BPC; c.HMAX = al.HMAX;
+    c.NH = al.NH; c.HMAX = al.HMAX;
     Cons *cons = reinterpret_cast<Cons *>(ab + al.cons);
     Cons *rcons = reinterpret_cast<Cons *>(ab + al.rcons);
     float *phaseProbs = reinterpret_cast<float *>(ab + al.probs);
     float *callConfs = reinterpret_cast<float *>(ab + al.confs);
     uint8_t *tg = ab + al.tg;
     const int64_t r0 = rowoff[t];
-    const size_t kw = eimp_kw(K);
     c.Mp = 2 * S + 1;
     c.rows = pbwt + (size_t)2 * r0 * kw;
     c.count0 = count0 + r0;
@@ -1094,7 +1268,7 @@ cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt,
                         float *totalconf, int32_t *ncallsites, uint32_t *status, cudaStream_t st) {
     ArenaLayout al = arena_layout(p, M);
     if (arena_bytes < al.total) return cudaErrorInvalidValue;
-    size_t sm = sizeof(WS) * BEAM_WARPS;
+    const size_t sm = (sizeof(WS) + beam_rows_bytes(p.K) + beam_canon_bytes(al.NH)) * BEAM_WARPS;
     cudaError_t e = cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     int blocks = (ntgt + BEAM_WARPS - 1) / BEAM_WARPS;
