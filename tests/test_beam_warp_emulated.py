@@ -1,0 +1,126 @@
+"""The beam phasing kernel (eimp_b200/csrc/beam.cu) run on the CPU under the
+host warp emulator (tests/warp_emu): every warp collective must be reached by
+all 32 lanes from the same call site, no access may leave its buffers
+(address and undefined-behaviour sanitizers), and the phased haplotypes,
+dosages and confidences must equal the golden fixtures made by the reference
+(beam 16) and the oracle restatement (beam 64 with pre-phasing, which runs
+the beam-path loops over more than one warp-width of paths)."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden_path
+
+CSRC = os.path.join(ROOT, "eimp_b200", "csrc")
+EMU = os.path.join(ROOT, "tests", "warp_emu")
+
+
+def split_rows(flat, counts):
+    out, o = [], 0
+    for c in counts:
+        out.append(flat[o:o + int(c)])
+        o += int(c)
+    return out
+
+
+@pytest.fixture(scope="module")
+def emu_exe(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    d = tmp_path_factory.mktemp("beam_emu")
+    shutil.copy(os.path.join(CSRC, "common.cuh"), d / "common.cuh")
+    kh = open(os.path.join(CSRC, "kernels.h")).read()
+    assert "#define BEAM_WARPS 4" in kh
+    # one warp per block: each warp's shared memory is its own allocation
+    (d / "kernels.h").write_text(kh.replace("#define BEAM_WARPS 4", "#define BEAM_WARPS 1"))
+    src = open(os.path.join(CSRC, "beam.cu")).read()
+    # the launcher (triple-chevron launch, runtime attributes) is device-only
+    i, j = src.index("cudaError_t launch_beam("), src.rindex("}  // namespace eimp")
+    src = src[:i] + src[j:]
+    decl = "extern __shared__ __align__(16) uint8_t smem_raw[];"
+    assert decl in src
+    src = src.replace(decl, "uint8_t *smem_raw = emu_smem_ptr;")
+    (d / "beam_emu.cpp").write_text('#include "emu.h"\n' + src)
+    exe = d / "beam_emu"
+    cmd = ["g++", "-std=c++20", "-O1", "-g", "-ffp-contract=off", "-fno-fast-math",
+           "-fsanitize=address,undefined", "-fno-sanitize-recover=undefined", "-I", EMU, "-I", str(d),
+           os.path.join(EMU, "beam_main.cpp"), "-o", str(exe), "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-4000:]
+    return str(exe)
+
+
+def write_inputs(d, gt, monos, splits, calls, cmd, pbwt, count0, rows, K, P, prephase):
+    nt, M = gt.shape
+    ns = np.array([len(s) for s in splits], np.int32)
+    nc = np.array([len(c) for c in calls], np.int32)
+    sp = np.zeros((nt, M), np.int32)
+    ca = np.zeros((nt, M), np.int32)
+    cm = np.zeros((nt, M + 1), np.float32)
+    for t in range(nt):
+        sp[t, :ns[t]] = splits[t]
+        ca[t, :nc[t]] = calls[t]
+        cm[t, :len(cmd[t])] = cmd[t]
+    rowoff = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
+    # history sizes of the reference defaults: HistorySize 100, HistorySizeFast 30, hist 1.0
+    pi = np.array([nt, M, K, 100, P, 24, 30, 64, 10, int(prephase), 1], np.int32)
+    pf = np.array([2.0, 0.003, 0.003, 0.5, 0.9, 0.99, 1.0], np.float32)
+    for name, a in [("params_i", pi), ("params_f", pf), ("gt", gt.astype(np.uint8)), ("monos", monos),
+                    ("splits", sp), ("nsplits", ns), ("calls", ca), ("ncalls", nc), ("cmd", cm),
+                    ("pbwt", pbwt.astype(np.uint32)), ("count0", count0.astype(np.int32)), ("rowoff", rowoff)]:
+        np.ascontiguousarray(a).tofile(os.path.join(d, name + ".bin"))
+
+
+def run_emu(exe, d, nt, M):
+    r = subprocess.run([exe, str(d)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    wM = ((M + 511) // 512) * 8
+    rd = lambda n, dt, shape: np.fromfile(os.path.join(d, n), dt).reshape(shape)
+    return (rd("o_mats.bin", np.uint64, (nt, wM)), rd("o_pats.bin", np.uint64, (nt, wM)),
+            rd("o_dm.bin", np.float32, (nt, M)), rd("o_dp.bin", np.float32, (nt, M)),
+            rd("o_tc.bin", np.float32, (nt,)), rd("o_nc.bin", np.int32, (nt,)), rd("o_st.bin", np.uint32, (nt,)))
+
+
+def golden_inputs(g, K):
+    pre = f"K{K}_"
+    ns = g[pre + "nsplits"]
+    return dict(gt=g["gt"], monos=g[pre + "monos"], splits=split_rows(g[pre + "splits"], ns),
+                calls=split_rows(g[pre + "calls"], g[pre + "ncalls"]),
+                cmd=split_rows(g[pre + "cmdiffs"], [s + 1 if s else 0 for s in ns]),
+                pbwt=g[pre + "pbwt"], count0=g[pre + "count0"], rows=g[pre + "rows"])
+
+
+def test_beam_emulated_matches_reference_golden(emu_exe, tmp_path):
+    g = np.load(golden_path("golden_tiny.npz"))
+    K = 64
+    write_inputs(tmp_path, K=K, P=16, prephase=False, **golden_inputs(g, K))
+    nt, M = g["gt"].shape
+    mats, pats, dm, dp, tc, nc, st = run_emu(emu_exe, tmp_path, nt, M)
+    assert not st.any()
+    np.testing.assert_array_equal(mats, g["K64_mat"])
+    np.testing.assert_array_equal(pats, g["K64_pat"])
+    np.testing.assert_array_equal(dm, g["K64_dos_mat"])
+    np.testing.assert_array_equal(dp, g["K64_dos_pat"])
+    np.testing.assert_array_equal(tc, g["K64_totalconf"])
+    np.testing.assert_array_equal(nc, g["K64_ncallsites"])
+
+
+def test_beam_emulated_wide_beam_prephasing_matches_oracle(emu_exe, tmp_path):
+    from oracle import restate as R
+    if not R.available():
+        pytest.skip("oracle library not built")
+    g = np.load(golden_path("golden_tiny.npz"))
+    K = 64
+    write_inputs(tmp_path, K=K, P=64, prephase=True, **golden_inputs(g, K))
+    nt, M = g["gt"].shape
+    mats, pats, dm, dp, tc, nc, st = run_emu(emu_exe, tmp_path, nt, M)
+    assert not st.any()
+    om, op, odm, odp = R.phase_many(g["gt"], g["hapmajor_typed"], g["sitemajor_typed"], g["cm_typed"],
+                                    R.params_c(K=K, beamwidth=64, doPrePhasing=True), 4)
+    np.testing.assert_array_equal(mats, om)
+    np.testing.assert_array_equal(pats, op)
+    np.testing.assert_array_equal(dm, odm)
+    np.testing.assert_array_equal(dp, odp)
