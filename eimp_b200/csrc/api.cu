@@ -34,6 +34,12 @@ struct DBuf {
 struct eimp_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // the imputation reference (transposed panel, segment map, reference
+    // PBWT) is built on a side stream, so that it overlaps whatever the main
+    // stream runs next (the phasing of the same batch); ref_ready marks its
+    // end and every use on the main stream waits for it
+    cudaStream_t side = nullptr;
+    cudaEvent_t ref_ready = nullptr, main_mark = nullptr;
     std::string err;
     uint64_t launches = 0;
     DBuf status;
@@ -117,7 +123,14 @@ int eimp_create(int device, eimp_ctx **out) {
     eimp_ctx *ctx = new eimp_ctx();
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ref_ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->main_mark, cudaEventDisableTiming) != cudaSuccess ||
         ctx->status.reserve(sizeof(uint32_t)) != cudaSuccess || cudaMemset(ctx->status.p, 0, sizeof(uint32_t)) != cudaSuccess) {
+        if (ctx->main_mark) cudaEventDestroy(ctx->main_mark);
+        if (ctx->ref_ready) cudaEventDestroy(ctx->ref_ready);
+        if (ctx->side) cudaStreamDestroy(ctx->side);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
         return EIMP_E_CUDA;
     }
@@ -128,9 +141,14 @@ int eimp_create(int device, eimp_ctx **out) {
 void eimp_destroy(eimp_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = ctx->stream, sd = ctx->side;
+    cudaEvent_t e1 = ctx->ref_ready, e2 = ctx->main_mark;
     delete ctx;
+    if (e1) cudaEventDestroy(e1);
+    if (e2) cudaEventDestroy(e2);
+    if (sd) cudaStreamDestroy(sd);
     if (s) cudaStreamDestroy(s);
 }
 
@@ -138,6 +156,7 @@ const char *eimp_last_error(const eimp_ctx *ctx) { return ctx ? ctx->err.c_str()
 
 int eimp_synchronize(eimp_ctx *ctx) {
     if (!ctx) return EIMP_E_ARG;
+    CK(cudaStreamSynchronize(ctx->side));
     CK(cudaStreamSynchronize(ctx->stream));
     return check_status(ctx);
 }
@@ -153,7 +172,11 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
                                const uint64_t *d_sitemajor_typed) {
     if (!ctx || !Mref || !nhaps || !M || M > Mref) return fail(ctx, EIMP_E_ARG, "eimp_imp_set_reference: bad sizes");
     if (int r = use_device(ctx)) return r;
-    cudaStream_t st = ctx->stream;
+    // after everything already queued on the main stream (earlier batches
+    // may still read the buffers rewritten here)
+    CK(cudaEventRecord(ctx->main_mark, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->side, ctx->main_mark, 0));
+    cudaStream_t st = ctx->side;
     const size_t wN = eimp_W(nhaps), wMref = eimp_W(Mref), kw = eimp_kw(nhaps);
     ctx->i_Mref = Mref; ctx->i_nhaps = nhaps; ctx->i_M = M;
     CK(ctx->i_hapfull.reserve(nhaps * wMref * 8));
@@ -172,6 +195,7 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
                          ctx->i_common.as<uint8_t>(), st));
     LAUNCH(launch_refpbwt(d_sitemajor_typed, (int)M, (int)nhaps, (int)wN, ctx->i_compr.as<uint32_t>(),
                           ctx->i_absperm.as<int32_t>(), ctx->i_count0.as<int32_t>(), st));
+    CK(cudaEventRecord(ctx->ref_ready, st));
     return 0;
 }
 
@@ -193,7 +217,7 @@ int eimp_imp_set_reference(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint6
     int r = eimp_imp_set_reference_dev(ctx, Mref, nhaps, full.as<uint64_t>(), af.as<float>(), M, ty.as<int64_t>(),
                                        st.as<uint64_t>());
     if (r) return r;
-    CK(cudaStreamSynchronize(ctx->stream));   // temporaries are freed on return
+    CK(cudaStreamSynchronize(ctx->side));   // temporaries are freed on return
     return 0;
 }
 
@@ -204,6 +228,7 @@ int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phase
     if (int r = use_device(ctx)) return r;
     const size_t M = ctx->i_M, wM = eimp_W(M), nh = 2 * ntargets;
     size_t cap = match_cap ? match_cap : M / 4 + 64;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
     ctx->i_ntargets = ntargets;
     ctx->i_imputeCalls = imputeCalls;
     ctx->i_cap = cap;
@@ -245,6 +270,7 @@ int eimp_imp_bunch_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t
     if (ldb_words < (nsites + 63) / 64 || ldd < nsites) return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch: leading dimension too small");
     if (int r = use_device(ctx)) return r;
     const size_t M = ctx->i_M;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
     LAUNCH(launch_dosage(ctx->i_matches.as<int4>(), (int)ctx->i_cap, ctx->i_nmatch.as<int>(),
                          ctx->i_absperm.as<int32_t>(), (int)ctx->i_nhaps, ctx->i_hapfull.as<uint64_t>(),
                          (int)eimp_W(ctx->i_Mref), ctx->i_segm.as<int32_t>(), ctx->i_common.as<uint8_t>(),
@@ -291,6 +317,7 @@ int eimp_imp_refpbwt(eimp_ctx *ctx, uint32_t *compr, int32_t *absperm) {
     if (!ctx || !ctx->i_Mref) return fail(ctx, EIMP_E_ARG, "eimp_imp_refpbwt: no reference set");
     if (int r = use_device(ctx)) return r;
     const size_t M = ctx->i_M, K = ctx->i_nhaps;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
     if (compr) CK(cudaMemcpyAsync(compr, ctx->i_compr.p, M * eimp_kw(K) * 4, cudaMemcpyDeviceToHost, ctx->stream));
     if (absperm) CK(cudaMemcpyAsync(absperm, ctx->i_absperm.p, (M + 1) * K * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));

@@ -255,79 +255,115 @@ __device__ __forceinline__ void hp_mark_required(HPh &h, const Cons &cn) {   // 
 
 // HaplotypePath::extend with updateScaling and calculateHaplotypeProbabilities
 // (HaplotypePath.cpp:162-479) against the cursor's two PBWT rows in shared
-// memory; returns extscaleexp
+// memory; returns extscaleexp.
+//
+// The history is walked in chunks of HXC steps: the chunk's intervals and
+// probabilities are loaded together (the next chunk's loads are in flight
+// while this one is computed) and the interval mappings of the chunk, pure
+// functions of the loaded intervals, are computed before the sequential part
+// that accumulates the probabilities, appends the extension intervals and
+// stops at the first step where both extensions are empty, in the reference's
+// order.
+constexpr int HXC = 8;
+
 __device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
     HPh &h = c.hp[slot];
     float *ph = ph_ptr(c, slot);
     const int pm = w.phsize - 1;
+    const int niv = h.niv, phstart = h.phstart;
+    const int calc0 = h.toext0, calc1 = h.toext1;
+    const int2 *iv = iv_buf(c, h.biv);
+    int2 *e0 = iv_buf(c, h.bext0);
+    int2 *e1 = iv_buf(c, h.bext1);
+    int ns = h.scaleexp;
     {   // updateScaling (:224-258)
-        int e = ilogb_exact(h.p);
-        int ns = h.scaleexp;
+        const int e = ilogb_exact(h.p);
         if (abs(e) >= 20) {
             ns += e;
-            double f = pow2i(-e);
-            for (int i = 0; i <= h.niv; i++) {
-                float *x = &ph[(i + h.phstart) & pm];
+            const double f = pow2i(-e);
+            for (int i = 0; i <= niv; i++) {
+                float *x = &ph[(i + phstart) & pm];
                 *x = (float)((double)*x * f);
             }
         }
         h.extscaleexp = ns;
     }
-    const int calc0 = h.toext0, calc1 = h.toext1;
-    const int2 *iv = iv_buf(c, h.biv);
-    int2 *e0 = iv_buf(c, h.bext0);
-    int2 *e1 = iv_buf(c, h.bext1);
-    const int lim = w.H < h.niv + 1 ? w.H : h.niv + 1;
+    const int lim = w.H < niv + 1 ? w.H : niv + 1;
     float p0 = 0.0f, p1 = 0.0f;
     int n0 = 0, n1 = 0;
+    int2 last0 = make_int2(0, -1), last1 = make_int2(0, -1);   // the last entries appended
     const int cnt0 = w.c0ref;
-    const float t0 = __fmul_rn(ph[h.phstart & pm], w.prec[0]);
+    const float t0 = __fmul_rn(ph[phstart & pm], w.prec[0]);
     if (cnt0 > 0) {
         if (calc0) p0 = __fmul_rn((float)cnt0, t0);
-        e0[n0++] = make_int2(0, cnt0 - 1);
+        last0 = make_int2(0, cnt0 - 1);
+        e0[n0++] = last0;
     }
     if (cnt0 < c.K) {
         if (calc1) p1 = __fmul_rn((float)(c.K - cnt0), t0);
-        e1[n1++] = make_int2(cnt0, c.K - 1);
+        last1 = make_int2(cnt0, c.K - 1);
+        e1[n1++] = last1;
     }
     const uint32_t *rinc = w.rowinc, *rref = w.rowref;
     const int cinc = w.c0inc;
     int2 prevfrom = make_int2(0, -1);
-    int2 from = lim > 1 ? iv[0] : make_int2(0, -1);
-    for (int i = 1; i < lim; i++) {
-        const int2 nextfrom = i + 1 < lim ? iv[i] : make_int2(0, -1);   // prefetch
-        const float ti = __fmul_rn(ph[(i + h.phstart) & pm], w.prec[i]);
-        int a0 = 0, b0 = -1, a1 = 0, b1 = -1;
-        if (i > 1 && prevfrom.x == from.x && prevfrom.y == from.y) {   // :395-399
-            if (n0 == i) { a0 = e0[n0 - 1].x; b0 = e0[n0 - 1].y; }
-            if (n1 == i) { a1 = e1[n1 - 1].x; b1 = e1[n1 - 1].y; }
-        } else {
-            int cl, cr, il, ir;
-            pbwt_map(rinc, cinc, from.x, from.y, cl, cr, il, ir);
-            pbwt_map(rref, cnt0, cl, cr, a0, b0, a1, b1);
+    int2 fr[HXC], nfr[HXC];
+    float tph[HXC], ntph[HXC];
+#pragma unroll
+    for (int j = 0; j < HXC; j++)
+        if (1 + j < lim) { fr[j] = iv[j]; tph[j] = ph[(1 + j + phstart) & pm]; }
+    bool stop = false;
+    for (int base = 1; base < lim && !stop; base += HXC) {
+        const int nb = base + HXC;
+#pragma unroll
+        for (int j = 0; j < HXC; j++)   // the next chunk's loads
+            if (nb + j < lim) { nfr[j] = iv[nb + j - 1]; ntph[j] = ph[(nb + j + phstart) & pm]; }
+        int A0[HXC], B0[HXC], A1[HXC], B1[HXC];
+#pragma unroll
+        for (int j = 0; j < HXC; j++) {
+            A0[j] = 0; B0[j] = -1; A1[j] = 0; B1[j] = -1;
+            if (base + j < lim) {
+                int cl, cr, il, ir;
+                pbwt_map(rinc, cinc, fr[j].x, fr[j].y, cl, cr, il, ir);
+                pbwt_map(rref, cnt0, cl, cr, A0[j], B0[j], A1[j], B1[j]);
+            }
         }
-        prevfrom = from;
-        bool any = false;
-        if (a0 <= b0) {
-            if (calc0) p0 = __fadd_rn(p0, __fmul_rn((float)(b0 - a0 + 1), ti));
-            e0[n0++] = make_int2(a0, b0);
-            any = true;
+#pragma unroll
+        for (int j = 0; j < HXC; j++) {
+            const int i = base + j;
+            if (stop || i >= lim) break;
+            const int2 from = fr[j];
+            int a0 = A0[j], b0 = B0[j], a1 = A1[j], b1 = B1[j];
+            if (i > 1 && prevfrom.x == from.x && prevfrom.y == from.y) {   // :395-399
+                a0 = 0; b0 = -1; a1 = 0; b1 = -1;
+                if (n0 == i) { a0 = last0.x; b0 = last0.y; }
+                if (n1 == i) { a1 = last1.x; b1 = last1.y; }
+            }
+            prevfrom = from;
+            const float ti = __fmul_rn(tph[j], w.prec[i]);
+            bool any = false;
+            if (a0 <= b0) {
+                if (calc0) p0 = __fadd_rn(p0, __fmul_rn((float)(b0 - a0 + 1), ti));
+                last0 = make_int2(a0, b0);
+                e0[n0++] = last0;
+                any = true;
+            }
+            if (a1 <= b1) {
+                if (calc1) p1 = __fadd_rn(p1, __fmul_rn((float)(b1 - a1 + 1), ti));
+                last1 = make_int2(a1, b1);
+                e1[n1++] = last1;
+                any = true;
+            }
+            if (!any) stop = true;
         }
-        if (a1 <= b1) {
-            if (calc1) p1 = __fadd_rn(p1, __fmul_rn((float)(b1 - a1 + 1), ti));
-            e1[n1++] = make_int2(a1, b1);
-            any = true;
-        }
-        if (!any) break;
-        from = nextfrom;
+#pragma unroll
+        for (int j = 0; j < HXC; j++) { fr[j] = nfr[j]; tph[j] = ntph[j]; }
     }
     h.next0 = n0; h.next1 = n1;
     h.extp0 = p0; h.extp1 = p1;
-    h.active0 = h.toext0; h.active1 = h.toext1;
-    return h.extscaleexp;
+    h.active0 = calc0; h.active1 = calc1;
+    return ns;
 }
-
-
 
 // HaplotypePath::applyExtension (HaplotypePath.cpp:77-103)
 __device__ void hp_apply(const Ctx &c, const WS &w, int slot, int e) {
@@ -512,21 +548,95 @@ __device__ void beam_init(const Ctx &c, WS &w, const Cons *constr, int reverse, 
     __syncwarp();
 }
 
-// Beam::prunePaths (Beam.cpp:577-787), the filter and the min-max heap: lane
-// 0 over the beam in shared memory.  The reference counts of the haplotype
-// paths are decremented afterwards by the lanes (nothing in the heap pass
-// reads them).  Returns 0 when no extension survives.
+__device__ __forceinline__ float warp_minf(float v) {
+    for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_maxf(float v) {
+    for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_mini(int v) {
+    for (int o = 16; o; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_maxi(int v) {
+    for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_sumi(int v) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Beam::prunePaths (Beam.cpp:577-787), the filter and the min-max heap.  The
+// candidates are, per beam path in list order, the extension indices from
+// the active index down to 0 (unconstrained) or the active index alone.
+//
+// When at most P candidates reach the limit the heap never evicts: exactly
+// the candidates below the limit are deleted, and the heap's minimum and
+// maximum are a candidate with the smallest and one with the largest key.
+// The lanes then decide everything with warp reductions, provided all
+// candidates tied at the smallest key give the same weightScaleExp and all
+// tied at the largest the same deleteErr (else which tied element the heap
+// holds at its root would matter).  Otherwise lane 0 runs the heap over the
+// beam in shared memory in the reference's order.  The reference counts of the
+// haplotype paths are decremented afterwards by the lanes (nothing in the
+// selection reads them).  Returns 0 when no extension survives.
 __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn) {
     const int lane = lane_id();
     BPh *bp = w.bp[w.bpsel];
-    for (int it = lane; it < w.nbp; it += 32) w.delmask[it] = 0;
+    const int nbp = w.nbp;
+    const float limit = __fmul_rn(c.pLimit, maxP);
+    const bool allext = cn.type == C_NONE;
+    for (int it = lane; it < nbp; it += 32) w.delmask[it] = 0;
+    // read-only pass: candidates at or above the limit and their extreme keys
+    int nA = 0;
+    float kmin = __int_as_float(0x7f800000), kmax = -__int_as_float(0x7f800000);
+    for (int it = lane; it < nbp; it += 32) {
+        const BPh &b = bp[it];
+        for (int ex = b.actidx; ex >= 0; ex = allext ? ex - 1 : -1) {
+            const float p = b.extp[ex];
+            if (p >= limit) { nA++; kmin = fminf(kmin, p); kmax = fmaxf(kmax, p); }
+        }
+    }
+    nA = warp_sumi(nA);
+    kmin = warp_minf(kmin);
+    kmax = warp_maxf(kmax);
+    bool fast = nA <= w.P;
+    int wse = 0, delerr = 0;
+    if (fast && nA > 0) {
+        int lo0 = INT_MAX, hi0 = INT_MIN, lo1 = 1, hi1 = 0;
+        for (int it = lane; it < nbp; it += 32) {
+            const BPh &b = bp[it];
+            for (int ex = b.actidx; ex >= 0; ex = allext ? ex - 1 : -1) {
+                const float p = b.extp[ex];
+                if (!(p >= limit)) continue;
+                if (p == kmin) { const int e = -ilogb_exact(b.weight); lo0 = min(lo0, e); hi0 = max(hi0, e); }
+                if (p == kmax) { const int f = b.nErr > 0; lo1 = min(lo1, f); hi1 = max(hi1, f); }
+            }
+        }
+        lo0 = warp_mini(lo0); hi0 = warp_maxi(hi0);
+        lo1 = warp_mini(lo1); hi1 = warp_maxi(hi1);
+        fast = lo0 == hi0 && lo1 == hi1;
+        wse = lo0;
+        delerr = lo1;
+    }
     __syncwarp();
-    if (lane == 0) {
-        const float limit = __fmul_rn(c.pLimit, maxP);
+    if (fast) {
+        for (int it = lane; it < nbp; it += 32) {
+            BPh &b = bp[it];
+            unsigned dm = 0;
+            for (int ex = b.actidx; ex >= 0; ex = allext ? ex - 1 : -1)
+                if (!(b.extp[ex] >= limit)) { b.active[ex] = 0; dm |= 1u << ex; }
+            if (dm) { bp_update_actidx(b); w.delmask[it] = (unsigned char)dm; }
+        }
+        if (lane == 0) { w.ires = nA; w.wse = wse; w.delerr = delerr; }
+    } else if (lane == 0) {
         Hel *hq = w.heap;
         const int P = w.P;
         int n = 0;
-        for (int it = 0; it < w.nbp; it++) {
+        for (int it = 0; it < nbp; it++) {
             BPh &b = bp[it];
             int ex = b.actidx;
             while (ex >= 0) {
@@ -540,7 +650,7 @@ __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn
                         heap_push(hq, n, p, it, ex);
                     } else bp_mark_deleted_deferred(w, b, it, ex);
                 } else bp_mark_deleted_deferred(w, b, it, ex);
-                ex = cn.type == C_NONE ? ex - 1 : -1;
+                ex = allext ? ex - 1 : -1;
             }
         }
         w.ires = n;
@@ -551,7 +661,7 @@ __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn
     }
     __syncwarp();
     const int n = w.ires;
-    for (int it = lane; it < w.nbp; it += 32) {
+    for (int it = lane; it < nbp; it += 32) {
         const unsigned dm = w.delmask[it];
         if (!dm) continue;
         HPh &pm = c.hp[c.happ[bp[it].mat]];

@@ -142,7 +142,10 @@ int eimp_phase_targets(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, c
  * VCFData.h:211), its allele frequencies (Mref floats), the typed sites (M
  * ascending indices into the full reference, VCFData::indexToRefFull) and the
  * typed reference in site-major layout (M x W(nhaps) words).  Builds the
- * reference PBWT with its prefix arrays on the device. */
+ * reference PBWT with its prefix arrays on the device.  The build runs on a
+ * second stream of the context, after the work already queued on the main
+ * stream and concurrently with what is queued there next (e.g. the phasing of
+ * the same batch); the calls that read the reference wait for it. */
 int eimp_imp_set_reference(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint64_t *sitemajor_full,
                            const float *af_full, size_t M, const int64_t *typed, const uint64_t *sitemajor_typed);
 

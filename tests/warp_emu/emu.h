@@ -116,6 +116,7 @@ inline int __clzll(long long x) { return x ? __builtin_clzll((unsigned long long
 inline int __ffs(int x) { return __builtin_ffs(x); }
 inline unsigned __float_as_uint(float f) { unsigned u; std::memcpy(&u, &f, 4); return u; }
 inline float __uint_as_float(unsigned u) { float f; std::memcpy(&f, &u, 4); return f; }
+inline float __int_as_float(int u) { float f; std::memcpy(&f, &u, 4); return f; }
 // IEEE round-to-nearest, one operation each (built with -ffp-contract=off)
 inline float __fadd_rn(float a, float b) { volatile float r = a + b; return r; }
 inline float __fmul_rn(float a, float b) { volatile float r = a * b; return r; }
