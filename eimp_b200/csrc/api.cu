@@ -46,7 +46,7 @@ struct eimp_ctx {
 
     // GPUEngine drop-in
     size_t g_K = 0, g_Kwords = 0, g_M = 0, g_Ncorr = 0, g_NAD = 0, g_refTcap = 0;
-    DBuf g_refT, g_gt, g_splits, g_nsplits, g_bh, g_rowoff, g_cref, g_count0, g_pbwt;
+    DBuf g_refT, g_hapT, g_gt, g_splits, g_nsplits, g_bh, g_rowoff, g_cref, g_count0, g_pbwt;
 
     // phasing reference
     size_t p_M = 0, p_nhaps = 0;
@@ -386,9 +386,9 @@ int run_cref_pbwt(eimp_ctx *ctx, size_t K, size_t ntgt, const uint8_t *d_gt, std
     CK(ctx->b_count0.reserve(rows * 4));
     CK(ctx->b_pbwt.reserve(2 * rows * kw * 4));
     CK(cudaMemcpyAsync(ctx->b_rowoff.p, rowoff.data(), (ntgt + 1) * 8, cudaMemcpyHostToDevice, st));
-    LAUNCH(launch_cref(d_gt, (int)ntgt, (int)M, ctx->p_sitemajor.as<uint64_t>(), (int)nh, (int)wN,
+    LAUNCH(launch_cref(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)eimp_W(M), (int)nh,
                        ctx->b_bh.as<int32_t>(), (int)K, ctx->b_splits.as<int32_t>(), ctx->b_nsplits.as<int32_t>(),
-                       ctx->b_rowoff.as<int64_t>(), ctx->b_cref.as<uint64_t>(), ctx->b_count0.as<int32_t>(), st));
+                       ctx->b_rowoff.as<int64_t>(), ctx->b_cref.as<uint64_t>(), st));
     LAUNCH(launch_pbwt(ctx->b_cref.as<uint64_t>(), ctx->b_count0.as<int32_t>(), ctx->b_rowoff.as<int64_t>(),
                        (int)ntgt, (int)K, ctx->b_pbwt.as<uint32_t>(), kw, 0, st));
     return 0;
@@ -546,6 +546,12 @@ int eimp_gpu_initialize(eimp_ctx *ctx, size_t K, size_t Kwords, size_t M, size_t
     ctx->g_refTcap = refTCapacity;
     CK(ctx->g_refT.reserve(M * refTCapacity));
     CK(cudaMemcpyAsync(ctx->g_refT.p, refTData, M * refTCapacity, cudaMemcpyHostToDevice, ctx->stream));
+    // haplotype-major copy for the condensed-reference kernel
+    const size_t wM = eimp_W(M);
+    CK(ctx->g_hapT.reserve(NrefhapsAD * wM * 8));
+    CK(cudaMemsetAsync(ctx->g_hapT.p, 0, NrefhapsAD * wM * 8, ctx->stream));
+    LAUNCH(launch_transpose(ctx->g_refT.as<uint64_t>(), M, refTCapacity / 8, ctx->g_hapT.as<uint64_t>(), NrefhapsAD,
+                            wM, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return 0;
 }
@@ -622,9 +628,9 @@ extern "C" int eimp_gpu_run_cref_pbwt(eimp_ctx *ctx, size_t ntgt, const uint64_t
     CK(ctx->g_count0.reserve(rows * 4));
     CK(ctx->g_pbwt.reserve(2 * rows * stride * 4));
     CK(cudaMemcpyAsync(ctx->g_rowoff.p, ro.data(), (ntgt + 1) * 8, cudaMemcpyHostToDevice, st));
-    LAUNCH(launch_cref(ctx->g_gt.as<uint8_t>(), (int)ntgt, (int)M, ctx->g_refT.as<uint64_t>(), (int)nh, (int)wN,
+    LAUNCH(launch_cref(ctx->g_gt.as<uint8_t>(), (int)ntgt, (int)M, ctx->g_hapT.as<uint64_t>(), (int)wM, (int)nh,
                        ctx->g_bh.as<int32_t>(), (int)K, ctx->g_splits.as<int32_t>(), ctx->g_nsplits.as<int32_t>(),
-                       ctx->g_rowoff.as<int64_t>(), ctx->g_cref.as<uint64_t>(), ctx->g_count0.as<int32_t>(), st));
+                       ctx->g_rowoff.as<int64_t>(), ctx->g_cref.as<uint64_t>(), st));
     LAUNCH(launch_pbwt(ctx->g_cref.as<uint64_t>(), ctx->g_count0.as<int32_t>(), ctx->g_rowoff.as<int64_t>(), (int)ntgt,
                        (int)K, ctx->g_pbwt.as<uint32_t>(), stride, 1, st));
     for (size_t t = 0; t < ntgt; t++) {

@@ -37,10 +37,12 @@ cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_
                                const int32_t *besthaps, int K, const float *cm, float cMmaxsplit, uint64_t *monos,
                                int32_t *splits, int32_t *calls, float *cmdiffs, int32_t *nsplits, int32_t *ncalls,
                                cudaStream_t st);
-cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *sitemajor, int nhaps, int wN,
+// condensed reference from the haplotype-major reference (nhaps x wM words)
+cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM, int nhaps,
                         const int32_t *besthaps, int K, const int32_t *splits, const int32_t *nsplits,
-                        const int64_t *rowoff, uint64_t *cref, int32_t *count0, cudaStream_t st);
-cudaError_t launch_pbwt(const uint64_t *cref, const int32_t *count0, const int64_t *rowoff, int ntgt, int K,
+                        const int64_t *rowoff, uint64_t *cref, cudaStream_t st);
+// forward and backward PBWT of the condensed references; writes count0 too
+cudaError_t launch_pbwt(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
                         uint32_t *pbwt, size_t rowstride, int emit_padded, cudaStream_t st);
 
 // ---- beam phasing (beam.cu)

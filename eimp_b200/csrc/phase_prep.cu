@@ -5,7 +5,8 @@
 //                        (Datatypes.cpp:107-116); exact K-smallest selection
 //                        by (errors, index) via a threshold search.
 //  monos_calls_kernel -- Target::findMonos + findCallLocs (Target.cpp:878-950)
-//  cref_kernel        -- Target::condensedReferenceT (Target.cpp:953-1059)
+//  cref_kernel        -- Target::condensedReferenceT (Target.cpp:953-1059),
+//                        one lane per selected haplotype (haplotype-major).
 //  pbwt_kernel        -- PBWT::buildComprPBWT (PBWT.cpp:207-285), forward and
 //                        backward, one CTA per (target, direction).
 #include "common.cuh"
@@ -211,198 +212,192 @@ cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_
 }
 
 // ---------------------------------------------------------------------------
-// compact a full-width row (smem) to the K best haps -> dst (wK words)
-__device__ int compact_row(const uint64_t *src, int nhaps, const int32_t *bh, int K, int wK, uint64_t *dst,
-                           int *buf) {
-    int cnt1 = 0;
-    if (K == nhaps) {
-        int nopad = (nhaps + 63) / 64;
-        for (int w = threadIdx.x; w < wK; w += blockDim.x) {
-            uint64_t x = 0;
-            if (w < nopad) {
-                x = src[w];
-                if (w == nopad - 1 && (nhaps & 63)) x &= (1ull << (nhaps & 63)) - 1;
-            }
-            dst[w] = x;
-            cnt1 += __popcll(x);
-        }
-    } else {
-        for (int w = threadIdx.x; w < wK; w += blockDim.x) {
-            uint64_t x = 0;
-            int k0 = w * 64;
-            int kn = min(64, K - k0);
-            for (int b = 0; b < kn; b++) {
-                int h = bh[k0 + b];
-                x |= ((src[h >> 6] >> (h & 63)) & 1ull) << b;
-            }
-            dst[w] = x;
-            cnt1 += __popcll(x);
-        }
-    }
-    return K - block_sum_int(cnt1, buf);
-}
+// Target::condensedReferenceT (Target.cpp:953-1059): the condensed reference of
+// a target has 2S+1 rows of K bits, one column per selected reference
+// haplotype (in besthaps order; identity when K == nhaps, Target.cpp:969-974).
+// Row 2j holds the inconsistency of each haplotype over the sites between
+// split j-1 and split j (a homozygous target genotype the haplotype does not
+// carry), row 2j+1 the haplotype's allele at split site j, row 2S the
+// inconsistency after the last split.
+//
+// Haplotype-major: lane = column.  A lane walks its haplotype's row of the
+// haplotype-major reference once (each segment is an OR over a short word
+// range), the warp's ballot is the 32-bit word of the output row.  Grid:
+// (target, 8 output words of 32 columns per CTA); the columns past K are
+// written as zero padding up to W(K) words.
+// ---------------------------------------------------------------------------
+constexpr int CREF_WARPS = 8;
 
-__global__ void __launch_bounds__(256) cref_kernel(const uint8_t *__restrict__ gt, int M,
-                                                  const uint64_t *__restrict__ sitemajor, int nhaps, int wN,
-                                                  const int32_t *__restrict__ besthaps, int K,
-                                                  const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits,
-                                                  const int64_t *__restrict__ rowoff, uint64_t *__restrict__ cref,
-                                                  int32_t *__restrict__ count0) {
+__global__ void __launch_bounds__(32 * CREF_WARPS) cref_kernel(
+    const uint8_t *__restrict__ gt, int M, const uint64_t *__restrict__ hapmajor, int wM, int nhaps,
+    const int32_t *__restrict__ besthaps, int K, const int32_t *__restrict__ splits,
+    const int32_t *__restrict__ nsplits, const int64_t *__restrict__ rowoff, uint64_t *__restrict__ cref) {
     extern __shared__ uint64_t sm[];
-    uint64_t *incon = sm, *srow = sm + wN;
-    __shared__ int buf[32];
-    const int t = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
-    const int S = nsplits[t];
-    const int wK = (int)eimp_W(K);
+    uint64_t *is0 = sm, *is2 = sm + wM;   // the target's homozygous genotypes as bit masks
+    const int t = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint8_t *g = gt + (size_t)t * M;
-    const int32_t *bh = besthaps + (size_t)t * K;
-    const int32_t *sp = splits + (size_t)t * M;
-    uint64_t *out = cref + (size_t)rowoff[t] * wK;
-    int32_t *c0 = count0 + rowoff[t];
-    const int nopad = (nhaps + 63) / 64;
-    for (int w = tid; w < wN; w += nt) incon[w] = 0ull;
-    __syncthreads();
-    int si = 0;
-    int next = S > 0 ? sp[0] : -1;
-    int row = 0;
-    for (int m = 0; m < M; m++) {
-        const uint64_t *r = sitemajor + (size_t)m * wN;
-        if (m == next) {
-            __syncthreads();
-            int z = compact_row(incon, nhaps, bh, K, wK, out + (size_t)row * wK, buf);
-            if (tid == 0) c0[row] = z;
-            row++;
-            for (int w = tid; w < wN; w += nt) { incon[w] = 0ull; srow[w] = r[w]; }
-            __syncthreads();
-            z = compact_row(srow, nhaps, bh, K, wK, out + (size_t)row * wK, buf);
-            if (tid == 0) c0[row] = z;
-            row++;
-            si++;
-            next = si < S ? sp[si] : -1;
-        } else {
-            uint8_t c = g[m];
-            if (c == 0) for (int w = tid; w < nopad; w += nt) incon[w] |= r[w];
-            else if (c == 2) for (int w = tid; w < nopad; w += nt) incon[w] |= ~r[w];
+    for (int w = tid; w < wM; w += blockDim.x) {
+        uint64_t a = 0, b = 0;
+        const int m0 = w * 64;
+        for (int j = 0; j < 64 && m0 + j < M; j++) {
+            const uint8_t c = g[m0 + j];
+            a |= (uint64_t)(c == 0) << j;
+            b |= (uint64_t)(c == 2) << j;
         }
+        is0[w] = a; is2[w] = b;
     }
     __syncthreads();
-    int z = compact_row(incon, nhaps, bh, K, wK, out + (size_t)row * wK, buf);
-    if (tid == 0) c0[row] = z;
+    const int wK = (int)eimp_W(K);
+    const int col32 = blockIdx.y * CREF_WARPS + warp;   // 32-bit word of the output rows
+    if (col32 >= 2 * wK) return;
+    const int k = col32 * 32 + lane;
+    const bool valid = k < K;
+    const int h = valid ? (K == nhaps ? k : besthaps[(size_t)t * K + k]) : 0;
+    const uint64_t *hm = hapmajor + (size_t)h * wM;
+    const size_t rstride = 2 * (size_t)wK;   // 32-bit words per row
+    uint32_t *out = reinterpret_cast<uint32_t *>(cref + (size_t)rowoff[t] * wK) + col32;
+    const int S = nsplits[t];
+    const int32_t *sp = splits + (size_t)t * M;
+    int lo = 0;
+    for (int j = 0; j <= S; j++) {
+        const int hi = j < S ? sp[j] : M;   // segment [lo, hi)
+        bool inc = false;
+        if (valid && lo < hi) {
+            const int q0 = lo >> 6, q1 = (hi - 1) >> 6;
+            for (int q = q0; q <= q1; q++) {
+                const uint64_t x = hm[q];
+                uint64_t mask = ~0ull;
+                if (q == q0) mask &= ~0ull << (lo & 63);
+                if (q == q1) mask &= ~0ull >> (63 - ((hi - 1) & 63));
+                if (((x & is0[q]) | (~x & is2[q])) & mask) { inc = true; break; }
+            }
+        }
+        const unsigned wi = __ballot_sync(0xffffffffu, inc);
+        if (lane == 0) out[(size_t)(2 * j) * rstride] = wi;
+        if (j < S) {
+            const int m = hi;
+            const bool a = valid && ((hm[m >> 6] >> (m & 63)) & 1ull);
+            const unsigned ws = __ballot_sync(0xffffffffu, a);
+            if (lane == 0) out[(size_t)(2 * j + 1) * rstride] = ws;
+            lo = m + 1;
+        }
+    }
 }
 
-cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *sitemajor, int nhaps, int wN,
+cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM, int nhaps,
                         const int32_t *besthaps, int K, const int32_t *splits, const int32_t *nsplits,
-                        const int64_t *rowoff, uint64_t *cref, int32_t *count0, cudaStream_t st) {
-    size_t sm = (size_t)2 * wN * sizeof(uint64_t);
+                        const int64_t *rowoff, uint64_t *cref, cudaStream_t st) {
+    const size_t sm = (size_t)2 * wM * sizeof(uint64_t);
     if (sm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(cref_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
-    cref_kernel<<<ntgt, 256, sm, st>>>(gt, M, sitemajor, nhaps, wN, besthaps, K, splits, nsplits, rowoff, cref,
-                                       count0);
+    const int wK = (int)eimp_W(K);
+    dim3 grid((unsigned)ntgt, (unsigned)((2 * wK + CREF_WARPS - 1) / CREF_WARPS));
+    cref_kernel<<<grid, 32 * CREF_WARPS, sm, st>>>(gt, M, hapmajor, wM, nhaps, besthaps, K, splits, nsplits, rowoff,
+                                                   cref);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-__device__ void block_exscan_small(int *a, int n, int *warpbuf, int *total) {
-    // n <= a few thousand: chunked per-thread sums, then a warp-level scan
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int per = (n + nt - 1) / nt;
-    const int lo = tid * per, hi = min(n, lo + per);
-    int s = 0;
-    for (int i = lo; i < hi; i++) s += a[i];
-    int lane = tid & 31, wid = tid >> 5;
-    int v = s;
-    for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += t;
-    }
-    if (lane == 31) warpbuf[wid] = v;
-    __syncthreads();
-    if (wid == 0) {
-        int nw = (nt + 31) >> 5;
-        int w = lane < nw ? warpbuf[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += t;
-        }
-        if (lane < nw) warpbuf[lane] = w;
-    }
-    __syncthreads();
-    int excl = v - s + (wid ? warpbuf[wid - 1] : 0);
-    for (int i = lo; i < hi; i++) { int t = a[i]; a[i] = excl; excl += t; }
-    if (total && tid == nt - 1) *total = excl;
-    __syncthreads();
-}
+// PBWT::buildComprPBWT (PBWT.cpp:207-285) of each target's condensed
+// reference, forward and backward (rows in sweep order), one CTA per (target,
+// direction).  Per row: every warp reads the row bits of its 32-haplotype
+// blocks in the current prefix order (one ballot = one data word) and scans
+// its blocks' zero counts; after one barrier each warp places its haplotypes
+// in the next prefix order (zeros first, stable) and writes the compressed
+// words [data, zeros through the word].  The next row is copied into shared
+// memory asynchronously while the current one is processed.  The forward CTA
+// also writes each row's zero count.
+// ---------------------------------------------------------------------------
+constexpr int PBWT_WARPS = 8;
 
-__global__ void __launch_bounds__(512) pbwt_kernel(const uint64_t *__restrict__ cref, const int64_t *__restrict__ rowoff,
-                                                  int K, uint32_t *__restrict__ pbwt, size_t rowstride,
-                                                  int emit_padded) {
-    extern __shared__ uint8_t smem[];
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__global__ void __launch_bounds__(32 * PBWT_WARPS) pbwt_kernel(const uint64_t *__restrict__ cref,
+                                                               const int64_t *__restrict__ rowoff, int K,
+                                                               uint32_t *__restrict__ pbwt, size_t rowstride,
+                                                               int emit_padded, int32_t *__restrict__ count0) {
+    extern __shared__ __align__(16) uint8_t smem[];
     const int t = blockIdx.x >> 1, dir = blockIdx.x & 1;
     const int wK = (int)eimp_W(K);
     const int nwords = (K + 31) / 32;
-    int32_t *perm = reinterpret_cast<int32_t *>(smem);
-    int32_t *nperm = perm + K;
-    uint32_t *row = reinterpret_cast<uint32_t *>(nperm + K);   // 2*wK
-    uint32_t *data = row + 2 * wK;                              // nwords
-    int *pz = reinterpret_cast<int *>(data + nwords);           // nwords
-    int *warpbuf = pz + nwords;                                 // 32
-    int *tot = warpbuf + 32;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
+    uint64_t *rowbuf = reinterpret_cast<uint64_t *>(smem);                // 2 x wK
+    int32_t *perm = reinterpret_cast<int32_t *>(rowbuf + 2 * wK);         // K
+    int32_t *nperm = perm + K;                                            // K
+    uint32_t *data = reinterpret_cast<uint32_t *>(nperm + K);             // nwords
+    int *wtot = reinterpret_cast<int *>(data + nwords);                   // PBWT_WARPS
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t r0 = rowoff[t];
     const int Mp = (int)(rowoff[t + 1] - r0);
     const uint64_t *rows = cref + (size_t)r0 * wK;
     uint32_t *out = pbwt + (size_t)(2 * r0 + (dir ? Mp : 0)) * rowstride;
+    const int per = (nwords + PBWT_WARPS - 1) / PBWT_WARPS;   // words of a warp
+    const int w0 = warp * per, w1 = min(nwords, w0 + per);
+    const unsigned lt = (1u << lane) - 1u;
+    const int nchunk = wK / 2;                                 // 16-byte pieces of a row
     for (int i = tid; i < K; i += blockDim.x) perm[i] = i;
-    __syncthreads();
+    if (Mp > 0) {
+        const uint64_t *src = rows + (size_t)(dir ? Mp - 1 : 0) * wK;
+        for (int c = tid; c < nchunk; c += blockDim.x) cp_async16(rowbuf + 2 * c, src + 2 * c);
+    }
+    cp_async_commit();
     for (int midx = 0; midx < Mp; midx++) {
         const int m = dir ? Mp - 1 - midx : midx;
-        const uint64_t *src = rows + (size_t)m * wK;
-        for (int w = tid; w < wK; w += blockDim.x) {
-            uint64_t x = src[w];
-            row[2 * w] = (uint32_t)x;
-            row[2 * w + 1] = (uint32_t)(x >> 32);
+        const uint64_t *row = rowbuf + (midx & 1) * wK;
+        cp_async_wait_all();
+        __syncthreads();   // this row has landed; the previous row's placements are done
+        if (midx + 1 < Mp) {
+            const uint64_t *src = rows + (size_t)(dir ? m - 1 : m + 1) * wK;
+            uint64_t *dst = rowbuf + ((midx + 1) & 1) * wK;
+            for (int c = tid; c < nchunk; c += blockDim.x) cp_async16(dst + 2 * c, src + 2 * c);
         }
-        __syncthreads();
-        for (int w = wid; w < nwords; w += nwarps) {
-            int i = w * 32 + lane;
-            int bit = 1;
-            if (i < K) { int h = perm[i]; bit = (row[h >> 5] >> (h & 31)) & 1; }
-            uint32_t b = __ballot_sync(0xffffffffu, bit);
-            if (lane == 0) { data[w] = b; pz[w] = __popc(~b); }
+        cp_async_commit();
+        // data words in the current prefix order, zeros per warp
+        int z = 0;
+        for (int w = w0; w < w1; w++) {
+            const int i = w * 32 + lane;
+            int bit = 1;   // tail padded with ones (PBWT.cpp:261-267)
+            if (i < K) { const int h = perm[i]; bit = (int)((row[h >> 6] >> (h & 63)) & 1ull); }
+            const unsigned b = __ballot_sync(0xffffffffu, bit);
+            if (lane == 0) data[w] = b;
+            z += __popc(~b);
         }
+        if (lane == 0) wtot[warp] = z;
         __syncthreads();
-        block_exscan_small(pz, nwords, warpbuf, tot);
-        const int cnt0 = *tot;
+        int zb = 0, cnt0 = 0;
+        for (int q = 0; q < PBWT_WARPS; q++) { const int v = wtot[q]; cnt0 += v; if (q < warp) zb += v; }
         uint32_t *o = out + (size_t)midx * rowstride;
-        for (int w = wid; w < nwords; w += nwarps) {
-            int i = w * 32 + lane;
-            uint32_t b = data[w];
-            int zb = pz[w];
+        for (int w = w0; w < w1; w++) {
+            const unsigned b = data[w];
+            const int i = w * 32 + lane;
             if (i < K) {
-                int h = perm[i];
-                uint32_t lt = (1u << lane) - 1u;
-                int dst = ((b >> lane) & 1) ? cnt0 + (w * 32 - zb) + __popc(b & lt) : zb + __popc(~b & lt);
-                nperm[dst] = h;
+                const int zi = zb + __popc(~b & lt);   // zeros before position i
+                nperm[((b >> lane) & 1u) ? cnt0 + (i - zi) : zi] = perm[i];
             }
-            if (lane == 0) { o[2 * w] = b; o[2 * w + 1] = (uint32_t)(zb + __popc(~b)); }
+            zb += __popc(~b);
+            if (lane == 0) { o[2 * w] = b; o[2 * w + 1] = (uint32_t)zb; }
         }
         if (emit_padded)
             for (size_t j = 2 * (size_t)nwords + tid; j < rowstride; j += blockDim.x) o[j] = 0u;
-        __syncthreads();
+        if (dir == 0 && tid == 0) count0[r0 + m] = cnt0;
         int32_t *tp = perm; perm = nperm; nperm = tp;
     }
+    cp_async_wait_all();
 }
 
-cudaError_t launch_pbwt(const uint64_t *cref, const int32_t *count0, const int64_t *rowoff, int ntgt, int K,
+cudaError_t launch_pbwt(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
                         uint32_t *pbwt, size_t rowstride, int emit_padded, cudaStream_t st) {
-    (void)count0;
     const int wK = (int)eimp_W(K), nwords = (K + 31) / 32;
-    size_t sm = (size_t)2 * K * 4 + (size_t)2 * wK * 4 + (size_t)nwords * 4 * 2 + 33 * 4;
+    const size_t sm = (size_t)2 * wK * 8 + (size_t)2 * K * 4 + (size_t)nwords * 4 + PBWT_WARPS * 4;
     cudaError_t e = cudaFuncSetAttribute(pbwt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    pbwt_kernel<<<2 * ntgt, 512, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded);
+    pbwt_kernel<<<2 * ntgt, 32 * PBWT_WARPS, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0);
     return cudaGetLastError();
 }
 
