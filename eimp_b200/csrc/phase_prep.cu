@@ -221,10 +221,12 @@ cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_
 // inconsistency after the last split.
 //
 // Haplotype-major: lane = column.  A lane walks its haplotype's row of the
-// haplotype-major reference once (each segment is an OR over a short word
-// range), the warp's ballot is the 32-bit word of the output row.  Grid:
-// (target, 8 output words of 32 columns per CTA); the columns past K are
-// written as zero padding up to W(K) words.
+// haplotype-major reference word by word, once: the split sites of the
+// target are a bit mask, so within a word every split closes the running
+// segment (its inconsistency row, then the split site's allele row) and the
+// rest of the word opens the next one.  The warp's ballot is the 32-bit word
+// of an output row.  Grid: (target, 8 output words of 32 columns per CTA);
+// the columns past K are written as zero padding up to W(K) words.
 // ---------------------------------------------------------------------------
 constexpr int CREF_WARPS = 8;
 
@@ -233,9 +235,12 @@ __global__ void __launch_bounds__(32 * CREF_WARPS) cref_kernel(
     const int32_t *__restrict__ besthaps, int K, const int32_t *__restrict__ splits,
     const int32_t *__restrict__ nsplits, const int64_t *__restrict__ rowoff, uint64_t *__restrict__ cref) {
     extern __shared__ uint64_t sm[];
-    uint64_t *is0 = sm, *is2 = sm + wM;   // the target's homozygous genotypes as bit masks
+    // the target's homozygous genotypes and its split sites as bit masks
+    uint64_t *is0 = sm, *is2 = sm + wM, *ssp = sm + 2 * wM;
     const int t = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint8_t *g = gt + (size_t)t * M;
+    const int S = nsplits[t];
+    const int32_t *sp = splits + (size_t)t * M;
     for (int w = tid; w < wM; w += blockDim.x) {
         uint64_t a = 0, b = 0;
         const int m0 = w * 64;
@@ -244,8 +249,10 @@ __global__ void __launch_bounds__(32 * CREF_WARPS) cref_kernel(
             a |= (uint64_t)(c == 0) << j;
             b |= (uint64_t)(c == 2) << j;
         }
-        is0[w] = a; is2[w] = b;
+        is0[w] = a; is2[w] = b; ssp[w] = 0ull;
     }
+    __syncthreads();
+    for (int j = tid; j < S; j += blockDim.x) atomicOr((unsigned long long *)&ssp[sp[j] >> 6], 1ull << (sp[j] & 63));
     __syncthreads();
     const int wK = (int)eimp_W(K);
     const int col32 = blockIdx.y * CREF_WARPS + warp;   // 32-bit word of the output rows
@@ -256,38 +263,37 @@ __global__ void __launch_bounds__(32 * CREF_WARPS) cref_kernel(
     const uint64_t *hm = hapmajor + (size_t)h * wM;
     const size_t rstride = 2 * (size_t)wK;   // 32-bit words per row
     uint32_t *out = reinterpret_cast<uint32_t *>(cref + (size_t)rowoff[t] * wK) + col32;
-    const int S = nsplits[t];
-    const int32_t *sp = splits + (size_t)t * M;
-    int lo = 0;
-    for (int j = 0; j <= S; j++) {
-        const int hi = j < S ? sp[j] : M;   // segment [lo, hi)
-        bool inc = false;
-        if (valid && lo < hi) {
-            const int q0 = lo >> 6, q1 = (hi - 1) >> 6;
-            for (int q = q0; q <= q1; q++) {
-                const uint64_t x = hm[q];
-                uint64_t mask = ~0ull;
-                if (q == q0) mask &= ~0ull << (lo & 63);
-                if (q == q1) mask &= ~0ull >> (63 - ((hi - 1) & 63));
-                if (((x & is0[q]) | (~x & is2[q])) & mask) { inc = true; break; }
-            }
+    bool any = false;   // inconsistency of the open segment
+    int row = 0;
+    uint64_t hw = valid ? hm[0] : 0ull;
+    for (int q = 0; q < wM; q++) {
+        const uint64_t a = hw;
+        if (q + 1 < wM) hw = valid ? hm[q + 1] : 0ull;   // next word in flight
+        const uint64_t x = (a & is0[q]) | (~a & is2[q]);
+        uint64_t bnd = ssp[q];
+        int start = 0;
+        while (bnd) {
+            const int b = __ffsll((long long)bnd) - 1;
+            const uint64_t seg = b > start ? (x >> start) & (~0ull >> (64 - (b - start))) : 0ull;
+            any = any || seg != 0ull;
+            const unsigned wi = __ballot_sync(0xffffffffu, valid && any);
+            const unsigned ws = __ballot_sync(0xffffffffu, valid && ((a >> b) & 1ull));
+            if (lane == 0) { out[(size_t)row * rstride] = wi; out[(size_t)(row + 1) * rstride] = ws; }
+            row += 2;
+            any = false;
+            start = b + 1;
+            bnd &= bnd - 1;
         }
-        const unsigned wi = __ballot_sync(0xffffffffu, inc);
-        if (lane == 0) out[(size_t)(2 * j) * rstride] = wi;
-        if (j < S) {
-            const int m = hi;
-            const bool a = valid && ((hm[m >> 6] >> (m & 63)) & 1ull);
-            const unsigned ws = __ballot_sync(0xffffffffu, a);
-            if (lane == 0) out[(size_t)(2 * j + 1) * rstride] = ws;
-            lo = m + 1;
-        }
+        if (start < 64) any = any || (x >> start) != 0ull;
     }
+    const unsigned wi = __ballot_sync(0xffffffffu, valid && any);
+    if (lane == 0) out[(size_t)row * rstride] = wi;
 }
 
 cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM, int nhaps,
                         const int32_t *besthaps, int K, const int32_t *splits, const int32_t *nsplits,
                         const int64_t *rowoff, uint64_t *cref, cudaStream_t st) {
-    const size_t sm = (size_t)2 * wM * sizeof(uint64_t);
+    const size_t sm = (size_t)3 * wM * sizeof(uint64_t);
     if (sm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(cref_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
@@ -302,16 +308,16 @@ cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapm
 // ---------------------------------------------------------------------------
 // PBWT::buildComprPBWT (PBWT.cpp:207-285) of each target's condensed
 // reference, forward and backward (rows in sweep order), one CTA per (target,
-// direction).  Per row: every warp reads the row bits of its 32-haplotype
-// blocks in the current prefix order (one ballot = one data word) and scans
-// its blocks' zero counts; after one barrier each warp places its haplotypes
-// in the next prefix order (zeros first, stable) and writes the compressed
-// words [data, zeros through the word].  The next row is copied into shared
-// memory asynchronously while the current one is processed.  The forward CTA
-// also writes each row's zero count.
+// direction).  Each warp owns PW consecutive 32-haplotype blocks of the prefix
+// order, lane j of the warp the j-th block's data word.  Per row: the warp
+// reads the row bits of its blocks in the current prefix order (a ballot per
+// block), scans the blocks' zero counts with shuffles and publishes its total;
+// after one barrier it places its haplotypes in the next prefix order (zeros
+// first, stable) and writes its compressed words [data, zeros through the
+// word] as one 8-byte store per lane.  Prefix arrays are 16-bit (K <= 65536).
+// The next row is copied into shared memory asynchronously while the current
+// one is processed.  The forward CTA also writes each row's zero count.
 // ---------------------------------------------------------------------------
-constexpr int PBWT_WARPS = 8;
-
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -319,29 +325,30 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-__global__ void __launch_bounds__(32 * PBWT_WARPS) pbwt_kernel(const uint64_t *__restrict__ cref,
-                                                               const int64_t *__restrict__ rowoff, int K,
-                                                               uint32_t *__restrict__ pbwt, size_t rowstride,
-                                                               int emit_padded, int32_t *__restrict__ count0) {
+template <int PW>
+__global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__ cref,
+                                                    const int64_t *__restrict__ rowoff, int K,
+                                                    uint32_t *__restrict__ pbwt, size_t rowstride, int emit_padded,
+                                                    int32_t *__restrict__ count0) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int t = blockIdx.x >> 1, dir = blockIdx.x & 1;
     const int wK = (int)eimp_W(K);
     const int nwords = (K + 31) / 32;
-    uint64_t *rowbuf = reinterpret_cast<uint64_t *>(smem);                // 2 x wK
-    int32_t *perm = reinterpret_cast<int32_t *>(rowbuf + 2 * wK);         // K
-    int32_t *nperm = perm + K;                                            // K
-    uint32_t *data = reinterpret_cast<uint32_t *>(nperm + K);             // nwords
-    int *wtot = reinterpret_cast<int *>(data + nwords);                   // PBWT_WARPS
+    const int nwarps = blockDim.x >> 5;
+    uint64_t *rowbuf = reinterpret_cast<uint64_t *>(smem);                 // 2 x wK
+    int *wtot = reinterpret_cast<int *>(rowbuf + 2 * wK);                  // 32
+    uint16_t *perm = reinterpret_cast<uint16_t *>(wtot + 32);              // K
+    uint16_t *nperm = perm + K;                                            // K
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t r0 = rowoff[t];
     const int Mp = (int)(rowoff[t + 1] - r0);
     const uint64_t *rows = cref + (size_t)r0 * wK;
     uint32_t *out = pbwt + (size_t)(2 * r0 + (dir ? Mp : 0)) * rowstride;
-    const int per = (nwords + PBWT_WARPS - 1) / PBWT_WARPS;   // words of a warp
-    const int w0 = warp * per, w1 = min(nwords, w0 + per);
+    const int w0 = warp * PW;                      // the warp's first block
+    const int nb = max(0, min(PW, nwords - w0));   // the warp's blocks
     const unsigned lt = (1u << lane) - 1u;
-    const int nchunk = wK / 2;                                 // 16-byte pieces of a row
-    for (int i = tid; i < K; i += blockDim.x) perm[i] = i;
+    const int nchunk = wK / 2;                     // 16-byte pieces of a row
+    for (int i = tid; i < K; i += blockDim.x) perm[i] = (uint16_t)i;
     if (Mp > 0) {
         const uint64_t *src = rows + (size_t)(dir ? Mp - 1 : 0) * wK;
         for (int c = tid; c < nchunk; c += blockDim.x) cp_async16(rowbuf + 2 * c, src + 2 * c);
@@ -358,47 +365,77 @@ __global__ void __launch_bounds__(32 * PBWT_WARPS) pbwt_kernel(const uint64_t *_
             for (int c = tid; c < nchunk; c += blockDim.x) cp_async16(dst + 2 * c, src + 2 * c);
         }
         cp_async_commit();
-        // data words in the current prefix order, zeros per warp
-        int z = 0;
-        for (int w = w0; w < w1; w++) {
-            const int i = w * 32 + lane;
-            int bit = 1;   // tail padded with ones (PBWT.cpp:261-267)
-            if (i < K) { const int h = perm[i]; bit = (int)((row[h >> 6] >> (h & 63)) & 1ull); }
-            const unsigned b = __ballot_sync(0xffffffffu, bit);
-            if (lane == 0) data[w] = b;
-            z += __popc(~b);
-        }
-        if (lane == 0) wtot[warp] = z;
-        __syncthreads();
-        int zb = 0, cnt0 = 0;
-        for (int q = 0; q < PBWT_WARPS; q++) { const int v = wtot[q]; cnt0 += v; if (q < warp) zb += v; }
-        uint32_t *o = out + (size_t)midx * rowstride;
-        for (int w = w0; w < w1; w++) {
-            const unsigned b = data[w];
-            const int i = w * 32 + lane;
-            if (i < K) {
-                const int zi = zb + __popc(~b & lt);   // zeros before position i
-                nperm[((b >> lane) & 1u) ? cnt0 + (i - zi) : zi] = perm[i];
+        // data words in the current prefix order
+        uint16_t hreg[PW];
+        unsigned myb = 0;
+#pragma unroll
+        for (int q = 0; q < PW; q++) {
+            if (q < nb) {
+                const int i = (w0 + q) * 32 + lane;
+                int bit = 1;   // tail padded with ones (PBWT.cpp:261-267)
+                hreg[q] = 0;
+                if (i < K) {
+                    const int h = perm[i];
+                    hreg[q] = (uint16_t)h;
+                    bit = (int)((row[h >> 6] >> (h & 63)) & 1ull);
+                }
+                const unsigned b = __ballot_sync(0xffffffffu, bit);
+                if (lane == q) myb = b;
             }
-            zb += __popc(~b);
-            if (lane == 0) { o[2 * w] = b; o[2 * w + 1] = (uint32_t)zb; }
         }
+        // zeros per block, scanned over the warp's blocks
+        const int zc = lane < nb ? __popc(~myb) : 0;
+        int inc = zc;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) wtot[warp] = inc;
+        __syncthreads();
+        int zw = 0, cnt0 = 0;
+        for (int q = 0; q < nwarps; q++) { const int v = wtot[q]; cnt0 += v; if (q < warp) zw += v; }
+        const int excl = zw + inc - zc;   // zeros before this lane's block
+#pragma unroll
+        for (int q = 0; q < PW; q++) {
+            if (q < nb) {
+                const unsigned b = __shfl_sync(0xffffffffu, myb, q);
+                const int zb = __shfl_sync(0xffffffffu, excl, q);
+                const int i = (w0 + q) * 32 + lane;
+                if (i < K) {
+                    const int zi = zb + __popc(~b & lt);   // zeros before position i
+                    nperm[((b >> lane) & 1u) ? cnt0 + (i - zi) : zi] = hreg[q];
+                }
+            }
+        }
+        uint32_t *o = out + (size_t)midx * rowstride;
+        if (lane < nb) reinterpret_cast<uint2 *>(o)[w0 + lane] = make_uint2(myb, (uint32_t)(excl + zc));
         if (emit_padded)
             for (size_t j = 2 * (size_t)nwords + tid; j < rowstride; j += blockDim.x) o[j] = 0u;
         if (dir == 0 && tid == 0) count0[r0 + m] = cnt0;
-        int32_t *tp = perm; perm = nperm; nperm = tp;
+        uint16_t *tp = perm; perm = nperm; nperm = tp;
     }
     cp_async_wait_all();
 }
 
+template <int PW>
+static cudaError_t launch_pbwt_pw(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
+                                  uint32_t *pbwt, size_t rowstride, int emit_padded, cudaStream_t st) {
+    const int wK = (int)eimp_W(K), nwords = (K + 31) / 32;
+    const int nwarps = max(4, (nwords + PW - 1) / PW);
+    const size_t sm = (size_t)2 * wK * 8 + 32 * 4 + (size_t)2 * K * 2;
+    cudaError_t e = cudaFuncSetAttribute(pbwt_kernel<PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    pbwt_kernel<PW><<<2 * ntgt, 32 * nwarps, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_pbwt(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
                         uint32_t *pbwt, size_t rowstride, int emit_padded, cudaStream_t st) {
-    const int wK = (int)eimp_W(K), nwords = (K + 31) / 32;
-    const size_t sm = (size_t)2 * wK * 8 + (size_t)2 * K * 4 + (size_t)nwords * 4 + PBWT_WARPS * 4;
-    cudaError_t e = cudaFuncSetAttribute(pbwt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    pbwt_kernel<<<2 * ntgt, 32 * PBWT_WARPS, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0);
-    return cudaGetLastError();
+    // the 8-byte pair stores need 8-byte aligned rows
+    if (K < 1 || K > 65536 || rowstride % 2) return cudaErrorInvalidValue;
+    const int nwords = (K + 31) / 32;
+    if (nwords <= 32 * 32) return launch_pbwt_pw<32>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, st);
+    return launch_pbwt_pw<64>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, st);
 }
 
 }  // namespace eimp
