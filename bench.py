@@ -336,6 +336,20 @@ def main():
     def step_imp():
         step_timed()
 
+    # beam-kernel roofline inputs: the library times its phasing stages with
+    # CUDA events on its stream; the condensed rows of the batch (sum of 2S+1
+    # over the targets) give the PBWT bytes the beam reads
+    STAGES = ("prep", "split_readback", "cref", "pbwt", "beam")
+    rows_total = 0
+    if do_phase:
+        ctx.check(L.eimp_set_timing(h, 1))
+        rows_c = C.c_size_t(0)
+        gt_host = np.ascontiguousarray(tg.gt, dtype=np.uint8)
+        ctx.check(L.eimp_phase_cref_pbwt(h, C.byref(pparams), nt, gt_host.ctypes.data, C.byref(rows_c),
+                                         None, None, None, None))
+        rows_total = rows_c.value
+    stage_ms = {k: [] for k in STAGES}
+
     for _ in range(args.warmup):
         step_imp()
     ctx.synchronize()
@@ -348,10 +362,15 @@ def main():
     sampler.start()
     launches0 = ctx.launches
     evs = []
+    st5 = (C.c_float * 5)()
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
         evs.append(step_timed())
+        if do_phase:   # read before the next step's phasing records over them
+            ctx.check(L.eimp_phase_stage_ms(h, st5, 5))
+            for k, v in zip(STAGES, st5):
+                stage_ms[k].append(float(v))
     ctx.synchronize()
     torch.cuda.synchronize()
     launches = ctx.launches - launches0
@@ -370,17 +389,39 @@ def main():
     dos_per_step = imputed_count(tg, Mref)
     value = world * dos_per_step * args.steps / (tot_ms / 1e3)
 
-    # roofline of the dominant kernel (dosages): algorithmic bytes per launch =
-    # dosage + bit outputs of every (haplotype, site) + one read of the
-    # haplotype-major panel
+    # roofline of the dominant kernel.  With phasing that is the beam kernel
+    # (more than half of the device time): its algorithmic bytes per launch are
+    # one read of every target's condensed PBWT in both directions (2 x rows x
+    # 2*ceil(K/32) uint32) plus the rows' zero counts, the genotype bytes it
+    # reads and the phased haplotypes and dosages it writes.  Without phasing
+    # it is the dosage kernel: dosage + bit outputs of every (haplotype, site)
+    # + one read of the haplotype-major panel.
+    peak, peak_kind = measured_peak_hbm()
     dos_ms = float(np.mean(kern["dosage"]))
     bytes_dos = 2 * nt * Mref * 4 + 2 * nt * ldb * 8 + nh_ref * W(Mref) * 8
-    peak, peak_kind = measured_peak_hbm()
-    achieved = bytes_dos / (dos_ms / 1e3) / 1e9
-    roofline = {"kernel": "dosage_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": bytes_dos, "avg_launch_ms": dos_ms,
-                "stage_ms": {k: float(np.mean(v)) for k, v in kern.items()}}
+    stage_means = {k: float(np.mean(v)) for k, v in kern.items()}
+    if do_phase:
+        stage_means.update({"phase_" + k: float(np.mean(v)) for k, v in stage_ms.items()})
+        kw = 2 * ((min(cfg.K, nh_ref) + 31) // 32)
+        beam_ms = float(np.mean(stage_ms["beam"]))
+        bytes_beam = 2 * rows_total * kw * 4 + rows_total * 4 + nt * (M + 2 * W(M) * 8 + 2 * M * 4)
+        achieved = bytes_beam / (beam_ms / 1e3) / 1e9
+        # DRAM bytes of one beam launch: the ncu capture of the 64-target cfg2
+        # launch (profiles/beam_kernel_cfg2_64targets.md: 159.7 MB read + 18.8
+        # MB written), scaled to the batch by the number of targets
+        traffic = (178.5e6 / 64) * nt if args.config == "cfg2" else None
+        roofline = {"kernel": "beam_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                    "algorithmic_bytes_per_launch": bytes_beam, "avg_launch_ms": beam_ms,
+                    "note": "latency-bound: one warp per target walks the beam sequentially",
+                    "stage_ms": stage_means,
+                    "dosage_kernel": {"achieved": bytes_dos / (dos_ms / 1e3) / 1e9, "avg_launch_ms": dos_ms,
+                                      "algorithmic_bytes_per_launch": bytes_dos}}
+    else:
+        achieved = bytes_dos / (dos_ms / 1e3) / 1e9
+        roofline = {"kernel": "dosage_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                    "algorithmic_bytes_per_launch": bytes_dos, "avg_launch_ms": dos_ms, "stage_ms": stage_means}
 
     # end to end through the public API: host (pinned) targets in, host dosages out
     e2e = None

@@ -37,6 +37,8 @@ _PROTOS = [
     ("eimp_synchronize", _i32, [_vp]),
     ("eimp_kernel_launches", C.c_uint64, [_vp]),
     ("eimp_stream", _vp, [_vp]),
+    ("eimp_set_timing", C.c_int, [_vp, C.c_int]),
+    ("eimp_phase_stage_ms", C.c_int, [_vp, _vp, C.c_int]),
     ("eimp_gpu_initialize", _i32, [_vp, _sz, _sz, _sz, _sz, _sz, _sz, _vp]),
     ("eimp_gpu_block_size", _sz, [_vp]),
     ("eimp_gpu_run_cref_pbwt", _i32, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -40,6 +40,9 @@ struct eimp_ctx {
     // end and every use on the main stream waits for it
     cudaStream_t side = nullptr;
     cudaEvent_t ref_ready = nullptr, main_mark = nullptr;
+    // optional device timing of the phasing stages (eimp_set_timing)
+    bool timing = false, tvalid = false;
+    cudaEvent_t tev[6] = {};
     std::string err;
     uint64_t launches = 0;
     DBuf status;
@@ -96,6 +99,13 @@ int use_device(eimp_ctx *ctx) {
     return 0;
 }
 
+// phasing stage boundaries: 0 start, 1 after prep, 2 before the condensed
+// reference (after the host read of the split counts), 3 after it, 4 after
+// the PBWT, 5 after the beam
+void tmark(eimp_ctx *ctx, int i) {
+    if (ctx->timing) cudaEventRecord(ctx->tev[i], ctx->stream);
+}
+
 int check_status(eimp_ctx *ctx) {
     uint32_t st = 0;
     CK(cudaMemcpyAsync(&st, ctx->status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -145,6 +155,8 @@ void eimp_destroy(eimp_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaStream_t s = ctx->stream, sd = ctx->side;
     cudaEvent_t e1 = ctx->ref_ready, e2 = ctx->main_mark;
+    for (cudaEvent_t e : ctx->tev)
+        if (e) cudaEventDestroy(e);
     delete ctx;
     if (e1) cudaEventDestroy(e1);
     if (e2) cudaEventDestroy(e2);
@@ -162,6 +174,26 @@ int eimp_synchronize(eimp_ctx *ctx) {
 }
 
 uint64_t eimp_kernel_launches(const eimp_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int eimp_set_timing(eimp_ctx *ctx, int on) {
+    if (!ctx) return EIMP_E_ARG;
+    if (int r = use_device(ctx)) return r;
+    if (on)
+        for (cudaEvent_t &e : ctx->tev)
+            if (!e) CK(cudaEventCreate(&e));
+    ctx->timing = on != 0;
+    ctx->tvalid = false;
+    return 0;
+}
+
+int eimp_phase_stage_ms(eimp_ctx *ctx, float *ms, int n) {
+    if (!ctx || !ms || n < 0) return EIMP_E_ARG;
+    if (!ctx->tvalid) return fail(ctx, EIMP_E_ARG, "eimp_phase_stage_ms: timing off or no phasing call since it was set");
+    if (int r = use_device(ctx)) return r;
+    CK(cudaEventSynchronize(ctx->tev[5]));
+    for (int i = 0; i < n && i < 5; i++) CK(cudaEventElapsedTime(&ms[i], ctx->tev[i], ctx->tev[i + 1]));
+    return 0;
+}
 
 void *eimp_stream(eimp_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
@@ -386,9 +418,11 @@ int run_cref_pbwt(eimp_ctx *ctx, size_t K, size_t ntgt, const uint8_t *d_gt, std
     CK(ctx->b_count0.reserve(rows * 4));
     CK(ctx->b_pbwt.reserve(2 * rows * kw * 4));
     CK(cudaMemcpyAsync(ctx->b_rowoff.p, rowoff.data(), (ntgt + 1) * 8, cudaMemcpyHostToDevice, st));
+    tmark(ctx, 2);
     LAUNCH(launch_cref(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)eimp_W(M), (int)nh,
                        ctx->b_bh.as<int32_t>(), (int)K, ctx->b_splits.as<int32_t>(), ctx->b_nsplits.as<int32_t>(),
                        ctx->b_rowoff.as<int64_t>(), ctx->b_cref.as<uint64_t>(), st));
+    tmark(ctx, 3);
     LAUNCH(launch_pbwt(ctx->b_cref.as<uint64_t>(), ctx->b_count0.as<int32_t>(), ctx->b_rowoff.as<int64_t>(),
                        (int)ntgt, (int)K, ctx->b_pbwt.as<uint32_t>(), kw, 0, st));
     return 0;
@@ -476,16 +510,22 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
     bp.minfixsize = p->minfixsize; bp.maxfixsize = p->maxfixsize;
     bp.minfixthr = p->minfixthr; bp.maxfixthr = p->maxfixthr;
     bp.doPrePhasing = p->doPrePhasing; bp.doRevPhasing = p->doRevPhasing;
+    ctx->tvalid = false;
+    tmark(ctx, 0);
     if (int r = run_prep(ctx, p, ntgt, d_gt)) return r;
+    tmark(ctx, 1);
     std::vector<int64_t> ro;
     if (int r = run_cref_pbwt(ctx, K, ntgt, d_gt, ro)) return r;
     const size_t ab = beam_arena_bytes(bp, (int)M);
     CK(ctx->b_arena.reserve(ntgt * ab));
+    tmark(ctx, 4);
     LAUNCH(launch_beam(bp, (int)ntgt, (int)M, d_gt, ctx->b_monos.as<uint64_t>(), ctx->b_splits.as<int32_t>(),
                        ctx->b_nsplits.as<int32_t>(), ctx->b_calls.as<int32_t>(), ctx->b_ncalls.as<int32_t>(),
                        ctx->b_cmd.as<float>(), ctx->b_pbwt.as<uint32_t>(), ctx->b_count0.as<int32_t>(),
                        ctx->b_rowoff.as<int64_t>(), ctx->b_arena.p, ab, d_mats, d_pats, d_dm, d_dp, d_tc, d_nc,
                        ctx->status.as<uint32_t>(), ctx->stream));
+    tmark(ctx, 5);
+    ctx->tvalid = ctx->timing;
     return 0;
 }
 

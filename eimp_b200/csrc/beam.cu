@@ -264,7 +264,7 @@ __device__ __forceinline__ void hp_mark_required(HPh &h, const Cons &cn) {   // 
 // that accumulates the probabilities, appends the extension intervals and
 // stops at the first step where both extensions are empty, in the reference's
 // order.
-constexpr int HXC = 8;
+constexpr int HXC = 6;
 
 __device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
     HPh &h = c.hp[slot];

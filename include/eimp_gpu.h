@@ -78,6 +78,15 @@ uint64_t eimp_kernel_launches(const eimp_ctx *ctx);
  * work with it. */
 void *eimp_stream(eimp_ctx *ctx);
 
+/* Device timing of the phasing stages (no counterpart in the reference; a
+ * diagnostic).  With timing on, every eimp_phase_targets* call records CUDA
+ * events on the context's stream around its stages; eimp_phase_stage_ms then
+ * waits for the last call and writes up to n of its stage times in ms: best
+ * haplotypes + call sites, the host read of the split counts, the condensed
+ * reference, the PBWTs, the beam. */
+int eimp_set_timing(eimp_ctx *ctx, int on);
+int eimp_phase_stage_ms(eimp_ctx *ctx, float *ms, int n);
+
 /* ------------------------------------------ GPUEngine drop-in (cref + PBWT) */
 
 /* GPUEngine::initialize (GPUEngine.h:50, GPUEngine.cu:44-96): uploads the typed
