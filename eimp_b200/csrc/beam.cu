@@ -755,11 +755,25 @@ __device__ void beam_apply_hap(const Ctx &c, WS &w) {
     }
     if (lane == 0) { w.nfree = nf - ncp; w.nivfree = nvf - 3 * ncp; w.nhap = one; }
     __syncwarp();
-    // probability rings of the copies
+    // probability rings of the copies: 16-byte pieces, one per lane, four
+    // copies' loads in flight before their stores
     const int phs = w.phsize;
-    for (int e = lane; e < ncp * phs; e += 32) {
-        const int k = e / phs, i = e % phs;
-        ph_ptr(c, c.copies[3 * k + 1])[i] = ph_ptr(c, c.copies[3 * k])[i];
+    if (phs >= 4) {
+        const int n4 = phs / 4;
+        for (int k0 = 0; k0 < ncp; k0 += 4) {
+            float4 v[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (k0 + j < ncp && lane < n4)
+                    v[j] = reinterpret_cast<const float4 *>(ph_ptr(c, c.copies[3 * (k0 + j)]))[lane];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (k0 + j < ncp && lane < n4)
+                    reinterpret_cast<float4 *>(ph_ptr(c, c.copies[3 * (k0 + j) + 1]))[lane] = v[j];
+        }
+    } else {
+        for (int k = 0; k < ncp; k++)
+            if (lane < phs) ph_ptr(c, c.copies[3 * k + 1])[lane] = ph_ptr(c, c.copies[3 * k])[lane];
     }
     __syncwarp();
     // the copies: push bit 1 and the extension-1 probability

@@ -33,11 +33,13 @@ enum { cudaSuccess = 0, cudaErrorInvalidValue = 1 };
 
 struct dim3 { unsigned x = 0, y = 0, z = 0; };
 struct int2 { int x, y; };
+struct short2 { short x, y; };
 struct uint2 { unsigned x, y; };
 struct uint4 { unsigned x, y, z, w; };
 struct float4 { float x, y, z, w; };
 struct int4 { int x, y, z, w; };
 inline int2 make_int2(int x, int y) { return int2{x, y}; }
+inline short2 make_short2(short x, short y) { return short2{x, y}; }
 inline int4 make_int4(int x, int y, int z, int w) { return int4{x, y, z, w}; }
 
 extern thread_local dim3 threadIdx, blockIdx;
