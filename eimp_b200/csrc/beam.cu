@@ -441,12 +441,6 @@ __device__ float bp_extend(const Ctx &c, BPh &b, int g, const Cons &cn, int bpsc
     return maxP;
 }
 
-__device__ __forceinline__ void hp_mark_deleted_atomic(HPh &h, int e) {   // HaplotypePath.cpp:105-109
-    // the decrements of one prune commute: the extension becomes inactive iff
-    // one of them brings its count to zero
-    if (e == 0) { if (atomicSub(&h.refcnt0, 1) == 1) h.active0 = 0; }
-    else { if (atomicSub(&h.refcnt1, 1) == 1) h.active1 = 0; }
-}
 
 // BeamPath::markExtensionDeleted (BeamPath.cpp:101-112) on the beam path; the
 // haplotype-path side is applied after the heap pass from delmask
@@ -573,48 +567,89 @@ __device__ __forceinline__ int warp_sumi(int v) {
 // candidates are, per beam path in list order, the extension indices from
 // the active index down to 0 (unconstrained) or the active index alone.
 //
-// When at most P candidates reach the limit the heap never evicts: exactly
-// the candidates below the limit are deleted, and the heap's minimum and
-// maximum are a candidate with the smallest and one with the largest key.
-// The lanes then decide everything with warp reductions, provided all
-// candidates tied at the smallest key give the same weightScaleExp and all
-// tied at the largest the same deleteErr (else which tied element the heap
-// holds at its root would matter).  Otherwise lane 0 runs the heap over the
-// beam in shared memory in the reference's order.  The reference counts of the
-// haplotype paths are decremented afterwards by the lanes (nothing in the
-// selection reads them).  Returns 0 when no extension survives.
+// The reference streams the candidates at or above the limit through a
+// min-max heap of capacity P that replaces its minimum only by a strictly
+// larger key.  When at most P candidates reach the limit nothing is evicted;
+// when more do but the P-th largest key is strictly larger than the
+// (P+1)-th, the heap ends holding exactly the P largest (every candidate
+// outside it is at most the final minimum, every one inside at least).  In
+// both cases the lanes decide everything: the P-th largest key comes from a
+// bitwise search over the keys (non-negative floats order like their bit
+// patterns), and the heap's minimum and maximum are a survivor with the
+// smallest and one with the largest key, provided all survivors tied at the
+// smallest key give the same weightScaleExp and all tied at the largest the
+// same deleteErr (else which tied element the heap holds at its root would
+// matter).  Otherwise lane 0 runs the heap in the reference's order.  The
+// reference counts of the haplotype paths are decremented afterwards by the
+// lanes (nothing in the selection reads them).  Returns 0 when no extension
+// survives.
+constexpr int PRR = (BPMAX + 31) / 32;   // beam paths per lane
+
+__device__ __forceinline__ unsigned key_bits(float p) { return p == 0.0f ? 0u : __float_as_uint(p); }
+
 __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn) {
     const int lane = lane_id();
     BPh *bp = w.bp[w.bpsel];
-    const int nbp = w.nbp;
+    const int nbp = w.nbp, P = w.P;
     const float limit = __fmul_rn(c.pLimit, maxP);
     const bool allext = cn.type == C_NONE;
     for (int it = lane; it < nbp; it += 32) w.delmask[it] = 0;
-    // read-only pass: candidates at or above the limit and their extreme keys
-    int nA = 0;
+    // the candidates at or above the limit: bit 4r+ex of sel for extension ex
+    // of beam path lane+32r (their keys are read back from shared memory)
+    unsigned sel = 0;
     float kmin = __int_as_float(0x7f800000), kmax = -__int_as_float(0x7f800000);
-    for (int it = lane; it < nbp; it += 32) {
-        const BPh &b = bp[it];
-        for (int ex = b.actidx; ex >= 0; ex = allext ? ex - 1 : -1) {
-            const float p = b.extp[ex];
-            if (p >= limit) { nA++; kmin = fminf(kmin, p); kmax = fmaxf(kmax, p); }
+#pragma unroll
+    for (int r = 0; r < PRR; r++) {
+        const int it = lane + 32 * r;
+        const BPh *b = &bp[it < nbp ? it : 0];
+        const int ai = it < nbp ? b->actidx : -1;
+#pragma unroll
+        for (int ex = 0; ex < 4; ex++) {
+            if (ex <= ai && (allext || ex == ai)) {
+                const float p = b->extp[ex];
+                if (p >= limit) {
+                    sel |= 1u << (4 * r + ex);
+                    kmin = fminf(kmin, p); kmax = fmaxf(kmax, p);
+                }
+            }
         }
     }
-    nA = warp_sumi(nA);
+    const int nA = warp_sumi(__popc(sel));
     kmin = warp_minf(kmin);
     kmax = warp_maxf(kmax);
-    bool fast = nA <= w.P;
+    // survivors: the selected candidates with key >= thr
+    unsigned thr = 0u;
+    bool fast = true;
+    if (nA > P) {
+        for (int bit = 31; bit >= 0; bit--) {
+            const unsigned cand = thr | (1u << bit);
+            int cnt = 0;
+#pragma unroll
+            for (int q = 0; q < PRR * 4; q++) cnt += ((sel >> q) & 1u) && key_bits(bp[lane + 32 * (q >> 2)].extp[q & 3]) >= cand;
+            if (warp_sumi(cnt) >= P) thr = cand;
+        }
+        int cnt = 0;
+#pragma unroll
+        for (int q = 0; q < PRR * 4; q++) cnt += ((sel >> q) & 1u) && key_bits(bp[lane + 32 * (q >> 2)].extp[q & 3]) >= thr;
+        fast = warp_sumi(cnt) == P;   // else ties straddle the P-th place
+    }
+    unsigned surv = sel;
+    if (thr)
+#pragma unroll
+        for (int q = 0; q < PRR * 4; q++)
+            if (((sel >> q) & 1u) && key_bits(bp[lane + 32 * (q >> 2)].extp[q & 3]) < thr) surv &= ~(1u << q);
     int wse = 0, delerr = 0;
-    if (fast && nA > 0) {
+    const int nsurv = nA > P ? P : nA;
+    if (fast && nsurv > 0) {
+        const unsigned kminb = nA > P ? thr : key_bits(kmin), kmaxb = key_bits(kmax);
         int lo0 = INT_MAX, hi0 = INT_MIN, lo1 = 1, hi1 = 0;
-        for (int it = lane; it < nbp; it += 32) {
-            const BPh &b = bp[it];
-            for (int ex = b.actidx; ex >= 0; ex = allext ? ex - 1 : -1) {
-                const float p = b.extp[ex];
-                if (!(p >= limit)) continue;
-                if (p == kmin) { const int e = -ilogb_exact(b.weight); lo0 = min(lo0, e); hi0 = max(hi0, e); }
-                if (p == kmax) { const int f = b.nErr > 0; lo1 = min(lo1, f); hi1 = max(hi1, f); }
-            }
+#pragma unroll
+        for (int q = 0; q < PRR * 4; q++) {
+            if (!((surv >> q) & 1u)) continue;
+            const BPh &b = bp[lane + 32 * (q >> 2)];
+            const unsigned kq = key_bits(b.extp[q & 3]);
+            if (kq == kminb) { const int e = -ilogb_exact(b.weight); lo0 = min(lo0, e); hi0 = max(hi0, e); }
+            if (kq == kmaxb) { const int f = b.nErr > 0; lo1 = min(lo1, f); hi1 = max(hi1, f); }
         }
         lo0 = warp_mini(lo0); hi0 = warp_maxi(hi0);
         lo1 = warp_mini(lo1); hi1 = warp_maxi(hi1);
@@ -624,17 +659,19 @@ __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn
     }
     __syncwarp();
     if (fast) {
-        for (int it = lane; it < nbp; it += 32) {
+#pragma unroll
+        for (int r = 0; r < PRR; r++) {
+            const int it = lane + 32 * r;
+            if (it >= nbp) continue;
             BPh &b = bp[it];
             unsigned dm = 0;
             for (int ex = b.actidx; ex >= 0; ex = allext ? ex - 1 : -1)
-                if (!(b.extp[ex] >= limit)) { b.active[ex] = 0; dm |= 1u << ex; }
+                if (!((surv >> (4 * r + ex)) & 1u)) { b.active[ex] = 0; dm |= 1u << ex; }
             if (dm) { bp_update_actidx(b); w.delmask[it] = (unsigned char)dm; }
         }
-        if (lane == 0) { w.ires = nA; w.wse = wse; w.delerr = delerr; }
+        if (lane == 0) { w.ires = nsurv; w.wse = wse; w.delerr = delerr; }
     } else if (lane == 0) {
         Hel *hq = w.heap;
-        const int P = w.P;
         int n = 0;
         for (int it = 0; it < nbp; it++) {
             BPh &b = bp[it];
@@ -661,13 +698,27 @@ __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn
     }
     __syncwarp();
     const int n = w.ires;
+    // the deletions (HaplotypePath::markExtensionDeleted, HaplotypePath.cpp:
+    // 105-109), aggregated per haplotype-path extension: a count reaches
+    // zero (the extension becomes inactive) in exactly the decrement that
+    // takes it from >= 1 to <= 0, however the decrements are grouped
     for (int it = lane; it < nbp; it += 32) {
         const unsigned dm = w.delmask[it];
         if (!dm) continue;
         HPh &pm = c.hp[c.happ[bp[it].mat]];
         HPh &pp = c.hp[c.happ[bp[it].pat]];
-        for (int ex = 0; ex < 4; ex++)
-            if (dm & (1u << ex)) { hp_mark_deleted_atomic(pm, ex >> 1); hp_mark_deleted_atomic(pp, ex & 1); }
+        const int dm0 = (int)(dm & 1u) + (int)((dm >> 1) & 1u);          // mat extension 0: ext 0, 1
+        const int dm1 = (int)((dm >> 2) & 1u) + (int)((dm >> 3) & 1u);   // mat extension 1: ext 2, 3
+        const int dp0 = (int)(dm & 1u) + (int)((dm >> 2) & 1u);          // pat extension 0: ext 0, 2
+        const int dp1 = (int)((dm >> 1) & 1u) + (int)((dm >> 3) & 1u);   // pat extension 1: ext 1, 3
+        const int om0 = dm0 ? atomicSub(&pm.refcnt0, dm0) : 0;
+        const int om1 = dm1 ? atomicSub(&pm.refcnt1, dm1) : 0;
+        const int op0 = dp0 ? atomicSub(&pp.refcnt0, dp0) : 0;
+        const int op1 = dp1 ? atomicSub(&pp.refcnt1, dp1) : 0;
+        if (dm0 && om0 >= 1 && om0 - dm0 <= 0) pm.active0 = 0;
+        if (dm1 && om1 >= 1 && om1 - dm1 <= 0) pm.active1 = 0;
+        if (dp0 && op0 >= 1 && op0 - dp0 <= 0) pp.active0 = 0;
+        if (dp1 && op1 >= 1 && op1 - dp1 <= 0) pp.active1 = 0;
     }
     __syncwarp();
     return n > 0;

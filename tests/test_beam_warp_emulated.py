@@ -3,8 +3,7 @@ host warp emulator (tests/warp_emu): every warp collective must be reached by
 all 32 lanes from the same call site, no access may leave its buffers
 (address and undefined-behaviour sanitizers), and the phased haplotypes,
 dosages and confidences must equal the golden fixtures made by the reference
-(beam 16) and the oracle restatement (beam 64 with pre-phasing, which runs
-the beam-path loops over more than one warp-width of paths)."""
+(beam 16) and the oracle restatement (beams 64 and 4 with pre-phasing)."""
 import os
 import shutil
 import subprocess
@@ -108,18 +107,21 @@ def test_beam_emulated_matches_reference_golden(emu_exe, tmp_path):
     np.testing.assert_array_equal(nc, g["K64_ncallsites"])
 
 
-def test_beam_emulated_wide_beam_prephasing_matches_oracle(emu_exe, tmp_path):
+@pytest.mark.parametrize("P", [64, 4])
+def test_beam_emulated_prephasing_matches_oracle(emu_exe, tmp_path, P):
+    """Beam 64 runs the beam-path loops over more than one warp-width of paths;
+    beam 4 makes most prunes select the P best of more candidates."""
     from oracle import restate as R
     if not R.available():
         pytest.skip("oracle library not built")
     g = np.load(golden_path("golden_tiny.npz"))
     K = 64
-    write_inputs(tmp_path, K=K, P=64, prephase=True, **golden_inputs(g, K))
+    write_inputs(tmp_path, K=K, P=P, prephase=True, **golden_inputs(g, K))
     nt, M = g["gt"].shape
     mats, pats, dm, dp, tc, nc, st = run_emu(emu_exe, tmp_path, nt, M)
     assert not st.any()
     om, op, odm, odp = R.phase_many(g["gt"], g["hapmajor_typed"], g["sitemajor_typed"], g["cm_typed"],
-                                    R.params_c(K=K, beamwidth=64, doPrePhasing=True), 4)
+                                    R.params_c(K=K, beamwidth=P, doPrePhasing=True), 4)
     np.testing.assert_array_equal(mats, om)
     np.testing.assert_array_equal(pats, op)
     np.testing.assert_array_equal(dm, odm)

@@ -38,8 +38,9 @@ def test_phase_golden(ctx, g, K):
     np.testing.assert_array_equal(nc, g[pre + "ncallsites"])
 
 
-@pytest.mark.parametrize("prephase", [False, True])
-def test_phase_vs_oracle_smalltest(ctx, smalltest, prephase):
+@pytest.mark.parametrize("prephase,beam", [(False, 32), (True, 32), (True, 4)])
+def test_phase_vs_oracle_smalltest(ctx, smalltest, prephase, beam):
+    """beam 4: most prunes keep the 4 best of more candidates."""
     from eimp_b200.engine import PhaseParams, Phaser
     from eimp_b200.synth import typed_views
     from oracle import restate as R
@@ -47,9 +48,9 @@ def test_phase_vs_oracle_smalltest(ctx, smalltest, prephase):
     tg = groups[0]
     hm, sm, cm = typed_views(panel, tg.typed)
     ph = Phaser(ctx, hm, sm, cm)
-    pp = PhaseParams(K=200, beamwidth=32, doPrePhasing=prephase)
+    pp = PhaseParams(K=200, beamwidth=beam, doPrePhasing=prephase)
     mats, pats, dm, dp, tc, nc = ph.phase(pp, tg.gt)
-    P = R.params_c(K=200, beamwidth=32, doPrePhasing=prephase)
+    P = R.params_c(K=200, beamwidth=beam, doPrePhasing=prephase)
     om, op, odm, odp = R.phase_many(tg.gt, hm, sm, cm, P, 8)
     for t in range(tg.gt.shape[0]):
         assert np.array_equal(mats[t], om[t]), (t, first_diff(mats[t], om[t], len(tg.typed)))
