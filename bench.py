@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--plain-targets", type=int, default=16,
+                    help="targets timed one per call for the plain-form comparison (0: skip)")
+    ap.add_argument("--serving-requests", type=int, default=40, help="requests of the serving run (0: skip)")
+    ap.add_argument("--serving-rate", type=float, default=40.0, help="mean request arrivals per second")
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--stages", default="phase,impute", help="comma list of: phase, impute")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -467,6 +471,67 @@ def main():
         e2e = {"value": world * dos_per_step / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3}
 
+    # the plain drop-in form: one target per call (phase, matches, dosages),
+    # device-resident inputs, on a sample of targets; same metric
+    plain = None
+    if rank == 0 and args.plain_targets > 0:
+        npl = min(args.plain_targets, nt)
+        ep = [ev() for _ in range(2)]
+        torch.cuda.synchronize()
+        ep[0].record(stream)
+        for i in range(npl):
+            if do_phase:
+                ctx.check(L.eimp_phase_targets_dev(h, C.byref(pparams), 1, d_gt[i:i + 1].data_ptr(),
+                                                   d_mats[i:i + 1].data_ptr(), d_pats[i:i + 1].data_ptr(),
+                                                   d_pdm[i:i + 1].data_ptr(), d_pdp[i:i + 1].data_ptr(),
+                                                   d_tc[i:i + 1].data_ptr(), d_nc[i:i + 1].data_ptr()))
+                with torch.cuda.stream(stream):
+                    d_ph3[i, 0].copy_(d_mats[i])
+                    d_ph3[i, 1].copy_(d_pats[i])
+                src1 = d_ph3[i]
+            else:
+                src1 = d_phased[2 * i:2 * i + 2]
+            ctx.check(L.eimp_imp_prepare_dev(h, 1, src1.data_ptr(), d_gt[i:i + 1].data_ptr(), 0, 0, 0))
+            ctx.check(L.eimp_imp_bunch_dev(h, 0, Mref, d_bits[2 * i:2 * i + 2].data_ptr(), ldb,
+                                           d_dos[2 * i:2 * i + 2].data_ptr(), Mref))
+        ep[1].record(stream)
+        ctx.synchronize()
+        pl_ms = ep[0].elapsed_time(ep[1])
+        sub = synth.Targets(tg.typed, tg.gt[:npl], tg.truth[:2 * npl])
+        pl_value = imputed_count(sub, Mref) / (pl_ms / 1e3)
+        plain = {"value": pl_value, "unit": UNIT, "targets": npl, "ms_per_target": pl_ms / npl,
+                 "batched_over_plain": (value / world) / pl_value,
+                 "form": "one target per call: eimp_phase_targets_dev, eimp_imp_prepare_dev, eimp_imp_bunch_dev"}
+
+    # serving: continuous batching of requests of 1..256 targets arriving as a
+    # Poisson stream, two slots (contexts) on this device; host buffers in
+    # and out; latency from submission to result
+    serving = None
+    if rank == 0 and args.serving_requests > 0 and do_phase:
+        from eimp_b200.engine import PhaseParams as PP
+        from eimp_b200.serving import GpuSlot, Server, device_bytes_per_target, load_test
+        srng = np.random.default_rng(cfg.seed + 7)
+        sizes = np.exp(srng.uniform(0.0, np.log(256.0), size=args.serving_requests)).astype(int).clip(1, 256)
+        reqs, o = [], 0
+        for sz in sizes:
+            idx = (o + np.arange(sz)) % nt
+            reqs.append(np.ascontiguousarray(tg.gt[idx]))
+            o += sz
+        pp = PP(K=cfg.K, beamwidth=cfg.beam)
+        slots = [GpuSlot(local, hm, sm, cm, panel.sitemajor, panel.af.astype(np.float32), tg.typed, nh_ref, pp)
+                 for _ in range(2)]
+        bpt = device_bytes_per_target(M, Mref, min(cfg.K, nh_ref), P=cfg.beam)
+        free_b, _tot = torch.cuda.mem_get_info(dev)
+        srv = Server(slots, max_batch_targets=512, mem_budget=0.5 * free_b, bytes_per_target=bpt)
+        srv.submit(reqs[0][:1]).result()   # first launch of each slot's kernels
+        srv.submit(reqs[0][:1]).result()
+        rate = args.serving_rate
+        cnt = lambda g: int(2 * ((Mref - M) * g.shape[0] + (g == 3).sum()))  # noqa: E731
+        serving = load_test(srv, reqs, rate, seed=cfg.seed, count=cnt)
+        srv.close()
+        serving.update({"unit": UNIT, "slots": 2, "max_batch_targets": 512,
+                        "request_sizes": "log-uniform 1..256 targets", "arrivals": "Poisson"})
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu, _ = cpu_baseline(cfg, panel, tg, args.cpu_sample_targets, stages)
@@ -477,7 +542,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64/f32",
                 "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
                 "config": config_block(cfg, panel, tg, stages), "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches)}
+                "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches), "plain": plain, "serving": serving}
         if do_phase:
             line["phased_samples_per_sec"] = world * nt * args.steps / (tot_ms / 1e3)
             line["phase_ms_per_step"] = float(np.mean(kern["phase"]))
