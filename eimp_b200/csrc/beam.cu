@@ -318,11 +318,16 @@ __device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
 #pragma unroll
         for (int j = 0; j < HXC; j++)   // the next chunk's loads
             if (nb + j < lim) { nfr[j] = iv[nb + j - 1]; ntph[j] = ph[(nb + j + phstart) & pm]; }
+        // mappings of the chunk's intervals; a step whose interval equals the
+        // previous step's takes the reference's reuse branch below and needs
+        // none (about 60 % of the steps, mostly the same for all lanes)
         int A0[HXC], B0[HXC], A1[HXC], B1[HXC];
 #pragma unroll
         for (int j = 0; j < HXC; j++) {
             A0[j] = 0; B0[j] = -1; A1[j] = 0; B1[j] = -1;
-            if (base + j < lim) {
+            const int2 pf = j == 0 ? prevfrom : fr[j - 1];
+            const bool same = base + j > 1 && pf.x == fr[j].x && pf.y == fr[j].y;
+            if (base + j < lim && !same) {
                 int cl, cr, il, ir;
                 pbwt_map(rinc, cinc, fr[j].x, fr[j].y, cl, cr, il, ir);
                 pbwt_map(rref, cnt0, cl, cr, A0[j], B0[j], A1[j], B1[j]);
