@@ -523,8 +523,7 @@ def main():
         bpt = device_bytes_per_target(M, Mref, min(cfg.K, nh_ref), P=cfg.beam)
         free_b, _tot = torch.cuda.mem_get_info(dev)
         srv = Server(slots, max_batch_targets=512, mem_budget=0.5 * free_b, bytes_per_target=bpt)
-        srv.submit(reqs[0][:1]).result()   # first launch of each slot's kernels
-        srv.submit(reqs[0][:1]).result()
+        srv.warmup(tg.gt[np.arange(512) % nt])   # buffers at their working size
         rate = args.serving_rate
         cnt = lambda g: int(2 * ((Mref - M) * g.shape[0] + (g == 3).sum()))  # noqa: E731
         serving = load_test(srv, reqs, rate, seed=cfg.seed, count=cnt)
