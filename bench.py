@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--plain-targets", type=int, default=16,
                     help="targets timed one per call for the plain-form comparison (0: skip)")
     ap.add_argument("--serving-requests", type=int, default=40, help="requests of the serving run (0: skip)")
+    ap.add_argument("--graph-steps", type=int, default=3, help="replays timed in the CUDA-graph form (0: skip)")
     ap.add_argument("--serving-rate", type=float, default=40.0, help="mean request arrivals per second")
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--stages", default="phase,impute", help="comma list of: phase, impute")
@@ -311,6 +312,21 @@ def main():
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     kern = {"phase": [], "smm": [], "dosage": []}
 
+    def step_body():
+        # the batch step without timing events (the CUDA-graph form captures this)
+        ctx.check(L.eimp_imp_set_reference_dev(h, Mref, nh_ref, d_full.data_ptr(), d_af.data_ptr(), M,
+                                               d_typed.data_ptr(), d_sitetyped.data_ptr()))
+        if do_phase:
+            ctx.check(L.eimp_phase_targets_dev(h, C.byref(pparams), nt, d_gt.data_ptr(), d_mats.data_ptr(),
+                                               d_pats.data_ptr(), d_pdm.data_ptr(), d_pdp.data_ptr(),
+                                               d_tc.data_ptr(), d_nc.data_ptr()))
+            with torch.cuda.stream(stream):
+                d_ph3[:, 0].copy_(d_mats)
+                d_ph3[:, 1].copy_(d_pats)
+        src = d_ph3 if do_phase else d_phased
+        ctx.check(L.eimp_imp_prepare_dev(h, nt, src.data_ptr(), d_gt.data_ptr(), 0, 0, 0))
+        ctx.check(L.eimp_imp_bunch_dev(h, 0, Mref, d_bits.data_ptr(), ldb, d_dos.data_ptr(), Mref))
+
     def step_timed():
         e = [ev() for _ in range(5)]
         e[0].record(stream)
@@ -471,6 +487,40 @@ def main():
         e2e = {"value": world * dos_per_step / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3}
 
+    # the CUDA-graph form: the same step captured once (phasing in capacity
+    # mode, the rows reserved for this batch) and replayed; its outputs must
+    # equal the eager step's
+    graph = None
+    if args.graph_steps > 0 and do_phase:
+        ref_out = [d_dos.clone(), d_bits.clone(), d_mats.clone(), d_pats.clone()]
+        ctx.check(L.eimp_set_timing(h, 0))
+        ctx.check(L.eimp_phase_reserve(h, C.byref(pparams), nt, rows_total))
+        step_body()
+        ctx.synchronize()
+        ctx.check(L.eimp_capture_begin(h))
+        step_body()
+        ctx.check(L.eimp_capture_end(h))
+        for _ in range(args.warmup):
+            ctx.check(L.eimp_graph_launch(h))
+        ctx.synchronize()
+        gms = []
+        for _ in range(args.graph_steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            g0, g1 = ev(), ev()
+            g0.record(stream)
+            ctx.check(L.eimp_graph_launch(h))
+            g1.record(stream)
+            gms.append((g0, g1))
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        g_ms = float(np.mean([a.elapsed_time(b) for a, b in gms]))
+        same = all(torch.equal(a, b) for a, b in zip(ref_out, [d_dos, d_bits, d_mats, d_pats]))
+        graph = {"value": world * dos_per_step / (g_ms / 1e3), "unit": UNIT, "ms_per_step": g_ms,
+                 "steps": args.graph_steps, "equal_to_eager": bool(same), "rows_reserved": int(rows_total)}
+        ctx.check(L.eimp_phase_reserve(h, C.byref(pparams), nt, 0))
+        ctx.check(L.eimp_set_timing(h, 1))
+
     # the plain drop-in form: one target per call (phase, matches, dosages),
     # device-resident inputs, on a sample of targets; same metric
     plain = None
@@ -541,7 +591,8 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64/f32",
                 "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
                 "config": config_block(cfg, panel, tg, stages), "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches), "plain": plain, "serving": serving}
+                "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches), "plain": plain, "serving": serving,
+                "graph": graph}
         if do_phase:
             line["phased_samples_per_sec"] = world * nt * args.steps / (tot_ms / 1e3)
             line["phase_ms_per_step"] = float(np.mean(kern["phase"]))

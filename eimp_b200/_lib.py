@@ -39,6 +39,10 @@ _PROTOS = [
     ("eimp_stream", _vp, [_vp]),
     ("eimp_set_timing", C.c_int, [_vp, C.c_int]),
     ("eimp_phase_stage_ms", C.c_int, [_vp, _vp, C.c_int]),
+    ("eimp_capture_begin", C.c_int, [_vp]),
+    ("eimp_capture_end", C.c_int, [_vp]),
+    ("eimp_graph_launch", C.c_int, [_vp]),
+    ("eimp_phase_reserve", C.c_int, [_vp, C.POINTER(EimpPhaseParams), _sz, _sz]),
     ("eimp_gpu_initialize", _i32, [_vp, _sz, _sz, _sz, _sz, _sz, _sz, _vp]),
     ("eimp_gpu_block_size", _sz, [_vp]),
     ("eimp_gpu_run_cref_pbwt", _i32, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),

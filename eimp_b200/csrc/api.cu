@@ -43,6 +43,16 @@ struct eimp_ctx {
     // optional device timing of the phasing stages (eimp_set_timing)
     bool timing = false, tvalid = false;
     cudaEvent_t tev[6] = {};
+    // capacity mode (eimp_phase_reserve): row offsets computed on the device
+    // against a reserved row capacity; cur_skip = the device flag the
+    // phasing kernels check (null outside capacity mode)
+    int64_t rows_cap = 0;
+    DBuf skipbuf;
+    const int *cur_skip = nullptr;
+    // stream capture (eimp_capture_begin / _end) and the instantiated graph
+    bool capturing = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
     std::string err;
     uint64_t launches = 0;
     DBuf status;
@@ -103,7 +113,7 @@ int use_device(eimp_ctx *ctx) {
 // reference (after the host read of the split counts), 3 after it, 4 after
 // the PBWT, 5 after the beam
 void tmark(eimp_ctx *ctx, int i) {
-    if (ctx->timing) cudaEventRecord(ctx->tev[i], ctx->stream);
+    if (ctx->timing && !ctx->capturing) cudaEventRecord(ctx->tev[i], ctx->stream);
 }
 
 int check_status(eimp_ctx *ctx) {
@@ -157,6 +167,8 @@ void eimp_destroy(eimp_ctx *ctx) {
     cudaEvent_t e1 = ctx->ref_ready, e2 = ctx->main_mark;
     for (cudaEvent_t e : ctx->tev)
         if (e) cudaEventDestroy(e);
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    if (ctx->graph) cudaGraphDestroy(ctx->graph);
     delete ctx;
     if (e1) cudaEventDestroy(e1);
     if (e2) cudaEventDestroy(e2);
@@ -192,6 +204,42 @@ int eimp_phase_stage_ms(eimp_ctx *ctx, float *ms, int n) {
     if (int r = use_device(ctx)) return r;
     CK(cudaEventSynchronize(ctx->tev[5]));
     for (int i = 0; i < n && i < 5; i++) CK(cudaEventElapsedTime(&ms[i], ctx->tev[i], ctx->tev[i + 1]));
+    return 0;
+}
+
+int eimp_capture_begin(eimp_ctx *ctx) {
+    if (!ctx) return EIMP_E_ARG;
+    if (ctx->capturing) return fail(ctx, EIMP_E_ARG, "eimp_capture_begin: already capturing");
+    if (int r = use_device(ctx)) return r;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+    ctx->capturing = true;
+    return 0;
+}
+
+int eimp_capture_end(eimp_ctx *ctx) {
+    if (!ctx) return EIMP_E_ARG;
+    if (!ctx->capturing) return fail(ctx, EIMP_E_ARG, "eimp_capture_end: not capturing");
+    if (int r = use_device(ctx)) return r;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->capturing = false;
+    CK(e);
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    ctx->graph = g;
+    CK(cudaGraphInstantiate(&ctx->gexec, g, 0));
+    // events last recorded inside the capture belong to the graph; record
+    // them again on their streams so that eager calls can wait on them
+    CK(cudaEventRecord(ctx->ref_ready, ctx->side));
+    CK(cudaEventRecord(ctx->main_mark, ctx->stream));
+    return 0;
+}
+
+int eimp_graph_launch(eimp_ctx *ctx) {
+    if (!ctx) return EIMP_E_ARG;
+    if (!ctx->gexec) return fail(ctx, EIMP_E_ARG, "eimp_graph_launch: nothing captured");
+    if (int r = use_device(ctx)) return r;
+    CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
     return 0;
 }
 
@@ -404,27 +452,42 @@ int run_prep(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8
 // condensed reference + PBWT for the prepared batch; fills ctx->b_rows and the
 // host copy of the row offsets
 int run_cref_pbwt(eimp_ctx *ctx, size_t K, size_t ntgt, const uint8_t *d_gt, std::vector<int64_t> &rowoff) {
-    const size_t M = ctx->p_M, nh = ctx->p_nhaps, wN = eimp_W(nh), wK = eimp_W(K), kw = eimp_kw(K);
+    const size_t M = ctx->p_M, nh = ctx->p_nhaps, wK = eimp_W(K), kw = eimp_kw(K);
     cudaStream_t st = ctx->stream;
-    std::vector<int32_t> ns(ntgt);
-    CK(cudaMemcpyAsync(ns.data(), ctx->b_nsplits.p, ntgt * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    rowoff.assign(ntgt + 1, 0);
-    for (size_t t = 0; t < ntgt; t++) rowoff[t + 1] = rowoff[t] + 2 * (int64_t)ns[t] + 1;
-    const size_t rows = (size_t)rowoff[ntgt];
-    ctx->b_rows = rows;
-    CK(ctx->b_rowoff.reserve((ntgt + 1) * 8));
+    size_t rows;
+    if (ctx->rows_cap > 0) {
+        // capacity mode: no host round trip; the offsets are scanned on the
+        // device and the kernels skip the batch when it needs more rows
+        rows = (size_t)ctx->rows_cap;
+        CK(ctx->skipbuf.reserve(sizeof(int)));
+        CK(ctx->b_rowoff.reserve((ntgt + 1) * 8));
+        LAUNCH(launch_rowoff(ctx->b_nsplits.as<int32_t>(), (int)ntgt, ctx->b_rowoff.as<int64_t>(), ctx->rows_cap,
+                             ctx->skipbuf.as<int>(), ctx->status.as<uint32_t>(), st));
+        ctx->cur_skip = ctx->skipbuf.as<int>();
+        ctx->b_rows = 0;   // not known on the host
+        rowoff.clear();
+    } else {
+        std::vector<int32_t> ns(ntgt);
+        CK(cudaMemcpyAsync(ns.data(), ctx->b_nsplits.p, ntgt * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        rowoff.assign(ntgt + 1, 0);
+        for (size_t t = 0; t < ntgt; t++) rowoff[t + 1] = rowoff[t] + 2 * (int64_t)ns[t] + 1;
+        rows = (size_t)rowoff[ntgt];
+        ctx->b_rows = rows;
+        ctx->cur_skip = nullptr;
+        CK(ctx->b_rowoff.reserve((ntgt + 1) * 8));
+        CK(cudaMemcpyAsync(ctx->b_rowoff.p, rowoff.data(), (ntgt + 1) * 8, cudaMemcpyHostToDevice, st));
+    }
     CK(ctx->b_cref.reserve(rows * wK * 8));
     CK(ctx->b_count0.reserve(rows * 4));
     CK(ctx->b_pbwt.reserve(2 * rows * kw * 4));
-    CK(cudaMemcpyAsync(ctx->b_rowoff.p, rowoff.data(), (ntgt + 1) * 8, cudaMemcpyHostToDevice, st));
     tmark(ctx, 2);
     LAUNCH(launch_cref(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)eimp_W(M), (int)nh,
                        ctx->b_bh.as<int32_t>(), (int)K, ctx->b_splits.as<int32_t>(), ctx->b_nsplits.as<int32_t>(),
-                       ctx->b_rowoff.as<int64_t>(), ctx->b_cref.as<uint64_t>(), st));
+                       ctx->b_rowoff.as<int64_t>(), ctx->b_cref.as<uint64_t>(), ctx->cur_skip, st));
     tmark(ctx, 3);
     LAUNCH(launch_pbwt(ctx->b_cref.as<uint64_t>(), ctx->b_count0.as<int32_t>(), ctx->b_rowoff.as<int64_t>(),
-                       (int)ntgt, (int)K, ctx->b_pbwt.as<uint32_t>(), kw, 0, st));
+                       (int)ntgt, (int)K, ctx->b_pbwt.as<uint32_t>(), kw, 0, ctx->cur_skip, st));
     return 0;
 }
 
@@ -476,6 +539,12 @@ int eimp_phase_cref_pbwt(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt,
     if (int r = run_prep(ctx, p, ntgt, ctx->b_gt.as<uint8_t>())) return r;
     std::vector<int64_t> ro;
     if (int r = run_cref_pbwt(ctx, K, ntgt, ctx->b_gt.as<uint8_t>(), ro)) return r;
+    if (ctx->rows_cap > 0) {   // offsets were computed on the device
+        ro.assign(ntgt + 1, 0);
+        CK(cudaMemcpyAsync(ro.data(), ctx->b_rowoff.p, (ntgt + 1) * 8, cudaMemcpyDeviceToHost, st));
+        if (int r = check_status(ctx)) return r;
+        ctx->b_rows = (size_t)ro[ntgt];
+    }
     *rows_out = ctx->b_rows;
     if (rowoff) memcpy(rowoff, ro.data(), (ntgt + 1) * 8);
     if (cref) CK(cudaMemcpyAsync(cref, ctx->b_cref.p, ctx->b_rows * eimp_W(K) * 8, cudaMemcpyDeviceToHost, st));
@@ -492,11 +561,7 @@ size_t hist_len(int hsize, float hist) {
     return (size_t)((double)((float)hsize * hist) + 0.5);
 }
 
-int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt, uint64_t *d_mats,
-              uint64_t *d_pats, float *d_dm, float *d_dp, float *d_tc, int32_t *d_nc) {
-    const size_t M = ctx->p_M, nh = ctx->p_nhaps;
-    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
-    BeamParams bp;
+int make_beam_params(eimp_ctx *ctx, const eimp_phase_params *p, size_t K, BeamParams &bp) {
     bp.K = (int)K;
     bp.H = (int)hist_len(p->hsize, p->hist);
     bp.Hf = (int)hist_len(p->hsize_fast, p->hist);
@@ -510,6 +575,15 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
     bp.minfixsize = p->minfixsize; bp.maxfixsize = p->maxfixsize;
     bp.minfixthr = p->minfixthr; bp.maxfixthr = p->maxfixthr;
     bp.doPrePhasing = p->doPrePhasing; bp.doRevPhasing = p->doRevPhasing;
+    return 0;
+}
+
+int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt, uint64_t *d_mats,
+              uint64_t *d_pats, float *d_dm, float *d_dp, float *d_tc, int32_t *d_nc) {
+    const size_t M = ctx->p_M, nh = ctx->p_nhaps;
+    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    BeamParams bp;
+    if (int r = make_beam_params(ctx, p, K, bp)) return r;
     ctx->tvalid = false;
     tmark(ctx, 0);
     if (int r = run_prep(ctx, p, ntgt, d_gt)) return r;
@@ -523,7 +597,7 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
                        ctx->b_nsplits.as<int32_t>(), ctx->b_calls.as<int32_t>(), ctx->b_ncalls.as<int32_t>(),
                        ctx->b_cmd.as<float>(), ctx->b_pbwt.as<uint32_t>(), ctx->b_count0.as<int32_t>(),
                        ctx->b_rowoff.as<int64_t>(), ctx->b_arena.p, ab, d_mats, d_pats, d_dm, d_dp, d_tc, d_nc,
-                       ctx->status.as<uint32_t>(), ctx->stream));
+                       ctx->status.as<uint32_t>(), ctx->cur_skip, ctx->stream));
     tmark(ctx, 5);
     ctx->tvalid = ctx->timing;
     return 0;
@@ -532,6 +606,40 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
 }  // namespace
 
 extern "C" {
+
+int eimp_phase_reserve(eimp_ctx *ctx, const eimp_phase_params *p, size_t max_targets, size_t max_rows) {
+    if (!max_rows) {   // back to host-sized offsets
+        if (!ctx) return EIMP_E_ARG;
+        ctx->rows_cap = 0;
+        return 0;
+    }
+    if (int r = check_phase_args(ctx, p, max_targets)) return r;
+    if (int r = use_device(ctx)) return r;
+    const size_t M = ctx->p_M, nh = ctx->p_nhaps, wM = eimp_W(M), wN = eimp_W(nh);
+    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    BeamParams bp;
+    bp.K = (int)K;
+    if (int r = make_beam_params(ctx, p, K, bp)) return r;
+    const size_t n = max_targets;
+    CK(ctx->b_gt.reserve(n * M));
+    CK(ctx->b_nerr.reserve(n * nh * 4));
+    CK(ctx->b_bh.reserve(n * K * 4));
+    CK(ctx->b_flags.reserve(n * wN * 8));
+    CK(ctx->b_monos.reserve(n * wM * 8));
+    CK(ctx->b_splits.reserve(n * M * 4));
+    CK(ctx->b_calls.reserve(n * M * 4));
+    CK(ctx->b_cmd.reserve(n * (M + 1) * 4));
+    CK(ctx->b_nsplits.reserve(n * 4));
+    CK(ctx->b_ncalls.reserve(n * 4));
+    CK(ctx->b_rowoff.reserve((n + 1) * 8));
+    CK(ctx->b_cref.reserve(max_rows * eimp_W(K) * 8));
+    CK(ctx->b_count0.reserve(max_rows * 4));
+    CK(ctx->b_pbwt.reserve(2 * max_rows * eimp_kw(K) * 4));
+    CK(ctx->b_arena.reserve(n * beam_arena_bytes(bp, (int)M)));
+    CK(ctx->skipbuf.reserve(sizeof(int)));
+    ctx->rows_cap = (int64_t)max_rows;
+    return 0;
+}
 
 int eimp_phase_targets_dev(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt,
                            uint64_t *d_mats, uint64_t *d_pats, float *d_dos_mats, float *d_dos_pats,
@@ -670,9 +778,9 @@ extern "C" int eimp_gpu_run_cref_pbwt(eimp_ctx *ctx, size_t ntgt, const uint64_t
     CK(cudaMemcpyAsync(ctx->g_rowoff.p, ro.data(), (ntgt + 1) * 8, cudaMemcpyHostToDevice, st));
     LAUNCH(launch_cref(ctx->g_gt.as<uint8_t>(), (int)ntgt, (int)M, ctx->g_hapT.as<uint64_t>(), (int)wM, (int)nh,
                        ctx->g_bh.as<int32_t>(), (int)K, ctx->g_splits.as<int32_t>(), ctx->g_nsplits.as<int32_t>(),
-                       ctx->g_rowoff.as<int64_t>(), ctx->g_cref.as<uint64_t>(), st));
+                       ctx->g_rowoff.as<int64_t>(), ctx->g_cref.as<uint64_t>(), nullptr, st));
     LAUNCH(launch_pbwt(ctx->g_cref.as<uint64_t>(), ctx->g_count0.as<int32_t>(), ctx->g_rowoff.as<int64_t>(), (int)ntgt,
-                       (int)K, ctx->g_pbwt.as<uint32_t>(), stride, 1, st));
+                       (int)K, ctx->g_pbwt.as<uint32_t>(), stride, 1, nullptr, st));
     for (size_t t = 0; t < ntgt; t++) {
         size_t nr = (size_t)(ro[t + 1] - ro[t]);
         CK(cudaMemcpyAsync(cPBWT[t], ctx->g_pbwt.as<uint32_t>() + 2 * (size_t)ro[t] * stride, 2 * nr * stride * 4,

@@ -1206,7 +1206,8 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS) beam_kernel(
     const int32_t *__restrict__ count0, const int64_t *__restrict__ rowoff, uint8_t *__restrict__ arena,
     size_t arena_bytes, uint64_t *__restrict__ mats, uint64_t *__restrict__ pats, float *__restrict__ dmat,
     float *__restrict__ dpat, float *__restrict__ totalconf, int32_t *__restrict__ ncallsites,
-    uint32_t *__restrict__ status) {
+    uint32_t *__restrict__ status, const int *__restrict__ skip) {
+    if (skip && *skip) return;   // the batch exceeds the reserved rows
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int t = blockIdx.x * BEAM_WARPS + wid;
@@ -1445,7 +1446,7 @@ cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt,
                         const int32_t *splits, const int32_t *nsplits, const int32_t *calls, const int32_t *ncalls,
                         const float *cmdiffs, const uint32_t *pbwt, const int32_t *count0, const int64_t *rowoff,
                         void *arena, size_t arena_bytes, uint64_t *mats, uint64_t *pats, float *dmat, float *dpat,
-                        float *totalconf, int32_t *ncallsites, uint32_t *status, cudaStream_t st) {
+                        float *totalconf, int32_t *ncallsites, uint32_t *status, const int *skip, cudaStream_t st) {
     ArenaLayout al = arena_layout(p, M);
     if (arena_bytes < al.total) return cudaErrorInvalidValue;
     const size_t sm = (sizeof(WS) + beam_rows_bytes(p.K) + beam_canon_bytes(al.NH)) * BEAM_WARPS;
@@ -1454,7 +1455,7 @@ cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt,
     int blocks = (ntgt + BEAM_WARPS - 1) / BEAM_WARPS;
     beam_kernel<<<blocks, 32 * BEAM_WARPS, sm, st>>>(p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls,
                                                      cmdiffs, pbwt, count0, rowoff, (uint8_t *)arena, arena_bytes,
-                                                     mats, pats, dmat, dpat, totalconf, ncallsites, status);
+                                                     mats, pats, dmat, dpat, totalconf, ncallsites, status, skip);
     return cudaGetLastError();
 }
 

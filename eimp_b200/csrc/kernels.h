@@ -40,10 +40,14 @@ cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_
 // condensed reference from the haplotype-major reference (nhaps x wM words)
 cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM, int nhaps,
                         const int32_t *besthaps, int K, const int32_t *splits, const int32_t *nsplits,
-                        const int64_t *rowoff, uint64_t *cref, cudaStream_t st);
+                        const int64_t *rowoff, uint64_t *cref, const int *skip, cudaStream_t st);
 // forward and backward PBWT of the condensed references; writes count0 too
 cudaError_t launch_pbwt(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
-                        uint32_t *pbwt, size_t rowstride, int emit_padded, cudaStream_t st);
+                        uint32_t *pbwt, size_t rowstride, int emit_padded, const int *skip, cudaStream_t st);
+// row offsets of the condensed references on the device (exclusive prefix of
+// 2*nsplits+1); sets *skip (and the status flag) when they exceed cap rows
+cudaError_t launch_rowoff(const int32_t *nsplits, int ntgt, int64_t *rowoff, int64_t cap, int *skip,
+                          uint32_t *status, cudaStream_t st);
 
 // ---- beam phasing (beam.cu)
 struct BeamParams {
@@ -59,6 +63,6 @@ cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt,
                         const int32_t *splits, const int32_t *nsplits, const int32_t *calls, const int32_t *ncalls,
                         const float *cmdiffs, const uint32_t *pbwt, const int32_t *count0, const int64_t *rowoff,
                         void *arena, size_t arena_bytes, uint64_t *mats, uint64_t *pats, float *dmat, float *dpat,
-                        float *totalconf, int32_t *ncallsites, uint32_t *status, cudaStream_t st);
+                        float *totalconf, int32_t *ncallsites, uint32_t *status, const int *skip, cudaStream_t st);
 
 }  // namespace eimp

@@ -233,7 +233,9 @@ constexpr int CREF_WARPS = 8;
 __global__ void __launch_bounds__(32 * CREF_WARPS) cref_kernel(
     const uint8_t *__restrict__ gt, int M, const uint64_t *__restrict__ hapmajor, int wM, int nhaps,
     const int32_t *__restrict__ besthaps, int K, const int32_t *__restrict__ splits,
-    const int32_t *__restrict__ nsplits, const int64_t *__restrict__ rowoff, uint64_t *__restrict__ cref) {
+    const int32_t *__restrict__ nsplits, const int64_t *__restrict__ rowoff, uint64_t *__restrict__ cref,
+    const int *__restrict__ skip) {
+    if (skip && *skip) return;   // the batch exceeds the reserved rows
     extern __shared__ uint64_t sm[];
     // the target's homozygous genotypes and its split sites as bit masks
     uint64_t *is0 = sm, *is2 = sm + wM, *ssp = sm + 2 * wM;
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(32 * CREF_WARPS) cref_kernel(
 
 cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM, int nhaps,
                         const int32_t *besthaps, int K, const int32_t *splits, const int32_t *nsplits,
-                        const int64_t *rowoff, uint64_t *cref, cudaStream_t st) {
+                        const int64_t *rowoff, uint64_t *cref, const int *skip, cudaStream_t st) {
     const size_t sm = (size_t)3 * wM * sizeof(uint64_t);
     if (sm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(cref_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -301,7 +303,7 @@ cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapm
     const int wK = (int)eimp_W(K);
     dim3 grid((unsigned)ntgt, (unsigned)((2 * wK + CREF_WARPS - 1) / CREF_WARPS));
     cref_kernel<<<grid, 32 * CREF_WARPS, sm, st>>>(gt, M, hapmajor, wM, nhaps, besthaps, K, splits, nsplits, rowoff,
-                                                   cref);
+                                                   cref, skip);
     return cudaGetLastError();
 }
 
@@ -329,7 +331,8 @@ template <int PW>
 __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__ cref,
                                                     const int64_t *__restrict__ rowoff, int K,
                                                     uint32_t *__restrict__ pbwt, size_t rowstride, int emit_padded,
-                                                    int32_t *__restrict__ count0) {
+                                                    int32_t *__restrict__ count0, const int *__restrict__ skip) {
+    if (skip && *skip) return;   // the batch exceeds the reserved rows
     extern __shared__ __align__(16) uint8_t smem[];
     const int t = blockIdx.x >> 1, dir = blockIdx.x & 1;
     const int wK = (int)eimp_W(K);
@@ -419,23 +422,65 @@ __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__
 
 template <int PW>
 static cudaError_t launch_pbwt_pw(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
-                                  uint32_t *pbwt, size_t rowstride, int emit_padded, cudaStream_t st) {
+                                  uint32_t *pbwt, size_t rowstride, int emit_padded, const int *skip,
+                                  cudaStream_t st) {
     const int wK = (int)eimp_W(K), nwords = (K + 31) / 32;
     const int nwarps = max(4, (nwords + PW - 1) / PW);
     const size_t sm = (size_t)2 * wK * 8 + 32 * 4 + (size_t)2 * K * 2;
     cudaError_t e = cudaFuncSetAttribute(pbwt_kernel<PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    pbwt_kernel<PW><<<2 * ntgt, 32 * nwarps, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0);
+    pbwt_kernel<PW><<<2 * ntgt, 32 * nwarps, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0, skip);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pbwt(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
-                        uint32_t *pbwt, size_t rowstride, int emit_padded, cudaStream_t st) {
+                        uint32_t *pbwt, size_t rowstride, int emit_padded, const int *skip, cudaStream_t st) {
     // the 8-byte pair stores need 8-byte aligned rows
     if (K < 1 || K > 65536 || rowstride % 2) return cudaErrorInvalidValue;
     const int nwords = (K + 31) / 32;
-    if (nwords <= 32 * 32) return launch_pbwt_pw<32>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, st);
-    return launch_pbwt_pw<64>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, st);
+    if (nwords <= 32 * 32)
+        return launch_pbwt_pw<32>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
+    return launch_pbwt_pw<64>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
+}
+
+// ---------------------------------------------------------------------------
+// Row offsets of the batch's condensed references (the exclusive prefix of
+// 2*nsplits+1, GPUHandler.cpp:139-143) computed on the device, so that no
+// host round trip sits between the preparation and the condensed reference.
+// One CTA: per-thread chunk sums, a block scan, then the chunk prefixes.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) rowoff_kernel(const int32_t *__restrict__ nsplits, int ntgt,
+                                                      int64_t *__restrict__ rowoff, int64_t cap, int *__restrict__ skip,
+                                                      uint32_t *__restrict__ status) {
+    __shared__ long long part[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
+    const int per = (ntgt + nt - 1) / nt;
+    const int lo = min(ntgt, tid * per), hi = min(ntgt, lo + per);
+    long long sum = 0;
+    for (int t = lo; t < hi; t++) sum += 2 * (long long)nsplits[t] + 1;
+    long long inc = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) part[warp] = inc;
+    __syncthreads();
+    long long base = 0;
+    for (int q = 0; q < warp; q++) base += part[q];
+    long long run = base + inc - sum;
+    for (int t = lo; t < hi; t++) { rowoff[t] = run; run += 2 * (long long)nsplits[t] + 1; }
+    if (tid == nt - 1) {
+        rowoff[ntgt] = run;
+        const int over = run > cap;
+        *skip = over;
+        if (over) atomicOr(status, (uint32_t)EIMP_ERR_ROWS_OVERFLOW);
+    }
+}
+
+cudaError_t launch_rowoff(const int32_t *nsplits, int ntgt, int64_t *rowoff, int64_t cap, int *skip,
+                          uint32_t *status, cudaStream_t st) {
+    rowoff_kernel<<<1, 1024, 0, st>>>(nsplits, ntgt, rowoff, cap, skip, status);
+    return cudaGetLastError();
 }
 
 }  // namespace eimp

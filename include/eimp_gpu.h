@@ -87,6 +87,19 @@ void *eimp_stream(eimp_ctx *ctx);
 int eimp_set_timing(eimp_ctx *ctx, int on);
 int eimp_phase_stage_ms(eimp_ctx *ctx, float *ms, int n);
 
+/* CUDA-graph form of a batch step (no counterpart in the reference; the
+ * reference launches per block from host threads).  eimp_capture_begin starts
+ * capturing the context's stream; the *_dev entry points called next are
+ * recorded instead of run (their work on the context's second stream joins
+ * the capture through the events that order it); eimp_capture_end
+ * instantiates the graph, and eimp_graph_launch replays it on the context's
+ * stream with the same buffers.  Phasing must run in capacity mode
+ * (eimp_phase_reserve) to be captured: in the default mode it reads the
+ * split counts back to the host to size the condensed reference. */
+int eimp_capture_begin(eimp_ctx *ctx);
+int eimp_capture_end(eimp_ctx *ctx);
+int eimp_graph_launch(eimp_ctx *ctx);
+
 /* ------------------------------------------ GPUEngine drop-in (cref + PBWT) */
 
 /* GPUEngine::initialize (GPUEngine.h:50, GPUEngine.cu:44-96): uploads the typed
@@ -140,6 +153,15 @@ int eimp_phase_cref_pbwt(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt,
 /* Target::phase (Target.cpp:166-289) for a batch of diploid targets: mats/pats
  * ntgt x W(M) words, dos_mats/dos_pats ntgt x M floats, totalconf and
  * ncallsites per target (Target.h:73-74). */
+/* Capacity mode for phasing (no counterpart in the reference): reserves the
+ * batch buffers for up to max_targets targets and max_rows condensed rows
+ * (sum over the targets of 2*S_t+1).  Afterwards the row offsets are computed
+ * on the device, so a phasing call makes no host round trip and can be
+ * captured; a batch that needs more rows skips the condensed reference, the
+ * PBWT and the beam and reports EIMP_E_CAPACITY at the next status check.
+ * max_rows = 0 returns to the default mode. */
+int eimp_phase_reserve(eimp_ctx *ctx, const eimp_phase_params *p, size_t max_targets, size_t max_rows);
+
 int eimp_phase_targets(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *gt,
                        uint64_t *mats, uint64_t *pats, float *dos_mats, float *dos_pats, float *totalconf,
                        int32_t *ncallsites);
