@@ -310,15 +310,17 @@ cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapm
 // ---------------------------------------------------------------------------
 // PBWT::buildComprPBWT (PBWT.cpp:207-285) of each target's condensed
 // reference, forward and backward (rows in sweep order), one CTA per (target,
-// direction).  Each warp owns PW consecutive 32-haplotype blocks of the prefix
-// order, lane j of the warp the j-th block's data word.  Per row: the warp
-// reads the row bits of its blocks in the current prefix order (a ballot per
-// block), scans the blocks' zero counts with shuffles and publishes its total;
-// after one barrier it places its haplotypes in the next prefix order (zeros
-// first, stable) and writes its compressed words [data, zeros through the
-// word] as one 8-byte store per lane.  Prefix arrays are 16-bit (K <= 65536).
-// The next row is copied into shared memory asynchronously while the current
-// one is processed.  The forward CTA also writes each row's zero count.
+// direction).  Each thread owns WPT consecutive 32-position words of the
+// prefix order.  Per row: the thread gathers its words' bits in the current
+// prefix order (a word is the row format's data word, the tail padded with
+// ones) and counts their zeros; one block scan gives every word's zeros
+// before it; the thread writes its [data, zeros through the word] pairs and
+// places its haplotypes in the next prefix order (zeros first, stable).  The
+// prefix arrays are 16-bit (K <= 65536) and XOR-swizzled within each 32-entry
+// block, so that the 32 lanes reading position j of their own words hit 32
+// different banks.  The next row is copied into shared memory asynchronously
+// while the current one is processed.  The forward CTA also writes each
+// row's zero count.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -327,7 +329,10 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int PW>
+// position p of the prefix order -> its slot in the swizzled array
+__device__ __forceinline__ int pswz(int p) { return p ^ ((p >> 5) & 31); }
+
+template <int WPT>
 __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__ cref,
                                                     const int64_t *__restrict__ rowoff, int K,
                                                     uint32_t *__restrict__ pbwt, size_t rowstride, int emit_padded,
@@ -337,99 +342,108 @@ __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__
     const int t = blockIdx.x >> 1, dir = blockIdx.x & 1;
     const int wK = (int)eimp_W(K);
     const int nwords = (K + 31) / 32;
-    const int nwarps = blockDim.x >> 5;
+    const int nthreads = blockDim.x, nwarps = nthreads >> 5;
     uint64_t *rowbuf = reinterpret_cast<uint64_t *>(smem);                 // 2 x wK
     int *wtot = reinterpret_cast<int *>(rowbuf + 2 * wK);                  // 32
-    uint16_t *perm = reinterpret_cast<uint16_t *>(wtot + 32);              // K
-    uint16_t *nperm = perm + K;                                            // K
+    uint16_t *perm = reinterpret_cast<uint16_t *>(wtot + 32);              // nwords*32, swizzled
+    uint16_t *nperm = perm + nwords * 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t r0 = rowoff[t];
     const int Mp = (int)(rowoff[t + 1] - r0);
     const uint64_t *rows = cref + (size_t)r0 * wK;
     uint32_t *out = pbwt + (size_t)(2 * r0 + (dir ? Mp : 0)) * rowstride;
-    const int w0 = warp * PW;                      // the warp's first block
-    const int nb = max(0, min(PW, nwords - w0));   // the warp's blocks
-    const unsigned lt = (1u << lane) - 1u;
+    const int w0 = tid * WPT;                      // the thread's first word
     const int nchunk = wK / 2;                     // 16-byte pieces of a row
-    for (int i = tid; i < K; i += blockDim.x) perm[i] = (uint16_t)i;
+    // identity order; the padding positions past K hold haplotype 0 in both
+    // arrays (never written later, never used for a bit)
+    for (int i = tid; i < nwords * 32; i += nthreads) perm[pswz(i)] = nperm[pswz(i)] = (uint16_t)(i < K ? i : 0);
     if (Mp > 0) {
         const uint64_t *src = rows + (size_t)(dir ? Mp - 1 : 0) * wK;
-        for (int c = tid; c < nchunk; c += blockDim.x) cp_async16(rowbuf + 2 * c, src + 2 * c);
+        for (int c = tid; c < nchunk; c += nthreads) cp_async16(rowbuf + 2 * c, src + 2 * c);
     }
     cp_async_commit();
     for (int midx = 0; midx < Mp; midx++) {
         const int m = dir ? Mp - 1 - midx : midx;
-        const uint64_t *row = rowbuf + (midx & 1) * wK;
+        const uint32_t *row = reinterpret_cast<const uint32_t *>(rowbuf + (midx & 1) * wK);
         cp_async_wait_all();
         __syncthreads();   // this row has landed; the previous row's placements are done
         if (midx + 1 < Mp) {
             const uint64_t *src = rows + (size_t)(dir ? m - 1 : m + 1) * wK;
             uint64_t *dst = rowbuf + ((midx + 1) & 1) * wK;
-            for (int c = tid; c < nchunk; c += blockDim.x) cp_async16(dst + 2 * c, src + 2 * c);
+            for (int c = tid; c < nchunk; c += nthreads) cp_async16(dst + 2 * c, src + 2 * c);
         }
         cp_async_commit();
-        // data words in the current prefix order
-        uint16_t hreg[PW];
-        unsigned myb = 0;
+        // the thread's data words in the current prefix order
+        uint32_t word[WPT];
+        int zsum = 0;
 #pragma unroll
-        for (int q = 0; q < PW; q++) {
-            if (q < nb) {
-                const int i = (w0 + q) * 32 + lane;
-                int bit = 1;   // tail padded with ones (PBWT.cpp:261-267)
-                hreg[q] = 0;
-                if (i < K) {
-                    const int h = perm[i];
-                    hreg[q] = (uint16_t)h;
-                    bit = (int)((row[h >> 6] >> (h & 63)) & 1ull);
+        for (int q = 0; q < WPT; q++) {
+            const int w = w0 + q;
+            uint32_t b = ~0u;
+            if (w < nwords) {
+                const uint16_t *pw = perm + w * 32;
+                const int key = w & 31;
+                b = 0u;
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const int h = pw[j ^ key];
+                    const uint32_t bit = (w * 32 + j < K) ? (row[h >> 5] >> (h & 31)) & 1u : 1u;
+                    b |= bit << j;
                 }
-                const unsigned b = __ballot_sync(0xffffffffu, bit);
-                if (lane == q) myb = b;
+                zsum += __popc(~b);
             }
+            word[q] = b;
         }
-        // zeros per block, scanned over the warp's blocks
-        const int zc = lane < nb ? __popc(~myb) : 0;
-        int inc = zc;
+        // zeros before the thread's words: warp scan, then the warps' totals
+        int inc = zsum;
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, inc, o);
             if (lane >= o) inc += y;
         }
         if (lane == 31) wtot[warp] = inc;
         __syncthreads();
-        int zw = 0, cnt0 = 0;
-        for (int q = 0; q < nwarps; q++) { const int v = wtot[q]; cnt0 += v; if (q < warp) zw += v; }
-        const int excl = zw + inc - zc;   // zeros before this lane's block
-#pragma unroll
-        for (int q = 0; q < PW; q++) {
-            if (q < nb) {
-                const unsigned b = __shfl_sync(0xffffffffu, myb, q);
-                const int zb = __shfl_sync(0xffffffffu, excl, q);
-                const int i = (w0 + q) * 32 + lane;
-                if (i < K) {
-                    const int zi = zb + __popc(~b & lt);   // zeros before position i
-                    nperm[((b >> lane) & 1u) ? cnt0 + (i - zi) : zi] = hreg[q];
-                }
-            }
-        }
+        int zb = inc - zsum, cnt0 = 0;
+        for (int q = 0; q < nwarps; q++) { const int v = wtot[q]; cnt0 += v; if (q < warp) zb += v; }
         uint32_t *o = out + (size_t)midx * rowstride;
-        if (lane < nb) reinterpret_cast<uint2 *>(o)[w0 + lane] = make_uint2(myb, (uint32_t)(excl + zc));
+#pragma unroll
+        for (int q = 0; q < WPT; q++) {
+            const int w = w0 + q;
+            if (w >= nwords) continue;
+            const uint32_t b = word[q];
+            const uint16_t *pw = perm + w * 32;
+            const int key = w & 31;
+            int z = zb;   // zeros before position w*32 + j
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const int p = w * 32 + j;
+                if (p < K) {
+                    const int h = pw[j ^ key];
+                    const int dst = ((b >> j) & 1u) ? cnt0 + (p - z) : z;
+                    nperm[pswz(dst)] = (uint16_t)h;
+                }
+                z += (int)((~b >> j) & 1u);
+            }
+            reinterpret_cast<uint2 *>(o)[w] = make_uint2(b, (uint32_t)z);
+            zb = z;
+        }
         if (emit_padded)
-            for (size_t j = 2 * (size_t)nwords + tid; j < rowstride; j += blockDim.x) o[j] = 0u;
-        if (dir == 0 && tid == 0) count0[r0 + m] = cnt0;
+            for (size_t jj = 2 * (size_t)nwords + tid; jj < rowstride; jj += nthreads) o[jj] = 0u;
+        if (dir == 0 && tid == nthreads - 1) count0[r0 + m] = cnt0;
         uint16_t *tp = perm; perm = nperm; nperm = tp;
     }
     cp_async_wait_all();
 }
 
-template <int PW>
-static cudaError_t launch_pbwt_pw(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
-                                  uint32_t *pbwt, size_t rowstride, int emit_padded, const int *skip,
-                                  cudaStream_t st) {
+template <int WPT>
+static cudaError_t launch_pbwt_w(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
+                                 uint32_t *pbwt, size_t rowstride, int emit_padded, const int *skip,
+                                 cudaStream_t st) {
     const int wK = (int)eimp_W(K), nwords = (K + 31) / 32;
-    const int nwarps = max(4, (nwords + PW - 1) / PW);
-    const size_t sm = (size_t)2 * wK * 8 + 32 * 4 + (size_t)2 * K * 2;
-    cudaError_t e = cudaFuncSetAttribute(pbwt_kernel<PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int nthreads = ((nwords + WPT - 1) / WPT + 31) / 32 * 32;
+    const size_t sm = (size_t)2 * wK * 8 + 32 * 4 + (size_t)2 * nwords * 32 * 2;
+    cudaError_t e = cudaFuncSetAttribute(pbwt_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    pbwt_kernel<PW><<<2 * ntgt, 32 * nwarps, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0, skip);
+    pbwt_kernel<WPT><<<2 * ntgt, nthreads, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0, skip);
     return cudaGetLastError();
 }
 
@@ -438,9 +452,8 @@ cudaError_t launch_pbwt(const uint64_t *cref, int32_t *count0, const int64_t *ro
     // the 8-byte pair stores need 8-byte aligned rows
     if (K < 1 || K > 65536 || rowstride % 2) return cudaErrorInvalidValue;
     const int nwords = (K + 31) / 32;
-    if (nwords <= 32 * 32)
-        return launch_pbwt_pw<32>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
-    return launch_pbwt_pw<64>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
+    if (nwords <= 1024) return launch_pbwt_w<1>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
+    return launch_pbwt_w<2>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
 }
 
 // ---------------------------------------------------------------------------
