@@ -94,7 +94,7 @@ int main(int argc, char **argv) {
                                   ncalls.data() + t, cmd.data() + (size_t)t * (M + 1), pbwt.data() + 2 * r0 * kw,
                                   count0.data() + r0, &zero, arena, al.total, mats.data() + (size_t)t * wM,
                                   pats.data() + (size_t)t * wM, dm.data() + (size_t)t * M, dp.data() + (size_t)t * M,
-                                  tc.data() + t, nc.data() + t, &status);
+                                  tc.data() + t, nc.data() + t, &status, nullptr);
             });
         for (auto &x : lanes) x.join();
         st[t] = status;
