@@ -161,28 +161,47 @@ struct SNode {
     unsigned char pad;
 };
 
-struct SmmWarpSmem {
-    SNode A[SMM_NODES];     // tree in pre-order
-    SNode B[SMM_NODES];     // tree being built
-    int4 mp[SMM_NODES];     // mappings (to0, to1); reused by the merge pass
-    short idx0[SMM_NODES];  // position of a node's 0-extension in B (-1: none)
-    short idx1[SMM_NODES];  // position of a node's 1-extension in B (-1: none)
+template <int NODES> struct SmmWarpSmem {
+    SNode A[NODES];         // tree in pre-order
+    SNode B[NODES];         // tree being built
+    int4 mp[NODES];         // mappings (to0, to1); reused by the merge pass
+    short idx0[NODES];      // position of a node's 0-extension in B (-1: none)
+    short idx1[NODES];      // position of a node's 1-extension in B (-1: none)
 };
 
 __device__ __forceinline__ int de_depth(int de) { return de & 0xffffff; }
 __device__ __forceinline__ int de_err(int de) { return (int)((unsigned)de >> 24); }
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
 
-__global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
+// A match search runs first with a small node pool (many warps per SM); a
+// haplotype whose tree outgrows it ends with its match count set to
+// SMM_RETRY and no error, and a second launch with a large pool (one warp
+// per CTA) redoes exactly those haplotypes.  Only a tree that outgrows the
+// large pool too is an error (EIMP_ERR_NODE_OVERFLOW).  set-maximal errors
+// make the trees grow: on a 5000-haplotype panel at 2000 sites the largest
+// trees held 148, 718, 1733 and 3093 nodes at 0, 1, 2 and 3 errors.
+constexpr int SMM_RETRY = -2;
+__device__ __forceinline__ void smm_finish(int lane, uint32_t err, bool retry_pass, int nres, int *nmatch, int hap,
+                                           uint32_t *status) {
+    if (lane) return;
+    if (!err) { nmatch[hap] = nres; return; }
+    if (!retry_pass && err == EIMP_ERR_NODE_OVERFLOW) { nmatch[hap] = SMM_RETRY; return; }
+    nmatch[hap] = -1;
+    atomicOr(status, err);
+}
+
+template <int NODES, int WARPS, bool RETRY>
+__global__ void __launch_bounds__(WARPS * 32) smm_kernel(
     const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
     const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
     int setmaxerrors, int4 *__restrict__ matches, int cap, int *__restrict__ nmatch,
     uint32_t *__restrict__ status) {
     extern __shared__ uint8_t smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int hap = blockIdx.x * SMM_WARPS + wid;
+    const int hap = blockIdx.x * WARPS + wid;
     if (hap >= nhaps) return;
-    SmmWarpSmem &S = reinterpret_cast<SmmWarpSmem *>(smem_raw)[wid];
+    if (RETRY && nmatch[hap] != SMM_RETRY) return;
+    SmmWarpSmem<NODES> &S = reinterpret_cast<SmmWarpSmem<NODES> *>(smem_raw)[wid];
     const uint8_t *g = gt + (size_t)(hap >> 1) * M;
     const uint64_t *hw = phased + (size_t)hap * wM;
     int4 *out = matches + (size_t)hap * cap;
@@ -241,7 +260,7 @@ __global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
             break;
         }
         const int nb = 1 + cnt0 + cnt1;
-        if (nb > SMM_NODES) { err |= EIMP_ERR_NODE_OVERFLOW; break; }
+        if (nb > NODES) { err |= EIMP_ERR_NODE_OVERFLOW; break; }
         // pass 2: build B = [new root] ++ 0-tree ++ 1-tree
         for (int i = lane; i < n; i += 32) {
             const SNode v = S.A[i];
@@ -327,10 +346,200 @@ __global__ void __launch_bounds__(SMM_WARPS * 32) smm_kernel(
         td = md;
     }
     for (int o = 16; o; o >>= 1) err |= __shfl_xor_sync(FULL, err, o);
-    if (lane == 0) {
-        nmatch[hap] = err ? -1 : nres;
-        if (err) atomicOr(status, err);
+    smm_finish(lane, err, RETRY, nres, nmatch, hap, status);
+}
+
+// ---------------------------------------------------------------------------
+// The same set-maximal match search with a compact tree (typed sites < 65536):
+// structure of arrays with the depth in 16 bits, packed with the parent index
+// and side, and the errors in a byte -- 30 bytes per node instead of 52, so
+// that a warp holds 15.5 KB of shared memory and 2000 target haplotypes fit
+// on the device at once (14 warps per SM instead of 8).  The mapped intervals
+// are not kept in an array of their own: pass 1 writes a node's 0-extension
+// interval straight into the new tree and its 1-extension interval over the
+// node's own interval, which pass 2 reads back; the merge pass keeps its
+// bookkeeping in the extension-index arrays.  Same algorithm and output as
+// smm_kernel above.
+// ---------------------------------------------------------------------------
+template <int NODES> struct SmmTree {
+    int l[NODES], r[NODES];
+    unsigned dps[NODES];              // depth | (parent + 1) << 16 | side << 31
+    unsigned char e[NODES];           // errors
+};
+template <int NODES> struct SmmWarpSmemC {
+    SmmTree<NODES> A, B;
+    short idx0[NODES];                // extension positions; kept positions in the merge pass
+    short idx1[NODES];                // extension positions; run starts in the merge pass
+    unsigned cflag[NODES / 16];       // 2 bits per node: which children it has
+};
+
+__device__ __forceinline__ int dps_depth(unsigned x) { return (int)(x & 0xffffu); }
+__device__ __forceinline__ int dps_parent(unsigned x) { return (int)((x >> 16) & 0x7fffu) - 1; }
+__device__ __forceinline__ int dps_side(unsigned x) { return (int)(x >> 31); }
+__device__ __forceinline__ unsigned dps_make(int depth, int parent, int side) {
+    return (unsigned)depth | ((unsigned)(parent + 1) << 16) | ((unsigned)side << 31);
+}
+
+template <int NODES, int WARPS, bool RETRY>
+__global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
+    const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
+    const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
+    int setmaxerrors, int4 *__restrict__ matches, int cap, int *__restrict__ nmatch,
+    uint32_t *__restrict__ status) {
+    extern __shared__ uint8_t smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int hap = blockIdx.x * WARPS + wid;
+    if (hap >= nhaps) return;
+    if (RETRY && nmatch[hap] != SMM_RETRY) return;
+    SmmWarpSmemC<NODES> &S = reinterpret_cast<SmmWarpSmemC<NODES> *>(smem_raw)[wid];
+    SmmTree<NODES> &A = S.A, &B = S.B;
+    const uint8_t *g = gt + (size_t)(hap >> 1) * M;
+    const uint64_t *hw = phased + (size_t)hap * wM;
+    int4 *out = matches + (size_t)hap * cap;
+    const size_t kw = eimp_kw(K);
+    const unsigned FULL = 0xffffffffu;
+
+    // missingness > 50 %: no matches (TargetImp.cpp:79-80)
+    int nmiss = 0;
+    for (int m = lane; m < M; m += 32) nmiss += g[m] == 3;
+    for (int o = 16; o; o >>= 1) nmiss += __shfl_xor_sync(FULL, nmiss, o);
+    if (nmiss > M / 2) { if (lane == 0) nmatch[hap] = 0; return; }
+
+    uint32_t err = 0;
+    int n = 1, nres = 0, td = 0;
+    if (lane == 0) { A.l[0] = 0; A.r[0] = K - 1; A.dps[0] = dps_make(0, -1, 0); A.e[0] = 0; }
+    __syncwarp();
+
+    for (int m = 0; m <= M; m++) {
+        const bool final = (m == M);   // TargetImp.cpp:144: erase pass, every node reports
+        const int curr = final ? 0 : bit_at(hw, m);
+        const int missing = final ? 0 : (g[m] == 3);
+        const uint32_t *crow = compr + (size_t)(final ? 0 : m) * kw;
+        const int c0 = final ? 0 : count0[m];
+        // pass 1: mappings, extension flags, matches of nodes that end here;
+        // the 0-extension interval goes to its place in B, the 1-extension
+        // interval over the node's own
+        int cnt0 = 0, cnt1 = 0, newcount = 0;
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            bool e0 = false, e1 = false, dead = false;
+            int l0 = 0, r0 = -1, l1 = 0, r1 = -1, vl = 0, vr = -1, d = 0;
+            if (i < n) {
+                vl = A.l[i]; vr = A.r[i];
+                d = dps_depth(A.dps[i]);
+                const int ne = A.e[i];
+                if (!final) pbwt_map(crow, c0, vl, vr, l0, r0, l1, r1);
+                e0 = l0 <= r0 && (missing || !curr || ne < setmaxerrors);
+                e1 = l1 <= r1 && (missing || curr || ne < setmaxerrors);
+                dead = !e0 && !e1 && d == td && td > 0;
+            }
+            const unsigned b0 = __ballot_sync(FULL, e0), b1 = __ballot_sync(FULL, e1), bd = __ballot_sync(FULL, dead);
+            if (i < n) {
+                const int p0 = e0 ? 1 + cnt0 + __popc(b0 & lanemask_lt()) : -1;
+                S.idx0[i] = (short)p0;
+                S.idx1[i] = e1 ? (short)(cnt1 + __popc(b1 & lanemask_lt())) : (short)-1;   // offset added below
+                if (p0 >= 0 && p0 < NODES) { B.l[p0] = l0; B.r[p0] = r0; }
+                A.l[i] = l1; A.r[i] = r1;
+            }
+            if (dead) {
+                const int pos = nres + newcount + __popc(bd & lanemask_lt());
+                if (pos < cap) out[pos] = make_int4(m - d, m, vl, vr);
+                else err |= EIMP_ERR_MATCH_OVERFLOW;
+            }
+            cnt0 += __popc(b0); cnt1 += __popc(b1); newcount += __popc(bd);
+        }
+        __syncwarp();
+        if (final) {
+            if (nres + newcount <= cap) nres += newcount;
+            break;
+        }
+        const int nb = 1 + cnt0 + cnt1;
+        if (nb > NODES) { err |= EIMP_ERR_NODE_OVERFLOW; break; }
+        // pass 2: the rest of B = [new root] ++ 0-tree ++ 1-tree
+        for (int i = lane; i < n; i += 32) {
+            const unsigned vd = A.dps[i];
+            const int d = dps_depth(vd) + 1, ne = A.e[i];
+            const int vp = dps_parent(vd), vs = dps_side(vd);
+            const int p0 = S.idx0[i], p1 = S.idx1[i];
+            if (p0 >= 0) {
+                B.dps[p0] = dps_make(d, i == 0 ? 0 : S.idx0[vp], i == 0 ? 0 : vs);
+                B.e[p0] = (unsigned char)((curr && !missing) ? ne + 1 : ne);
+            }
+            if (p1 >= 0) {
+                const int q = 1 + cnt0 + p1;
+                B.l[q] = A.l[i]; B.r[q] = A.r[i];
+                B.dps[q] = dps_make(d, i == 0 ? 0 : 1 + cnt0 + S.idx1[vp], i == 0 ? 1 : vs);
+                B.e[q] = (unsigned char)((!curr && !missing) ? ne + 1 : ne);
+            }
+        }
+        if (lane == 0) { B.l[0] = 0; B.r[0] = K - 1; B.dps[0] = dps_make(0, -1, 0); B.e[0] = 0; }
+        for (int q = lane; q < (nb + 15) / 16; q += 32) S.cflag[q] = 0u;
+        __syncwarp();
+        // pass 3: merges (TargetImp.cpp:405-432).  Child flags first.
+        for (int u = 1 + lane; u < nb; u += 32) {
+            const unsigned x = B.dps[u];
+            const int pa = dps_parent(x);
+            atomicOr(&S.cflag[pa >> 4], (1u << dps_side(x)) << ((pa & 15) * 2));
+        }
+        __syncwarp();
+        // removal flags, kept-position scan (-> idx0, -1 when removed), start
+        // of each removed run (-> idx1)
+        int kept = 0, laststart = -1;
+        for (int base = 0; base < nb; base += 32) {
+            const int v = base + lane;
+            bool rm = false;
+            if (v >= 1 && v < nb) {
+                const unsigned cf = (S.cflag[v >> 4] >> ((v & 15) * 2)) & 3u;
+                if (cf == 1u || cf == 2u)   // exactly one child: the next entry
+                    rm = B.l[v] == B.l[v + 1] && B.r[v] == B.r[v + 1] && B.e[v] == B.e[v + 1];
+            }
+            const unsigned brm = __ballot_sync(FULL, rm);
+            // a removed run starts where the previous entry is kept
+            const unsigned prevrm = (brm << 1) | (base > 0 ? (unsigned)(S.idx0[base - 1] < 0) : 0u);
+            const bool start = rm && !((prevrm >> lane) & 1u);
+            const unsigned bst = __ballot_sync(FULL, start);
+            const unsigned upto = bst & (lanemask_lt() | (1u << lane));
+            const int ls = upto ? base + (31 - __clz(upto)) : laststart;
+            const bool keep = v < nb && !rm;
+            const unsigned bk = __ballot_sync(FULL, keep);
+            __syncwarp();   // every lane has read idx0[base - 1]
+            if (v < nb) {
+                S.idx0[v] = keep ? (short)(kept + __popc(bk & lanemask_lt())) : (short)-1;
+                S.idx1[v] = (short)ls;
+            }
+            kept += __popc(bk);
+            if (bst) laststart = base + (31 - __clz(bst));
+            __syncwarp();
+        }
+        // compact into A with remapped parents
+        for (int u = lane; u < nb; u += 32) {
+            const int np = S.idx0[u];
+            if (np < 0) continue;
+            unsigned x = B.dps[u];
+            if (u > 0) {
+                int p = dps_parent(x), side = dps_side(x);
+                if (S.idx0[p] < 0) {   // parent removed: take the place of its run's first node
+                    const int q = S.idx1[p];
+                    const unsigned xq = B.dps[q];
+                    p = dps_parent(xq);
+                    side = dps_side(xq);
+                }
+                x = dps_make(dps_depth(x), S.idx0[p], side);
+            }
+            A.l[np] = B.l[u]; A.r[np] = B.r[u]; A.dps[np] = x; A.e[np] = B.e[u];
+        }
+        __syncwarp();
+        n = kept;
+        int md = 0;
+        for (int i = lane; i < n; i += 32) md = max(md, dps_depth(A.dps[i]));
+        for (int o = 16; o; o >>= 1) md = max(md, __shfl_xor_sync(FULL, md, o));
+        // TargetImp.cpp:132-136: the site's matches are set-maximal only if no
+        // longer path is still alive
+        if (newcount && td >= md && nres + newcount <= cap) nres += newcount;
+        td = md;
     }
+    for (int o = 16; o; o >>= 1) err |= __shfl_xor_sync(FULL, err, o);
+    smm_finish(lane, err, RETRY, nres, nmatch, hap, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -478,16 +687,38 @@ cudaError_t launch_transpose(const uint64_t *src, size_t rows, size_t srcw, uint
     return cudaGetLastError();
 }
 
+template <class Smem, class Kern>
+static cudaError_t smm_launch(Kern kern, int warps, const uint32_t *compr, const int32_t *count0, int M, int K,
+                              const uint64_t *phased, int wM, const uint8_t *gt, int nhaps, int setmaxerrors,
+                              int4 *matches, int cap, int *nmatch, uint32_t *status, cudaStream_t st) {
+    const size_t sm = sizeof(Smem) * warps;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    const int blocks = (nhaps + warps - 1) / warps;
+    kern<<<blocks, warps * 32, sm, st>>>(compr, count0, M, K, phased, wM, gt, nhaps, setmaxerrors, matches, cap,
+                                        nmatch, status);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
                        const uint8_t *gt, int nhaps, int setmaxerrors, int4 *matches, int cap, int *nmatch,
                        uint32_t *status, cudaStream_t st) {
-    size_t sm = sizeof(SmmWarpSmem) * SMM_WARPS;
-    cudaError_t e = cudaFuncSetAttribute(smm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e;
+    if (M < 65536) {   // depths fit the compact tree
+        e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false>, SMMC_WARPS,
+                                                compr, count0, M, K, phased, wM, gt, nhaps, setmaxerrors, matches,
+                                                cap, nmatch, status, st);
+        if (e != cudaSuccess) return e;
+        return smm_launch<SmmWarpSmemC<SMM_NODES_RETRY>>(smm_compact_kernel<SMM_NODES_RETRY, 1, true>, 1, compr,
+                                                         count0, M, K, phased, wM, gt, nhaps, setmaxerrors,
+                                                         matches, cap, nmatch, status, st);
+    }
+    e = smm_launch<SmmWarpSmem<SMM_NODES>>(smm_kernel<SMM_NODES, SMM_WARPS, false>, SMM_WARPS, compr, count0, M, K,
+                                           phased, wM, gt, nhaps, setmaxerrors, matches, cap, nmatch, status, st);
     if (e != cudaSuccess) return e;
-    int blocks = (nhaps + SMM_WARPS - 1) / SMM_WARPS;
-    smm_kernel<<<blocks, SMM_WARPS * 32, sm, st>>>(compr, count0, M, K, phased, wM, gt, nhaps, setmaxerrors,
-                                                   matches, cap, nmatch, status);
-    return cudaGetLastError();
+    return smm_launch<SmmWarpSmem<SMM_NODES_RETRY>>(smm_kernel<SMM_NODES_RETRY, 1, true>, 1, compr, count0, M, K,
+                                                    phased, wM, gt, nhaps, setmaxerrors, matches, cap, nmatch,
+                                                    status, st);
 }
 
 cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,

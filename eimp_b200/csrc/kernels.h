@@ -5,10 +5,13 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-// set-maximal match search: warps (target haplotypes) per CTA and the size of
-// the per-warp match-tree node pool in shared memory
+// set-maximal match search: warps (target haplotypes) per CTA of the wide
+// and the compact kernel, and the per-warp match-tree node pools in shared
+// memory of the first launch and of the retry launch (one warp per CTA)
 #define SMM_WARPS 4
+#define SMMC_WARPS 2
 #define SMM_NODES 512
+#define SMM_NODES_RETRY 4096
 // beam phasing: warps (targets) per CTA
 #define BEAM_WARPS 4
 

@@ -116,3 +116,71 @@ def test_imputation_vs_oracle_cfg1_sample(ctx):
         ob, od, oi = R.impute(om, ap, panel.sitemajor, tg.typed, panel.af, panel.nhaps, miss, phased[h])
         np.testing.assert_array_equal(dos[h], od)
         np.testing.assert_array_equal(bits[h], ob)
+
+
+@pytest.mark.parametrize("setmaxerrors", [1, 2, 3])
+def test_setmaxerrors_vs_oracle_cfg1(ctx, setmaxerrors):
+    """Set-maximal matches with tolerated errors (--setmaxerrors): the match
+    trees grow past the first launch's node pool (up to 718, 1733 and 3093
+    nodes at 1, 2 and 3 errors on this panel) and those haplotypes are redone
+    by the retry launch.  Matches and dosages bit-exact against the oracle."""
+    from eimp_b200 import synth
+    from eimp_b200.engine import PBWTImputer
+    from eimp_b200.synth import typed_views
+    from oracle import restate as R
+    panel, groups = synth.generate("cfg1")
+    tg = groups[0]
+    nt = 16
+    _, sm, _ = typed_views(panel, tg.typed)
+    M = len(tg.typed)
+    phased = pack_rows(tg.truth[:2 * nt], W(M))
+    imp = PBWTImputer(ctx, panel.sitemajor, panel.af, tg.typed, sm, panel.nhaps, setmaxerrors=setmaxerrors)
+    imp.prepareImputation(phased, tg.gt[:nt])
+    bits, dos = imp.impute_window(0, panel.nsites)
+    compr, c0, ap = R.pbwt(sm, panel.nhaps, absperm=True)
+    for h in range(2 * nt):
+        miss = np.where(tg.gt[h // 2] == 3)[0].astype(np.int64)
+        om = R.smmatches(compr, c0, M, panel.nhaps, phased[h], miss, setmaxerrors)
+        np.testing.assert_array_equal(imp.matches(h).astype(np.int64), om)
+        ob, od, oi = R.impute(om, ap, panel.sitemajor, tg.typed, panel.af, panel.nhaps, miss, phased[h])
+        np.testing.assert_array_equal(dos[h], od)
+        np.testing.assert_array_equal(bits[h], ob)
+
+
+def test_many_typed_sites_wide_tree(ctx):
+    """70000 typed sites (more than the compact tree's 16-bit depths hold):
+    the match search runs on the wide-tree kernel.  Panel of 512 haplotypes
+    copied in segments from 40 founders with 0.2 % mutations; targets copied
+    the same way, 2 % of their genotypes missing.  Matches and dosages
+    bit-exact against the oracle."""
+    from eimp_b200.engine import PBWTImputer
+    from oracle import restate as R
+    rng = np.random.default_rng(70000)
+    M, K, nt, nf, seg = 70000, 512, 3, 40, 2500
+    founders = (rng.random((nf, M)) < rng.beta(0.5, 0.5, M)).astype(np.uint8)
+
+    def mosaic(n):
+        src = rng.integers(0, nf, (n, (M + seg - 1) // seg)).repeat(seg, axis=1)[:, :M]
+        h = founders[src, np.arange(M)]
+        return h ^ (rng.random((n, M)) < 0.002).astype(np.uint8)
+
+    ref = mosaic(K)
+    tgt = mosaic(2 * nt)
+    gt = (tgt[0::2] + tgt[1::2]).astype(np.uint8)
+    gt[rng.random(gt.shape) < 0.02] = 3
+    sm = pack_rows(ref.T.copy(), W(K))
+    af = ref.mean(axis=0).astype(np.float32)
+    typed = np.arange(M, dtype=np.int64)
+    phased = pack_rows(tgt, W(M))
+    imp = PBWTImputer(ctx, sm, af, typed, sm, K)
+    imp.prepareImputation(phased, gt)
+    bits, dos = imp.impute_window(0, M)
+    compr, c0, ap = R.pbwt(sm, K, absperm=True)
+    for h in range(2 * nt):
+        miss = np.where(gt[h // 2] == 3)[0].astype(np.int64)
+        om = R.smmatches(compr, c0, M, K, phased[h], miss)
+        assert len(om) > 0
+        np.testing.assert_array_equal(imp.matches(h).astype(np.int64), om)
+        ob, od, oi = R.impute(om, ap, sm, typed, af, K, miss, phased[h])
+        np.testing.assert_array_equal(dos[h], od)
+        np.testing.assert_array_equal(bits[h], ob)

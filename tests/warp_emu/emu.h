@@ -11,7 +11,7 @@
 // or divergence instead of hiding behind lock-step execution.
 #pragma once
 #include <atomic>
-#include <barrier>
+#include <sched.h>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -44,8 +44,25 @@ inline int4 make_int4(int x, int y, int z, int w) { return int4{x, y, z, w}; }
 
 extern thread_local dim3 threadIdx, blockIdx;
 
+// Barrier of the 32 lane threads: the last to arrive opens the next
+// generation; the others yield the core while they wait (lanes outnumber the
+// cores, and a futex wake-up of 31 threads per collective costs far more).
+struct EmuBarrier {
+    std::atomic<int> count{0};
+    std::atomic<unsigned> gen{0};
+    void arrive_and_wait() {
+        const unsigned g = gen.load(std::memory_order_acquire);
+        if (count.fetch_add(1, std::memory_order_acq_rel) == 31) {
+            count.store(0, std::memory_order_relaxed);
+            gen.fetch_add(1, std::memory_order_release);
+        } else {
+            while (gen.load(std::memory_order_acquire) == g) sched_yield();
+        }
+    }
+};
+
 struct EmuWarp {
-    std::barrier<> bar{32};
+    EmuBarrier bar;
     uint64_t vals[32];
     int sites[32];
 };
@@ -142,3 +159,4 @@ inline int atomicMin(int *p, int v) {
     return o;
 }
 inline unsigned atomicOr(unsigned *p, unsigned v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }
+inline int atomicOr(int *p, int v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }

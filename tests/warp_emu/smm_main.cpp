@@ -1,0 +1,97 @@
+// Runs the set-maximal match kernels (generated host copy of the match
+// section of eimp_b200/csrc/imp_kernels.cu) one target haplotype at a time
+// under the warp emulator.
+//
+//   smm_emu <dir> <kernel>      kernel 0: smm_kernel, 1: smm_compact_kernel
+//
+// Both launches of launch_smm run: the small node pool first, then the retry
+// pass with the large pool.  <dir> holds the inputs as raw little-endian arrays in the layout of the
+// device buffers: params_i.bin (nhaps, M, K, setmaxerrors, cap), compr.bin
+// (M x kw u32), count0.bin (M i32), phased.bin (nhaps x W(M) u64), gt.bin
+// (nhaps/2 x M u8).  Outputs: o_matches.bin (nhaps x cap int4), o_nmatch.bin,
+// o_status.bin, o_retried.bin (haplotypes redone by the retry pass).  Each haplotype gets its own shared-memory block so the
+// address sanitizer sees accesses past it.  Exit status 3: a divergent warp
+// collective was seen.
+#include "smm_emu.cpp"
+
+#include <string>
+#include <thread>
+#include <vector>
+
+thread_local dim3 threadIdx, blockIdx;
+thread_local EmuWarp *emu_warp;
+thread_local uint8_t *emu_smem_ptr;
+std::atomic<int> emu_divergence{0};
+
+template <class T> static std::vector<T> rd(const std::string &d, const char *name) {
+    const std::string p = d + "/" + name;
+    FILE *f = fopen(p.c_str(), "rb");
+    if (!f) { perror(p.c_str()); exit(1); }
+    fseek(f, 0, SEEK_END);
+    const long n = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    std::vector<T> v(n / sizeof(T));
+    if (fread(v.data(), 1, n, f) != (size_t)n) exit(2);
+    fclose(f);
+    return v;
+}
+template <class T> static void wr(const std::string &d, const char *name, const std::vector<T> &v) {
+    const std::string p = d + "/" + name;
+    FILE *f = fopen(p.c_str(), "wb");
+    if (!f) { perror(p.c_str()); exit(1); }
+    fwrite(v.data(), sizeof(T), v.size(), f);
+    fclose(f);
+}
+
+int main(int argc, char **argv) {
+    if (argc < 3) { fprintf(stderr, "usage: %s <dir> <kernel>\n", argv[0]); return 1; }
+    const std::string d = argv[1];
+    const int which = atoi(argv[2]);
+    const auto pi = rd<int32_t>(d, "params_i.bin");
+    const int nhaps = pi[0], M = pi[1], K = pi[2], sme = pi[3], cap = pi[4];
+    const auto compr = rd<uint32_t>(d, "compr.bin");
+    const auto count0 = rd<int32_t>(d, "count0.bin");
+    const auto phased = rd<uint64_t>(d, "phased.bin");
+    const auto gt = rd<uint8_t>(d, "gt.bin");
+    const int wM = (int)eimp_W(M);
+    std::vector<int4> matches((size_t)nhaps * cap, int4{-7, -7, -7, -7});
+    std::vector<int32_t> nmatch(nhaps, -7);
+    uint32_t status = 0;
+    int retried = 0;
+    // the launches of launch_smm: the small node pool, then the retry pass
+    for (int pass = 0; pass < 2; pass++) {
+        const size_t smb = which ? (pass ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY>)
+                                         : sizeof(eimp::SmmWarpSmemC<SMM_NODES>))
+                                 : (pass ? sizeof(eimp::SmmWarpSmem<SMM_NODES_RETRY>)
+                                         : sizeof(eimp::SmmWarpSmem<SMM_NODES>));
+        for (int h = 0; h < nhaps; h++) {
+            if (pass) retried += nmatch[h] == eimp::SMM_RETRY;
+            // a fill pattern instead of zeros: the kernel must not read what it has not written
+            uint8_t *smem = (uint8_t *)aligned_alloc(16, (smb + 15) / 16 * 16);
+            memset(smem, 0x5A, smb);
+            EmuWarp warp;
+            std::vector<std::thread> lanes;
+            for (int l = 0; l < 32; l++)
+                lanes.emplace_back([&, l] {
+                    threadIdx.x = l;
+                    blockIdx.x = h;
+                    emu_warp = &warp;
+                    emu_smem_ptr = smem;
+                    auto kern = which ? (pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true>
+                                              : eimp::smm_compact_kernel<SMM_NODES, 1, false>)
+                                      : (pass ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true>
+                                              : eimp::smm_kernel<SMM_NODES, 1, false>);
+                    kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, sme, matches.data(),
+                         cap, nmatch.data(), &status);
+                });
+            for (auto &x : lanes) x.join();
+            free(smem);
+        }
+    }
+    wr(d, "o_retried.bin", std::vector<int32_t>{retried});
+    wr(d, "o_matches.bin", matches);
+    wr(d, "o_nmatch.bin", nmatch);
+    wr(d, "o_status.bin", std::vector<uint32_t>{status});
+    if (emu_divergence.load()) { fprintf(stderr, "divergent warp collectives: %d\n", emu_divergence.load()); return 3; }
+    return 0;
+}
