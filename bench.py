@@ -443,6 +443,45 @@ def main():
                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
                     "algorithmic_bytes_per_launch": bytes_dos, "avg_launch_ms": dos_ms, "stage_ms": stage_means}
 
+    # output statistics of the step's imputed bunch (the numbers of
+    # VCFData::writeVCFImputedBunch: allele dosages and alleles written, r2,
+    # AF, MAF, AC, AN, filters), timed on their own after the step: reads the
+    # dosages and alleles of every (haplotype, site), writes the allele
+    # dosages and alleles, 30 B per site of per-site inputs and outputs
+    if do_phase:
+        from eimp_b200._lib import EimpSiteStatsOpts
+        d_ads = torch.empty_like(d_dos)
+        d_gtb = torch.empty_like(d_bits)
+        d_site = torch.empty(Mref * 6, dtype=torch.int32, device=dev)
+        d_conf = torch.zeros(1, dtype=torch.int64, device=dev)
+        so = EimpSiteStatsOpts(0, 0, 0.0, 0.0)
+        sp = d_site.data_ptr()
+
+        def stats_call():
+            ctx.check(L.eimp_imp_site_stats_dev(h, 0, Mref, d_bits.data_ptr(), ldb, d_dos.data_ptr(), Mref,
+                                                d_pdm.data_ptr(), d_pdp.data_ptr(), M, C.byref(so),
+                                                d_ads.data_ptr(), Mref, d_gtb.data_ptr(), ldb, None, None, sp,
+                                                sp + 4 * Mref, sp + 8 * Mref, sp + 12 * Mref, sp + 16 * Mref,
+                                                sp + 20 * Mref, d_conf.data_ptr()))
+        for _ in range(3):
+            stats_call()
+        st_ms = []
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0, e1 = ev(), ev()
+            e0.record(stream)
+            stats_call()
+            e1.record(stream)
+            ctx.synchronize()
+            st_ms.append(e0.elapsed_time(e1))
+        st_ms = float(np.mean(st_ms))
+        bytes_st = 2 * (2 * nt * Mref * 4 + 2 * nt * ldb * 8) + Mref * 30
+        roofline["site_stats_kernel"] = {"achieved": bytes_st / (st_ms / 1e3) / 1e9, "avg_launch_ms": st_ms,
+                                         "algorithmic_bytes_per_launch": bytes_st,
+                                         "frac": bytes_st / (st_ms / 1e3) / 1e9 / peak}
+        del d_ads, d_gtb
+
     # end to end through the public API: host (pinned) targets in, host dosages out
     e2e = None
     if rank == 0 or world > 1:

@@ -19,6 +19,12 @@ _sz = C.c_size_t
 _i32 = C.c_int
 
 
+class EimpSiteStatsOpts(C.Structure):
+    """eimp_site_stats_opts (include/eimp_gpu.h)"""
+    _fields_ = [("overwriteCalls", C.c_int), ("improveCalls", C.c_int), ("r2filter", C.c_float),
+                ("maffilter", C.c_float)]
+
+
 class EimpPhaseParams(C.Structure):
     """eimp_phase_params (include/eimp_gpu.h)"""
     _fields_ = [("K", C.c_int), ("hsize", C.c_int), ("beamwidth", C.c_int), ("delta", C.c_int),
@@ -58,6 +64,10 @@ _PROTOS = [
     ("eimp_imp_bunch", _i32, [_vp, _sz, _sz, _vp, _vp]),
     ("eimp_imp_bunch_dev", _i32, [_vp, _sz, _sz, _vp, _sz, _vp, _sz]),
     ("eimp_imp_matches", _i32, [_vp, _sz, _vp, _sz, C.POINTER(_sz)]),
+    ("eimp_imp_phased_dosages", _i32, [_vp, _vp, _vp]),
+    ("eimp_imp_bunch_stats", _i32, [_vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("eimp_imp_site_stats_dev", _i32, [_vp, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _sz,
+                                       _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("eimp_imp_refpbwt", _i32, [_vp, _vp, _vp]),
     ("eimp_besthaps_noalloc", _i32, [_vp, _sz, _sz, _vp, _vp, _sz, _sz, _vp, _vp]),
 ]

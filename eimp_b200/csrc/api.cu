@@ -80,6 +80,9 @@ struct eimp_ctx {
     DBuf i_phased, i_gt, i_matches, i_nmatch;
     // host <-> device staging for bunches
     DBuf i_bits, i_dos;
+    // phased dosages (eimp_imp_phased_dosages) and staging of the output statistics
+    DBuf i_pdm, i_pdp, s_ads, s_gt, s_ds, s_gp, s_site, s_conf;
+    bool i_have_pdos = false;
 };
 
 namespace {
@@ -310,6 +313,7 @@ int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phase
     size_t cap = match_cap ? match_cap : M / 4 + 64;
     CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
     ctx->i_ntargets = ntargets;
+    ctx->i_have_pdos = false;   // phased dosages belong to the previous targets
     ctx->i_imputeCalls = imputeCalls;
     ctx->i_cap = cap;
     CK(ctx->i_phased.reserve(nh * wM * 8));
@@ -373,6 +377,104 @@ int eimp_imp_bunch(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t *bi
     if (r) return r;
     CK(cudaMemcpyAsync(bits, ctx->i_bits.p, nh * wb * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(dos, ctx->i_dos.p, nh * nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int eimp_imp_phased_dosages(eimp_ctx *ctx, const float *dos_mat, const float *dos_pat) {
+    if (!ctx || !dos_mat || !dos_pat) return fail(ctx, EIMP_E_ARG, "eimp_imp_phased_dosages: NULL argument");
+    if (!ctx->i_ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_phased_dosages: imputation not prepared");
+    if (int r = use_device(ctx)) return r;
+    const size_t bytes = ctx->i_ntargets * ctx->i_M * 4;
+    CK(ctx->i_pdm.reserve(bytes));
+    CK(ctx->i_pdp.reserve(bytes));
+    CK(cudaMemcpyAsync(ctx->i_pdm.p, dos_mat, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->i_pdp.p, dos_pat, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->i_have_pdos = true;
+    return 0;
+}
+
+int eimp_imp_site_stats_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const uint64_t *d_bits,
+                            size_t ldb_words, const float *d_dos, size_t ldd, const float *d_pdos_mat,
+                            const float *d_pdos_pat, size_t ldp, const eimp_site_stats_opts *opts, float *d_ads,
+                            size_t lda, uint64_t *d_gtbits, size_t ldg_words, float *d_ds, float *d_gp,
+                            float *d_r2, float *d_af, float *d_maf, int32_t *d_ac, int32_t *d_an, uint8_t *d_pass,
+                            uint64_t *d_conflicts) {
+    if (!ctx || !ctx->i_ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: imputation not prepared");
+    if (!opts || !d_bits || !d_dos || !d_ads || !d_gtbits || !d_r2 || !d_af || !d_maf || !d_ac || !d_an || !d_pass ||
+        !d_conflicts)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: NULL argument");
+    if (mref_begin + nsites > ctx->i_Mref || !nsites) return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: window out of range");
+    const size_t wb = (nsites + 63) / 64;
+    if (ldb_words < wb || ldg_words < wb || ldd < nsites || lda < nsites)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: leading dimension too small");
+    const float *pm = d_pdos_mat ? d_pdos_mat : (ctx->i_have_pdos ? ctx->i_pdm.as<float>() : nullptr);
+    const float *pp = d_pdos_pat ? d_pdos_pat : (ctx->i_have_pdos ? ctx->i_pdp.as<float>() : nullptr);
+    if (!d_pdos_mat) ldp = ctx->i_M;
+    if (!pm || !pp || ldp < ctx->i_M)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: no phased dosages (eimp_imp_phased_dosages)");
+    if (int r = use_device(ctx)) return r;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
+    SiteStatsArgs a;
+    a.ntgt = (int)ctx->i_ntargets; a.mref_begin = (int)mref_begin; a.nsites = (int)nsites;
+    a.bits = d_bits; a.ldb = (int)ldb_words; a.dos = d_dos; a.ldd = (int)ldd;
+    a.phased = ctx->i_phased.as<uint64_t>(); a.wM = (int)eimp_W(ctx->i_M);
+    a.pdos_mat = pm; a.pdos_pat = pp; a.ldp = (int)ldp;
+    a.gt = ctx->i_gt.as<uint8_t>(); a.M = (int)ctx->i_M;
+    a.segm = ctx->i_segm.as<int32_t>(); a.common = ctx->i_common.as<uint8_t>(); a.af = ctx->i_af.as<float>();
+    a.overwriteCalls = opts->overwriteCalls; a.improveCalls = opts->improveCalls;
+    a.r2filter = opts->r2filter; a.maffilter = opts->maffilter;
+    a.ads = d_ads; a.lda = (int)lda; a.gtbits = d_gtbits; a.ldg = (int)ldg_words; a.ds = d_ds; a.gp = d_gp;
+    a.r2 = d_r2; a.af_out = d_af; a.maf = d_maf; a.ac = d_ac; a.an = d_an; a.pass = d_pass;
+    a.conflicts = reinterpret_cast<unsigned long long *>(d_conflicts);
+    LAUNCH(launch_site_stats(a, ctx->stream));
+    return 0;
+}
+
+int eimp_imp_bunch_stats(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const eimp_site_stats_opts *opts,
+                         float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2, float *af, float *maf,
+                         int32_t *ac, int32_t *an, uint8_t *pass, uint64_t *conflicts) {
+    if (!ctx || !opts || !ads || !gtbits || !r2 || !af || !maf || !ac || !an || !pass || !conflicts)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch_stats: NULL argument");
+    if (!ctx->i_ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch_stats: imputation not prepared");
+    if (!ctx->i_have_pdos) return fail(ctx, EIMP_E_ARG, "eimp_imp_bunch_stats: no phased dosages (eimp_imp_phased_dosages)");
+    if (int r = use_device(ctx)) return r;
+    const size_t N = ctx->i_ntargets, nh = 2 * N, wb = eimp_W(nsites);
+    CK(ctx->i_bits.reserve(nh * wb * 8));
+    CK(ctx->i_dos.reserve(nh * nsites * 4));
+    CK(ctx->s_ads.reserve(nh * nsites * 4));
+    CK(ctx->s_gt.reserve(nh * wb * 8));
+    if (ds) CK(ctx->s_ds.reserve(N * nsites * 4));
+    if (gp) CK(ctx->s_gp.reserve(3 * N * nsites * 4));
+    const size_t site_bytes = nsites * (4 * 3 + 4 * 2 + 1) + 64;
+    CK(ctx->s_site.reserve(site_bytes));
+    CK(ctx->s_conf.reserve(8));
+    CK(cudaMemsetAsync(ctx->i_bits.p, 0, nh * wb * 8, ctx->stream));
+    CK(cudaMemsetAsync(ctx->s_gt.p, 0, nh * wb * 8, ctx->stream));
+    CK(cudaMemsetAsync(ctx->s_conf.p, 0, 8, ctx->stream));
+    int r = eimp_imp_bunch_dev(ctx, mref_begin, nsites, ctx->i_bits.as<uint64_t>(), wb, ctx->i_dos.as<float>(), nsites);
+    if (r) return r;
+    uint8_t *sb = ctx->s_site.as<uint8_t>();
+    float *d_r2 = reinterpret_cast<float *>(sb), *d_af = d_r2 + nsites, *d_maf = d_af + nsites;
+    int32_t *d_ac = reinterpret_cast<int32_t *>(d_maf + nsites), *d_an = d_ac + nsites;
+    uint8_t *d_pass = reinterpret_cast<uint8_t *>(d_an + nsites);
+    r = eimp_imp_site_stats_dev(ctx, mref_begin, nsites, ctx->i_bits.as<uint64_t>(), wb, ctx->i_dos.as<float>(), nsites,
+                                nullptr, nullptr, 0, opts, ctx->s_ads.as<float>(), nsites, ctx->s_gt.as<uint64_t>(), wb,
+                                ds ? ctx->s_ds.as<float>() : nullptr, gp ? ctx->s_gp.as<float>() : nullptr, d_r2, d_af,
+                                d_maf, d_ac, d_an, d_pass, ctx->s_conf.as<uint64_t>());
+    if (r) return r;
+    CK(cudaMemcpyAsync(ads, ctx->s_ads.p, nh * nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(gtbits, ctx->s_gt.p, nh * wb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (ds) CK(cudaMemcpyAsync(ds, ctx->s_ds.p, N * nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (gp) CK(cudaMemcpyAsync(gp, ctx->s_gp.p, 3 * N * nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(r2, d_r2, nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(af, d_af, nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(maf, d_maf, nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ac, d_ac, nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(an, d_an, nsites * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(pass, d_pass, nsites, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(conflicts, ctx->s_conf.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return 0;
 }

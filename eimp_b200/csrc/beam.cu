@@ -105,7 +105,7 @@ struct Ctx {
     // arena
     HPh *hp;
     float *ph;
-    int2 *ivpool;
+    uint32_t *ivpool;            // intervals [l, r] packed l | r << 16 (K <= 65536)
     int *ivfree;
     int *happ, *happ_old;
     int2 *hapmap;
@@ -161,7 +161,11 @@ __device__ __forceinline__ int bh_equal(const HPh &a, const HPh &b) {
 }
 
 __device__ __forceinline__ float *ph_ptr(const Ctx &c, int slot) { return c.ph + (size_t)slot * PHMAX; }
-__device__ __forceinline__ int2 *iv_buf(const Ctx &c, int b) { return c.ivpool + (size_t)b * c.HMAX; }
+__device__ __forceinline__ uint32_t *iv_buf(const Ctx &c, int b) { return c.ivpool + (size_t)b * c.HMAX; }
+// the interval lists hold non-empty intervals of positions < K <= 65536
+__device__ __forceinline__ uint32_t iv_pack(int l, int r) { return (uint32_t)l | ((uint32_t)r << 16); }
+__device__ __forceinline__ int iv_l(uint32_t v) { return (int)(v & 0xffffu); }
+__device__ __forceinline__ int iv_r(uint32_t v) { return (int)(v >> 16); }
 
 // ------------------------------------------------------------------ min-max heap (MinMaxHeap.h)
 __device__ __forceinline__ int hlt(const Hel &x, const Hel &y) { return x.key < y.key; }
@@ -272,9 +276,9 @@ __device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
     const int pm = w.phsize - 1;
     const int niv = h.niv, phstart = h.phstart;
     const int calc0 = h.toext0, calc1 = h.toext1;
-    const int2 *iv = iv_buf(c, h.biv);
-    int2 *e0 = iv_buf(c, h.bext0);
-    int2 *e1 = iv_buf(c, h.bext1);
+    const uint32_t *iv = iv_buf(c, h.biv);
+    uint32_t *e0 = iv_buf(c, h.bext0);
+    uint32_t *e1 = iv_buf(c, h.bext1);
     int ns = h.scaleexp;
     {   // updateScaling (:224-258)
         const int e = ilogb_exact(h.p);
@@ -291,23 +295,23 @@ __device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
     const int lim = w.H < niv + 1 ? w.H : niv + 1;
     float p0 = 0.0f, p1 = 0.0f;
     int n0 = 0, n1 = 0;
-    int2 last0 = make_int2(0, -1), last1 = make_int2(0, -1);   // the last entries appended
+    uint32_t last0 = 0u, last1 = 0u;   // the last entries appended (read only after an append)
     const int cnt0 = w.c0ref;
     const float t0 = __fmul_rn(ph[phstart & pm], w.prec[0]);
     if (cnt0 > 0) {
         if (calc0) p0 = __fmul_rn((float)cnt0, t0);
-        last0 = make_int2(0, cnt0 - 1);
+        last0 = iv_pack(0, cnt0 - 1);
         e0[n0++] = last0;
     }
     if (cnt0 < c.K) {
         if (calc1) p1 = __fmul_rn((float)(c.K - cnt0), t0);
-        last1 = make_int2(cnt0, c.K - 1);
+        last1 = iv_pack(cnt0, c.K - 1);
         e1[n1++] = last1;
     }
     const uint32_t *rinc = w.rowinc, *rref = w.rowref;
     const int cinc = w.c0inc;
-    int2 prevfrom = make_int2(0, -1);
-    int2 fr[HXC], nfr[HXC];
+    uint32_t prevfrom = 0u;   // compared only from the second step on
+    uint32_t fr[HXC], nfr[HXC];
     float tph[HXC], ntph[HXC];
 #pragma unroll
     for (int j = 0; j < HXC; j++)
@@ -325,11 +329,11 @@ __device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
 #pragma unroll
         for (int j = 0; j < HXC; j++) {
             A0[j] = 0; B0[j] = -1; A1[j] = 0; B1[j] = -1;
-            const int2 pf = j == 0 ? prevfrom : fr[j - 1];
-            const bool same = base + j > 1 && pf.x == fr[j].x && pf.y == fr[j].y;
+            const uint32_t pf = j == 0 ? prevfrom : fr[j - 1];
+            const bool same = base + j > 1 && pf == fr[j];
             if (base + j < lim && !same) {
                 int cl, cr, il, ir;
-                pbwt_map(rinc, cinc, fr[j].x, fr[j].y, cl, cr, il, ir);
+                pbwt_map(rinc, cinc, iv_l(fr[j]), iv_r(fr[j]), cl, cr, il, ir);
                 pbwt_map(rref, cnt0, cl, cr, A0[j], B0[j], A1[j], B1[j]);
             }
         }
@@ -337,25 +341,25 @@ __device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
         for (int j = 0; j < HXC; j++) {
             const int i = base + j;
             if (stop || i >= lim) break;
-            const int2 from = fr[j];
+            const uint32_t from = fr[j];
             int a0 = A0[j], b0 = B0[j], a1 = A1[j], b1 = B1[j];
-            if (i > 1 && prevfrom.x == from.x && prevfrom.y == from.y) {   // :395-399
+            if (i > 1 && prevfrom == from) {   // :395-399
                 a0 = 0; b0 = -1; a1 = 0; b1 = -1;
-                if (n0 == i) { a0 = last0.x; b0 = last0.y; }
-                if (n1 == i) { a1 = last1.x; b1 = last1.y; }
+                if (n0 == i) { a0 = iv_l(last0); b0 = iv_r(last0); }
+                if (n1 == i) { a1 = iv_l(last1); b1 = iv_r(last1); }
             }
             prevfrom = from;
             const float ti = __fmul_rn(tph[j], w.prec[i]);
             bool any = false;
             if (a0 <= b0) {
                 if (calc0) p0 = __fadd_rn(p0, __fmul_rn((float)(b0 - a0 + 1), ti));
-                last0 = make_int2(a0, b0);
+                last0 = iv_pack(a0, b0);
                 e0[n0++] = last0;
                 any = true;
             }
             if (a1 <= b1) {
                 if (calc1) p1 = __fadd_rn(p1, __fmul_rn((float)(b1 - a1 + 1), ti));
-                last1 = make_int2(a1, b1);
+                last1 = iv_pack(a1, b1);
                 e1[n1++] = last1;
                 any = true;
             }
@@ -1171,7 +1175,7 @@ static ArenaLayout arena_layout(const BeamParams &p, int M) {
     a.ph = o; o = align256(o + sizeof(float) * PHMAX * a.NH);
     // the interval pool doubles as the storage of the pre-phasing constraint
     // heaps (one entry per split site) once the fast beam is done
-    const size_t ivb = sizeof(int2) * (size_t)H * 3 * a.NH, heapb = sizeof(Hel) * (size_t)(M + 1);
+    const size_t ivb = sizeof(uint32_t) * (size_t)H * 3 * a.NH, heapb = sizeof(Hel) * (size_t)(M + 1);
     a.ivpool = o; o = align256(o + (ivb > heapb ? ivb : heapb));
     a.ivfree = o; o = align256(o + sizeof(int) * 3 * a.NH);
     a.happ = o; o = align256(o + sizeof(int) * a.NH);
@@ -1199,7 +1203,7 @@ __device__ __forceinline__ void setbit_(uint64_t *v, int i) { v[i >> 6] |= 1ull 
 __device__ __forceinline__ void clrbit_(uint64_t *v, int i) { v[i >> 6] &= ~(1ull << (i & 63)); }
 
 // One warp per target: Target::phaseExtPBWT (Target.cpp:291-777)
-__global__ void __launch_bounds__(32 * BEAM_WARPS) beam_kernel(
+__global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
     const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
     const int32_t *__restrict__ ncalls, const float *__restrict__ cmdiffs, const uint32_t *__restrict__ pbwt,
@@ -1238,7 +1242,7 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS) beam_kernel(
     uint8_t *ab = arena + (size_t)t * arena_bytes;
     c.hp = reinterpret_cast<HPh *>(ab + al.hp);
     c.ph = reinterpret_cast<float *>(ab + al.ph);
-    c.ivpool = reinterpret_cast<int2 *>(ab + al.ivpool);
+    c.ivpool = reinterpret_cast<uint32_t *>(ab + al.ivpool);
     c.ivfree = reinterpret_cast<int *>(ab + al.ivfree);
     c.happ = reinterpret_cast<int *>(ab + al.happ);
     c.happ_old = reinterpret_cast<int *>(ab + al.happ_old);

@@ -3,10 +3,12 @@
 //  refpbwt_kernel   -- PBWT::buildComprPBWT with refPBWT=true (PBWT.cpp:207-285,
 //                      136-142): compressed rows + prefix arrays gAbsPerm.
 //  transpose_kernel -- site-major -> haplotype-major bit matrix (64x64 tiles).
-//  smm_kernel       -- TargetImp::calcSMMatches / processHistorySubTree
-//                      (TargetImp.cpp:74-246, 346-435), one warp per target
-//                      haplotype: the rank queries of all tree nodes of a site
-//                      run across the lanes, the tree update runs on lane 0.
+//  smm_kernel,      -- TargetImp::calcSMMatches / processHistorySubTree
+//  smm_compact_kernel  (TargetImp.cpp:74-246, 346-435), one warp per target
+//                      haplotype: the rank queries of all tree nodes of a
+//                      site and the rebuild of the tree run across the lanes;
+//                      the compact kernel stores the tree in 30 B per node
+//                      (typed sites < 65536).
 //  dosage_kernel    -- TargetImp::imputeBunch (TargetImp.cpp:474-558), one
 //                      warp per (target haplotype, 64-site tile).
 #include "common.cuh"

@@ -33,6 +33,27 @@ cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const
                           uint64_t *bits, int ldb, cudaStream_t st);
 cudaError_t launch_segmap(const int64_t *typed, int M, int Mref, int32_t *segm, uint8_t *common, cudaStream_t st);
 
+// ---- output statistics of an imputed bunch (site_stats.cu)
+struct SiteStatsArgs {
+    int ntgt, mref_begin, nsites;
+    const uint64_t *bits; int ldb;            // imputed alleles, 2*ntgt rows of ldb words
+    const float *dos; int ldd;                // imputed dosages, 2*ntgt rows (-1: conflict)
+    const uint64_t *phased; int wM;           // phased haplotypes at the typed sites
+    const float *pdos_mat, *pdos_pat; int ldp;   // phased dosages, ntgt rows each
+    const uint8_t *gt; int M;                 // target genotypes at the typed sites (3: missing)
+    const int32_t *segm; const uint8_t *common; const float *af;   // per reference site
+    int overwriteCalls, improveCalls;
+    float r2filter, maffilter;
+    float *ads; int lda;                      // allele dosages written, 2*ntgt rows
+    uint64_t *gtbits; int ldg;                // alleles written, 2*ntgt rows of ldg words
+    float *ds, *gp;                           // optional: ntgt rows / 3*ntgt rows of lda floats
+    float *r2, *af_out, *maf;                 // per site of the bunch
+    int32_t *ac, *an;
+    uint8_t *pass;
+    unsigned long long *conflicts;            // incremented by the conflicts found
+};
+cudaError_t launch_site_stats(const SiteStatsArgs &a, cudaStream_t st);
+
 // ---- phasing preparation, condensed reference, PBWT (phase_prep.cu)
 cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int nhaps, int wM, int K,
                             uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, cudaStream_t st);

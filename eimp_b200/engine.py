@@ -250,6 +250,41 @@ class PBWTImputer:
         self.ctx.check(self.ctx.L.eimp_imp_bunch(self.ctx.h, mref_begin, nsites, ptr(bits), ptr(dos)))
         return bits, dos
 
+    def setPhasedDosages(self, dos_mat: np.ndarray, dos_pat: np.ndarray):
+        """phasedDosages of the prepared targets (N x M floats each, the mat and
+        pat dosages phasing returned), kept on the device for the output
+        statistics of writeVCFImputedBunch."""
+        dm = np.ascontiguousarray(dos_mat, np.float32)
+        dp = np.ascontiguousarray(dos_pat, np.float32)
+        if dm.shape != (self.ntargets, self.M) or dp.shape != dm.shape:
+            raise ValueError(f"phased dosages must be {self.ntargets} x {self.M}")
+        self.ctx.check(self.ctx.L.eimp_imp_phased_dosages(self.ctx.h, ptr(dm), ptr(dp)))
+
+    def writeImputedBunchStats(self, mref_begin: int, nsites: int, overwriteCalls: bool = False,
+                               improveCalls: bool = False, r2filter: float = 0.0, maffilter: float = 0.0,
+                               ds: bool = False, gp: bool = False) -> dict:
+        """imputeBunch for the window plus the numbers VCFData::writeVCFImputedBunch
+        (VCFData.cpp:3068-3446) writes for it: per haplotype and site the
+        allele dosage (ads) and allele (gtbits); optionally DS and GP; per site
+        r2, af, maf, ac, an and passed (the r2/MAF output filters); the number
+        of imputation conflicts."""
+        from ._lib import EimpSiteStatsOpts
+        nh, N = 2 * self.ntargets, self.ntargets
+        o = EimpSiteStatsOpts(int(overwriteCalls), int(improveCalls), float(r2filter), float(maffilter))
+        out = dict(ads=np.zeros((nh, nsites), np.float32), gtbits=np.zeros((nh, W(nsites)), np.uint64),
+                   ds=np.zeros((N, nsites), np.float32) if ds else None,
+                   gp=np.zeros((3 * N, nsites), np.float32) if gp else None,
+                   r2=np.zeros(nsites, np.float32), af=np.zeros(nsites, np.float32),
+                   maf=np.zeros(nsites, np.float32), ac=np.zeros(nsites, np.int32), an=np.zeros(nsites, np.int32),
+                   passed=np.zeros(nsites, np.uint8))
+        conf = np.zeros(1, np.uint64)
+        self.ctx.check(self.ctx.L.eimp_imp_bunch_stats(
+            self.ctx.h, mref_begin, nsites, C.byref(o), ptr(out["ads"]), ptr(out["gtbits"]),
+            ptr(out["ds"]) if ds else None, ptr(out["gp"]) if gp else None, ptr(out["r2"]), ptr(out["af"]),
+            ptr(out["maf"]), ptr(out["ac"]), ptr(out["an"]), ptr(out["passed"]), ptr(conf)))
+        out["conflicts"] = int(conf[0])
+        return out
+
     def matches(self, hap: int) -> np.ndarray:
         n = C.c_size_t(0)
         self.ctx.check(self.ctx.L.eimp_imp_matches(self.ctx.h, hap, None, 0, C.byref(n)))

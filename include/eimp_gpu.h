@@ -204,6 +204,41 @@ int eimp_imp_matches(eimp_ctx *ctx, size_t hap, int32_t *out, size_t cap, size_t
  * and prefix arrays ((M+1) x nhaps int32, PBWT::getSortOrder, PBWT.h:67). */
 int eimp_imp_refpbwt(eimp_ctx *ctx, uint32_t *compr, int32_t *absperm);
 
+/* Output statistics of an imputed bunch: the numeric part of
+ * VCFData::writeVCFImputedBunch (VCFData.cpp:3068-3446), which main.cpp:454
+ * calls after PBWTImputer::imputeBunch for every bunch.  Diploid targets.
+ * Per target haplotype and site: the allele dosage written (ADS; an imputation
+ * conflict takes the reference panel allele frequency RefPanelAF and the
+ * allele RefPanelAF > 0.5; a typed, non-missing call keeps the phased allele
+ * and dosage unless overwriteCalls, or improveCalls and the imputed dosage is
+ * closer to 0/1), and the allele written (GT).  Optional per target and site:
+ * DS = ADS0 + ADS1 and GP (three floats, VCFData.cpp:3159-3166).  Per site:
+ * AF and MAF from the dosages, minimac4's r2, AC, AN and whether the record
+ * passes the --imputeR2filter / --imputeMAFfilter thresholds.  `conflicts`
+ * receives the number of conflicts (VCFData::conflictcnt).  The per-category
+ * counters that --improveCalls adds to the run statistics are not produced. */
+typedef struct {
+    int overwriteCalls;   /* --overwriteCalls (Args.cpp:304) */
+    int improveCalls;     /* --improveCalls (Args.cpp:305) */
+    float r2filter;       /* --imputeR2filter (Args.cpp:283), default 0 */
+    float maffilter;      /* --imputeMAFfilter (Args.cpp:284), default 0 */
+} eimp_site_stats_opts;
+
+/* Phased dosages of the prepared targets (phasedDosages of main.cpp: the mat
+ * and pat dosage of each target at the typed sites, ntargets x M floats each,
+ * as eimp_phase_targets returns them), kept on the device for the output
+ * statistics; a new eimp_imp_prepare drops them. */
+int eimp_imp_phased_dosages(eimp_ctx *ctx, const float *dos_mat, const float *dos_pat);
+
+/* imputeBunch + the output statistics for the window [mref_begin,
+ * mref_begin + nsites): ads 2*ntargets x nsites floats, gtbits 2*ntargets x
+ * W(nsites) words, ds (NULL: skipped) ntargets x nsites, gp (NULL: skipped)
+ * 3*ntargets x nsites floats (rows GP0, GP1, GP2 of each target), per site r2,
+ * af, maf, ac, an, pass (nsites each), *conflicts. */
+int eimp_imp_bunch_stats(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const eimp_site_stats_opts *opts,
+                         float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2, float *af, float *maf,
+                         int32_t *ac, int32_t *an, uint8_t *pass, uint64_t *conflicts);
+
 /* ------------------------------------------- device-resident variants ----
  * Same operations on device pointers (inputs already in HBM; outputs written to
  * device memory; no host<->device copies, no synchronisation). */
@@ -214,6 +249,17 @@ int eimp_imp_bunch_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t
 int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint64_t *d_sitemajor_full,
                                const float *d_af_full, size_t M, const int64_t *d_typed,
                                const uint64_t *d_sitemajor_typed);
+/* The output statistics of a bunch already imputed into d_bits / d_dos
+ * (eimp_imp_bunch_dev); phased dosages from d_pdos_mat / d_pdos_pat (ntargets
+ * rows of ldp floats) or, when those are NULL, from eimp_imp_phased_dosages.
+ * d_ads / d_gtbits may be d_dos / d_bits (in place, with lda == ldd); the
+ * statistics add to *d_conflicts. */
+int eimp_imp_site_stats_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const uint64_t *d_bits,
+                            size_t ldb_words, const float *d_dos, size_t ldd, const float *d_pdos_mat,
+                            const float *d_pdos_pat, size_t ldp, const eimp_site_stats_opts *opts, float *d_ads,
+                            size_t lda, uint64_t *d_gtbits, size_t ldg_words, float *d_ds, float *d_gp,
+                            float *d_r2, float *d_af, float *d_maf, int32_t *d_ac, int32_t *d_an, uint8_t *d_pass,
+                            uint64_t *d_conflicts);
 int eimp_phase_targets_dev(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt,
                            uint64_t *d_mats, uint64_t *d_pats, float *d_dos_mats, float *d_dos_pats,
                            float *d_totalconf, int32_t *d_ncallsites);

@@ -461,3 +461,107 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
         if (mref == mmap) mmap = (currm + 1) < M ? (size_t)typed[currm + 1] : Mref;
     }
 }
+
+
+/* ------------------------------------------------------------------------
+ * Output statistics: VCFData::writeVCFImputedBunch (VCFData.cpp:3068-3446),
+ * diploid targets, in the reference's order of operations.
+ * ---------------------------------------------------------------------- */
+static int eo_getbit(const uint64_t *row, size_t i) { return (int)((row[i >> 6] >> (i & 63)) & 1u); }
+static void eo_setbit(uint64_t *row, size_t i, int v) { if (v) row[i >> 6] |= 1ull << (i & 63); }
+
+long eo_site_stats(size_t ntgt, size_t mref_begin, size_t nsites, const uint64_t *bits, size_t wb,
+                   const float *dos, const uint64_t *phased, size_t wM, const float *pdm, const float *pdp,
+                   const uint8_t *gt, size_t M, const int32_t *typed_idx, const uint8_t *is_typed,
+                   const float *af_full, int overwriteCalls, int improveCalls, float r2filter, float maffilter,
+                   float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2o, float *afo, float *mafo,
+                   int32_t *aco, int32_t *ano, uint8_t *pass) {
+    long conflictcnt = 0;
+    for (size_t isite = 0; isite < nsites; isite++) {
+        const size_t idx = mref_begin + isite;
+        const float rpaf = af_full[idx];                       /* :3118 */
+        const int isimputed = !is_typed[idx];
+        const size_t psite = (size_t)typed_idx[idx];
+        double adsum = 0.0, ad2sum = 0.0;                      /* :3119-3123 */
+        int nval = 0, ac1 = 0, an = 0;
+        for (size_t i = 0; i < ntgt; i++) {
+            const size_t h0 = 2 * i, h1 = 2 * i + 1;
+            int hap0, hap1;
+            float ads0, ads1;
+            const int missing = !isimputed && gt[i * M + psite] == 3;   /* :3238 */
+            if (isimputed || missing || overwriteCalls) {      /* :3126-3152, :3246-3270 */
+                hap0 = eo_getbit(bits + h0 * wb, isite);
+                hap1 = eo_getbit(bits + h1 * wb, isite);
+                ads0 = dos[h0 * nsites + isite];
+                if (ads0 < 0) { ads0 = rpaf; hap0 = rpaf > 0.5; conflictcnt++; }
+                ads1 = dos[h1 * nsites + isite];
+                if (ads1 < 0) { ads1 = rpaf; hap1 = rpaf > 0.5; conflictcnt++; }
+            } else {                                           /* :3272-3340 */
+                hap0 = eo_getbit(phased + h0 * wM, psite);
+                hap1 = eo_getbit(phased + h1 * wM, psite);
+                ads0 = pdm[i * M + psite];
+                ads1 = pdp[i * M + psite];
+                if (improveCalls) {
+                    float idos0 = dos[h0 * nsites + isite];
+                    float idos1 = dos[h1 * nsites + isite];
+                    float pdos0 = ads0;
+                    float pdos1 = ads1;
+                    if (idos0 < 0) idos0 = rpaf;
+                    if (idos1 < 0) idos1 = rpaf;
+                    if (idos0 > 0.5) idos0 = 1.0 - idos0;
+                    if (idos1 > 0.5) idos1 = 1.0 - idos1;
+                    if (pdos0 > 0.5) pdos0 = 1.0 - pdos0;
+                    if (pdos1 > 0.5) pdos1 = 1.0 - pdos1;
+                    float improve0 = pdos0 - idos0;
+                    float improve1 = pdos1 - idos1;
+                    if (improve0 + improve1 > 0) {
+                        if (dos[h0 * nsites + isite] < 0) conflictcnt++;
+                        if (dos[h1 * nsites + isite] < 0) conflictcnt++;
+                        hap0 = eo_getbit(bits + h0 * wb, isite);
+                        hap1 = eo_getbit(bits + h1 * wb, isite);
+                        ads0 = hap0 ? 1.0 - idos0 : idos0;
+                        ads1 = hap1 ? 1.0 - idos1 : idos1;
+                    }
+                }
+            }
+            ads[h0 * nsites + isite] = ads0;
+            ads[h1 * nsites + isite] = ads1;
+            adsum += ads0 + ads1;                              /* :3154-3155 */
+            ad2sum += ads0 * ads0 + ads1 * ads1;
+            if (ds) ds[i * nsites + isite] = ads0 + ads1;
+            if (gp) {                                          /* :3159-3166 */
+                double gp0 = (1.0 - ads0) * (1.0 - ads1);
+                double gp2 = ads0 * ads1;
+                double gp1 = 1.0 - gp0 - gp2;
+                gp[(3 * i) * nsites + isite] = (float)gp0;
+                gp[(3 * i + 1) * nsites + isite] = (float)gp1;
+                gp[(3 * i + 2) * nsites + isite] = (float)gp2;
+            }
+            if (hap0) ac1++;                                   /* :3169-3174 */
+            if (hap1) ac1++;
+            an += 2;
+            nval += 2;
+            eo_setbit(gtbits + h0 * wb, isite, hap0);
+            eo_setbit(gtbits + h1 * wb, isite, hap1);
+        }
+        double r2 = 1.0, af = 0.0, evar = 0.0, ovar = 0.0;    /* :3363-3383 */
+        if (nval) {
+            af = adsum / nval;
+            evar = af * (1.0 - af);
+            ovar = (ad2sum - adsum * af) / nval;
+            if (evar > 0.0 && ovar > 0.0) r2 = ovar / evar;
+            else r2 = 0.0;
+        }
+        float r2f = r2;
+        float aff = af;
+        float maff = aff > 0.5 ? 1 - aff : aff;
+        r2o[isite] = r2f;
+        afo[isite] = aff;
+        mafo[isite] = maff;
+        aco[isite] = ac1;
+        ano[isite] = an;
+        pass[isite] = !(r2f < r2filter || maff < maffilter);   /* :3389 */
+    }
+    return conflictcnt;
+}
+

@@ -82,6 +82,27 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
                size_t nmiss, int imputeCalls, const uint64_t *hap, uint64_t *bits, float *dos,
                uint8_t *imputed);
 
+/* Output statistics of an imputed bunch: the numeric part of
+ * VCFData::writeVCFImputedBunch (VCFData.cpp:3068-3446) for diploid targets.
+ * Site-major over the bunch's nsites sites (site s = reference site
+ * mref_begin + s):
+ *   bits   2*ntgt rows of wb words (imputed alleles), dos 2*ntgt x nsites
+ *   phased 2*ntgt rows of wM words, pdm/pdp ntgt x M phased dosages
+ *   gt     ntgt x M genotype codes (3 = missing), typed_idx / is_typed per
+ *          reference site (the typed index of the last typed site <= mref)
+ * Outputs: ads 2*ntgt x nsites, gtbits 2*ntgt rows of wb words (zeroed by the
+ * caller), ds ntgt x nsites (optional), gp 3*ntgt x nsites (optional, rows
+ * GP0, GP1, GP2 per target), per site r2, af, maf, ac, an, pass; returns the
+ * number of imputation conflicts.
+ * The reference's writer needs htslib and cannot be compiled here: this
+ * restatement is pinned by hand-worked cases in the tests only. */
+long eo_site_stats(size_t ntgt, size_t mref_begin, size_t nsites, const uint64_t *bits, size_t wb,
+                   const float *dos, const uint64_t *phased, size_t wM, const float *pdm, const float *pdp,
+                   const uint8_t *gt, size_t M, const int32_t *typed_idx, const uint8_t *is_typed,
+                   const float *af_full, int overwriteCalls, int improveCalls, float r2filter, float maffilter,
+                   float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2, float *af, float *maf,
+                   int32_t *ac, int32_t *an, uint8_t *pass);
+
 /* a7: phasing parameters (Args.cpp:274-299 defaults) */
 typedef struct {
     int K;

@@ -67,6 +67,11 @@ def lib():
         L.eo_impute.argtypes = [_i64p, C.c_size_t, _i32p, C.c_size_t, _u64p, C.c_size_t, C.c_size_t, _i64p,
                                 C.c_size_t, _f32p, C.c_size_t, _i64p, C.c_size_t, C.c_int, _u64p, _u64p,
                                 _f32p, _u8p]
+        L.eo_site_stats.restype = C.c_long
+        L.eo_site_stats.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t, _u64p, C.c_size_t, _f32p, _u64p, C.c_size_t,
+                                    _f32p, _f32p, _u8p, C.c_size_t, _i32p, _u8p, _f32p, C.c_int, C.c_int,
+                                    C.c_float, C.c_float, _f32p, _u64p, C.c_void_p, C.c_void_p, _f32p, _f32p,
+                                    _f32p, _i32p, _i32p, _u8p]
         L.eo_phase.restype = C.c_int
         L.eo_phase.argtypes = [_u8p, _u64p, _u64p, _f32p, C.c_size_t, C.c_size_t, C.POINTER(PhaseParamsC),
                                _u64p, _u64p, _f32p, _f32p, C.POINTER(C.c_float), C.POINTER(C.c_size_t)]
@@ -151,6 +156,42 @@ def impute(matches, absperm, sitemajor_full, typed, af_full, nrefhaps, miss, hap
                     np.ascontiguousarray(miss, np.int64) if len(miss) else np.zeros(1, np.int64), len(miss),
                     int(imputeCalls), np.ascontiguousarray(hap_words, np.uint64), bits, dos, imp)
     return bits, dos, imp
+
+
+def site_stats(mref_begin, bits, dos, phased, pdm, pdp, gt, typed, Mref, af_full, overwriteCalls=False,
+               improveCalls=False, r2filter=0.0, maffilter=0.0, want_ds=False, want_gp=False):
+    """VCFData::writeVCFImputedBunch's numbers for one bunch (eo_site_stats).
+    bits: 2N x wb words, dos: 2N x nsites floats, phased: 2N x wM words,
+    pdm/pdp: N x M phased dosages, gt: N x M, typed: ascending typed site
+    indices into the Mref reference sites."""
+    nh, nsites = dos.shape
+    N, M = gt.shape
+    typed = np.asarray(typed, np.int64)
+    cnt = np.searchsorted(typed, np.arange(Mref), side="right")
+    typed_idx = np.maximum(cnt - 1, 0).astype(np.int32)
+    is_typed = np.zeros(Mref, np.uint8)
+    is_typed[typed] = 1
+    wb = bits.shape[1]
+    ads = np.zeros((nh, nsites), np.float32)
+    gtbits = np.zeros((nh, wb), np.uint64)
+    ds = np.zeros((N, nsites), np.float32) if want_ds else None
+    gp = np.zeros((3 * N, nsites), np.float32) if want_gp else None
+    r2 = np.zeros(nsites, np.float32)
+    af = np.zeros(nsites, np.float32)
+    maf = np.zeros(nsites, np.float32)
+    ac = np.zeros(nsites, np.int32)
+    an = np.zeros(nsites, np.int32)
+    ps = np.zeros(nsites, np.uint8)
+    conf = lib().eo_site_stats(N, mref_begin, nsites, np.ascontiguousarray(bits, np.uint64), wb,
+                               np.ascontiguousarray(dos, np.float32), np.ascontiguousarray(phased, np.uint64),
+                               phased.shape[1], np.ascontiguousarray(pdm, np.float32),
+                               np.ascontiguousarray(pdp, np.float32), np.ascontiguousarray(gt, np.uint8), M,
+                               typed_idx, is_typed, np.ascontiguousarray(af_full, np.float32), int(overwriteCalls),
+                               int(improveCalls), r2filter, maffilter, ads, gtbits,
+                               ds.ctypes.data if ds is not None else None, gp.ctypes.data if gp is not None else None,
+                               r2, af, maf, ac, an, ps)
+    return dict(ads=ads, gtbits=gtbits, ds=ds, gp=gp, r2=r2, af=af, maf=maf, ac=ac, an=an, passed=ps,
+                conflicts=int(conf))
 
 
 def phase(gt_row, hapmajor, sitemajor, cm, params: PhaseParamsC):

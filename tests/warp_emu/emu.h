@@ -23,7 +23,8 @@
 #define __global__
 #define __host__
 #define __forceinline__ inline
-#define __launch_bounds__(x)
+#define __noinline__
+#define __launch_bounds__(...)
 #define __align__(n) __attribute__((aligned(n)))
 #define __restrict__ __restrict
 
@@ -42,7 +43,7 @@ inline int2 make_int2(int x, int y) { return int2{x, y}; }
 inline short2 make_short2(short x, short y) { return short2{x, y}; }
 inline int4 make_int4(int x, int y, int z, int w) { return int4{x, y, z, w}; }
 
-extern thread_local dim3 threadIdx, blockIdx;
+extern thread_local dim3 threadIdx, blockIdx, blockDim;
 
 // Barrier of the 32 lane threads: the last to arrive opens the next
 // generation; the others yield the core while they wait (lanes outnumber the
@@ -142,6 +143,9 @@ inline float __fmul_rn(float a, float b) { volatile float r = a * b; return r; }
 inline float __fdiv_rn(float a, float b) { volatile float r = a / b; return r; }
 inline double __dadd_rn(double a, double b) { volatile double r = a + b; return r; }
 inline double __dmul_rn(double a, double b) { volatile double r = a * b; return r; }
+inline double __dsub_rn(double a, double b) { volatile double r = a - b; return r; }
+inline double __ddiv_rn(double a, double b) { volatile double r = a / b; return r; }
+inline float __fsub_rn(float a, float b) { volatile float r = a - b; return r; }
 using std::ldexp;
 inline int min(int a, int b) { return a < b ? a : b; }
 inline int max(int a, int b) { return a > b ? a : b; }
@@ -159,4 +163,7 @@ inline int atomicMin(int *p, int v) {
     return o;
 }
 inline unsigned atomicOr(unsigned *p, unsigned v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned long long atomicAdd(unsigned long long *p, unsigned long long v) {
+    return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);
+}
 inline int atomicOr(int *p, int v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }

@@ -18,7 +18,7 @@
 #include <thread>
 #include <vector>
 
-thread_local dim3 threadIdx, blockIdx;
+thread_local dim3 threadIdx, blockIdx, blockDim;
 thread_local EmuWarp *emu_warp;
 thread_local uint8_t *emu_smem_ptr;
 std::atomic<int> emu_divergence{0};
