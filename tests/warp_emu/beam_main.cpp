@@ -18,6 +18,7 @@
 
 thread_local dim3 threadIdx, blockIdx, blockDim;
 thread_local EmuWarp *emu_warp;
+thread_local EmuBarrier *emu_block;
 thread_local uint8_t *emu_smem_ptr;
 std::atomic<int> emu_divergence{0};
 

@@ -51,9 +51,10 @@ extern thread_local dim3 threadIdx, blockIdx, blockDim;
 struct EmuBarrier {
     std::atomic<int> count{0};
     std::atomic<unsigned> gen{0};
+    int n = 32;   // participating threads
     void arrive_and_wait() {
         const unsigned g = gen.load(std::memory_order_acquire);
-        if (count.fetch_add(1, std::memory_order_acq_rel) == 31) {
+        if (count.fetch_add(1, std::memory_order_acq_rel) == n - 1) {
             count.store(0, std::memory_order_relaxed);
             gen.fetch_add(1, std::memory_order_release);
         } else {
@@ -68,6 +69,12 @@ struct EmuWarp {
     int sites[32];
 };
 extern thread_local EmuWarp *emu_warp;
+// __syncthreads: a barrier of all the block's threads (drivers that run whole
+// blocks set emu_block; a block's __shared__ arrays are function statics,
+// shared by its threads -- blocks run one after the other)
+extern thread_local EmuBarrier *emu_block;
+#define __shared__ static
+#define __syncthreads() emu_block->arrive_and_wait()
 extern thread_local uint8_t *emu_smem_ptr;
 extern std::atomic<int> emu_divergence;
 

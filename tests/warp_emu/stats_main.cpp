@@ -1,6 +1,6 @@
 // Runs site_stats_kernel (generated host copy of
-// eimp_b200/csrc/site_stats.cu) under the warp emulator, one warp of its
-// 128-thread blocks at a time.
+// eimp_b200/csrc/site_stats.cu) under the warp emulator, one block (all its
+// warps, meeting at __syncthreads) at a time.
 //
 //   stats_emu <dir>
 //
@@ -19,6 +19,7 @@
 
 thread_local dim3 threadIdx, blockIdx, blockDim;
 thread_local EmuWarp *emu_warp;
+thread_local EmuBarrier *emu_block;
 thread_local uint8_t *emu_smem_ptr;
 std::atomic<int> emu_divergence{0};
 
@@ -73,21 +74,24 @@ int main(int argc, char **argv) {
     a.ads = ads.data(); a.lda = (int)ns; a.gtbits = gtbits.data(); a.ldg = a.ldb; a.ds = ds.data(); a.gp = gp.data();
     a.r2 = site_f.data(); a.af_out = site_f.data() + ns; a.maf = site_f.data() + 2 * ns;
     a.ac = site_i.data(); a.an = site_i.data() + ns; a.pass = pass.data(); a.conflicts = conf.data();
-    const int blocks = (a.nsites + 127) / 128;
-    for (int b = 0; b < blocks; b++)
-        for (int w = 0; w < 4; w++) {
-            EmuWarp warp;
-            std::vector<std::thread> lanes;
-            for (int l = 0; l < 32; l++)
-                lanes.emplace_back([&, l] {
-                    threadIdx.x = w * 32 + l;
-                    blockIdx.x = b;
-                    blockDim.x = 128;
-                    emu_warp = &warp;
-                    eimp::site_stats_kernel(a);
-                });
-            for (auto &x : lanes) x.join();
-        }
+    // whole blocks: the producer warps and the summing warp meet at __syncthreads
+    const int blocks = (a.nsites + 31) / 32, nw = eimp::SS_PROD + 1;
+    for (int b = 0; b < blocks; b++) {
+        std::vector<EmuWarp> warps(nw);
+        EmuBarrier block;
+        block.n = 32 * nw;
+        std::vector<std::thread> threads;
+        for (int t = 0; t < 32 * nw; t++)
+            threads.emplace_back([&, t] {
+                threadIdx.x = t;
+                blockIdx.x = b;
+                blockDim.x = 32 * nw;
+                emu_warp = &warps[t / 32];
+                emu_block = &block;
+                eimp::site_stats_kernel(a);
+            });
+        for (auto &x : threads) x.join();
+    }
     wr(d, "o_ads.bin", ads); wr(d, "o_gtbits.bin", gtbits); wr(d, "o_ds.bin", ds); wr(d, "o_gp.bin", gp);
     wr(d, "o_site_f.bin", site_f); wr(d, "o_site_i.bin", site_i); wr(d, "o_pass.bin", pass);
     wr(d, "o_conf.bin", conf);
