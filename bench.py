@@ -52,6 +52,8 @@ def parse():
                     help="targets timed one per call for the plain-form comparison (0: skip)")
     ap.add_argument("--serving-requests", type=int, default=40, help="requests of the serving run (0: skip)")
     ap.add_argument("--graph-steps", type=int, default=3, help="replays timed in the CUDA-graph form (0: skip)")
+    ap.add_argument("--qref-steps", type=int, default=5,
+                    help="timed decodes of the panel's Qref haplotype section (0: skip)")
     ap.add_argument("--serving-rate", type=float, default=40.0, help="mean request arrivals per second")
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--stages", default="phase,impute", help="comma list of: phase, impute")
@@ -560,6 +562,65 @@ def main():
         ctx.check(L.eimp_phase_reserve(h, C.byref(pparams), nt, 0))
         ctx.check(L.eimp_set_timing(h, 1))
 
+    # the panel's Qref haplotype section (qref_spec.md section I) decoded on
+    # the device into the site-major rows: the section already in HBM (value),
+    # and through the host API from host memory (index walk, one copy,
+    # decode); the reference's own decoder on one host core beside it
+    qref = None
+    if args.qref_steps > 0 and rank == 0:
+        sec = synth.qref_section(panel.sitemajor)
+        nwq = W(nh_ref)
+        offs = np.zeros(Mref, np.int64)
+        assert L.eimp_qref_index(sec.ctypes.data, sec.size, Mref, nh_ref // 2, offs.ctypes.data) == 0
+        d_sec = torch.zeros(sec.size + 16, dtype=torch.uint8, device=dev)
+        d_sec[:sec.size].copy_(torch.from_numpy(sec))
+        d_offs = torch.from_numpy(offs).to(dev)
+        d_rows = torch.empty(Mref * nwq, dtype=torch.int64, device=dev)
+        torch.cuda.synchronize()
+
+        def qcall():
+            ctx.check(L.eimp_qref_decode_dev(h, d_sec.data_ptr(), d_offs.data_ptr(), Mref, nh_ref // 2,
+                                             d_rows.data_ptr(), nwq))
+        for _ in range(3):
+            qcall()
+        ctx.synchronize()
+        qms = []
+        for _ in range(args.qref_steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            q0, q1 = ev(), ev()
+            q0.record(stream)
+            qcall()
+            q1.record(stream)
+            ctx.synchronize()
+            qms.append(q0.elapsed_time(q1))
+        q_ms = float(np.mean(qms))
+        same = torch.equal(d_rows.view(Mref, nwq), d_full.view(Mref, -1))
+        sec_pin = torch.from_numpy(sec).pin_memory()
+        t0 = time.perf_counter()
+        ctx.check(L.eimp_qref_decode(h, sec_pin.data_ptr(), sec.size, Mref, nh_ref // 2, d_rows.data_ptr(), nwq,
+                                     None))
+        e2e_ms = (time.perf_counter() - t0) * 1e3
+        qbytes = sec.size + Mref * nwq * 8
+        qref = {"variants": Mref, "haplotypes": nh_ref, "section_bytes": int(sec.size),
+                "coded_variants": int(sum(1 for o in offs if int(sec[o:o + 8].view(np.uint64)[0]) > 0)),
+                "value": Mref / (q_ms / 1e3), "unit": "variants/s", "ms": q_ms,
+                "roofline": {"bound": "hbm", "achieved": qbytes / (q_ms / 1e3) / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": qbytes / (q_ms / 1e3) / 1e9 / peak,
+                             "algorithmic_bytes_per_launch": qbytes},
+                "e2e": {"value": Mref / (e2e_ms / 1e3), "unit": "variants/s", "ms": e2e_ms,
+                        "h2d_bytes": int(sec.size), "d2h_bytes": 0},
+                "equal_to_panel": bool(same)}
+        if not args.no_cpu_baseline:
+            from oracle import refcore
+            if refcore.available():
+                t0 = time.perf_counter()
+                _, rc = refcore.qref_decode(sec, Mref, nwq)
+                c_s = time.perf_counter() - t0
+                qref["cpu_baseline"] = {"value": Mref / c_s, "unit": "variants/s", "cores": 1, "kind": "reference",
+                                        "sample": f"all {Mref} variants, runlengthDecode of utils.h", "ok": rc == 0}
+        del d_sec, d_rows, d_offs
+
     # the plain drop-in form: one target per call (phase, matches, dosages),
     # device-resident inputs, on a sample of targets; same metric
     plain = None
@@ -631,7 +692,7 @@ def main():
                 "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
                 "config": config_block(cfg, panel, tg, stages), "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches), "plain": plain, "serving": serving,
-                "graph": graph}
+                "graph": graph, "qref_decode": qref}
         if do_phase:
             line["phased_samples_per_sec"] = world * nt * args.steps / (tot_ms / 1e3)
             line["phase_ms_per_step"] = float(np.mean(kern["phase"]))

@@ -82,6 +82,8 @@ struct eimp_ctx {
     DBuf i_bits, i_dos;
     // phased dosages (eimp_imp_phased_dosages) and staging of the output statistics
     DBuf i_pdm, i_pdp, s_ads, s_gt, s_ds, s_gp, s_site, s_conf;
+    // Qref haplotype section staging
+    DBuf q_sec, q_offs, q_out;
     bool i_have_pdos = false;
 };
 
@@ -126,6 +128,7 @@ int check_status(eimp_ctx *ctx) {
     if (st) {
         CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(uint32_t), ctx->stream));
         if (st & EIMP_ERR_BEAM_EMPTY) return fail(ctx, EIMP_E_BEAM_EMPTY, "Beam is empty. No paths left.");
+        if (st & EIMP_ERR_QREF_TRUNCATED) return fail(ctx, EIMP_E_ARG, "Truncated runlength sequence!");
         char b[160];
         snprintf(b, sizeof b, "device structure capacity exceeded (status 0x%x)", st);
         return fail(ctx, EIMP_E_CAPACITY, b);
@@ -477,6 +480,69 @@ int eimp_imp_bunch_stats(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const 
     CK(cudaMemcpyAsync(conflicts, ctx->s_conf.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return 0;
+}
+
+int eimp_qref_index(const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref, int64_t *offsets) {
+    if ((!section && nbytes) || (!offsets && Mref)) return EIMP_E_ARG;
+    const size_t raw = eimp_W(2 * Nref) * 8;   // hapcapacity: 2*Nref bits in 512-bit units
+    size_t off = 0;
+    for (size_t v = 0; v < Mref; v++) {
+        if (off + 8 > nbytes) return EIMP_E_ARG;   // "Failed reading haplotypes from reference."
+        uint64_t encsize;
+        memcpy(&encsize, section + off, 8);
+        offsets[v] = (int64_t)off;
+        const size_t len = encsize ? encsize : raw;
+        if (len > nbytes - off - 8) return EIMP_E_ARG;
+        off += 8 + len;
+    }
+    return 0;
+}
+
+int eimp_qref_decode_dev(eimp_ctx *ctx, const uint8_t *d_section, const int64_t *d_offsets, size_t Mref,
+                         size_t Nref, uint64_t *d_out, size_t ldw_words) {
+    if (!ctx || (Mref && (!d_section || !d_offsets || !d_out))) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode: NULL argument");
+    const size_t nw = eimp_W(2 * Nref);
+    if (ldw_words < nw) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode: leading dimension too small");
+    if (Mref > (size_t)INT32_MAX || nw > (size_t)INT32_MAX) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode: too many variants");
+    if (int r = use_device(ctx)) return r;
+    LAUNCH(launch_qref_decode(d_section, d_offsets, (int)Mref, (int)nw, d_out, ldw_words, ctx->status.as<uint32_t>(),
+                              ctx->stream));
+    return 0;
+}
+
+int eimp_qref_decode(eimp_ctx *ctx, const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref,
+                     uint64_t *d_out, size_t ldw_words, uint64_t *host_out) {
+    if (!ctx || (!section && nbytes)) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode: NULL argument");
+    const size_t nw = eimp_W(2 * Nref);
+    if (!d_out) ldw_words = nw;
+    if (ldw_words < nw) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode: leading dimension too small");
+    std::vector<int64_t> offs(Mref);
+    if (eimp_qref_index(section, nbytes, Mref, Nref, offs.data()))
+        return fail(ctx, EIMP_E_ARG, "Failed reading haplotypes from reference.");
+    if (int r = use_device(ctx)) return r;
+    // the decoder reads whole aligned 32-bit words: 16 bytes of slack past the section
+    CK(ctx->q_sec.reserve(nbytes + 16));
+    CK(ctx->q_offs.reserve(Mref * 8 + 8));
+    CK(cudaMemsetAsync(ctx->q_sec.as<uint8_t>() + nbytes, 0, 16, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->q_sec.p, section, nbytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->q_offs.p, offs.data(), Mref * 8, cudaMemcpyHostToDevice, ctx->stream));
+    uint64_t *dst = d_out;
+    if (!dst) {
+        CK(ctx->q_out.reserve(Mref * nw * 8 + 8));
+        dst = ctx->q_out.as<uint64_t>();
+    }
+    int r = eimp_qref_decode_dev(ctx, ctx->q_sec.as<uint8_t>(), ctx->q_offs.as<int64_t>(), Mref, Nref, dst, ldw_words);
+    if (r) return r;
+    if (host_out) {
+        if (ldw_words == nw) {
+            CK(cudaMemcpyAsync(host_out, dst, Mref * nw * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        } else {
+            CK(cudaMemcpy2DAsync(host_out, nw * 8, dst, ldw_words * 8, nw * 8, Mref, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
 }
 
 int eimp_imp_matches(eimp_ctx *ctx, size_t hap, int32_t *out, size_t cap, size_t *n) {

@@ -54,6 +54,10 @@ struct SiteStatsArgs {
 };
 cudaError_t launch_site_stats(const SiteStatsArgs &a, cudaStream_t st);
 
+// ---- Qref haplotype section (qref_decode.cu)
+cudaError_t launch_qref_decode(const uint8_t *sec, const int64_t *offs, int Mref, int nwords, uint64_t *out,
+                               size_t ldw, uint32_t *status, cudaStream_t st);
+
 // ---- phasing preparation, condensed reference, PBWT (phase_prep.cu)
 cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int nhaps, int wM, int K,
                             uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, cudaStream_t st);

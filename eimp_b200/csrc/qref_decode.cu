@@ -1,0 +1,113 @@
+// Qref reference panel: decoding of the haplotype section on the device
+// (sm_100a).
+//
+//  qref_decode_kernel -- VCFData::qRefLoadNextVariant (VCFData.cpp:2378-2535)
+//                        with runlengthDecode (utils.h:194-), no masked
+//                        samples: every variant's haplotype vector, stored
+//                        raw or run-length coded (qref_spec.md section I),
+//                        into its row of the site-major panel
+//                        (referenceFullT).
+//
+// The host copies the section as it lies in the file (one transfer) and the
+// byte offset of every variant's <encsize> field (a walk over the size
+// fields, qref_index on the host); one warp then decodes one variant.  A raw
+// vector is copied with 32-bit loads realigned by funnel shifts (the section
+// interleaves 8-byte sizes with odd-length codes, so a vector can start at
+// any byte).  A run-length code is read 32 bytes at a time: a ballot of the
+// bytes' high bits and a walk along them give the bytes that start a run
+// length (a length is one byte, or two when the first has its high bit set);
+// a warp scan of the lengths gives every run's first bit; runs alternate
+// 0/1 starting with 0, and the lanes holding runs of ones set them in the
+// zeroed row.  HBM-bound: each variant reads its code and writes its row.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace eimp {
+
+__device__ __forceinline__ void set_ones(uint64_t *row, uint64_t a, uint64_t b) {   // bits [a, b), b > a
+    const uint64_t wa = a >> 6, wb = (b - 1) >> 6;
+    const int la = (int)(a & 63), lb = (int)((b - 1) & 63);
+    if (wa == wb) {
+        const uint64_t m = (lb == 63 ? ~0ull : ((1ull << (lb + 1)) - 1ull)) & (~0ull << la);
+        atomicOr(reinterpret_cast<unsigned long long *>(row + wa), m);
+        return;
+    }
+    atomicOr(reinterpret_cast<unsigned long long *>(row + wa), ~0ull << la);
+    for (uint64_t w = wa + 1; w < wb; w++) row[w] = ~0ull;   // words inside the run belong to it alone
+    atomicOr(reinterpret_cast<unsigned long long *>(row + wb), lb == 63 ? ~0ull : ((1ull << (lb + 1)) - 1ull));
+}
+
+__global__ void __launch_bounds__(128) qref_decode_kernel(const uint8_t *__restrict__ sec,
+                                                          const int64_t *__restrict__ offs, int Mref, int nwords,
+                                                          uint64_t *__restrict__ out, size_t ldw,
+                                                          uint32_t *__restrict__ status) {
+    const int lane = threadIdx.x & 31;
+    const int v = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (v >= Mref) return;
+    const uint8_t *p = sec + offs[v];
+    uint64_t encsize = 0;
+    if (lane < 8) encsize = (uint64_t)p[lane] << (8 * lane);
+    for (int o = 4; o; o >>= 1) encsize |= __shfl_xor_sync(0xffffffffu, encsize, o);
+    encsize = __shfl_sync(0xffffffffu, encsize, 0);
+    const uint8_t *enc = p + 8;
+    uint64_t *row = out + (size_t)v * ldw;
+    if (encsize == 0) {   // the raw vector (VCFData.cpp:2434-2446)
+        const size_t mis = reinterpret_cast<uintptr_t>(enc) & 3u;
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(enc - mis);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(row);
+        const unsigned sh = (unsigned)mis * 8u;
+        for (int k = lane; k < 2 * nwords; k += 32)
+            dst[k] = sh ? __funnelshift_r(src[k], src[k + 1], sh) : src[k];
+        return;
+    }
+    for (int k = lane; k < nwords; k += 32) row[k] = 0ull;
+    __syncwarp();
+    const uint64_t nbits = (uint64_t)nwords * 64;
+    int carry = 0;            // the chunk starts with the second byte of a run length
+    unsigned long long runs = 0, pos = 0, last_start = 0;
+    for (uint64_t base = 0; base < encsize; base += 32) {
+        const uint64_t i = base + lane;
+        const bool in = i < encsize;
+        const unsigned b = in ? enc[i] : 0u;
+        const unsigned hi = __ballot_sync(0xffffffffu, in && (b & 0x80u));
+        const int nvalid = (int)min((uint64_t)32, encsize - base);
+        unsigned sm = 0;
+        int q = carry;
+        while (q < nvalid) { sm |= 1u << q; q += 1 + (int)((hi >> q) & 1u); }
+        const int ncarry = q - nvalid;
+        const bool start = (sm >> lane) & 1u;
+        unsigned nb = __shfl_down_sync(0xffffffffu, b, 1);
+        if (lane == 31) nb = (i + 1 < encsize) ? enc[i + 1] : 0u;
+        const unsigned len = start ? ((b & 0x80u) ? ((nb & 0xffu) << 7) | (b & 0x7fu) : b) : 0u;
+        unsigned incl = len;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+        const unsigned long long rs = pos + (incl - len);
+        const unsigned long long ridx = runs + __popc(sm & ((1u << lane) - 1u));
+        if (start && (ridx & 1ull) && len && rs < nbits)   // a run of ones
+            set_ones(row, rs, min(rs + len, (unsigned long long)nbits));
+        const unsigned lastlane = sm ? 31 - __clz(sm) : 0;
+        const unsigned long long ls = __shfl_sync(0xffffffffu, rs, lastlane);
+        if (sm) last_start = ls;
+        pos += total;
+        runs += __popc(sm);
+        carry = ncarry;
+    }
+    // utils.h:222-240: a run length cut after its first byte, or runs that end
+    // inside a word the reference still decodes, are a truncated sequence
+    const bool cut = carry != 0;
+    const bool midword = (pos & 63ull) && (pos >> 6) <= max((unsigned long long)nwords - 1, last_start >> 6);
+    if (lane == 0 && (cut || midword)) atomicOr(status, EIMP_ERR_QREF_TRUNCATED);
+}
+
+cudaError_t launch_qref_decode(const uint8_t *sec, const int64_t *offs, int Mref, int nwords, uint64_t *out,
+                               size_t ldw, uint32_t *status, cudaStream_t st) {
+    if (Mref <= 0) return cudaSuccess;
+    qref_decode_kernel<<<(Mref + 3) / 4, 128, 0, st>>>(sec, offs, Mref, nwords, out, ldw, status);
+    return cudaGetLastError();
+}
+
+}  // namespace eimp

@@ -299,3 +299,16 @@ class PBWTImputer:
         ap = np.zeros((self.M + 1, self.nhaps), np.int32)
         self.ctx.check(self.ctx.L.eimp_imp_refpbwt(self.ctx.h, ptr(compr), ptr(ap)))
         return compr, ap
+
+
+def decode_qref_haplotypes(ctx: Context, section: np.ndarray, Mref: int, Nref: int) -> np.ndarray:
+    """The haplotype section of a Qref reference file (qref_spec.md section I:
+    per variant <encsize u64> and a run-length code, or the raw vector) decoded
+    on the device -- the decode of VCFData::qRefLoadNextVariant -- into Mref
+    site-major rows of W(2*Nref) words (referenceFullT)."""
+    sec = np.ascontiguousarray(section, np.uint8)
+    out = np.zeros((Mref, W(2 * Nref)), np.uint64)
+    ctx.check(ctx.L.eimp_qref_decode(ctx.h, ptr(sec) if sec.size else None, sec.size, Mref, Nref, None, 0,
+                                     ptr(out)))
+    return out
+

@@ -214,3 +214,54 @@ def typed_views(panel: Panel, typed: np.ndarray):
     hapmajor_typed = pack_rows(np.ascontiguousarray(dense.T), W(M))
     cm_typed = panel.cm[typed].astype(np.float32)
     return hapmajor_typed, sitemajor_typed, cm_typed
+
+
+# ---------------------------------------------------------------- Qref panels
+_RLE_MAX = 32767
+
+
+def _rle_row(row: np.ndarray):
+    """The run-length code of one haplotype vector as the Qref writer stores
+    it (runlengthEncode / addRunlength, utils.h:133-191): alternating run
+    lengths starting with the 0-bit run, one byte below 128, two bytes (low 7
+    bits with the high bit set, then the rest) below 32768, longer runs split
+    into 32767-runs joined by empty runs.  None where the code would not be
+    shorter than the vector."""
+    nbytes_raw = row.size * 8
+    bits = np.unpackbits(row.view(np.uint8), bitorder="little")
+    change = np.flatnonzero(bits[1:] != bits[:-1]) + 1
+    bounds = np.concatenate([[0], change, [bits.size]])
+    runs = np.diff(bounds)
+    if bits[0]:
+        runs = np.concatenate([[0], runs])
+    out = []
+    for k, L in enumerate(runs.tolist()):
+        while L > _RLE_MAX:
+            out += [0xff, 0xff, 0x00]
+            L -= _RLE_MAX
+        if L >= 128:
+            out += [(L & 0x7f) | 0x80, L >> 7]
+        else:
+            out.append(L)
+        last = k == len(runs) - 1
+        if not last and len(out) >= nbytes_raw:   # the writer gives up while it encodes
+            return None
+    if len(out) > nbytes_raw:
+        return None
+    return np.array(out, np.uint8)
+
+
+def qref_section(rows: np.ndarray) -> np.ndarray:
+    """The haplotype section of a Qref file (qref_spec.md section I) for
+    site-major panel rows (one row of W(2*Nref) words per variant): per
+    variant the uint64 size of its run-length code and the code, or size 0
+    and the raw row where the code is not shorter."""
+    rows = np.ascontiguousarray(rows, np.uint64)
+    parts = []
+    for r in rows:
+        enc = _rle_row(r)
+        if enc is None:
+            parts += [np.zeros(8, np.uint8), r.view(np.uint8)]
+        else:
+            parts += [np.array([enc.size], np.uint64).view(np.uint8), enc]
+    return np.concatenate(parts) if parts else np.zeros(0, np.uint8)

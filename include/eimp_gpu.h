@@ -239,6 +239,26 @@ int eimp_imp_bunch_stats(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const 
                          float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2, float *af, float *maf,
                          int32_t *ac, int32_t *an, uint8_t *pass, uint64_t *conflicts);
 
+/* Qref reference panel, haplotype section (qref_spec.md section I; read by
+ * VCFData::qRefLoadNextVariant, VCFData.cpp:2378-2535, with runlengthDecode,
+ * utils.h:194-): Mref variants, each <encsize uint64> followed by encsize
+ * run-length bytes, or by the raw vector of W(2*Nref) words when encsize is
+ * 0.  Decoded into Mref rows of W(2*Nref) words (bit 2s mat, 2s+1 pat of
+ * sample s; the site-major referenceFullT layout, VCFData.h:211).  Masked
+ * reference samples (--excludeRefSamples) are not supported.
+ *
+ * eimp_qref_index (host only, no device): the byte offset of every variant's
+ * <encsize> field; EIMP_E_ARG when the section is shorter than its variants
+ * ("Failed reading haplotypes from reference.").
+ * eimp_qref_decode: the section from host memory (copied once), decoded into
+ * d_out (device, Mref rows of ldw_words words) or, when d_out is NULL, into a
+ * buffer of the context; with host_out non-NULL the rows are also copied
+ * there (Mref x W(2*Nref) words).  Returns EIMP_E_ARG for a truncated
+ * run-length sequence ("Truncated runlength sequence!", utils.h:222-240). */
+int eimp_qref_index(const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref, int64_t *offsets);
+int eimp_qref_decode(eimp_ctx *ctx, const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref,
+                     uint64_t *d_out, size_t ldw_words, uint64_t *host_out);
+
 /* ------------------------------------------- device-resident variants ----
  * Same operations on device pointers (inputs already in HBM; outputs written to
  * device memory; no host<->device copies, no synchronisation). */
@@ -260,6 +280,12 @@ int eimp_imp_site_stats_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, con
                             size_t lda, uint64_t *d_gtbits, size_t ldg_words, float *d_ds, float *d_gp,
                             float *d_r2, float *d_af, float *d_maf, int32_t *d_ac, int32_t *d_an, uint8_t *d_pass,
                             uint64_t *d_conflicts);
+/* The Qref haplotype section already in device memory (readable up to the
+ * next multiple of 4 bytes past its end) with its variant offsets from
+ * eimp_qref_index; only enqueues the decode: a truncated sequence is
+ * reported by the next eimp_synchronize. */
+int eimp_qref_decode_dev(eimp_ctx *ctx, const uint8_t *d_section, const int64_t *d_offsets, size_t Mref,
+                         size_t Nref, uint64_t *d_out, size_t ldw_words);
 int eimp_phase_targets_dev(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt,
                            uint64_t *d_mats, uint64_t *d_pats, float *d_dos_mats, float *d_dos_pats,
                            float *d_totalconf, int32_t *d_ncallsites);

@@ -565,3 +565,111 @@ long eo_site_stats(size_t ntgt, size_t mref_begin, size_t nsites, const uint64_t
     return conflictcnt;
 }
 
+
+/* ------------------------------------------------------------------------
+ * Qref run-length coding of haplotype vectors: utils.h:133-191 (encode),
+ * utils.h:194- (decode, here without masked samples), qref_spec.md:110-173.
+ * ---------------------------------------------------------------------- */
+static size_t eo_add_run(size_t len, uint8_t *dest, size_t n) {   /* utils.h:133-149 */
+    while (len > 32767) {
+        dest[n++] = 0xff;
+        dest[n++] = 0xff;
+        dest[n++] = 0;
+        len -= 32767;
+    }
+    if (len >= 128) {
+        dest[n++] = (uint8_t)((len & 0x7f) | 0x80);
+        dest[n++] = (uint8_t)(len >> 7);
+    } else {
+        dest[n++] = (uint8_t)len;
+    }
+    return n;
+}
+
+long eo_rle_encode(const uint64_t *src, size_t nwords, uint8_t *enc) {
+    size_t n = 0, cur = 0;
+    int bit = 0;
+    for (size_t i = 0; i < nwords; i++) {
+        uint64_t word = bit ? ~src[i] : src[i];
+        int rem = 64;
+        while (rem > 0) {
+            int tr = word == 0 ? rem : __builtin_ctzll(word);
+            if (tr < rem) {
+                cur += (size_t)tr;
+                rem -= tr;
+                word >>= tr;
+                n = eo_add_run(cur, enc, n);
+                if (n >= nwords * 8) return -1;
+                cur = 0;
+                bit = !bit;
+                word = ~word;
+            } else {
+                cur += (size_t)rem;
+                rem = 0;
+            }
+        }
+    }
+    if (cur) n = eo_add_run(cur, enc, n);
+    if (n > nwords * 8) return -1;
+    return (long)n;
+}
+
+int eo_rle_decode(const uint8_t *enc, size_t encsize, uint64_t *dest, size_t nwords) {
+    size_t e = 0;
+    uint64_t remlength = 0;
+    int bit = 1;   /* toggled before the first run */
+    for (size_t i = 0; i < nwords || e < encsize; i++) {
+        uint64_t rem = 64;
+        while (rem > 0) {
+            while (remlength == 0) {
+                if (e == encsize) {
+                    if (rem % 64 == 0) {   /* ends on a word boundary: the rest is zero padding */
+                        remlength = rem + (i < nwords ? (nwords - i - 1) * 64 : 0);
+                        bit = 0;
+                        break;
+                    }
+                    return -1;
+                }
+                remlength = enc[e] & 0x7f;
+                if (enc[e] & 0x80) {
+                    e++;
+                    if (e == encsize) return -1;
+                    remlength |= (uint64_t)enc[e] << 7;
+                }
+                e++;
+                bit = !bit;
+            }
+            uint64_t fill;
+            if (remlength >= rem) { fill = rem; remlength -= rem; rem = 0; }
+            else { fill = remlength; rem -= remlength; remlength = 0; }
+            if (bit && i < nwords) {
+                uint64_t v = fill == 64 ? ~0ull : ((1ull << fill) - 1ull);
+                dest[i] |= v << (64 - (rem + fill));
+            }
+        }
+    }
+    return 0;
+}
+
+int eo_qref_decode(const uint8_t *section, size_t nbytes, size_t Mref, size_t nwords, uint64_t *out) {
+    size_t off = 0;
+    for (size_t v = 0; v < Mref; v++) {
+        uint64_t encsize;
+        if (off + 8 > nbytes) return -2;
+        memcpy(&encsize, section + off, 8);
+        off += 8;
+        uint64_t *row = out + v * nwords;
+        memset(row, 0, nwords * 8);
+        if (encsize) {
+            if (off + encsize > nbytes) return -2;
+            if (eo_rle_decode(section + off, encsize, row, nwords)) return -1;
+            off += encsize;
+        } else {
+            if (off + nwords * 8 > nbytes) return -2;
+            memcpy(row, section + off, nwords * 8);
+            off += nwords * 8;
+        }
+    }
+    return 0;
+}
+

@@ -96,6 +96,20 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
  * number of imputation conflicts.
  * The reference's writer needs htslib and cannot be compiled here: this
  * restatement is pinned by hand-worked cases in the tests only. */
+/* Qref haplotype vectors (qref_spec.md section I).
+ * eo_rle_encode: runlengthEncode + addRunlength (utils.h:133-191) of nwords
+ * words; returns the encoded length, or -1 where the reference gives up (the
+ * encoding would not be shorter than the source).  enc needs nwords*8+3 bytes.
+ * eo_rle_decode: runlengthDecode (utils.h:194-) without masked samples into
+ * nwords zeroed words; returns 0, or -1 for a truncated sequence.
+ * eo_qref_decode: the section of Mref variants (<encsize u64> then encsize
+ * bytes, or the raw capacity bytes when encsize is 0 -- VCFData.cpp:2378-2535)
+ * into Mref rows of nwords words; returns 0, -1 for a truncated sequence, -2
+ * for a section shorter than its variants. */
+long eo_rle_encode(const uint64_t *src, size_t nwords, uint8_t *enc);
+int eo_rle_decode(const uint8_t *enc, size_t encsize, uint64_t *dest, size_t nwords);
+int eo_qref_decode(const uint8_t *section, size_t nbytes, size_t Mref, size_t nwords, uint64_t *out);
+
 long eo_site_stats(size_t ntgt, size_t mref_begin, size_t nsites, const uint64_t *bits, size_t wb,
                    const float *dos, const uint64_t *phased, size_t wM, const float *pdm, const float *pdp,
                    const uint8_t *gt, size_t M, const int32_t *typed_idx, const uint8_t *is_typed,

@@ -49,6 +49,7 @@
 
 #include "StatusFile.h"
 #include "MyMalloc.h"
+#include "utils.h"
 
 StatusFile StatusFile::instance;
 MyMalloc MyMalloc::mm;
@@ -314,6 +315,51 @@ void refo_imp_bunch(void *ip, size_t bsize, unsigned nthreads, uint64_t *bits, f
     ih->imp->setNumThreads(nthreads);
     ih->imp->imputeBunch(0, bsize, it, id);
     for (size_t i = 0; i < nh; i++) memcpy(dos + i * bsize, id[i].data(), bsize * sizeof(float));
+}
+
+// Qref haplotype vectors: the reference's own run-length coder (utils.h)
+long refo_rle_encode(const uint64_t *src, size_t nwords, uint8_t *enc) {
+    vector<char> out;
+    if (!runlengthEncode(src, nwords, out)) return -1;
+    memcpy(enc, out.data(), out.size());
+    return (long)out.size();
+}
+
+void refo_rle_decode(const uint8_t *enc, size_t encsize, uint64_t *dest, size_t nwords) {
+    vector<char> in((const char *)enc, (const char *)enc + encsize);
+    vector<size_t> masked;
+    vector<bool> maskedhap;
+    size_t maskedalleles = 0;
+    runlengthDecode(in, dest, nwords, masked, maskedhap, maskedalleles);
+}
+
+// the haplotype section of a Qref file decoded variant by variant with the
+// reference's runlengthDecode, as qRefLoadNextVariant does after its reads
+// (VCFData.cpp:2378-2535; no masked samples); returns -2 for a short section
+int refo_qref_decode(const uint8_t *sec, size_t nbytes, size_t Mref, size_t nwords, uint64_t *out) {
+    vector<size_t> masked;
+    vector<bool> maskedhap;
+    size_t off = 0;
+    for (size_t v = 0; v < Mref; v++) {
+        if (off + 8 > nbytes) return -2;
+        size_t encsize;
+        memcpy(&encsize, sec + off, 8);
+        off += 8;
+        uint64_t *row = out + v * nwords;
+        memset(row, 0, nwords * 8);
+        if (encsize) {
+            if (off + encsize > nbytes) return -2;
+            vector<char> enc((const char *)sec + off, (const char *)sec + off + encsize);
+            size_t maskedalleles = 0;
+            runlengthDecode(enc, row, nwords, masked, maskedhap, maskedalleles);
+            off += encsize;
+        } else {
+            if (off + nwords * 8 > nbytes) return -2;
+            memcpy(row, sec + off, nwords * 8);
+            off += nwords * 8;
+        }
+    }
+    return 0;
 }
 
 } // extern "C"

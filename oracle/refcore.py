@@ -60,8 +60,40 @@ def lib():
         L.refo_imp_matches.argtypes = [C.c_void_p, C.c_size_t, _i64p]
         L.refo_imp_refpbwt.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.refo_imp_bunch.argtypes = [C.c_void_p, C.c_size_t, C.c_uint, _u64p, _f32p]
+        L.refo_rle_encode.restype = C.c_long
+        L.refo_rle_encode.argtypes = [_u64p, C.c_size_t, _u8p]
+        L.refo_rle_decode.argtypes = [_u8p, C.c_size_t, _u64p, C.c_size_t]
+        L.refo_qref_decode.restype = C.c_int
+        L.refo_qref_decode.argtypes = [_u8p, C.c_size_t, C.c_size_t, C.c_size_t, _u64p]
         _lib = L
     return _lib
+
+
+def rle_encode(words: np.ndarray):
+    """The reference's runlengthEncode (utils.h:155-191): bytes, or None where
+    it gives up (the encoding would not be shorter)."""
+    w = np.ascontiguousarray(words, np.uint64)
+    out = np.zeros(w.size * 8 + 3, np.uint8)
+    n = lib().refo_rle_encode(w, w.size, out)
+    return None if n < 0 else out[:n].copy()
+
+
+def rle_decode(enc: np.ndarray, nwords: int) -> np.ndarray:
+    """The reference's runlengthDecode (utils.h:194-), no masked samples; the
+    sequence must be well-formed (the reference exits on a truncated one)."""
+    e = np.ascontiguousarray(enc, np.uint8)
+    out = np.zeros(nwords, np.uint64)
+    lib().refo_rle_decode(e if e.size else np.zeros(1, np.uint8), e.size, out, nwords)
+    return out
+
+
+def qref_decode(section: np.ndarray, Mref: int, nwords: int):
+    """A Qref haplotype section decoded by the reference's own runlengthDecode
+    (the decode part of VCFData::qRefLoadNextVariant): (rows, status)."""
+    sec = np.ascontiguousarray(section, np.uint8)
+    out = np.zeros((Mref, nwords), np.uint64)
+    rc = lib().refo_qref_decode(sec, sec.size, Mref, nwords, out)
+    return out, rc
 
 
 class PhaseParams:

@@ -72,6 +72,12 @@ def lib():
                                     _f32p, _f32p, _u8p, C.c_size_t, _i32p, _u8p, _f32p, C.c_int, C.c_int,
                                     C.c_float, C.c_float, _f32p, _u64p, C.c_void_p, C.c_void_p, _f32p, _f32p,
                                     _f32p, _i32p, _i32p, _u8p]
+        L.eo_rle_encode.restype = C.c_long
+        L.eo_rle_encode.argtypes = [_u64p, C.c_size_t, _u8p]
+        L.eo_rle_decode.restype = C.c_int
+        L.eo_rle_decode.argtypes = [_u8p, C.c_size_t, _u64p, C.c_size_t]
+        L.eo_qref_decode.restype = C.c_int
+        L.eo_qref_decode.argtypes = [_u8p, C.c_size_t, C.c_size_t, C.c_size_t, _u64p]
         L.eo_phase.restype = C.c_int
         L.eo_phase.argtypes = [_u8p, _u64p, _u64p, _f32p, C.c_size_t, C.c_size_t, C.POINTER(PhaseParamsC),
                                _u64p, _u64p, _f32p, _f32p, C.POINTER(C.c_float), C.POINTER(C.c_size_t)]
@@ -156,6 +162,46 @@ def impute(matches, absperm, sitemajor_full, typed, af_full, nrefhaps, miss, hap
                     np.ascontiguousarray(miss, np.int64) if len(miss) else np.zeros(1, np.int64), len(miss),
                     int(imputeCalls), np.ascontiguousarray(hap_words, np.uint64), bits, dos, imp)
     return bits, dos, imp
+
+
+def rle_encode(words: np.ndarray):
+    """runlengthEncode (utils.h:155-191): bytes, or None (not shorter)."""
+    w = np.ascontiguousarray(words, np.uint64)
+    out = np.zeros(w.size * 8 + 3, np.uint8)
+    n = lib().eo_rle_encode(w, w.size, out)
+    return None if n < 0 else out[:n].copy()
+
+
+def rle_decode(enc: np.ndarray, nwords: int):
+    """runlengthDecode (utils.h:194-) without masked samples: (words, status)
+    with status -1 for a truncated sequence."""
+    e = np.ascontiguousarray(enc, np.uint8)
+    out = np.zeros(nwords, np.uint64)
+    rc = lib().eo_rle_decode(e if e.size else np.zeros(1, np.uint8), e.size, out, nwords)
+    return out, rc
+
+
+def qref_section(rows: np.ndarray) -> np.ndarray:
+    """The haplotype section of a Qref file (qref_spec.md section I) for the
+    site-major rows: each variant as <encsize u64><run-length bytes>, or
+    <0><raw row> where the run-length code is not shorter."""
+    parts = []
+    for r in np.ascontiguousarray(rows, np.uint64):
+        enc = rle_encode(r)
+        if enc is None:
+            parts += [np.zeros(8, np.uint8), r.view(np.uint8)]
+        else:
+            parts += [np.array([len(enc)], np.uint64).view(np.uint8), enc]
+    return np.concatenate(parts) if parts else np.zeros(0, np.uint8)
+
+
+def qref_decode(section: np.ndarray, Mref: int, nwords: int):
+    """The Qref haplotype section decoded into Mref rows (VCFData::qRefLoadNextVariant):
+    (rows, status) -- 0, -1 truncated run-length sequence, -2 short section."""
+    s = np.ascontiguousarray(section, np.uint8)
+    out = np.zeros((Mref, nwords), np.uint64)
+    rc = lib().eo_qref_decode(s if s.size else np.zeros(1, np.uint8), s.size, Mref, nwords, out)
+    return out, rc
 
 
 def site_stats(mref_begin, bits, dos, phased, pdm, pdp, gt, typed, Mref, af_full, overwriteCalls=False,

@@ -123,6 +123,13 @@ template <class T> inline T emu_shfl_up(int site, T v, int d) {
     emu_leave();
     return r;
 }
+template <class T> inline T emu_shfl_down(int site, T v, int d) {
+    emu_enter(site, emu_bits(v), true);
+    const int l = emu_lane();
+    T r = l + d < 32 ? emu_from<T>(emu_warp->vals[l + d]) : v;
+    emu_leave();
+    return r;
+}
 template <class T> inline T emu_shfl_xor(int site, T v, int m) {
     emu_enter(site, emu_bits(v), true);
     T r = emu_from<T>(emu_warp->vals[(emu_lane() ^ m) & 31]);
@@ -135,6 +142,7 @@ template <class T> inline T emu_shfl_xor(int site, T v, int m) {
 #define __shfl_sync(m, v, s) emu_shfl(__LINE__, (v), (s))
 #define __shfl_up_sync(m, v, d) emu_shfl_up(__LINE__, (v), (d))
 #define __shfl_xor_sync(m, v, x) emu_shfl_xor(__LINE__, (v), (x))
+#define __shfl_down_sync(m, v, d) emu_shfl_down(__LINE__, (v), (d))
 
 inline int __popc(unsigned x) { return __builtin_popcount(x); }
 inline int __popcll(unsigned long long x) { return __builtin_popcountll(x); }
@@ -170,6 +178,13 @@ inline int atomicMin(int *p, int v) {
     return o;
 }
 inline unsigned atomicOr(unsigned *p, unsigned v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned long long atomicOr(unsigned long long *p, unsigned long long v) {
+    return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST);
+}
+inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
+    const uint64_t v = ((uint64_t)hi << 32) | lo;
+    return (unsigned)(v >> (sh & 31));
+}
 inline unsigned long long atomicAdd(unsigned long long *p, unsigned long long v) {
     return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);
 }
