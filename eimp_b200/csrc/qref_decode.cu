@@ -14,8 +14,9 @@
 // vector is copied with 32-bit loads realigned by funnel shifts (the section
 // interleaves 8-byte sizes with odd-length codes, so a vector can start at
 // any byte).  A run-length code is read 32 bytes at a time: a ballot of the
-// bytes' high bits and a walk along them give the bytes that start a run
-// length (a length is one byte, or two when the first has its high bit set);
+// bytes' high bits and a few bit operations on it give the bytes that start
+// a run length (a length is one byte, or two when the first has its high bit
+// set);
 // a warp scan of the lengths gives every run's first bit; runs alternate
 // 0/1 starting with 0, and the lanes holding runs of ones set them in the
 // zeroed row.  HBM-bound: each variant reads its code and writes its row.
@@ -65,19 +66,34 @@ __global__ void __launch_bounds__(128) qref_decode_kernel(const uint8_t *__restr
     const uint64_t nbits = (uint64_t)nwords * 64;
     int carry = 0;            // the chunk starts with the second byte of a run length
     unsigned long long runs = 0, pos = 0, last_start = 0;
+    unsigned bnext = lane < encsize ? enc[lane] : 0u;   // the chunks are loaded one ahead
     for (uint64_t base = 0; base < encsize; base += 32) {
         const uint64_t i = base + lane;
         const bool in = i < encsize;
-        const unsigned b = in ? enc[i] : 0u;
+        const unsigned b = bnext;
+        bnext = i + 32 < encsize ? enc[i + 32] : 0u;
         const unsigned hi = __ballot_sync(0xffffffffu, in && (b & 0x80u));
         const int nvalid = (int)min((uint64_t)32, encsize - base);
-        unsigned sm = 0;
-        int q = carry;
-        while (q < nvalid) { sm |= 1u << q; q += 1 + (int)((hi >> q) & 1u); }
-        const int ncarry = q - nvalid;
+        // the bytes that start a run length, bit-parallel: inside every run of
+        // high-bit bytes that begins at a start p, the bytes p+1, p+3, ... (up
+        // to the byte after the run) are second bytes.  Adding a run's first
+        // bit to the run carries through it; the carried bits at odd distance
+        // from p are those second bytes.
+        const uint64_t vmask = (1ull << nvalid) - 1ull;
+        uint64_t H = (uint64_t)hi & vmask;
+        if (carry) H &= ~1ull;   // byte 0 is the second byte of the previous chunk's last length
+        const uint64_t P = H & ~(H << 1);
+        const uint64_t EV = 0x5555555555555555ull, OD = 0xAAAAAAAAAAAAAAAAull;
+        const uint64_t pe = P & EV, po = P & OD;
+        const uint64_t cont = (((H + pe) ^ H ^ pe) & OD) | (((H + po) ^ H ^ po) & EV);
+        uint64_t S = vmask & ~cont;
+        if (carry) S &= ~1ull;
+        const unsigned sm = (unsigned)S;
+        const int ncarry = (int)((cont >> nvalid) & 1ull);
         const bool start = (sm >> lane) & 1u;
         unsigned nb = __shfl_down_sync(0xffffffffu, b, 1);
-        if (lane == 31) nb = (i + 1 < encsize) ? enc[i + 1] : 0u;
+        const unsigned nb0 = __shfl_sync(0xffffffffu, bnext, 0);   // the next chunk's first byte
+        if (lane == 31) nb = nb0;
         const unsigned len = start ? ((b & 0x80u) ? ((nb & 0xffu) << 7) | (b & 0x7fu) : b) : 0u;
         unsigned incl = len;
         for (int o = 1; o < 32; o <<= 1) {
