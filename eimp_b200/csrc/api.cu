@@ -63,6 +63,8 @@ struct eimp_ctx {
 
     // phasing reference
     size_t p_M = 0, p_nhaps = 0;
+    // phasing iterations after the first: reference sample of target 0 (-1: none)
+    int64_t self0 = -1;
     DBuf p_hapmajor, p_sitemajor, p_cm;
     // phasing batch scratch
     DBuf b_gt, b_nerr, b_bh, b_flags, b_monos, b_splits, b_calls, b_cmd, b_nsplits, b_ncalls, b_rowoff, b_cref,
@@ -134,6 +136,15 @@ int check_status(eimp_ctx *ctx) {
         return fail(ctx, EIMP_E_CAPACITY, b);
     }
     return 0;
+}
+
+// K of a phasing call: at most the haplotypes a target may choose from --
+// all of the panel, or all but its own two in iterations after the first
+// (PBWTPhaser.cpp:408-476: localK = min(K, localNrefhapsCorr))
+size_t phase_K(const eimp_ctx *ctx, const eimp_phase_params *p) {
+    const size_t nh = ctx->p_nhaps;
+    const size_t corr = ctx->self0 >= 0 && nh >= 2 ? nh - 2 : nh;
+    return (size_t)p->K < corr ? (size_t)p->K : corr;
 }
 
 }  // namespace
@@ -482,6 +493,14 @@ int eimp_imp_bunch_stats(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const 
     return 0;
 }
 
+int eimp_phase_exclude_self(eimp_ctx *ctx, int64_t first_sample) {
+    if (!ctx) return EIMP_E_ARG;
+    if (first_sample >= 0 && (size_t)first_sample >= ctx->p_nhaps / 2)
+        return fail(ctx, EIMP_E_ARG, "eimp_phase_exclude_self: sample outside the phasing reference");
+    ctx->self0 = first_sample < 0 ? -1 : first_sample;
+    return 0;
+}
+
 int eimp_qref_index(const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref, int64_t *offsets) {
     if ((!section && nbytes) || (!offsets && Mref)) return EIMP_E_ARG;
     const size_t raw = eimp_W(2 * Nref) * 8;   // hapcapacity: 2*Nref bits in 512-bit units
@@ -597,7 +616,9 @@ namespace {
 // device-side prepPhase for ntgt targets whose genotypes are at d_gt
 int run_prep(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt) {
     const size_t M = ctx->p_M, nh = ctx->p_nhaps, wM = eimp_W(M), wN = eimp_W(nh);
-    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    const size_t K = phase_K(ctx, p);
+    if (ctx->self0 >= 0 && (size_t)ctx->self0 + ntgt > nh / 2)
+        return fail(ctx, EIMP_E_ARG, "the batch's own samples lie outside the phasing reference");
     cudaStream_t st = ctx->stream;
     CK(ctx->b_nerr.reserve(ntgt * nh * 4));
     CK(ctx->b_bh.reserve(ntgt * K * 4));
@@ -610,7 +631,7 @@ int run_prep(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8
     CK(ctx->b_ncalls.reserve(ntgt * 4));
     LAUNCH(launch_besthaps(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)nh, (int)wM, (int)K,
                            ctx->b_nerr.as<uint32_t>(), ctx->b_bh.as<int32_t>(), ctx->b_flags.as<uint64_t>(), (int)wN,
-                           st));
+                           (int)ctx->self0, st));
     LAUNCH(launch_monos_calls(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)wM,
                               ctx->b_bh.as<int32_t>(), (int)K, ctx->p_cm.as<float>(), p->cMmaxsplit,
                               ctx->b_monos.as<uint64_t>(), ctx->b_splits.as<int32_t>(), ctx->b_calls.as<int32_t>(),
@@ -678,7 +699,7 @@ int eimp_phase_prep(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, cons
     if (!gt) return fail(ctx, EIMP_E_ARG, "eimp_phase_prep: NULL genotypes");
     if (int r = use_device(ctx)) return r;
     const size_t M = ctx->p_M, nh = ctx->p_nhaps, wM = eimp_W(M), wN = eimp_W(nh);
-    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    const size_t K = phase_K(ctx, p);
     cudaStream_t st = ctx->stream;
     CK(ctx->b_gt.reserve(ntgt * M));
     CK(cudaMemcpyAsync(ctx->b_gt.p, gt, ntgt * M, cudaMemcpyHostToDevice, st));
@@ -701,7 +722,7 @@ int eimp_phase_cref_pbwt(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt,
     if (!gt || !rows_out) return fail(ctx, EIMP_E_ARG, "eimp_phase_cref_pbwt: NULL argument");
     if (int r = use_device(ctx)) return r;
     const size_t M = ctx->p_M, nh = ctx->p_nhaps;
-    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    const size_t K = phase_K(ctx, p);
     cudaStream_t st = ctx->stream;
     CK(ctx->b_gt.reserve(ntgt * M));
     CK(cudaMemcpyAsync(ctx->b_gt.p, gt, ntgt * M, cudaMemcpyHostToDevice, st));
@@ -750,7 +771,7 @@ int make_beam_params(eimp_ctx *ctx, const eimp_phase_params *p, size_t K, BeamPa
 int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8_t *d_gt, uint64_t *d_mats,
               uint64_t *d_pats, float *d_dm, float *d_dp, float *d_tc, int32_t *d_nc) {
     const size_t M = ctx->p_M, nh = ctx->p_nhaps;
-    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    const size_t K = phase_K(ctx, p);
     BeamParams bp;
     if (int r = make_beam_params(ctx, p, K, bp)) return r;
     ctx->tvalid = false;
@@ -785,7 +806,7 @@ int eimp_phase_reserve(eimp_ctx *ctx, const eimp_phase_params *p, size_t max_tar
     if (int r = check_phase_args(ctx, p, max_targets)) return r;
     if (int r = use_device(ctx)) return r;
     const size_t M = ctx->p_M, nh = ctx->p_nhaps, wM = eimp_W(M), wN = eimp_W(nh);
-    const size_t K = (size_t)p->K < nh ? (size_t)p->K : nh;
+    const size_t K = phase_K(ctx, p);
     BeamParams bp;
     bp.K = (int)K;
     if (int r = make_beam_params(ctx, p, K, bp)) return r;

@@ -60,7 +60,8 @@ cudaError_t launch_qref_decode(const uint8_t *sec, const int64_t *offs, int Mref
 
 // ---- phasing preparation, condensed reference, PBWT (phase_prep.cu)
 cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int nhaps, int wM, int K,
-                            uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, cudaStream_t st);
+                            uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, int self0,
+                            cudaStream_t st);
 cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM,
                                const int32_t *besthaps, int K, const float *cm, float cMmaxsplit, uint64_t *monos,
                                int32_t *splits, int32_t *calls, float *cmdiffs, int32_t *nsplits, int32_t *ncalls,

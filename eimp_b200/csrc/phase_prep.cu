@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
                                                       const uint64_t *__restrict__ hapmajor, int nhaps, int wM,
                                                       int K, uint32_t *__restrict__ nerr_scratch,
                                                       int32_t *__restrict__ besthaps, uint64_t *__restrict__ flags,
-                                                      int wN) {
+                                                      int wN, int self0) {
     extern __shared__ uint64_t sm[];
     uint64_t *is0 = sm, *is2 = sm + wM;
     __shared__ int buf[32];
@@ -69,6 +69,22 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
     int32_t *bh = besthaps + (size_t)t * K;
     uint64_t *fl = flags + (size_t)t * wN;
     for (int w = tid; w < wN; w += nt) fl[w] = 0ull;
+    // phasing iterations after the first: the panel ends with the phased
+    // targets and a target ignores its own two haplotypes (Target.cpp:791-796)
+    const int ign = self0 >= 0 ? 2 * (self0 + t) : -2;
+    if (ign >= 0 && K >= nhaps - 2) {   // all but the target's own (Target.cpp:798-811)
+        for (int h = tid; h < nhaps; h += nt)
+            if (h != ign && h != ign + 1) bh[h < ign ? h : h - 2] = h;
+        __syncthreads();
+        for (int w = tid; w < wN; w += nt) {
+            int lo = w * 64;
+            uint64_t f = lo + 64 <= nhaps ? ~0ull : (lo >= nhaps ? 0ull : ((1ull << (nhaps - lo)) - 1));
+            for (int j = ign; j <= ign + 1; j++)
+                if (j >= lo && j < lo + 64) f &= ~(1ull << (j - lo));
+            fl[w] = f;
+        }
+        return;
+    }
     if (K >= nhaps) {
         for (int h = tid; h < nhaps; h += nt) bh[h] = h;
         __syncthreads();
@@ -82,7 +98,7 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
         const uint64_t *row = hapmajor + (size_t)h * wM;
         uint32_t e = 0;
         for (int w = 0; w < wM; w++) e += __popcll((is0[w] & row[w]) | (is2[w] & ~row[w]));
-        nerr[h] = e;
+        nerr[h] = (h == ign || h == ign + 1) ? 0xffffffffu : e;   // never selected
     }
     __syncthreads();
     // smallest threshold thr with #(nerr <= thr) >= K
@@ -122,13 +138,14 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
 }
 
 cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int nhaps, int wM, int K,
-                            uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, cudaStream_t st) {
+                            uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, int self0,
+                            cudaStream_t st) {
     size_t sm = (size_t)2 * wM * sizeof(uint64_t);
     if (sm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(besthaps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
-    besthaps_kernel<<<ntgt, 512, sm, st>>>(gt, M, hapmajor, nhaps, wM, K, nerr_scratch, besthaps, flags, wN);
+    besthaps_kernel<<<ntgt, 512, sm, st>>>(gt, M, hapmajor, nhaps, wM, K, nerr_scratch, besthaps, flags, wN, self0);
     return cudaGetLastError();
 }
 

@@ -139,13 +139,25 @@ class Phaser:
         self.ctx = ctx
         self.nhaps, self.wM = hapmajor.shape
         self.M = sitemajor.shape[0]
+        self.self0 = -1
+        ctx.check(ctx.L.eimp_phase_exclude_self(ctx.h, -1))
         ctx.check(ctx.L.eimp_phase_set_reference(ctx.h, self.M, self.nhaps, ptr(_c(hapmajor, np.uint64)),
                                                  ptr(_c(sitemajor, np.uint64)), ptr(_c(cm, np.float32))))
+
+    def excludeSelf(self, first_sample: int):
+        """Phasing iterations after the first: target t is sample
+        first_sample + t of this reference and leaves its own haplotypes out
+        of its best haplotypes (Target.cpp:791-811); -1 turns it off."""
+        self.ctx.check(self.ctx.L.eimp_phase_exclude_self(self.ctx.h, int(first_sample)))
+        self.self0 = int(first_sample)
+
+    def _K(self, params: PhaseParams) -> int:
+        return min(params.K, self.nhaps - 2 if self.self0 >= 0 else self.nhaps)
 
     def prep(self, params: PhaseParams, gt: np.ndarray):
         gt = _c(gt, np.uint8)
         n, M = gt.shape
-        K = min(params.K, self.nhaps)
+        K = self._K(params)
         out = dict(besthaps=np.zeros((n, K), np.int32), flags=np.zeros((n, W(self.nhaps)), np.uint64),
                    monos=np.zeros((n, W(M)), np.uint64), splits=np.zeros((n, M), np.int32),
                    calls=np.zeros((n, M), np.int32), cmdiffs=np.zeros((n, M + 1), np.float32),
@@ -158,7 +170,7 @@ class Phaser:
     def cref_pbwt(self, params: PhaseParams, gt: np.ndarray):
         gt = _c(gt, np.uint8)
         n = gt.shape[0]
-        K = min(params.K, self.nhaps)
+        K = self._K(params)
         p = params.c()
         rows = C.c_size_t(0)
         self.ctx.check(self.ctx.L.eimp_phase_cref_pbwt(self.ctx.h, C.byref(p), n, ptr(gt), C.byref(rows),
@@ -191,6 +203,40 @@ class Phaser:
         n = d_gt.shape[0]
         self.ctx.check(self.ctx.L.eimp_phase_targets_dev(self.ctx.h, C.byref(p), n, ptr(d_gt), ptr(d_mats),
                                                          ptr(d_pats), ptr(d_dm), ptr(d_dp), ptr(d_tc), ptr(d_nc)))
+
+
+def _transpose_bits(rows: np.ndarray, ncols: int) -> np.ndarray:
+    """Bit matrix rows x ncols (row words) -> ncols x rows (padded rows)."""
+    from .bits import pack_rows, unpack_rows
+    return pack_rows(np.ascontiguousarray(unpack_rows(rows, ncols).T), W(rows.shape[0]))
+
+
+def phase_iterations(ctx: Context, hapmajor: np.ndarray, sitemajor: np.ndarray, cm: np.ndarray,
+                     params: PhaseParams, gt: np.ndarray, iters: int):
+    """PBWTPhaser's phasing iterations (PBWTPhaser.cpp:406-476, --phaseIters):
+    iteration 1 phases the targets against the reference; every further
+    iteration phases them again against the reference followed by the phased
+    targets of the previous iteration, each target leaving its own
+    haplotypes out; reverse phasing and the call confidences only in the last
+    iteration.  Returns the last iteration's (mats, pats, dm, dp, tc, nc)."""
+    import dataclasses
+    gt = _c(gt, np.uint8)
+    n, M = gt.shape
+    nh = hapmajor.shape[0]
+    ph = Phaser(ctx, hapmajor, sitemajor, cm)
+    out = None
+    for it in range(1, iters + 1):
+        p = dataclasses.replace(params, doRevPhasing=params.doRevPhasing and it == iters)
+        if it > 1:
+            mats, pats = out[0], out[1]
+            tgt = np.empty((2 * n, mats.shape[1]), np.uint64)
+            tgt[0::2], tgt[1::2] = mats, pats
+            aug = np.concatenate([_c(hapmajor, np.uint64), tgt])
+            ph = Phaser(ctx, aug, _transpose_bits(aug, M), cm)
+            ph.excludeSelf(nh // 2)
+        out = ph.phase(p, gt)
+    ph.excludeSelf(-1)
+    return out
 
 
 class PBWTImputer:

@@ -153,6 +153,16 @@ int eimp_phase_cref_pbwt(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt,
 /* Target::phase (Target.cpp:166-289) for a batch of diploid targets: mats/pats
  * ntgt x W(M) words, dos_mats/dos_pats ntgt x M floats, totalconf and
  * ncallsites per target (Target.h:73-74). */
+/* Phasing iterations after the first (PBWTPhaser.cpp:406-476): the phasing
+ * reference is the panel followed by the phased targets of the previous
+ * iteration (target t as sample first_sample + t), and target t of the
+ * following phasing calls leaves its own sample out of its best haplotypes
+ * (Target::findBestHaps, Target.cpp:791-811), K at most the panel's
+ * haplotypes minus 2.  first_sample < 0 turns it off (the first iteration).
+ * No counterpart function in the reference, which passes the index through
+ * its Target objects. */
+int eimp_phase_exclude_self(eimp_ctx *ctx, int64_t first_sample);
+
 /* Capacity mode for phasing (no counterpart in the reference): reserves the
  * batch buffers for up to max_targets targets and max_rows condensed rows
  * (sum over the targets of 2*S_t+1).  Afterwards the row offsets are computed

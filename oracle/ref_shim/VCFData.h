@@ -40,7 +40,10 @@ public:
     const RingBuffer<fp_type> &getCMPos() const { return cMs; }
     const vector<string> &getTargetIDs() const { return targetIDs; }
 
-    size_t getNReferenceHaps() const { return Nrefhaps; }
+    // in phasing iterations after the first the panel holds the reference
+    // haplotypes followed by the phased targets: getNReferenceHaps is the
+    // reference part, getNReferenceHapsMax all of it (VCFData.h of the reference)
+    size_t getNReferenceHaps() const { return NrefhapsOrig ? NrefhapsOrig : Nrefhaps; }
     size_t getNReferenceHapsMax() const { return Nrefhaps; }
     size_t getNTarget() const { return Ntarget; }
     size_t getNSNPs() const { return M; }
@@ -57,6 +60,7 @@ public:
     Haplotype getStartPhase(size_t targetidx) const { return toHap(chunkStartPhase[targetidx]); }
 
     // plain storage, filled by the oracle driver
+    size_t NrefhapsOrig = 0;
     vector<BooleanVector> reference;
     RingBuffer<BooleanVector> referenceT;
     vector<BooleanVector> referenceFullT;

@@ -60,6 +60,10 @@ size_t capBytes(size_t nbits) { return roundToMultiple(nbits, UNITWORDS * sizeof
 
 struct Handle {
     VCFData vd;
+    bool lastIter = true;
+    // NrefhapsCorrected of PBWTPhaser (PBWTPhaser.cpp:408-476): all
+    // haplotypes, or all but the target's own two in iterations after the first
+    size_t ncorr() const { return vd.NrefhapsOrig ? vd.Nrefhaps - 2 : vd.Nrefhaps; }
     std::vector<uint64_t*> bufs;
     ~Handle() { for (auto p : bufs) free(p); }
     uint64_t *alloc(size_t bytes) {
@@ -153,6 +157,16 @@ void *refo_create(size_t nhaps, size_t M, size_t Mref,
 
 void refo_destroy(void *hp) { delete (Handle*)hp; }
 
+/* Phasing iteration after the first (PBWTPhaser.cpp:406-476): the handle's
+ * panel is the reference (nhaps_orig haplotypes) followed by the phased
+ * targets; last_iter as Target's lastIter (reverse phasing and call
+ * confidences only in the last iteration). */
+void refo_set_iteration(void *hp, size_t nhaps_orig, int last_iter) {
+    Handle *h = (Handle*)hp;
+    h->vd.NrefhapsOrig = nhaps_orig;
+    h->lastIter = last_iter != 0;
+}
+
 void refo_set_params(int hsize, int beamwidth, int delta, float cMmaxsplit,
                      int hsize_fast, int beamwidth_fast, int delta_fast) {
     setParams(hsize, beamwidth, delta, cMmaxsplit, hsize_fast, beamwidth_fast, delta_fast);
@@ -167,7 +181,7 @@ long refo_prep(void *hp, size_t t, size_t K,
     Handle *h = (Handle*)hp;
     VCFData &v = h->vd;
     BooleanVector pm, pp; std::vector<float> dm, dp;
-    Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, v.Nrefhaps, K,
+    Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, h->ncorr(), K,
               2.0f, 1.0f, 0.003f, 0.003f, false, true, true, false, false, false);
     tg.prepPhase();
     for (size_t k = 0; k < K; k++) besthaps[k] = tg.bestHaps[k];
@@ -187,7 +201,7 @@ long refo_cref_pbwt(void *hp, size_t t, size_t K, uint64_t *cref, int *count0, u
     Handle *h = (Handle*)hp;
     VCFData &v = h->vd;
     BooleanVector pm, pp; std::vector<float> dm, dp;
-    Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, v.Nrefhaps, K,
+    Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, h->ncorr(), K,
               2.0f, 1.0f, 0.003f, 0.003f, false, true, true, false, false, false);
     tg.prepPhase();
     size_t Mp = 2 * tg.splitsites.size() + 1;
@@ -222,8 +236,8 @@ int refo_phase(void *hp, size_t t, size_t K, float expectIBDcM, float hist, floa
     BooleanVector pm(md, cap, 0), pp(pd, cap, 0);
     std::vector<float> dm, dp;
     {
-        Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, v.Nrefhaps, K,
-                  expectIBDcM, hist, pErr, pLimit, doPrePhasing, doRevPhasing, true, false, false, false);
+        Target tg(pm, pp, dm, dp, t, v.targetIDs[t], v, v.Nrefhaps, h->ncorr(), K,
+                  expectIBDcM, hist, pErr, pLimit, doPrePhasing, doRevPhasing, h->lastIter, false, false, false);
         tg.phase();
         *totalconf = tg.getTotalConfidence();
         *ncallsites = tg.getNCallSites();

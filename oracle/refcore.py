@@ -40,6 +40,7 @@ def lib():
         L.refo_create.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t, _u64p, _u64p, _u64p, _i64p,
                                   _f32p, _f32p, _f32p, C.c_size_t, _u8p]
         L.refo_destroy.argtypes = [C.c_void_p]
+        L.refo_set_iteration.argtypes = [C.c_void_p, C.c_size_t, C.c_int]
         L.refo_set_params.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int]
         L.refo_prep.restype = C.c_long
         L.refo_prep.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, _i64p, _u64p, _i64p, _i64p,
@@ -141,6 +142,42 @@ class RefCore:
                                cm, self.af_full, self.af_common, self.ntarget, self.gt)
         self.params = None
 
+    @classmethod
+    def typed_only(cls, hapmajor_typed, sitemajor_typed, cm_typed, gt, af_common):
+        """A handle over a typed-site panel only (phasing; no imputation) --
+        e.g. the panel of a phasing iteration after the first, the reference
+        haplotypes followed by the phased targets."""
+        self = cls.__new__(cls)
+        L = lib()
+        self.nhaps = hapmajor_typed.shape[0]
+        self.M = sitemajor_typed.shape[0]
+        self.Mref = self.M
+        self.typed = np.arange(self.M, dtype=np.int64)
+        self.ntarget = gt.shape[0]
+        self.hapmajor_typed = np.ascontiguousarray(hapmajor_typed, np.uint64)
+        self.sitemajor_typed = np.ascontiguousarray(sitemajor_typed, np.uint64)
+        self.cm_typed = np.ascontiguousarray(cm_typed, np.float32)
+        self.sitemajor_full = self.sitemajor_typed
+        self.af_common = np.ascontiguousarray(af_common, np.float32)
+        self.af_full = self.af_common
+        self.gt = np.ascontiguousarray(gt, np.uint8)
+        self.h = L.refo_create(self.nhaps, self.M, self.Mref, self.hapmajor_typed, self.sitemajor_typed,
+                               self.sitemajor_full, self.typed, self.cm_typed, self.af_full, self.af_common,
+                               self.ntarget, self.gt)
+        self.params = None
+        return self
+
+    @property
+    def ncorr(self) -> int:
+        """Haplotypes a target chooses its K best from (PBWTPhaser.cpp:408-476)."""
+        return self.nhaps - 2 if getattr(self, "nhaps_orig", 0) else self.nhaps
+
+    def set_iteration(self, nhaps_orig: int, last_iter: bool):
+        """Phasing iteration after the first: the first nhaps_orig haplotypes
+        are the reference, target t is sample nhaps_orig/2 + t of the panel."""
+        lib().refo_set_iteration(self.h, nhaps_orig, int(last_iter))
+        self.nhaps_orig = nhaps_orig
+
     def close(self):
         if self.h:
             lib().refo_destroy(self.h)
@@ -158,7 +195,7 @@ class RefCore:
                               p.beamwidth_fast, p.delta_fast)
 
     def prep(self, t: int):
-        K = min(self.params.K, self.nhaps)
+        K = min(self.params.K, self.ncorr)
         bh = np.zeros(K, np.int64)
         monos = np.zeros(W(self.M), np.uint64)
         splits = np.zeros(self.M + 1, np.int64)
@@ -170,7 +207,7 @@ class RefCore:
                     cmdiffs=diffs[:S + 1].copy() if nc.value else diffs[:0].copy())
 
     def cref_pbwt(self, t: int):
-        K = min(self.params.K, self.nhaps)
+        K = min(self.params.K, self.ncorr)
         Mp = lib().refo_cref_pbwt(self.h, t, K, None, None, None)
         cref = np.zeros((Mp, W(K)), np.uint64)
         c0 = np.zeros(Mp, np.int32)
@@ -181,7 +218,7 @@ class RefCore:
 
     def phase(self, t: int):
         p = self.params
-        K = min(p.K, self.nhaps)
+        K = min(p.K, self.ncorr)
         mat = np.zeros(W(self.M), np.uint64)
         pat = np.zeros(W(self.M), np.uint64)
         dm = np.zeros(self.M, np.float32)
@@ -194,7 +231,7 @@ class RefCore:
 
     def phase_range(self, t0: int, t1: int, nthreads: int):
         p = self.params
-        K = min(p.K, self.nhaps)
+        K = min(p.K, self.ncorr)
         n = t1 - t0
         mats = np.zeros((n, W(self.M)), np.uint64)
         pats = np.zeros((n, W(self.M)), np.uint64)

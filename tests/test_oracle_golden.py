@@ -88,3 +88,43 @@ def test_imputation(g):
         # a 60 %-missing target yields no matches and only dosage conflicts
         if h // 2 == gt.shape[0] - 1:
             assert len(m) == 0 and np.all(dos[sel] == -1.0)
+
+
+def test_transpose_bits_round_trip():
+    """The host transposition used to build the panel of a phasing iteration."""
+    from eimp_b200.bits import pack_rows, unpack_rows
+    from eimp_b200.engine import _transpose_bits
+    rng = np.random.default_rng(3)
+    b = (rng.random((37, 1000)) < 0.3).astype(np.uint8)
+    rows = pack_rows(b, W(1000))
+    t = _transpose_bits(rows, 1000)
+    assert t.shape == (1000, W(37))
+    np.testing.assert_array_equal(unpack_rows(t, 37), b.T)
+
+
+def test_reference_iteration_excludes_own_sample():
+    """The reference's findBestHaps in an iteration after the first
+    (Target.cpp:791-841), run from its own sources: a target never picks its
+    own two haplotypes from the panel of reference + phased targets, and with
+    K at least the other haplotypes it takes all of those in order."""
+    from oracle import refcore
+    if not refcore.available():
+        pytest.skip("reference sources not compiled (oracle/_ref)")
+    from eimp_b200.engine import _transpose_bits
+    g = np.load(golden_path("golden_tiny.npz"))
+    hm, cm, gt = g["hapmajor_typed"], g["cm_typed"], g["gt"]
+    n, M = gt.shape
+    nh = hm.shape[0]
+    tgt = np.empty((2 * n, hm.shape[1]), np.uint64)
+    tgt[0::2], tgt[1::2] = g["K64_mat"], g["K64_pat"]
+    aug = np.concatenate([hm, tgt])
+    rc = refcore.RefCore.typed_only(aug, _transpose_bits(aug, M), cm, gt, g["af_full"][g["typed"]])
+    rc.set_iteration(nh, True)
+    for K in (64, 1000):
+        rc.set_params(refcore.PhaseParams(K=K))
+        for t in range(n):
+            bh = rc.prep(t)["besthaps"]
+            assert nh + 2 * t not in bh and nh + 2 * t + 1 not in bh
+            if K == 1000:
+                np.testing.assert_array_equal(bh, [h for h in range(nh + 2 * n) if h // 2 != nh // 2 + t])
+    rc.close()
