@@ -34,6 +34,7 @@ __device__ __forceinline__ float one_minus(float x) {   // `1.0 - x` with x floa
     return (float)__dsub_rn(1.0, (double)x);
 }
 
+template <bool DS, bool GP>
 __global__ void __launch_bounds__((SS_PROD + 1) * 32, 3) site_stats_kernel(SiteStatsArgs a) {
     __shared__ float tsum[2][SS_CHUNK][32], tsq[2][SS_CHUNK][32];
     __shared__ int wac[SS_PROD][32];
@@ -46,6 +47,10 @@ __global__ void __launch_bounds__((SS_PROD + 1) * 32, 3) site_stats_kernel(SiteS
     const bool isimputed = !a.common[mref];
     const int psite = a.segm[mref];
     const int nchunks = (a.ntgt + SS_CHUNK - 1) / SS_CHUNK;
+    // row strides of one target (two haplotype rows); a producer warp's next
+    // target is SS_PROD targets further
+    const size_t sD = (size_t)2 * a.ldd, sA = (size_t)2 * a.lda;
+    const size_t sB = (size_t)4 * a.ldb, sG = (size_t)4 * a.ldg;   // in 32-bit words
     double adsum = 0.0, ad2sum = 0.0;   // summing warp
     int ac1 = 0;
     unsigned long long conflicts = 0;
@@ -53,18 +58,25 @@ __global__ void __launch_bounds__((SS_PROD + 1) * 32, 3) site_stats_kernel(SiteS
         if (wid < SS_PROD && c < nchunks) {
             float(*bs)[32] = tsum[c & 1];
             float(*bq)[32] = tsq[c & 1];
+            const int ib = c * SS_CHUNK + wid;   // this warp's first target of the chunk
+            const float *dp = a.dos + (size_t)ib * sD + s;
+            const uint32_t *bp = reinterpret_cast<const uint32_t *>(a.bits) + (size_t)ib * sB + (s >> 5);
+            float *ap = a.ads + (size_t)ib * sA + s;
+            uint32_t *gp32 = reinterpret_cast<uint32_t *>(a.gtbits) + (size_t)ib * sG + blockIdx.x;
             for (int k0 = 0; k0 < SS_PER; k0 += SS_U) {
                 float r0[SS_U], r1[SS_U], q0[SS_U], q1[SS_U];
                 uint32_t w0[SS_U], w1[SS_U], p01[SS_U];
                 uint8_t g[SS_U];
 #pragma unroll
                 for (int u = 0; u < SS_U; u++) {
-                    const int i = c * SS_CHUNK + (k0 + u) * SS_PROD + wid;
+                    const int i = ib + (k0 + u) * SS_PROD;
                     if (i < a.ntgt) {
-                        r0[u] = a.dos[(size_t)(2 * i) * a.ldd + s];
-                        r1[u] = a.dos[(size_t)(2 * i + 1) * a.ldd + s];
-                        w0[u] = reinterpret_cast<const uint32_t *>(a.bits + (size_t)(2 * i) * a.ldb)[s >> 5];
-                        w1[u] = reinterpret_cast<const uint32_t *>(a.bits + (size_t)(2 * i + 1) * a.ldb)[s >> 5];
+                        const float *d = dp + (size_t)(k0 + u) * SS_PROD * sD;
+                        const uint32_t *b = bp + (size_t)(k0 + u) * SS_PROD * sB;
+                        r0[u] = d[0];
+                        r1[u] = d[a.ldd];
+                        w0[u] = b[0];
+                        w1[u] = b[2 * a.ldb];
                         if (!isimputed) {   // the typed site's call: genotype, phased alleles and dosages
                             g[u] = a.gt[(size_t)i * a.M + psite];
                             p01[u] = bit_at(a.phased + (size_t)(2 * i) * a.wM, psite) |
@@ -77,9 +89,8 @@ __global__ void __launch_bounds__((SS_PROD + 1) * 32, 3) site_stats_kernel(SiteS
 #pragma unroll
                 for (int u = 0; u < SS_U; u++) {
                     const int k = k0 + u;
-                    const int i = c * SS_CHUNK + k * SS_PROD + wid;
+                    const int i = ib + k * SS_PROD;
                     if (i >= a.ntgt) break;   // uniform across the warp
-                    const int h0 = 2 * i, h1 = 2 * i + 1;
                     int hap0, hap1;
                     float ads0, ads1;
                     if (isimputed || a.overwriteCalls || g[u] == 3) {   // :3126-3152, :3246-3270
@@ -116,10 +127,11 @@ __global__ void __launch_bounds__((SS_PROD + 1) * 32, 3) site_stats_kernel(SiteS
                     bs[k * SS_PROD + wid][lane] = __fadd_rn(ads0, ads1);
                     bq[k * SS_PROD + wid][lane] = __fadd_rn(__fmul_rn(ads0, ads0), __fmul_rn(ads1, ads1));
                     if (valid) {
-                        a.ads[(size_t)h0 * a.lda + s] = ads0;
-                        a.ads[(size_t)h1 * a.lda + s] = ads1;
-                        if (a.ds) a.ds[(size_t)i * a.lda + s] = __fadd_rn(ads0, ads1);
-                        if (a.gp) {
+                        float *o = ap + (size_t)k * SS_PROD * sA;
+                        o[0] = ads0;
+                        o[a.lda] = ads1;
+                        if (DS) a.ds[(size_t)i * a.lda + s] = __fadd_rn(ads0, ads1);
+                        if (GP) {
                             const double g0 = __dmul_rn(__dsub_rn(1.0, (double)ads0), __dsub_rn(1.0, (double)ads1));
                             const double g2 = (double)__fmul_rn(ads0, ads1);
                             const double g1 = __dsub_rn(__dsub_rn(1.0, g0), g2);
@@ -133,9 +145,10 @@ __global__ void __launch_bounds__((SS_PROD + 1) * 32, 3) site_stats_kernel(SiteS
                     // the written alleles as bits: the warp's 32 sites are one 32-bit word of each row
                     const unsigned b0 = __ballot_sync(0xffffffffu, valid && hap0);
                     const unsigned b1 = __ballot_sync(0xffffffffu, valid && hap1);
-                    if (lane == 0 && blockIdx.x * 32 < a.nsites) {
-                        reinterpret_cast<uint32_t *>(a.gtbits + (size_t)h0 * a.ldg)[blockIdx.x] = b0;
-                        reinterpret_cast<uint32_t *>(a.gtbits + (size_t)h1 * a.ldg)[blockIdx.x] = b1;
+                    if (lane == 0) {
+                        uint32_t *gw = gp32 + (size_t)k * SS_PROD * sG;
+                        gw[0] = b0;
+                        gw[2 * a.ldg] = b1;
                     }
                 }
             }
@@ -181,7 +194,11 @@ __global__ void __launch_bounds__((SS_PROD + 1) * 32, 3) site_stats_kernel(SiteS
 
 cudaError_t launch_site_stats(const SiteStatsArgs &a, cudaStream_t st) {
     if (a.nsites <= 0) return cudaSuccess;
-    site_stats_kernel<<<(a.nsites + 31) / 32, (SS_PROD + 1) * 32, 0, st>>>(a);
+    const dim3 grid((a.nsites + 31) / 32), block((SS_PROD + 1) * 32);
+    if (a.ds && a.gp) site_stats_kernel<true, true><<<grid, block, 0, st>>>(a);
+    else if (a.ds) site_stats_kernel<true, false><<<grid, block, 0, st>>>(a);
+    else if (a.gp) site_stats_kernel<false, true><<<grid, block, 0, st>>>(a);
+    else site_stats_kernel<false, false><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
 

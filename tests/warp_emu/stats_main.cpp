@@ -88,7 +88,7 @@ int main(int argc, char **argv) {
                 blockDim.x = 32 * nw;
                 emu_warp = &warps[t / 32];
                 emu_block = &block;
-                eimp::site_stats_kernel(a);
+                eimp::site_stats_kernel<true, true>(a);
             });
         for (auto &x : threads) x.join();
     }
