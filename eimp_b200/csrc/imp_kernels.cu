@@ -513,11 +513,13 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
             if (bst) laststart = base + (31 - __clz(bst));
             __syncwarp();
         }
-        // compact into A with remapped parents
+        // compact into A with remapped parents; the largest depth on the way
+        int md = 0;
         for (int u = lane; u < nb; u += 32) {
             const int np = S.idx0[u];
             if (np < 0) continue;
             unsigned x = B.dps[u];
+            md = max(md, dps_depth(x));
             if (u > 0) {
                 int p = dps_parent(x), side = dps_side(x);
                 if (S.idx0[p] < 0) {   // parent removed: take the place of its run's first node
@@ -532,8 +534,6 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
         }
         __syncwarp();
         n = kept;
-        int md = 0;
-        for (int i = lane; i < n; i += 32) md = max(md, dps_depth(A.dps[i]));
         for (int o = 16; o; o >>= 1) md = max(md, __shfl_xor_sync(FULL, md, o));
         // TargetImp.cpp:132-136: the site's matches are set-maximal only if no
         // longer path is still alive
