@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
     if (hap >= nhaps) return;
     if (RETRY && nmatch[hap] != SMM_RETRY) return;
     SmmWarpSmemC<NODES> &S = reinterpret_cast<SmmWarpSmemC<NODES> *>(smem_raw)[wid];
-    SmmTree<NODES> &A = S.A, &B = S.B;
+    SmmTree<NODES> *A = &S.A, *B = &S.B;   // the tree and the one being built; swapped when a site merges nothing
     const uint8_t *g = gt + (size_t)(hap >> 1) * M;
     const uint64_t *hw = phased + (size_t)hap * wM;
     int4 *out = matches + (size_t)hap * cap;
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
 
     uint32_t err = 0;
     int n = 1, nres = 0, td = 0;
-    if (lane == 0) { A.l[0] = 0; A.r[0] = K - 1; A.dps[0] = dps_make(0, -1, 0); A.e[0] = 0; }
+    if (lane == 0) { A->l[0] = 0; A->r[0] = K - 1; A->dps[0] = dps_make(0, -1, 0); A->e[0] = 0; }
     __syncwarp();
 
     for (int m = 0; m <= M; m++) {
@@ -427,9 +427,9 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
             bool e0 = false, e1 = false, dead = false;
             int l0 = 0, r0 = -1, l1 = 0, r1 = -1, vl = 0, vr = -1, d = 0;
             if (i < n) {
-                vl = A.l[i]; vr = A.r[i];
-                d = dps_depth(A.dps[i]);
-                const int ne = A.e[i];
+                vl = A->l[i]; vr = A->r[i];
+                d = dps_depth(A->dps[i]);
+                const int ne = A->e[i];
                 if (!final) pbwt_map(crow, c0, vl, vr, l0, r0, l1, r1);
                 e0 = l0 <= r0 && (missing || !curr || ne < setmaxerrors);
                 e1 = l1 <= r1 && (missing || curr || ne < setmaxerrors);
@@ -440,8 +440,8 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
                 const int p0 = e0 ? 1 + cnt0 + __popc(b0 & lanemask_lt()) : -1;
                 S.idx0[i] = (short)p0;
                 S.idx1[i] = e1 ? (short)(cnt1 + __popc(b1 & lanemask_lt())) : (short)-1;   // offset added below
-                if (p0 >= 0 && p0 < NODES) { B.l[p0] = l0; B.r[p0] = r0; }
-                A.l[i] = l1; A.r[i] = r1;
+                if (p0 >= 0 && p0 < NODES) { B->l[p0] = l0; B->r[p0] = r0; }
+                A->l[i] = l1; A->r[i] = r1;
             }
             if (dead) {
                 const int pos = nres + newcount + __popc(bd & lanemask_lt());
@@ -457,29 +457,33 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
         }
         const int nb = 1 + cnt0 + cnt1;
         if (nb > NODES) { err |= EIMP_ERR_NODE_OVERFLOW; break; }
-        // pass 2: the rest of B = [new root] ++ 0-tree ++ 1-tree
+        // pass 2: the rest of B = [new root] ++ 0-tree ++ 1-tree.  The largest
+        // depth of B is the largest after the merges too: a merged node has a
+        // child, which is deeper
+        int md = 0;
         for (int i = lane; i < n; i += 32) {
-            const unsigned vd = A.dps[i];
-            const int d = dps_depth(vd) + 1, ne = A.e[i];
+            const unsigned vd = A->dps[i];
+            const int d = dps_depth(vd) + 1, ne = A->e[i];
+            if (S.idx0[i] >= 0 || S.idx1[i] >= 0) md = max(md, d);
             const int vp = dps_parent(vd), vs = dps_side(vd);
             const int p0 = S.idx0[i], p1 = S.idx1[i];
             if (p0 >= 0) {
-                B.dps[p0] = dps_make(d, i == 0 ? 0 : S.idx0[vp], i == 0 ? 0 : vs);
-                B.e[p0] = (unsigned char)((curr && !missing) ? ne + 1 : ne);
+                B->dps[p0] = dps_make(d, i == 0 ? 0 : S.idx0[vp], i == 0 ? 0 : vs);
+                B->e[p0] = (unsigned char)((curr && !missing) ? ne + 1 : ne);
             }
             if (p1 >= 0) {
                 const int q = 1 + cnt0 + p1;
-                B.l[q] = A.l[i]; B.r[q] = A.r[i];
-                B.dps[q] = dps_make(d, i == 0 ? 0 : 1 + cnt0 + S.idx1[vp], i == 0 ? 1 : vs);
-                B.e[q] = (unsigned char)((!curr && !missing) ? ne + 1 : ne);
+                B->l[q] = A->l[i]; B->r[q] = A->r[i];
+                B->dps[q] = dps_make(d, i == 0 ? 0 : 1 + cnt0 + S.idx1[vp], i == 0 ? 1 : vs);
+                B->e[q] = (unsigned char)((!curr && !missing) ? ne + 1 : ne);
             }
         }
-        if (lane == 0) { B.l[0] = 0; B.r[0] = K - 1; B.dps[0] = dps_make(0, -1, 0); B.e[0] = 0; }
+        if (lane == 0) { B->l[0] = 0; B->r[0] = K - 1; B->dps[0] = dps_make(0, -1, 0); B->e[0] = 0; }
         for (int q = lane; q < (nb + 15) / 16; q += 32) S.cflag[q] = 0u;
         __syncwarp();
         // pass 3: merges (TargetImp.cpp:405-432).  Child flags first.
         for (int u = 1 + lane; u < nb; u += 32) {
-            const unsigned x = B.dps[u];
+            const unsigned x = B->dps[u];
             const int pa = dps_parent(x);
             atomicOr(&S.cflag[pa >> 4], (1u << dps_side(x)) << ((pa & 15) * 2));
         }
@@ -493,7 +497,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
             if (v >= 1 && v < nb) {
                 const unsigned cf = (S.cflag[v >> 4] >> ((v & 15) * 2)) & 3u;
                 if (cf == 1u || cf == 2u)   // exactly one child: the next entry
-                    rm = B.l[v] == B.l[v + 1] && B.r[v] == B.r[v + 1] && B.e[v] == B.e[v + 1];
+                    rm = B->l[v] == B->l[v + 1] && B->r[v] == B->r[v + 1] && B->e[v] == B->e[v + 1];
             }
             const unsigned brm = __ballot_sync(FULL, rm);
             // a removed run starts where the previous entry is kept
@@ -513,25 +517,24 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
             if (bst) laststart = base + (31 - __clz(bst));
             __syncwarp();
         }
-        // compact into A with remapped parents; the largest depth on the way
-        int md = 0;
-        for (int u = lane; u < nb; u += 32) {
+        // compact into A with remapped parents, or take B as it is
+        for (int u = lane; kept < nb && u < nb; u += 32) {
             const int np = S.idx0[u];
             if (np < 0) continue;
-            unsigned x = B.dps[u];
-            md = max(md, dps_depth(x));
+            unsigned x = B->dps[u];
             if (u > 0) {
                 int p = dps_parent(x), side = dps_side(x);
                 if (S.idx0[p] < 0) {   // parent removed: take the place of its run's first node
                     const int q = S.idx1[p];
-                    const unsigned xq = B.dps[q];
+                    const unsigned xq = B->dps[q];
                     p = dps_parent(xq);
                     side = dps_side(xq);
                 }
                 x = dps_make(dps_depth(x), S.idx0[p], side);
             }
-            A.l[np] = B.l[u]; A.r[np] = B.r[u]; A.dps[np] = x; A.e[np] = B.e[u];
+            A->l[np] = B->l[u]; A->r[np] = B->r[u]; A->dps[np] = x; A->e[np] = B->e[u];
         }
+        if (kept == nb) { SmmTree<NODES> *t = A; A = B; B = t; }
         __syncwarp();
         n = kept;
         for (int o = 16; o; o >>= 1) md = max(md, __shfl_xor_sync(FULL, md, o));
