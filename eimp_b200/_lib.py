@@ -66,6 +66,7 @@ _PROTOS = [
     ("eimp_imp_matches", _i32, [_vp, _sz, _vp, _sz, C.POINTER(_sz)]),
     ("eimp_imp_phased_dosages", _i32, [_vp, _vp, _vp]),
     ("eimp_phase_exclude_self", _i32, [_vp, C.c_int64]),
+    ("eimp_phase_start_phases", _i32, [_vp, _sz, _vp]),
     ("eimp_qref_index", _i32, [_vp, _sz, _sz, _sz, _vp]),
     ("eimp_qref_decode", _i32, [_vp, _vp, _sz, _sz, _sz, _vp, _sz, _vp]),
     ("eimp_qref_decode_dev", _i32, [_vp, _vp, _vp, _sz, _sz, _vp, _sz]),

@@ -65,6 +65,9 @@ struct eimp_ctx {
     size_t p_M = 0, p_nhaps = 0;
     // phasing iterations after the first: reference sample of target 0 (-1: none)
     int64_t self0 = -1;
+    // start phases of the targets of the next phasing calls (chunk carry)
+    DBuf startph;
+    size_t startph_n = 0;
     DBuf p_hapmajor, p_sitemajor, p_cm;
     // phasing batch scratch
     DBuf b_gt, b_nerr, b_bh, b_flags, b_monos, b_splits, b_calls, b_cmd, b_nsplits, b_ncalls, b_rowoff, b_cref,
@@ -501,6 +504,18 @@ int eimp_phase_exclude_self(eimp_ctx *ctx, int64_t first_sample) {
     return 0;
 }
 
+int eimp_phase_start_phases(eimp_ctx *ctx, size_t ntgt, const uint8_t *phases) {
+    if (!ctx || (ntgt && !phases)) return fail(ctx, EIMP_E_ARG, "eimp_phase_start_phases: NULL argument");
+    if (int r = use_device(ctx)) return r;
+    if (ntgt) {
+        CK(ctx->startph.reserve(ntgt));
+        CK(cudaMemcpyAsync(ctx->startph.p, phases, ntgt, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->startph_n = ntgt;
+    return 0;
+}
+
 int eimp_qref_index(const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref, int64_t *offsets) {
     if ((!section && nbytes) || (!offsets && Mref)) return EIMP_E_ARG;
     const size_t raw = eimp_W(2 * Nref) * 8;   // hapcapacity: 2*Nref bits in 512-bit units
@@ -774,6 +789,11 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
     const size_t K = phase_K(ctx, p);
     BeamParams bp;
     if (int r = make_beam_params(ctx, p, K, bp)) return r;
+    if (ctx->startph_n) {
+        if (ctx->startph_n != ntgt)
+            return fail(ctx, EIMP_E_ARG, "start phases were set for a different number of targets");
+        bp.startph = ctx->startph.as<uint8_t>();
+    }
     ctx->tvalid = false;
     tmark(ctx, 0);
     if (int r = run_prep(ctx, p, ntgt, d_gt)) return r;

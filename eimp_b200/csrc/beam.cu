@@ -1272,7 +1272,8 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     __syncwarp();
 
     int err = 0;
-    int cur = 0, lastph = 0;   // VCFData::getStartPhase: Ref
+    const int startph = p.startph ? (p.startph[t] != 0) : 0;   // VCFData::getStartPhase (Target.cpp:311-312)
+    int cur = startph, lastph = startph;
     if (p.doPrePhasing) {   // Target.cpp:324-438
         beam_init(c, w, cons, 0, p.Hf, p.Pf, p.Deltaf);
         if (lane == 0 && S > 0) { cons[0].type = C_HETKEEP; cons[0].refidx = 0; }
@@ -1343,7 +1344,7 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     }
 
     // fine phasing forward (Target.cpp:458-599)
-    cur = 0;
+    cur = startph;   // Target.cpp:443
     int nprobs = 0;
     if (lane == 0) phaseProbs[0] = 0.0f;
     nprobs = 1;

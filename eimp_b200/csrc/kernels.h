@@ -86,6 +86,9 @@ struct BeamParams {
     float expectIBDcM, pErr, pLimit;
     float minfixsize, maxfixsize, minfixthr, maxfixthr;
     int doPrePhasing, doRevPhasing;
+    // maternal phase of each target's first heterozygous site, carried over
+    // from the previous chunk (VCFData::getStartPhase; 0 = Ref); null: all Ref
+    const uint8_t *startph = nullptr;
 };
 size_t beam_arena_bytes(const BeamParams &p, int S_max);
 cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt, const uint64_t *monos,

@@ -151,6 +151,17 @@ class Phaser:
         self.ctx.check(self.ctx.L.eimp_phase_exclude_self(self.ctx.h, int(first_sample)))
         self.self0 = int(first_sample)
 
+    def setStartPhases(self, phases):
+        """The maternal phase of every target's first heterozygous site carried
+        over from the previous chunk (VCFData::getStartPhase; 0 = Ref) for the
+        next phase() calls, which must then have len(phases) targets; None
+        goes back to Ref for all."""
+        if phases is None:
+            self.ctx.check(self.ctx.L.eimp_phase_start_phases(self.ctx.h, 0, None))
+            return
+        ph = _c(phases, np.uint8)
+        self.ctx.check(self.ctx.L.eimp_phase_start_phases(self.ctx.h, ph.size, ptr(ph)))
+
     def _K(self, params: PhaseParams) -> int:
         return min(params.K, self.nhaps - 2 if self.self0 >= 0 else self.nhaps)
 
@@ -203,6 +214,26 @@ class Phaser:
         n = d_gt.shape[0]
         self.ctx.check(self.ctx.L.eimp_phase_targets_dev(self.ctx.h, C.byref(p), n, ptr(d_gt), ptr(d_mats),
                                                          ptr(d_pats), ptr(d_dm), ptr(d_dp), ptr(d_tc), ptr(d_nc)))
+
+
+def determine_start_phases(mats: np.ndarray, pats: np.ndarray, overlap_begin: int, M: int) -> np.ndarray:
+    """VCFData::determineStartPhases (VCFData.cpp:2802-2816): for every target
+    the maternal allele at its first heterozygous phased site from
+    overlap_begin on (the start of the overlap with the next chunk), or at the
+    last site when there is none -- the start phase of the next chunk."""
+    from .bits import unpack_rows
+    m = unpack_rows(_c(mats, np.uint64), M)
+    p = unpack_rows(_c(pats, np.uint64), M)
+    out = np.zeros(m.shape[0], np.uint8)
+    for t in range(m.shape[0]):
+        s = overlap_begin
+        while True:
+            mat, pat = m[t, s], p[t, s]
+            s += 1
+            if mat != pat or s >= M:
+                break
+        out[t] = mat
+    return out
 
 
 def _transpose_bits(rows: np.ndarray, ncols: int) -> np.ndarray:

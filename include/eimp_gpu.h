@@ -163,6 +163,13 @@ int eimp_phase_cref_pbwt(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt,
  * its Target objects. */
 int eimp_phase_exclude_self(eimp_ctx *ctx, int64_t first_sample);
 
+/* Chunked runs (VCFData.cpp:2802-2816, Target.cpp:311-312, 443): the maternal
+ * phase of every target's first heterozygous site, carried over from the
+ * overlap with the previous chunk (0 = Ref, 1 = Alt; VCFData::getStartPhase),
+ * for the next phasing calls, which must then phase exactly ntgt targets.
+ * ntgt = 0 goes back to Ref for all (the first chunk). */
+int eimp_phase_start_phases(eimp_ctx *ctx, size_t ntgt, const uint8_t *phases);
+
 /* Capacity mode for phasing (no counterpart in the reference): reserves the
  * batch buffers for up to max_targets targets and max_rows condensed rows
  * (sum over the targets of 2*S_t+1).  Afterwards the row offsets are computed

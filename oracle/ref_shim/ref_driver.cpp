@@ -157,6 +157,13 @@ void *refo_create(size_t nhaps, size_t M, size_t Mref,
 
 void refo_destroy(void *hp) { delete (Handle*)hp; }
 
+/* Start phases of the targets (VCFData::chunkStartPhase, carried over from
+ * the previous chunk, VCFData.cpp:2802-2816): ntarget bytes, 0 = Ref. */
+void refo_set_start_phases(void *hp, const uint8_t *ph) {
+    Handle *h = (Handle*)hp;
+    for (size_t t = 0; t < h->vd.chunkStartPhase.size(); t++) h->vd.chunkStartPhase[t] = ph[t] != 0;
+}
+
 /* Phasing iteration after the first (PBWTPhaser.cpp:406-476): the handle's
  * panel is the reference (nhaps_orig haplotypes) followed by the phased
  * targets; last_iter as Target's lastIter (reverse phasing and call

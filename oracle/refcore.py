@@ -41,6 +41,7 @@ def lib():
                                   _f32p, _f32p, _f32p, C.c_size_t, _u8p]
         L.refo_destroy.argtypes = [C.c_void_p]
         L.refo_set_iteration.argtypes = [C.c_void_p, C.c_size_t, C.c_int]
+        L.refo_set_start_phases.argtypes = [C.c_void_p, _u8p]
         L.refo_set_params.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int]
         L.refo_prep.restype = C.c_long
         L.refo_prep.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, _i64p, _u64p, _i64p, _i64p,
@@ -171,6 +172,10 @@ class RefCore:
     def ncorr(self) -> int:
         """Haplotypes a target chooses its K best from (PBWTPhaser.cpp:408-476)."""
         return self.nhaps - 2 if getattr(self, "nhaps_orig", 0) else self.nhaps
+
+    def set_start_phases(self, phases):
+        """VCFData::chunkStartPhase of every target (0 = Ref)."""
+        lib().refo_set_start_phases(self.h, np.ascontiguousarray(phases, np.uint8))
 
     def set_iteration(self, nhaps_orig: int, last_iter: bool):
         """Phasing iteration after the first: the first nhaps_orig haplotypes

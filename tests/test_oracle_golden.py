@@ -128,3 +128,20 @@ def test_reference_iteration_excludes_own_sample():
             if K == 1000:
                 np.testing.assert_array_equal(bh, [h for h in range(nh + 2 * n) if h // 2 != nh // 2 + t])
     rc.close()
+
+
+def test_determine_start_phases():
+    """VCFData::determineStartPhases (VCFData.cpp:2802-2816): the maternal
+    allele at the first heterozygous site from the overlap start on, else at
+    the last site."""
+    from eimp_b200.bits import pack_rows
+    from eimp_b200.engine import determine_start_phases
+    M = 10
+    mats = np.array([[0, 0, 1, 1, 0, 0, 0, 0, 0, 0],    # het at 4 (mat 0)
+                     [0, 0, 0, 0, 0, 1, 0, 0, 0, 0],    # het at 5 (mat 1)
+                     [1, 1, 1, 1, 1, 1, 1, 1, 1, 1]], np.uint8)   # no het: mat at the last site
+    pats = np.array([[0, 0, 1, 1, 1, 0, 0, 0, 0, 0],
+                     [0, 0, 0, 0, 0, 0, 0, 0, 0, 0],
+                     [1, 1, 1, 1, 1, 1, 1, 1, 1, 1]], np.uint8)
+    got = determine_start_phases(pack_rows(mats, W(M)), pack_rows(pats, W(M)), 3, M)
+    np.testing.assert_array_equal(got, [0, 1, 1])

@@ -50,7 +50,7 @@ int main(int argc, char **argv) {
     const int ntgt = pi[0], M = pi[1];
     int t0 = argc > 2 ? atoi(argv[2]) : 0, t1 = argc > 3 ? atoi(argv[3]) : ntgt;
     if (t1 > ntgt) t1 = ntgt;
-    eimp::BeamParams p;
+    eimp::BeamParams p;   // start phases: all Ref
     p.K = pi[2]; p.H = pi[3]; p.P = pi[4]; p.Delta = pi[5]; p.Hf = pi[6]; p.Pf = pi[7]; p.Deltaf = pi[8];
     p.doPrePhasing = pi[9]; p.doRevPhasing = pi[10];
     p.expectIBDcM = pf[0]; p.pErr = pf[1]; p.pLimit = pf[2];
