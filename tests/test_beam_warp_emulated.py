@@ -126,3 +126,33 @@ def test_beam_emulated_prephasing_matches_oracle(emu_exe, tmp_path, P):
     np.testing.assert_array_equal(pats, op)
     np.testing.assert_array_equal(dm, odm)
     np.testing.assert_array_equal(dp, odp)
+
+
+@pytest.mark.parametrize("prephase", [False, True])
+def test_beam_emulated_start_phases_match_reference(emu_exe, tmp_path, prephase):
+    """Start phases carried over from a previous chunk (VCFData::getStartPhase)
+    against the reference's own Target::phase with the same chunkStartPhase."""
+    from oracle import refcore
+    if not refcore.available():
+        pytest.skip("reference sources not compiled (oracle/_ref)")
+    g = np.load(golden_path("golden_tiny.npz"))
+    K = 64
+    nt, M = g["gt"].shape
+    phases = (np.arange(nt) % 3 != 0).astype(np.uint8)
+    write_inputs(tmp_path, K=K, P=16, prephase=prephase, **golden_inputs(g, K))
+    phases.tofile(os.path.join(tmp_path, "startph.bin"))
+    mats, pats, dm, dp, tc, nc, st = run_emu(emu_exe, tmp_path, nt, M)
+    assert not st.any()
+    rc = refcore.RefCore.typed_only(g["hapmajor_typed"], g["sitemajor_typed"], g["cm_typed"], g["gt"],
+                                    g["af_full"][g["typed"]])
+    rc.set_start_phases(phases)
+    rc.set_params(refcore.PhaseParams(K=K, beamwidth=16, doPrePhasing=prephase))
+    for t in range(nt):
+        m, p, a, b, c, n = rc.phase(t)
+        np.testing.assert_array_equal(mats[t], m)
+        np.testing.assert_array_equal(pats[t], p)
+        np.testing.assert_array_equal(dm[t], a)
+        np.testing.assert_array_equal(dp[t], b)
+        assert tc[t] == np.float32(c) and nc[t] == n
+    rc.close()
+

@@ -6,7 +6,8 @@
 // <dir> holds the kernel inputs as raw little-endian arrays (params_i.bin,
 // params_f.bin, gt.bin, monos.bin, splits.bin, nsplits.bin, calls.bin,
 // ncalls.bin, cmd.bin, pbwt.bin, count0.bin, rowoff.bin, in the layout the
-// device buffers have); the outputs are written next to them (o_*.bin).
+// device buffers have; optional startph.bin); the outputs are written next to
+// them (o_*.bin).
 // Each target gets its own arena and shared-memory block so the address
 // sanitizer sees accesses past either.  Exit status 3: a divergent warp
 // collective was seen.
@@ -50,7 +51,7 @@ int main(int argc, char **argv) {
     const int ntgt = pi[0], M = pi[1];
     int t0 = argc > 2 ? atoi(argv[2]) : 0, t1 = argc > 3 ? atoi(argv[3]) : ntgt;
     if (t1 > ntgt) t1 = ntgt;
-    eimp::BeamParams p;   // start phases: all Ref
+    eimp::BeamParams p;   // start phases: all Ref unless startph.bin is given
     p.K = pi[2]; p.H = pi[3]; p.P = pi[4]; p.Delta = pi[5]; p.Hf = pi[6]; p.Pf = pi[7]; p.Deltaf = pi[8];
     p.doPrePhasing = pi[9]; p.doRevPhasing = pi[10];
     p.expectIBDcM = pf[0]; p.pErr = pf[1]; p.pLimit = pf[2];
@@ -65,6 +66,9 @@ int main(int argc, char **argv) {
     const auto pbwt = rd<uint32_t>(d, "pbwt.bin");
     const auto count0 = rd<int32_t>(d, "count0.bin");
     const auto rowoff = rd<int64_t>(d, "rowoff.bin");
+    // optional: start phases of the targets (0 = Ref)
+    std::vector<uint8_t> startph;
+    if (FILE *f = fopen((d + "/startph.bin").c_str(), "rb")) { fclose(f); startph = rd<uint8_t>(d, "startph.bin"); }
     const int wM = (int)eimp_W(M);
     const size_t kw = eimp_kw(p.K);
     const eimp::ArenaLayout al = eimp::arena_layout(p, M);
@@ -90,7 +94,9 @@ int main(int argc, char **argv) {
                 blockIdx.x = 0;
                 emu_warp = &warp;
                 emu_smem_ptr = smem;
-                eimp::beam_kernel(p, al, 1, M, gt.data() + (size_t)t * M, monos.data() + (size_t)t * wM,
+                eimp::BeamParams pt = p;
+                pt.startph = startph.empty() ? nullptr : startph.data() + t;   // this target's entry at index 0
+                eimp::beam_kernel(pt, al, 1, M, gt.data() + (size_t)t * M, monos.data() + (size_t)t * wM,
                                   splits.data() + (size_t)t * M, nsplits.data() + t, calls.data() + (size_t)t * M,
                                   ncalls.data() + t, cmd.data() + (size_t)t * (M + 1), pbwt.data() + 2 * r0 * kw,
                                   count0.data() + r0, &zero, arena, al.total, mats.data() + (size_t)t * wM,
