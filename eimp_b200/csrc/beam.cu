@@ -267,8 +267,11 @@ __device__ __forceinline__ void hp_mark_required(HPh &h, const Cons &cn) {   // 
 // functions of the loaded intervals, are computed before the sequential part
 // that accumulates the probabilities, appends the extension intervals and
 // stops at the first step where both extensions are empty, in the reference's
-// order.
-constexpr int HXC = 6;
+// order.  One step per chunk measured fastest on cfg2 (beam 67 ms against 74,
+// 78, 83 and 93 ms for 2, 3, 4 and 6 steps): the smaller loop body costs the
+// warps sharing an SM fewer instruction-fetch stalls than the deeper
+// prefetch saves.
+constexpr int HXC = 1;
 
 __device__ int hp_extend(const Ctx &c, const WS &w, int slot) {
     HPh &h = c.hp[slot];
