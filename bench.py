@@ -429,9 +429,9 @@ def main():
         bytes_beam = 2 * rows_total * kw * 4 + rows_total * 4 + nt * (M + 2 * W(M) * 8 + 2 * M * 4)
         achieved = bytes_beam / (beam_ms / 1e3) / 1e9
         # DRAM bytes of one beam launch: an ncu capture of the 64-target cfg2
-        # launch (157.2 MB read + 12.6 MB written), scaled to the batch by the
-        # number of targets
-        traffic = (169.8e6 / 64) * nt if args.config == "cfg2" else None
+        # launch (158.3 MB read + 13.1 MB written), scaled to the batch by
+        # the number of targets
+        traffic = (171.3e6 / 64) * nt if args.config == "cfg2" else None
         roofline = {"kernel": "beam_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                     "algorithmic_bytes_per_launch": bytes_beam, "avg_launch_ms": beam_ms,
