@@ -636,18 +636,18 @@ __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn
         for (int bit = 31; bit >= 0; bit--) {
             const unsigned cand = thr | (1u << bit);
             int cnt = 0;
-#pragma unroll
+#pragma unroll 1
             for (int q = 0; q < PRR * 4; q++) cnt += ((sel >> q) & 1u) && key_bits(bp[lane + 32 * (q >> 2)].extp[q & 3]) >= cand;
             if (warp_sumi(cnt) >= P) thr = cand;
         }
         int cnt = 0;
-#pragma unroll
+#pragma unroll 1
         for (int q = 0; q < PRR * 4; q++) cnt += ((sel >> q) & 1u) && key_bits(bp[lane + 32 * (q >> 2)].extp[q & 3]) >= thr;
         fast = warp_sumi(cnt) == P;   // else ties straddle the P-th place
     }
     unsigned surv = sel;
     if (thr)
-#pragma unroll
+#pragma unroll 1
         for (int q = 0; q < PRR * 4; q++)
             if (((sel >> q) & 1u) && key_bits(bp[lane + 32 * (q >> 2)].extp[q & 3]) < thr) surv &= ~(1u << q);
     int wse = 0, delerr = 0;
@@ -655,7 +655,7 @@ __device__ int beam_prune_select(const Ctx &c, WS &w, float maxP, const Cons &cn
     if (fast && nsurv > 0) {
         const unsigned kminb = nA > P ? thr : key_bits(kmin), kmaxb = key_bits(kmax);
         int lo0 = INT_MAX, hi0 = INT_MIN, lo1 = 1, hi1 = 0;
-#pragma unroll
+#pragma unroll 1
         for (int q = 0; q < PRR * 4; q++) {
             if (!((surv >> q) & 1u)) continue;
             const BPh &b = bp[lane + 32 * (q >> 2)];
