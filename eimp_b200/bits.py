@@ -41,10 +41,55 @@ def unpack_rows(words: np.ndarray, n: int) -> np.ndarray:
     return np.unpackbits(b, axis=1, bitorder="little", count=n)
 
 
-def transpose_bits(words: np.ndarray, nrows: int, ncols: int, out_words: int | None = None) -> np.ndarray:
-    """Transpose a packed (nrows x ncols bits) matrix into (ncols x nrows bits)."""
-    dense = unpack_rows(words, ncols)[:nrows]
-    return pack_rows(np.ascontiguousarray(dense.T), out_words)
+_T64_MASKS = {j: np.uint64(sum(1 << b for b in range(64) if not b & j)) for j in (32, 16, 8, 4, 2, 1)}
+
+
+def _transpose64_inplace(a: np.ndarray) -> None:
+    """Transpose the 64 x 64 bit blocks along the last axis of ``a`` (uint64,
+    last axis 64 rows, bit c of row r is element (r, c)) in place: row c of
+    the result holds bit r of every input row r.  Six butterfly stages; at
+    stage j the bits (k, c + j) and (k + j, c) with k & j == c & j == 0 trade
+    places."""
+    lead = a.shape[:-1]
+    for j in (32, 16, 8, 4, 2, 1):
+        v = a.reshape(*lead, 64 // (2 * j), 2, j)
+        lo, hi = v[..., 0, :], v[..., 1, :]
+        t = ((lo >> np.uint64(j)) ^ hi) & _T64_MASKS[j]
+        lo ^= t << np.uint64(j)
+        hi ^= t
+
+
+def transpose_bits(words: np.ndarray, nrows: int, ncols: int, out_words: int | None = None,
+                   chunk_words: int = 256) -> np.ndarray:
+    """Transpose a packed (nrows x ncols bits) matrix into (ncols x nrows bits).
+
+    ``words`` is (>= nrows, >= ceil(ncols/64)) uint64, LSB first; the result is
+    (ncols, out_words) uint64 with ``out_words`` defaulting to W(nrows).  Works
+    on 64 x 64 bit blocks, ``chunk_words`` source words at a time."""
+    words = np.asarray(words, dtype=np.uint64)
+    if out_words is None:
+        out_words = W(nrows)
+    rb = (nrows + 63) // 64
+    cw_total = (ncols + 63) // 64
+    assert out_words >= rb
+    src = words[:nrows]
+    out = np.zeros((cw_total * 64, out_words), dtype=np.uint64)
+    for c0 in range(0, cw_total, chunk_words):
+        c1 = min(cw_total, c0 + chunk_words)
+        blk = np.zeros((rb * 64, c1 - c0), dtype=np.uint64)
+        blk[:nrows] = src[:, c0:c1]
+        b = np.ascontiguousarray(blk.reshape(rb, 64, c1 - c0).transpose(0, 2, 1))   # (rb, cw, 64 rows)
+        _transpose64_inplace(b)                                                     # (rb, cw, 64 cols)
+        out[c0 * 64:c1 * 64, :rb] = b.transpose(1, 2, 0).reshape((c1 - c0) * 64, rb)
+    return np.ascontiguousarray(out[:ncols])
+
+
+def gather_bits(words: np.ndarray, cols: np.ndarray) -> np.ndarray:
+    """Bits of every row of packed ``words`` at the bit positions ``cols``:
+    (rows, len(cols)) uint8."""
+    cols = np.asarray(cols, dtype=np.int64)
+    w = np.asarray(words, dtype=np.uint64)[:, cols >> 6]
+    return ((w >> (cols & 63).astype(np.uint64)) & np.uint64(1)).astype(np.uint8)
 
 
 def pack_genotypes(gt: np.ndarray) -> np.ndarray:

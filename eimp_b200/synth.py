@@ -30,7 +30,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .bits import W, pack_rows
+from .bits import W, gather_bits, pack_rows, transpose_bits
 
 
 @dataclass(frozen=True)
@@ -99,27 +99,63 @@ class Targets:
     truth: np.ndarray          # uint8 (2*ntargets, M) true haplotypes at typed sites
 
 
-def _mosaic_block(rng, founders_T, cm, nhap, mean_seg, copy_err):
-    """Return (nhap, nsites) uint8 mosaics of the founder matrix (nsites, F)."""
-    nsites, F = founders_T.shape
-    glen = float(cm[-1] - cm[0])
-    out = np.empty((nhap, nsites), dtype=np.uint8)
-    cols = np.arange(nsites)
-    for h in range(nhap):
-        nsw = rng.poisson(glen / mean_seg)
-        x = np.sort(rng.uniform(cm[0], cm[-1], nsw))
-        brk = np.searchsorted(cm, x, side="left")
-        brk = np.concatenate(([0], brk, [nsites]))
-        lens = np.diff(brk)
-        fid = rng.integers(0, F, len(lens))
-        fidx = np.repeat(fid, lens)
-        row = founders_T[cols, fidx]
-        nerr = rng.binomial(nsites, copy_err)
-        if nerr:
-            e = rng.integers(0, nsites, nerr)
-            row[e] ^= 1
-        out[h] = row
+def _founders_words(rng, f, nfounders, nw, chunk=64):
+    """Founder haplotypes as packed words (nfounders, nw): allele ~ Bernoulli(f)
+    per site, drawn for ``chunk`` founders at a time."""
+    n = f.size
+    out = np.zeros((nfounders, nw), dtype=np.uint64)
+    f32 = f.astype(np.float32)
+    for a in range(0, nfounders, chunk):
+        b = min(nfounders, a + chunk)
+        alle = (rng.random((b - a, n), dtype=np.float32) < f32[None, :]).astype(np.uint8)
+        out[a:b] = pack_rows(alle, nw)
     return out
+
+
+def _mosaic_words(rng, Fw, cm, nhap, mean_seg, copy_err):
+    """(nhap, nw) packed Li-Stephens mosaics of the packed founders Fw
+    (F, nw): every haplotype switches to a uniformly drawn founder at
+    Poisson(genetic length / mean_seg) uniform genetic positions (a switch at
+    genetic position x takes effect from the first site at or after x), and
+    each copied allele flips with probability copy_err.  Words are copied
+    whole; the words a switch falls into are merged at the switch's bit."""
+    F, nw = Fw.shape
+    n = cm.size
+    glen = float(cm[-1] - cm[0])
+    counts = rng.poisson(glen / mean_seg, nhap)
+    total = int(counts.sum())
+    hid = np.repeat(np.arange(nhap), counts)
+    x = rng.uniform(cm[0], cm[-1], total)
+    order = np.lexsort((x, hid))
+    x = x[order]
+    brk = np.searchsorted(cm, x, side="left").astype(np.int64)          # first site of the new segment
+    fid = rng.integers(0, F, total + nhap)                                # founder of every segment
+    bp0 = np.concatenate(([0], np.cumsum(counts)))                        # first breakpoint of each hap
+    seg0 = bp0[:-1] + np.arange(nhap)                                     # first segment of each hap
+    # founder in effect at the first site of every word: segments started at or before it
+    key = hid * (n + 1) + brk
+    wkey = (np.arange(nhap, dtype=np.int64) * (n + 1))[:, None] + 64 * np.arange(nw, dtype=np.int64)[None, :]
+    nbefore = np.searchsorted(key, wkey, side="right") - bp0[:-1, None]
+    founder = fid[seg0[:, None] + nbefore]
+    words = Fw[founder, np.arange(nw)[None, :]]
+    # switches inside a word, in order along each haplotype
+    rank = np.arange(total) - bp0[hid]
+    inner = (brk % 64 != 0) & (brk < n)
+    for r in range(int(counts.max()) if nhap else 0):
+        s = np.flatnonzero(inner & (rank == r))
+        if s.size == 0:
+            continue
+        h, b = hid[s], brk[s]
+        w = b >> 6
+        low = (np.uint64(1) << (b & 63).astype(np.uint64)) - np.uint64(1)
+        fnew = fid[seg0[h] + r + 1]
+        words[h, w] = (words[h, w] & low) | (Fw[fnew, w] & ~low)
+    # copying errors
+    nerr = rng.binomial(n, copy_err, nhap)
+    eh = np.repeat(np.arange(nhap), nerr)
+    ep = rng.integers(0, n, int(nerr.sum()))
+    np.bitwise_xor.at(words, (eh, ep >> 6), np.uint64(1) << (ep & 63).astype(np.uint64))
+    return words
 
 
 def _cache_dir() -> str:
@@ -128,11 +164,15 @@ def _cache_dir() -> str:
     return d
 
 
+# version of the generator's drawing order (part of the cache key)
+GENERATOR = 2
+
+
 def generate(cfg: SynthConfig | str, cache: bool = True):
     """Generate (or load from cache) ``(panel, [targets per group])``."""
     if isinstance(cfg, str):
         cfg = CONFIGS[cfg]
-    path = os.path.join(_cache_dir(), f"{cfg.name}-{cfg.key()}.npz")
+    path = os.path.join(_cache_dir(), f"{cfg.name}-g{GENERATOR}-{cfg.key()}.npz")
     if cache and os.path.exists(path):
         z = np.load(path)
         panel = Panel(cfg.nhaps, cfg.nsites, z["pos"], z["cm"], z["af"], z["hapmajor"], z["sitemajor"])
@@ -149,28 +189,18 @@ def generate(cfg: SynthConfig | str, cache: bool = True):
     f = cfg.maf_min * (0.5 / cfg.maf_min) ** u
     flip = rng.uniform(0.0, 1.0, n) < 0.5
     f = np.where(flip, 1.0 - f, f)
-    founders_T = (rng.uniform(0.0, 1.0, (n, cfg.founders)) < f[:, None]).astype(np.uint8)
-
-    # reference haplotypes, generated in blocks of 512 (a multiple of 64 so that
-    # the site-major words of a block are whole words)
-    nh = cfg.nhaps
     hap_w = W(n)
-    site_w = W(nh)
+    Fw = _founders_words(rng, f, cfg.founders, hap_w)
+
+    # reference haplotypes in blocks of 1024
+    nh = cfg.nhaps
     hapmajor = np.zeros((nh, hap_w), dtype=np.uint64)
-    sitemajor = np.zeros((n, site_w), dtype=np.uint64)
-    ac = np.zeros(n, dtype=np.int64)
-    blk = 512
+    blk = 1024
     for b0 in range(0, nh, blk):
         b1 = min(nh, b0 + blk)
-        block = _mosaic_block(rng, founders_T, cm, b1 - b0, cfg.mean_segment_cm, cfg.copy_err)
-        ac += block.sum(axis=0, dtype=np.int64)
-        hapmajor[b0:b1] = pack_rows(block, hap_w)
-        sm = np.packbits(np.ascontiguousarray(block.T), axis=1, bitorder="little")
-        nbytes = sm.shape[1]
-        sm_pad = np.zeros((n, ((nbytes + 7) // 8) * 8), dtype=np.uint8)
-        sm_pad[:, :nbytes] = sm
-        words = sm_pad.view("<u8")
-        sitemajor[:, b0 // 64: b0 // 64 + words.shape[1]] = words
+        hapmajor[b0:b1] = _mosaic_words(rng, Fw, cm, b1 - b0, cfg.mean_segment_cm, cfg.copy_err)
+    sitemajor = transpose_bits(hapmajor, nh, n)
+    ac = np.bitwise_count(sitemajor).sum(axis=1, dtype=np.int64)
     af = (ac / float(nh)).astype(np.float32)
     panel = Panel(nh, n, pos.astype(np.int64), cm, af, hapmajor, sitemajor)
 
@@ -178,8 +208,10 @@ def generate(cfg: SynthConfig | str, cache: bool = True):
     for g in cfg.groups:
         m = max(2, int(round(g.typed_frac * n)))
         typed = np.sort(rng.choice(n, m, replace=False)).astype(np.int64)
-        haps = _mosaic_block(rng, founders_T, cm, 2 * g.ntargets, cfg.mean_segment_cm, cfg.copy_err)
-        th = haps[:, typed]
+        th = np.zeros((2 * g.ntargets, m), dtype=np.uint8)
+        for a in range(0, 2 * g.ntargets, blk):
+            b = min(2 * g.ntargets, a + blk)
+            th[a:b] = gather_bits(_mosaic_words(rng, Fw, cm, b - a, cfg.mean_segment_cm, cfg.copy_err), typed)
         gt = (th[0::2].astype(np.uint8) + th[1::2]).astype(np.uint8)
         for t in range(g.ntargets):
             rate = rng.uniform(g.miss_lo, g.miss_hi) if g.miss_hi > g.miss_lo else g.miss_lo
@@ -207,11 +239,9 @@ def typed_views(panel: Panel, typed: np.ndarray):
     cm_typed float32 (M,))`` -- ``reference``, ``referenceT`` and ``cMs``
     (VCFData.h:199-205, 227).
     """
-    from .bits import unpack_rows
     M = len(typed)
     sitemajor_typed = np.ascontiguousarray(panel.sitemajor[typed])
-    dense = unpack_rows(sitemajor_typed, panel.nhaps)       # (M, nhaps)
-    hapmajor_typed = pack_rows(np.ascontiguousarray(dense.T), W(M))
+    hapmajor_typed = transpose_bits(sitemajor_typed, M, panel.nhaps)
     cm_typed = panel.cm[typed].astype(np.float32)
     return hapmajor_typed, sitemajor_typed, cm_typed
 
