@@ -137,9 +137,12 @@ def imputed_count(tg, Mref):
 
 
 # ---------------------------------------------------------------- reference arm / CPU baseline
-def cpu_reference_sample(cfg, panel, tg, ntgt, nthreads, stages):
+def cpu_reference_sample(cfg, panel, tg, ntgt, nthreads, stages, keep=None):
     """The reference's own CPU path (oracle/_ref) on a bounded target sample:
-    phasing (PBWTPhaser::phaseCPU loop) and/or PBWTImputer prepare + bunch."""
+    phasing (PBWTPhaser::phaseCPU loop) and/or PBWTImputer prepare + bunch.
+    With ``keep`` (a dict) its outputs are stored there after the timing:
+    phased haplotypes and dosages, imputed alleles and dosages, and the
+    matches and prefix arrays of the first haplotypes (for the FP64 oracle)."""
     from oracle import refcore
     sub = synth.Targets(tg.typed, np.ascontiguousarray(tg.gt[:ntgt]), np.ascontiguousarray(tg.truth[:2 * ntgt]))
     rc = refcore.RefCore(panel, sub)
@@ -147,7 +150,7 @@ def cpu_reference_sample(cfg, panel, tg, ntgt, nthreads, stages):
     M = len(tg.typed)
     t0 = time.perf_counter()
     if "phase" in stages:
-        mats, pats, _, _ = rc.phase_range(0, ntgt, nthreads)
+        mats, pats, dm, dp = rc.phase_range(0, ntgt, nthreads)
         phased = np.zeros((2 * ntgt, W(M)), np.uint64)
         phased[0::2] = mats
         phased[1::2] = pats
@@ -155,12 +158,21 @@ def cpu_reference_sample(cfg, panel, tg, ntgt, nthreads, stages):
         phased = pack_rows(sub.truth, W(M))
     t1 = time.perf_counter()
     dt_imp = 0.0
+    imp = None
     if "impute" in stages:
         imp = rc.imputer(phased, nthreads)
-        imp.bunch(panel.nsites, nthreads)
-        imp.close()
+        bits, dos = imp.bunch(panel.nsites, nthreads)
         dt_imp = time.perf_counter() - t1
     dt = time.perf_counter() - t0
+    if keep is not None:
+        keep["phased"] = phased
+        if "phase" in stages:
+            keep.update(mats=mats, pats=pats, dm=dm, dp=dp)
+        if imp is not None:
+            keep.update(bits=bits, dos=dos, absperm=imp.refpbwt()[1],
+                        matches=[imp.matches(h) for h in range(min(2 * ntgt, PARITY_FP64_HAPS))])
+    if imp is not None:
+        imp.close()
     rc.close()
     return dt, t1 - t0, dt_imp
 
@@ -190,7 +202,7 @@ def cpu_port_sample(cfg, panel, tg, ntgt, nthreads, stages):
     return t2 - t0, t1 - t0, t2 - t1
 
 
-def cpu_baseline(cfg, panel, tg, ntgt, stages):
+def cpu_baseline(cfg, panel, tg, ntgt, stages, keep=None):
     nthreads = os.cpu_count() or 1
     from oracle import refcore
     kind = "reference" if refcore.available() else "port"
@@ -199,7 +211,7 @@ def cpu_baseline(cfg, panel, tg, ntgt, stages):
     os.dup2(devnull, 1)   # the reference prints progress to stdout
     try:
         if kind == "reference":
-            dt, dtp, dti = cpu_reference_sample(cfg, panel, tg, ntgt, nthreads, stages)
+            dt, dtp, dti = cpu_reference_sample(cfg, panel, tg, ntgt, nthreads, stages, keep)
         else:
             dt, dtp, dti = cpu_port_sample(cfg, panel, tg, ntgt, nthreads if "phase" in stages else 1, stages)
     finally:
@@ -214,6 +226,53 @@ def cpu_baseline(cfg, panel, tg, ntgt, stages):
     if "phase" in stages:
         out["phased_samples_per_sec"] = ntgt / dtp
     return out, dt
+
+
+# haplotypes of the CPU sample whose dosages are also checked against the FP64
+# dosage oracle (score/sum in double, not rounded to float)
+PARITY_FP64_HAPS = 32
+
+
+def imputed_mask(tg, ntgt, Mref):
+    """(2*ntgt, Mref) bool: the sites TargetImp::imputeBunch writes for each
+    target haplotype -- untyped sites and the target's missing typed sites
+    (TargetImp.cpp:503)."""
+    m = np.ones((ntgt, Mref), bool)
+    m[:, tg.typed] = tg.gt[:ntgt] == 3
+    return np.repeat(m, 2, axis=0)
+
+
+def parity_block(gpu, ref, cfg, panel, tg, ntgt, stages):
+    """Compare the GPU step's outputs for the first ntgt targets with the
+    reference's own CPU outputs on the same targets (bit-exact), and state the
+    largest dosage error against the reference and against the FP64 oracle."""
+    from eimp_b200.bits import unpack_rows
+    out = {"targets": ntgt, "against": "reference CPU path (oracle/_ref) on the CPU sample"}
+    if "phase" in stages and "mats" in ref:
+        out["phased_equal"] = bool(np.array_equal(gpu["mats"], ref["mats"]) and np.array_equal(gpu["pats"], ref["pats"]))
+        out["phasing_dosages_equal"] = bool(np.array_equal(gpu["dm"], ref["dm"]) and np.array_equal(gpu["dp"], ref["dp"]))
+    if "impute" in stages and "dos" in ref:
+        Mref = panel.nsites
+        sel = imputed_mask(tg, ntgt, Mref)
+        gb = unpack_rows(gpu["bits"], Mref).astype(bool)
+        rb = unpack_rows(ref["bits"], Mref).astype(bool)
+        out["imputed_alleles_equal"] = bool(np.array_equal(gb[sel], rb[sel]))
+        d = np.abs(gpu["dos"][sel] - ref["dos"][sel])
+        out["dosage_max_abs_err"] = float(d.max(initial=0.0))
+        out["dosage_tolerance"] = 1e-5
+        from oracle import restate as R
+        worst = 0.0
+        for h, m in enumerate(ref["matches"]):
+            miss = np.where(tg.gt[h // 2] == 3)[0].astype(np.int64)
+            _, _, imp, d64 = R.impute(m, ref["absperm"], panel.sitemajor, tg.typed, panel.af, panel.nhaps, miss,
+                                      ref["phased"][h], fp64=True)
+            cov = imp.astype(bool) & (d64 >= 0)
+            worst = max(worst, float(np.abs(gpu["dos"][h][cov].astype(np.float64) - d64[cov]).max(initial=0.0)))
+        out["dosage_max_abs_err_fp64"] = worst
+        out["fp64_haplotypes"] = len(ref["matches"])
+    out["ok"] = all(v for k, v in out.items() if k.endswith("_equal")) and \
+        out.get("dosage_max_abs_err", 0.0) <= 1e-5
+    return out
 
 
 def run_reference_arm(args, rank):
@@ -397,6 +456,15 @@ def main():
     torch.cuda.synchronize()
     launches = ctx.launches - launches0
     clocks = sampler.stop()
+    # the last timed step's outputs for the CPU sample's targets (compared with
+    # the reference's own outputs once the CPU baseline has run)
+    npar = min(args.cpu_sample_targets, nt)
+    gpu_out = {"bits": d_bits[:2 * npar].cpu().numpy().view(np.uint64),
+               "dos": d_dos[:2 * npar].cpu().numpy()}
+    if do_phase:
+        gpu_out.update(mats=d_mats[:npar].cpu().numpy().view(np.uint64),
+                       pats=d_pats[:npar].cpu().numpy().view(np.uint64),
+                       dm=d_pdm[:npar].cpu().numpy(), dp=d_pdp[:npar].cpu().numpy())
     step_ms = [e[0].elapsed_time(e[4]) for e in evs]
     for e in evs:
         kern["phase"].append(e[0].elapsed_time(e[1]))
@@ -684,8 +752,12 @@ def main():
                         "request_sizes": "log-uniform 1..256 targets", "arrivals": "Poisson"})
 
     cpu = None
+    parity = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        cpu, _ = cpu_baseline(cfg, panel, tg, args.cpu_sample_targets, stages)
+        ref_out = {}
+        cpu, _ = cpu_baseline(cfg, panel, tg, npar, stages, keep=ref_out)
+        if ref_out:
+            parity = parity_block(gpu_out, ref_out, cfg, panel, tg, npar, stages)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -694,7 +766,7 @@ def main():
                 "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
                 "config": config_block(cfg, panel, tg, stages), "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches), "plain": plain, "serving": serving,
-                "graph": graph, "qref_decode": qref}
+                "graph": graph, "qref_decode": qref, "parity": parity}
         if do_phase:
             line["phased_samples_per_sec"] = world * nt * args.steps / (tot_ms / 1e3)
             line["phase_ms_per_step"] = float(np.mean(kern["phase"]))

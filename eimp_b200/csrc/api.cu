@@ -702,6 +702,12 @@ int check_phase_args(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt) {
     if (!p || p->K <= 0 || !ntgt) return fail(ctx, EIMP_E_ARG, "bad phasing parameters or empty batch");
     if (p->hsize <= 0 || p->hsize > 128 || p->hsize_fast <= 0 || p->hsize_fast > 128)
         return fail(ctx, EIMP_E_ARG, "hsize must be in 1..128 (BooleanHistory holds 128 sites)");
+    if (phase_K(ctx, p) > 65536)
+        return fail(ctx, EIMP_E_ARG, "K must be at most 65536 (the PBWT kernel keeps 16-bit prefix positions)");
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) == cudaSuccess &&
+        (size_t)16 * eimp_W(ctx->p_M) > (size_t)optin)
+        return fail(ctx, EIMP_E_CAPACITY, "too many typed sites: a target's genotype vectors do not fit a CTA's shared memory");
     return 0;
 }
 

@@ -30,7 +30,9 @@ constexpr int kMaxDevices = 64;
 uint32_t *g_nerr_addr[kMaxDevices] = {nullptr};
 std::mutex g_nerr_mutex;
 
-// device address of the array on the current device (set-up once per device)
+// device address of the array on the current device (set-up once per device;
+// the address stays valid for the life of the device's primary context, so a
+// cudaDeviceReset after the first call is not supported)
 int nerr_address(uint32_t **out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return EIMP_E_CUDA;
@@ -54,6 +56,13 @@ extern "C" int eimp_besthaps_noalloc(void *stream, size_t ntgt, size_t M, const 
     if (!ntgt || !M || !nhaps || !K || !d_gt || !d_hapmajor || !d_besthaps || !d_flags) return EIMP_E_ARG;
     if (ntgt > (size_t)EIMP_BESTHAPS_NOALLOC_MAX / nhaps) return EIMP_E_CAPACITY;
     if (M > (size_t)INT32_MAX || nhaps > (size_t)INT32_MAX) return EIMP_E_ARG;
+    // the kernel keeps the target's two genotype bit vectors in shared memory
+    // (16 * W(M) bytes per CTA): longer targets do not fit a CTA
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return EIMP_E_CUDA;
+    if ((size_t)16 * eimp_W(M) > (size_t)optin) return EIMP_E_CAPACITY;
     uint32_t *nerr = nullptr;
     if (int r = nerr_address(&nerr)) return r;
     const size_t Kc = K < nhaps ? K : nhaps;

@@ -40,7 +40,15 @@ enum {
 typedef struct eimp_ctx eimp_ctx;
 
 /* Phasing parameters; defaults of the reference in brackets (Args.cpp:274-299,
- * main.cpp:207-237, 305-306, 326). */
+ * main.cpp:207-237, 305-306, 326).
+ * Limits of this implementation, each returning EIMP_E_ARG when exceeded (the
+ * reference accepts any size_t): K after clamping at most 65,536; hsize,
+ * hsize_fast and the history lengths hsize*hist at most 128 (BooleanHistory
+ * keeps 128 sites); beamwidth and beamwidth_fast at most 128 (the beam
+ * kernel's per-warp arrays); the reference's defaults are inside all of them.
+ * A phasing reference whose typed sites need more than the device's opt-in
+ * shared memory per block for two genotype bit vectors (16 x W(M) bytes;
+ * 929,792 sites on a B200) returns EIMP_E_CAPACITY. */
 typedef struct {
     int K;              /* conditioning haplotypes [10000], clamped to Nrefhaps */
     int hsize;          /* history size H [100] */
@@ -323,8 +331,13 @@ int eimp_phase_targets_dev(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntg
  *    ntgt x W(nhaps) words -- the same values eimp_phase_prep returns;
  *  - ntgt x nhaps must not exceed EIMP_BESTHAPS_NOALLOC_MAX, otherwise the call
  *    returns EIMP_E_CAPACITY and does nothing (split the targets into batches);
+ *  - a target's genotype bit vectors are staged in shared memory (16 x W(M)
+ *    bytes per CTA): M above the device's opt-in shared memory per block
+ *    (929,792 typed sites on a B200) returns EIMP_E_CAPACITY as well;
  *  - the first call on a device looks up the array's device address
- *    (cudaGetSymbolAddress); make it before capturing a stream on that device;
+ *    (cudaGetSymbolAddress) and keeps it; make that call before capturing a
+ *    stream on that device, and do not reset the device (cudaDeviceReset)
+ *    after it, which would leave the kept address stale;
  *  - all calls on a device share the array: calls that overlap on the GPU
  *    (different streams, unsynchronised) race and give wrong results. */
 #define EIMP_BESTHAPS_NOALLOC_MAX (4u << 20)

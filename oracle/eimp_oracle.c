@@ -402,8 +402,11 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
                const uint64_t *sitemajor_full, size_t wN, size_t Mref, const int64_t *typed,
                size_t M, const float *af_full, size_t nrefhaps_total, const int64_t *miss,
                size_t nmiss, int imputeCalls, const uint64_t *hap, uint64_t *bits, float *dos,
-               uint8_t *imputed) {
-    /* TargetImp.cpp:474-558 (+ the constructor's initial state :28-59) */
+               uint8_t *imputed, double *dos64) {
+    /* TargetImp.cpp:474-558 (+ the constructor's initial state :28-59).
+     * dos64 (optional): the FP64 dosage oracle, score/sum in double without
+     * the reference's final rounding to float (-1 at uncovered sites, the
+     * written value elsewhere) */
     memset(bits, 0, eo_W(Mref) * sizeof(uint64_t));
     int beforefirst = 1;
     size_t currm = 0;
@@ -425,6 +428,7 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
             if (imputed) imputed[mref] = 1;
             if (idx0 >= nmatches || (size_t)matches[4 * idx0] > currm) {
                 dos[mref] = -1.0f;                       /* DOSAGE_CONFLICT (:26) */
+                if (dos64) dos64[mref] = -1.0;
             } else {
                 uint64_t score = 0, sum = 0;
                 float af = af_full[mref];
@@ -449,6 +453,7 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
                 }
                 if (score > sum / 2) setbit(bits, mref);
                 dos[mref] = (float)((double)score / (double)sum);
+                if (dos64) dos64[mref] = (double)score / (double)sum;
             }
         } else {
             /* typed, non-missing, calls not imputed: the reference writes
@@ -457,6 +462,7 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
             int b = getbit(hap, currm);
             if (b) setbit(bits, mref);
             dos[mref] = b ? 1.0f : 0.0f;
+            if (dos64) dos64[mref] = b ? 1.0 : 0.0;
         }
         if (mref == mmap) mmap = (currm + 1) < M ? (size_t)typed[currm + 1] : Mref;
     }

@@ -80,7 +80,7 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
                const uint64_t *sitemajor_full, size_t wN, size_t Mref, const int64_t *typed,
                size_t M, const float *af_full, size_t nrefhaps_total, const int64_t *miss,
                size_t nmiss, int imputeCalls, const uint64_t *hap, uint64_t *bits, float *dos,
-               uint8_t *imputed);
+               uint8_t *imputed, double *dos64);
 
 /* Output statistics of an imputed bunch: the numeric part of
  * VCFData::writeVCFImputedBunch (VCFData.cpp:3068-3446) for diploid targets.

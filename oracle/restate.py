@@ -66,7 +66,7 @@ def lib():
                                    _i64p, C.c_size_t]
         L.eo_impute.argtypes = [_i64p, C.c_size_t, _i32p, C.c_size_t, _u64p, C.c_size_t, C.c_size_t, _i64p,
                                 C.c_size_t, _f32p, C.c_size_t, _i64p, C.c_size_t, C.c_int, _u64p, _u64p,
-                                _f32p, _u8p]
+                                _f32p, _u8p, C.c_void_p]
         L.eo_site_stats.restype = C.c_long
         L.eo_site_stats.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t, _u64p, C.c_size_t, _f32p, _u64p, C.c_size_t,
                                     _f32p, _f32p, _u8p, C.c_size_t, _i32p, _u8p, _f32p, C.c_int, C.c_int,
@@ -149,19 +149,25 @@ def smmatches(refpbwt, count0, M, K, hap_words, miss, setmaxerrors=0, maxmatches
     return out[:n].copy()
 
 
-def impute(matches, absperm, sitemajor_full, typed, af_full, nrefhaps, miss, hap_words, imputeCalls=False):
+def impute(matches, absperm, sitemajor_full, typed, af_full, nrefhaps, miss, hap_words, imputeCalls=False,
+           fp64=False):
+    """TargetImp::imputeBunch of one haplotype over all panel sites: (bits,
+    dosages, imputed-site flags), plus the FP64 dosage oracle (score/sum in
+    double, not rounded to float) when fp64 is set."""
     Mref, wN = sitemajor_full.shape
     K = absperm.shape[1]
     bits = np.zeros(W(Mref), np.uint64)
     dos = np.zeros(Mref, np.float32)
     imp = np.zeros(Mref, np.uint8)
+    d64 = np.zeros(Mref, np.float64) if fp64 else None
     m = np.ascontiguousarray(matches, np.int64).reshape(-1, 4)
     lib().eo_impute(m.reshape(-1) if len(m) else np.zeros(4, np.int64), len(m), np.ascontiguousarray(absperm, np.int32),
                     K, np.ascontiguousarray(sitemajor_full), wN, Mref, np.ascontiguousarray(typed, np.int64),
                     len(typed), np.ascontiguousarray(af_full, np.float32), nrefhaps,
                     np.ascontiguousarray(miss, np.int64) if len(miss) else np.zeros(1, np.int64), len(miss),
-                    int(imputeCalls), np.ascontiguousarray(hap_words, np.uint64), bits, dos, imp)
-    return bits, dos, imp
+                    int(imputeCalls), np.ascontiguousarray(hap_words, np.uint64), bits, dos, imp,
+                    d64.ctypes.data if fp64 else None)
+    return (bits, dos, imp, d64) if fp64 else (bits, dos, imp)
 
 
 def rle_encode(words: np.ndarray):

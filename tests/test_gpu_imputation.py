@@ -109,13 +109,20 @@ def test_imputation_vs_oracle_cfg1_sample(ctx):
     gc, ga = imp.refpbwt()
     np.testing.assert_array_equal(gc, compr)
     np.testing.assert_array_equal(ga, ap)
+    worst = 0.0
     for h in range(2 * nt):
         miss = np.where(tg.gt[h // 2] == 3)[0].astype(np.int64)
         om = R.smmatches(compr, c0, M, panel.nhaps, phased[h], miss)
         np.testing.assert_array_equal(imp.matches(h).astype(np.int64), om)
-        ob, od, oi = R.impute(om, ap, panel.sitemajor, tg.typed, panel.af, panel.nhaps, miss, phased[h])
+        ob, od, oi, o64 = R.impute(om, ap, panel.sitemajor, tg.typed, panel.af, panel.nhaps, miss, phased[h],
+                                   fp64=True)
         np.testing.assert_array_equal(dos[h], od)
         np.testing.assert_array_equal(bits[h], ob)
+        cov = oi.astype(bool) & (o64 >= 0)
+        err = np.abs(dos[h][cov].astype(np.float64) - o64[cov])
+        assert err.max(initial=0.0) <= DOSAGE_TOL
+        worst = max(worst, float(err.max(initial=0.0)))
+    print(f"largest |dosage - FP64 score/sum| over {2 * nt} haplotypes x {panel.nsites} sites: {worst:.3e}")
 
 
 @pytest.mark.parametrize("setmaxerrors", [1, 2, 3])

@@ -5,7 +5,8 @@ device memory (a framework that owns the device budget through its own pool, a
 serving loop that forbids allocation after start-up): its scratch is a fixed
 device array inside the library.  It must give the same best haplotypes and
 flags as the regular entry point eimp_phase_prep, call after call -- the shared
-array keeps the previous call's contents, so two calls in a row are checked.
+array keeps the previous call's contents, so three calls in a row are checked,
+the last one filling the whole array.
 This file is collected last on purpose."""
 import ctypes as C
 
@@ -37,9 +38,21 @@ def test_besthaps_noalloc_matches_regular_entry_point():
     cases = [(g["gt"], g["hapmajor_typed"], g["sitemajor_typed"], g["cm_typed"], 50)]
     hm2, sm2, cm2 = synth.typed_views(panel, groups[0].typed)
     cases.append((groups[0].gt, hm2, sm2, cm2, 200))
+    # third call at the array's capacity: 8192 targets x 512 haplotypes fill
+    # all EIMP_BESTHAPS_NOALLOC_MAX entries (largest offsets into the array)
+    rng = np.random.default_rng(4096)
+    Mx, nhx, ntx = 700, 512, 8192
+    assert ntx * nhx == 4 << 20
+    dense = (rng.random((nhx, Mx)) < 0.3).astype(np.uint8)
+    from eimp_b200.bits import pack_rows, transpose_bits
+    hm3 = pack_rows(dense, W(Mx))
+    sm3 = transpose_bits(hm3, nhx, Mx)
+    gt3 = (dense[rng.integers(0, nhx, ntx)] + dense[rng.integers(0, nhx, ntx)]).astype(np.uint8)
+    gt3[rng.random(gt3.shape) < 0.01] = 3
+    cases.append((gt3, hm3, sm3, np.linspace(0.0, 3.0, Mx, dtype=np.float32), 64))
     ctx = Context(0)
     dev = torch.device("cuda", 0)
-    # two calls in a row (different panels, targets and K): each must match
+    # three calls in a row (different panels, targets and K): each must match
     # the regular entry point, whatever the previous call left in the array
     for gt, hm, sm, cm, K in cases:
         gt = np.ascontiguousarray(gt, dtype=np.uint8)
