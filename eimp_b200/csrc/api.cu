@@ -76,8 +76,8 @@ struct eimp_ctx {
 
     // imputation reference
     size_t i_Mref = 0, i_nhaps = 0, i_M = 0;
-    DBuf i_hapfull, i_sitefull_tmp, i_af, i_typed, i_segm, i_common, i_sitetyped_tmp, i_compr, i_absperm,
-        i_count0;
+    DBuf i_hapfull, i_sitefull_tmp, i_af, i_typed, i_segm, i_common, i_sinfo, i_sitetyped_tmp, i_compr,
+        i_absperm, i_count0;
     // prepared targets
     size_t i_ntargets = 0;
     int i_imputeCalls = 0;
@@ -284,6 +284,7 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
     CK(ctx->i_typed.reserve(M * 8));
     CK(ctx->i_segm.reserve(Mref * 4));
     CK(ctx->i_common.reserve(Mref));
+    CK(ctx->i_sinfo.reserve(Mref * sizeof(int2)));
     CK(ctx->i_compr.reserve(M * kw * 4));
     CK(ctx->i_absperm.reserve((M + 1) * nhaps * 4));
     CK(ctx->i_count0.reserve(M * 4));
@@ -291,8 +292,8 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
     CK(cudaMemcpyAsync(ctx->i_typed.p, d_typed, M * 8, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemsetAsync(ctx->i_hapfull.p, 0, nhaps * wMref * 8, st));
     LAUNCH(launch_transpose(d_sitemajor_full, Mref, wN, ctx->i_hapfull.as<uint64_t>(), nhaps, wMref, st));
-    LAUNCH(launch_segmap(ctx->i_typed.as<int64_t>(), (int)M, (int)Mref, ctx->i_segm.as<int32_t>(),
-                         ctx->i_common.as<uint8_t>(), st));
+    LAUNCH(launch_segmap(ctx->i_typed.as<int64_t>(), (int)M, (int)Mref, ctx->i_af.as<float>(), (int)nhaps,
+                         ctx->i_segm.as<int32_t>(), ctx->i_common.as<uint8_t>(), ctx->i_sinfo.as<int2>(), st));
     LAUNCH(launch_refpbwt(d_sitemajor_typed, (int)M, (int)nhaps, (int)wN, ctx->i_compr.as<uint32_t>(),
                           ctx->i_absperm.as<int32_t>(), ctx->i_count0.as<int32_t>(), st));
     CK(cudaEventRecord(ctx->ref_ready, st));
@@ -375,8 +376,7 @@ int eimp_imp_bunch_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t
     CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
     LAUNCH(launch_dosage(ctx->i_matches.as<int4>(), (int)ctx->i_cap, ctx->i_nmatch.as<int>(),
                          ctx->i_absperm.as<int32_t>(), (int)ctx->i_nhaps, ctx->i_hapfull.as<uint64_t>(),
-                         (int)eimp_W(ctx->i_Mref), ctx->i_segm.as<int32_t>(), ctx->i_common.as<uint8_t>(),
-                         ctx->i_af.as<float>(), (int)ctx->i_nhaps, ctx->i_phased.as<uint64_t>(), (int)eimp_W(M),
+                         (int)eimp_W(ctx->i_Mref), ctx->i_sinfo.as<int2>(), ctx->i_phased.as<uint64_t>(), (int)eimp_W(M),
                          ctx->i_gt.as<uint8_t>(), (int)M, (int)(2 * ctx->i_ntargets), (int)mref_begin, (int)nsites,
                          ctx->i_imputeCalls, d_dos, (int)ldd, d_bits, (int)ldb_words, ctx->stream));
     return 0;

@@ -10,7 +10,9 @@
 //                      the compact kernel stores the tree in 30 B per node
 //                      (typed sites < 65536).
 //  dosage_kernel    -- TargetImp::imputeBunch (TargetImp.cpp:474-558), one
-//                      warp per (target haplotype, 64-site tile).
+//                      warp per (target haplotype, span of 64-site tiles).
+#include <climits>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -548,124 +550,276 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// dosages.  One warp per (target haplotype, tile of 64 sites of the window).
-// Lane j handles sites base+j and base+32+j.
+// dosages (TargetImp::imputeBunch, TargetImp.cpp:474-558).
+//
+// One warp per (target haplotype, span of DOS_SPAN tiles of 64 sites); lane j
+// owns sites base+j and base+32+j of each tile.  A site's dosage sums, over
+// the set-maximal matches covering its last typed site k (start <= k < end),
+// single = (k-start+1)(end-k) once per reference of the match's interval, and
+// into the score where that reference carries the alternative allele.  The
+// matches are sorted by end and by start, so the warp keeps a window of 32
+// of them in registers (one per lane) and slides it along the span: matches
+// that end at or before a tile's first segment leave at the front, and the
+// covering ones are the window's prefix up to the first match that starts
+// after the tile's last segment.  The (match, reference) pairs ("slots") of
+// the covering matches are dealt out to the lanes; each lane keeps its
+// slot's reference haplotype for as long as the covering matches stay the
+// same (usually many tiles), loads that haplotype's 64 sites of the tile (one
+// word of the haplotype-major panel, two where the window is not
+// word-aligned), and the per-site counts come from shuffles of those words.
+// More than 32 slots or covering matches take a general path that deals the
+// slots out in chunks of 32 per tile.  score and sum are integers, so the
+// order of the additions does not change them and the dosage (double score /
+// double sum, rounded to float) is bit-exact.
+//
+// Per reference site the kernel reads one int2 (sinfo, built with the
+// segment map): x = last typed site k | typed-site flag << 31, y = the
+// smallest match height that takes the low-frequency shortcut of
+// TargetImp.cpp:522-531 (float maf * Nrefhaps < 0.01 * height, evaluated
+// once per site instead of once per match) | (af > 0.5) << 31.
 // ---------------------------------------------------------------------------
+constexpr int DOS_SPAN = 8;
+
+// uint64 -> double without the conversion unit: exact for x < 2^52 (the bits
+// of 2^52 + x as a double, minus 2^52)
+__device__ __forceinline__ double dos_u64_to_f64(uint64_t x) {
+    if (x < (1ull << 52)) return __longlong_as_double((long long)(0x4330000000000000ull | x)) - 4503599627370496.0;
+    return (double)x;
+}
+
+// a double q in [2^-126, 1] rounded to the nearest float, ties to even (the
+// rounding of a C cast), by integer operations on its bits: keep 23 of the 52
+// fraction bits, add half an ulp minus one plus the kept lowest bit, and let
+// a carry out of the fraction step the exponent
+__device__ __forceinline__ float dos_f64_to_f32(double q) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(q);
+    const unsigned e = (unsigned)(b >> 52);
+    const unsigned long long m = b & ((1ull << 52) - 1);
+    const unsigned long long r = m + 0x0FFFFFFFull + ((m >> 29) & 1ull);
+    return __uint_as_float(((e - 1023u + 127u) << 23) + (unsigned)(r >> 29));
+}
+
+// one covered site's share of a match: the shortcut adds height x single to
+// the sum (and to the score where the alternative allele is the major one),
+// otherwise single per reference of the match (n of them in this chunk,
+// cnt of them with the alternative allele)
+struct DosSite {
+    int k, hthr;
+    bool imp, altmajor;
+    uint64_t score, sum;
+    __device__ __forceinline__ void add(int st, int en, int h, int cnt, int n, bool first) {
+        if (!imp || st > k || k >= en) return;
+        const uint64_t single = (uint64_t)(k - st + 1) * (uint64_t)(en - k);
+        if (h >= hthr) {
+            if (first) {
+                const uint64_t t = (uint64_t)h * single;
+                sum += t;
+                if (altmajor) score += t;
+            }
+        } else {
+            score += single * (uint64_t)cnt;
+            sum += single * (uint64_t)n;
+        }
+    }
+    __device__ __forceinline__ float dosage(int &bit) const {
+        if (sum == 0) return -1.0f;   // DOSAGE_CONFLICT (TargetImp.cpp:26,507-509)
+        bit = score > sum / 2;
+        if (score == 0) return 0.0f;
+        return dos_f64_to_f32(dos_u64_to_f64(score) / dos_u64_to_f64(sum));
+    }
+};
+
+__device__ __forceinline__ void dos_word(const uint64_t *__restrict__ hr, int w0, int o0, int wMref, uint32_t &lo,
+                                         uint32_t &hi) {
+    uint64_t x = hr[w0];
+    if (o0) x = (x >> o0) | ((w0 + 1 < wMref ? hr[w0 + 1] : 0ull) << (64 - o0));
+    lo = (uint32_t)x;
+    hi = (uint32_t)(x >> 32);
+}
+
 __global__ void __launch_bounds__(256) dosage_kernel(
     const int4 *__restrict__ matches, int cap, const int *__restrict__ nmatch,
     const int32_t *__restrict__ absperm, int K, const uint64_t *__restrict__ hapmajor_full, int wMref,
-    const int32_t *__restrict__ segm, const uint8_t *__restrict__ common, const float *__restrict__ af,
-    int nrefhaps_total, const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int M,
-    int nhaps, int mref_begin, int nsites, int imputeCalls, float *__restrict__ dos, int ldd,
+    const int2 *__restrict__ sinfo, const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt,
+    int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *__restrict__ dos, int ldd,
     uint64_t *__restrict__ bits, int ldb) {
+    const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const long gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int ntiles = (nsites + 63) / 64;
-    const int hap = (int)(gw / ntiles);
-    const int tile = (int)(gw % ntiles);
+    const int nspans = (ntiles + DOS_SPAN - 1) / DOS_SPAN;
+    const int hap = (int)(gw / nspans);
     if (hap >= nhaps) return;
-    const int base = mref_begin + tile * 64;
+    const int t0 = (int)(gw % nspans) * DOS_SPAN, t1 = min(ntiles, t0 + DOS_SPAN);
     const int end = mref_begin + nsites;
     const uint8_t *g = gt + (size_t)(hap >> 1) * M;
     const uint64_t *hw = phased + (size_t)hap * wM;
-
-    int s[2] = {base + lane, base + 32 + lane};
-    bool valid[2], imp[2];
-    int k[2];
-    float afv[2];
-    bool shortc[2];
-    uint64_t score[2] = {0, 0}, sum[2] = {0, 0};
-    for (int j = 0; j < 2; j++) {
-        valid[j] = s[j] < end;
-        int ss = valid[j] ? s[j] : base;
-        k[j] = segm[ss];
-        afv[j] = af[ss];
-        imp[j] = valid[j] && (!common[ss] || g[k[j]] == 3 || imputeCalls);
-    }
-    // matches covering any site of the tile
-    const int n = nmatch[hap] < 0 ? 0 : nmatch[hap];
+    const int n = max(nmatch[hap], 0);
     const int4 *mt = matches + (size_t)hap * cap;
-    const int kmin = segm[base];
-    const int kmax = segm[min(base + 63, end - 1)];
-    int lo = 0, hi = n;
-    {   // first match with end > kmin
-        int a = 0, b = n;
-        while (a < b) { int c = (a + b) >> 1; if (mt[c].y > kmin) b = c; else a = c + 1; }
-        lo = a;
-        a = lo; b = n;   // first match with start > kmax
-        while (a < b) { int c = (a + b) >> 1; if (mt[c].x > kmax) b = c; else a = c + 1; }
-        hi = a;
+    // an empty window slot: it neither covers nor leaves
+    const int4 NONE = make_int4(INT_MAX, INT_MAX, 0, -1);
+    const int KMASK = 0x7fffffff;
+
+    // window start: the first match ending after the span's first segment
+    const int kmin0 = sinfo[mref_begin + t0 * 64].x & KMASK;
+    int wb = n;
+    for (int b = 0; b < n; b += 32) {
+        const unsigned f = __ballot_sync(FULL, b + lane < n && mt[b + lane].y > kmin0);
+        if (f) { wb = b + __ffs(f) - 1; break; }
     }
-    const int w0 = base >> 6;
-    for (int i = lo; i < hi; i++) {
-        const int4 mm = mt[i];
-        const int height = mm.w - mm.z + 1;
-        bool cov[2];
-        bool loop = false;
-        uint64_t single[2];
-        for (int j = 0; j < 2; j++) {
-            cov[j] = imp[j] && mm.x <= k[j] && k[j] < mm.y;
-            single[j] = (uint64_t)(k[j] - mm.x + 1) * (uint64_t)(mm.y - k[j]);
-            float maf = afv[j] > 0.5f ? 1.0f - afv[j] : afv[j];
-            // TargetImp.cpp:526: float maf * Nrefhaps (as float) against double 0.01 * height
-            shortc[j] = (double)__fmul_rn(maf, (float)nrefhaps_total) < 0.01 * (double)height;
-            if (cov[j] && shortc[j]) {
-                sum[j] += (uint64_t)height * single[j];
-                if (afv[j] > 0.5f) score[j] += (uint64_t)height * single[j];
-            }
-            loop |= cov[j] && !shortc[j];
+    int4 win = wb + lane < n ? mt[wb + lane] : NONE;
+    // slots of the covering set (cwb, cncov): per window lane its height and
+    // first slot, per lane its slot's reference haplotype (-1: none)
+    int cwb = -1, cncov = -1, hgt = 0, off = 0, total = 0, sref = -1;
+
+    for (int tile = t0; tile < t1; tile++) {
+        const int base = mref_begin + tile * 64;
+        const int kmin = sinfo[base].x & KMASK;
+        const int kmax = sinfo[min(base + 63, end - 1)].x & KMASK;
+        // matches ending at or before kmin leave the front of the window (TargetImp.cpp:489-490)
+        for (;;) {
+            const unsigned d = __ballot_sync(FULL, win.y <= kmin);
+            if (!(d & 1u)) break;
+            const int nd = ~d ? __ffs(~d) - 1 : 32;
+            wb += nd;
+            win = wb + lane < n ? mt[wb + lane] : NONE;
+            if (nd < 32) break;
         }
-        if (!__any_sync(0xffffffffu, loop)) continue;
-        const int32_t *ap = absperm + (size_t)mm.y * K;
-        for (int r = mm.z; r <= mm.w; r++) {
-            const int ref = ap[r];
-            const uint64_t *hr = hapmajor_full + (size_t)ref * wMref;
-            const uint64_t wa = hr[w0];
-            const uint64_t wb = (w0 + 1 < wMref) ? hr[w0 + 1] : 0ull;
-            for (int j = 0; j < 2; j++) {
-                if (cov[j] && !shortc[j]) {
-                    int off = s[j] - (w0 << 6);
-                    uint64_t word = off < 64 ? wa : wb;
-                    sum[j] += single[j];
-                    if ((word >> (off & 63)) & 1ull) score[j] += single[j];
+        DosSite S0, S1;
+        const int s0 = base + lane, s1 = base + 32 + lane;
+        const bool valid0 = s0 < end, valid1 = s1 < end;
+        {
+            const int2 i0 = sinfo[valid0 ? s0 : base], i1 = sinfo[valid1 ? s1 : base];
+            S0.k = i0.x & KMASK; S0.hthr = i0.y & KMASK; S0.altmajor = i0.y < 0;
+            S1.k = i1.x & KMASK; S1.hthr = i1.y & KMASK; S1.altmajor = i1.y < 0;
+            S0.imp = valid0 && (i0.x >= 0 || g[S0.k] == 3 || imputeCalls);
+            S1.imp = valid1 && (i1.x >= 0 || g[S1.k] == 3 || imputeCalls);
+            S0.score = S0.sum = S1.score = S1.sum = 0;
+        }
+        const int w0 = base >> 6, o0 = base & 63;
+        // covering matches: up to the first one starting after the tile (TargetImp.cpp:516)
+        const unsigned cb = __ballot_sync(FULL, win.x <= kmax);
+        const int ncov = ~cb ? __ffs(~cb) - 1 : 32;
+        if (ncov != cncov || wb != cwb) {
+            hgt = lane < ncov ? win.w - win.z + 1 : 0;
+            off = hgt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, off, o);
+                if (lane >= o) off += t;
+            }
+            total = __shfl_sync(FULL, off, 31);
+            off -= hgt;
+            int mi = 0;   // the match of this lane's slot: the last with first slot <= lane
+            for (int i = 1; i < ncov; i++) mi += __shfl_sync(FULL, off, i) <= lane;
+            const int my = __shfl_sync(FULL, win.y, mi), mz = __shfl_sync(FULL, win.z, mi);
+            const int mo = __shfl_sync(FULL, off, mi);
+            sref = lane < total ? absperm[(size_t)my * K + mz + (lane - mo)] : -1;
+            cwb = wb;
+            cncov = ncov;
+        }
+        if (ncov < 32 && total <= 32) {
+            // every slot has its lane
+            uint32_t xlo = 0u, xhi = 0u;
+            if (sref >= 0) dos_word(hapmajor_full + (size_t)sref * wMref, w0, o0, wMref, xlo, xhi);
+            for (int i = 0; i < ncov; i++) {
+                const int oi = __shfl_sync(FULL, off, i), hi = __shfl_sync(FULL, hgt, i);
+                const int st = __shfl_sync(FULL, win.x, i), en = __shfl_sync(FULL, win.y, i);
+                int cnt0 = 0, cnt1 = 0;
+                for (int q = oi; q < oi + hi; q++) {
+                    cnt0 += (__shfl_sync(FULL, xlo, q) >> lane) & 1u;
+                    cnt1 += (__shfl_sync(FULL, xhi, q) >> lane) & 1u;
                 }
+                S0.add(st, en, hi, cnt0, hi, true);
+                S1.add(st, en, hi, cnt1, hi, true);
             }
-        }
-    }
-    float* drow = dos + (size_t)hap * ldd;
-    uint32_t bw[2];
-    for (int j = 0; j < 2; j++) {
-        int b = 0;
-        float d = 0.0f;
-        if (valid[j]) {
-            if (imp[j]) {
-                if (sum[j] == 0) d = -1.0f;           // DOSAGE_CONFLICT (TargetImp.cpp:26,507-509)
-                else {
-                    b = score[j] > sum[j] / 2;
-                    d = (float)((double)score[j] / (double)sum[j]);
+        } else {
+            // general path: pages of 32 covering matches, chunks of 32 slots
+            for (int pb = 0;; pb += 32) {
+                const int4 pw = pb == 0 ? win : (wb + pb + lane < n ? mt[wb + pb + lane] : NONE);
+                const unsigned pc = __ballot_sync(FULL, pw.x <= kmax);
+                const int pn = ~pc ? __ffs(~pc) - 1 : 32;
+                if (pn == 0) break;
+                const int ph = lane < pn ? pw.w - pw.z + 1 : 0;
+                int po = ph;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(FULL, po, o);
+                    if (lane >= o) po += t;
                 }
-            } else {
-                b = bit_at(hw, k[j]);
-                d = b ? 1.0f : 0.0f;
+                const int ptot = __shfl_sync(FULL, po, 31);
+                po -= ph;
+                for (int c = 0; c < ptot; c += 32) {
+                    const int s = c + lane;
+                    int mi = 0;
+                    for (int i = 1; i < pn; i++) mi += __shfl_sync(FULL, po, i) <= s;
+                    const int my = __shfl_sync(FULL, pw.y, mi), mz = __shfl_sync(FULL, pw.z, mi);
+                    const int mo = __shfl_sync(FULL, po, mi);
+                    uint32_t xlo = 0u, xhi = 0u;
+                    if (s < ptot)
+                        dos_word(hapmajor_full + (size_t)absperm[(size_t)my * K + mz + (s - mo)] * wMref, w0, o0,
+                                 wMref, xlo, xhi);
+                    const int cend = min(ptot, c + 32);
+                    for (int i = 0; i < pn; i++) {
+                        const int oi = __shfl_sync(FULL, po, i), hi = __shfl_sync(FULL, ph, i);
+                        const int a = max(oi, c), b = min(oi + hi, cend);
+                        if (a >= b) continue;   // warp-uniform
+                        int cnt0 = 0, cnt1 = 0;
+                        for (int q = a; q < b; q++) {
+                            cnt0 += (__shfl_sync(FULL, xlo, q - c) >> lane) & 1u;
+                            cnt1 += (__shfl_sync(FULL, xhi, q - c) >> lane) & 1u;
+                        }
+                        const int st = __shfl_sync(FULL, pw.x, i), en = __shfl_sync(FULL, pw.y, i);
+                        S0.add(st, en, hi, cnt0, b - a, a == oi);
+                        S1.add(st, en, hi, cnt1, b - a, a == oi);
+                    }
+                }
+                if (pn < 32) break;
             }
-            drow[s[j] - mref_begin] = d;
         }
-        bw[j] = __ballot_sync(0xffffffffu, b);
+
+        float *drow = dos + (size_t)hap * ldd;
+        int b0 = 0, b1 = 0;
+        if (valid0) {
+            float d;
+            if (S0.imp) d = S0.dosage(b0);
+            else { b0 = bit_at(hw, S0.k); d = b0 ? 1.0f : 0.0f; }
+            drow[s0 - mref_begin] = d;
+        }
+        if (valid1) {
+            float d;
+            if (S1.imp) d = S1.dosage(b1);
+            else { b1 = bit_at(hw, S1.k); d = b1 ? 1.0f : 0.0f; }
+            drow[s1 - mref_begin] = d;
+        }
+        const unsigned bw0 = __ballot_sync(FULL, b0), bw1 = __ballot_sync(FULL, b1);
+        if (lane == 0) bits[(size_t)hap * ldb + tile] = (uint64_t)bw0 | ((uint64_t)bw1 << 32);
     }
-    if (lane == 0) bits[(size_t)hap * ldb + tile] = (uint64_t)bw[0] | ((uint64_t)bw[1] << 32);
 }
 
 // per-site segment map: segm[mref] = index of the last typed site <= mref
-// (0 before the first), common[mref] = 1 at typed sites
-__global__ void segmap_kernel(const int64_t *__restrict__ typed, int M, int Mref, int32_t *__restrict__ segm,
-                              uint8_t *__restrict__ common) {
+// (0 before the first), common[mref] = 1 at typed sites; sinfo[mref] (the
+// dosage kernel's per-site word pair) = {segm | common << 31, the smallest
+// match height h with (double)(float maf * (float)Nrefhaps) < 0.01 * (double)h
+// -- the low-frequency shortcut of TargetImp.cpp:526 -- | (af > 0.5) << 31}
+__global__ void segmap_kernel(const int64_t *__restrict__ typed, int M, int Mref, const float *__restrict__ af,
+                              int nrefhaps_total, int32_t *__restrict__ segm, uint8_t *__restrict__ common,
+                              int2 *__restrict__ sinfo) {
     int mref = blockIdx.x * blockDim.x + threadIdx.x;
     if (mref >= Mref) return;
     int a = 0, b = M;   // number of typed sites <= mref
     while (a < b) { int c = (a + b) >> 1; if (typed[c] <= mref) a = c + 1; else b = c; }
     int cnt = a;
-    segm[mref] = cnt > 0 ? cnt - 1 : 0;
-    common[mref] = (cnt > 0 && typed[cnt - 1] == mref) ? 1 : 0;
+    const int k = cnt > 0 ? cnt - 1 : 0;
+    const int cm = (cnt > 0 && typed[cnt - 1] == mref) ? 1 : 0;
+    segm[mref] = k;
+    common[mref] = (uint8_t)cm;
+    const float afv = af[mref];
+    const float maf = afv > 0.5f ? 1.0f - afv : afv;
+    const double x = (double)__fmul_rn(maf, (float)nrefhaps_total);
+    // 0.01 * h is monotone in h: step up from just below x / 0.01
+    double start = floor(x * 100.0) - 2.0;
+    int h = start < 1.0 ? 1 : (start > 1.0e9 ? 1000000000 : (int)start);
+    while (h < 1000000000 && !(x < 0.01 * (double)h)) h++;
+    sinfo[mref] = make_int2(k | (cm << 31), h | ((afv > 0.5f ? 1 : 0) << 31));
 }
 
 // ---------------------------------------------------------------------------
@@ -727,20 +881,21 @@ cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int 
 }
 
 cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,
-                          const uint64_t *hapmajor_full, int wMref, const int32_t *segm, const uint8_t *common,
-                          const float *af, int nrefhaps_total, const uint64_t *phased, int wM, const uint8_t *gt,
-                          int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *dos, int ldd,
-                          uint64_t *bits, int ldb, cudaStream_t st) {
-    long warps = (long)nhaps * ((nsites + 63) / 64);
+                          const uint64_t *hapmajor_full, int wMref, const int2 *sinfo, const uint64_t *phased, int wM,
+                          const uint8_t *gt, int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *dos,
+                          int ldd, uint64_t *bits, int ldb, cudaStream_t st) {
+    const long ntiles = (nsites + 63) / 64;
+    long warps = (long)nhaps * ((ntiles + DOS_SPAN - 1) / DOS_SPAN);
     long blocks = (warps + 7) / 8;
-    dosage_kernel<<<(unsigned)blocks, 256, 0, st>>>(matches, cap, nmatch, absperm, K, hapmajor_full, wMref, segm,
-                                                    common, af, nrefhaps_total, phased, wM, gt, M, nhaps,
-                                                    mref_begin, nsites, imputeCalls, dos, ldd, bits, ldb);
+    dosage_kernel<<<(unsigned)blocks, 256, 0, st>>>(matches, cap, nmatch, absperm, K, hapmajor_full, wMref, sinfo,
+                                                    phased, wM, gt, M, nhaps, mref_begin, nsites, imputeCalls, dos,
+                                                    ldd, bits, ldb);
     return cudaGetLastError();
 }
 
-cudaError_t launch_segmap(const int64_t *typed, int M, int Mref, int32_t *segm, uint8_t *common, cudaStream_t st) {
-    segmap_kernel<<<(Mref + 255) / 256, 256, 0, st>>>(typed, M, Mref, segm, common);
+cudaError_t launch_segmap(const int64_t *typed, int M, int Mref, const float *af, int nrefhaps_total, int32_t *segm,
+                          uint8_t *common, int2 *sinfo, cudaStream_t st) {
+    segmap_kernel<<<(Mref + 255) / 256, 256, 0, st>>>(typed, M, Mref, af, nrefhaps_total, segm, common, sinfo);
     return cudaGetLastError();
 }
 

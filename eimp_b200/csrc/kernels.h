@@ -27,11 +27,13 @@ cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int 
                        const uint8_t *gt, int nhaps, int setmaxerrors, int4 *matches, int cap, int *nmatch,
                        uint32_t *status, cudaStream_t st);
 cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,
-                          const uint64_t *hapmajor_full, int wMref, const int32_t *segm, const uint8_t *common,
-                          const float *af, int nrefhaps_total, const uint64_t *phased, int wM, const uint8_t *gt,
-                          int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *dos, int ldd,
-                          uint64_t *bits, int ldb, cudaStream_t st);
-cudaError_t launch_segmap(const int64_t *typed, int M, int Mref, int32_t *segm, uint8_t *common, cudaStream_t st);
+                          const uint64_t *hapmajor_full, int wMref, const int2 *sinfo, const uint64_t *phased, int wM,
+                          const uint8_t *gt, int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *dos,
+                          int ldd, uint64_t *bits, int ldb, cudaStream_t st);
+// segment map of the typed sites over the reference sites, plus the dosage
+// kernel's per-site pair (segment | typed << 31, shortcut height | af>0.5 << 31)
+cudaError_t launch_segmap(const int64_t *typed, int M, int Mref, const float *af, int nrefhaps_total, int32_t *segm,
+                          uint8_t *common, int2 *sinfo, cudaStream_t st);
 
 // ---- output statistics of an imputed bunch (site_stats.cu)
 struct SiteStatsArgs {

@@ -152,6 +152,8 @@ inline int __ffs(int x) { return __builtin_ffs(x); }
 inline unsigned __float_as_uint(float f) { unsigned u; std::memcpy(&u, &f, 4); return u; }
 inline float __uint_as_float(unsigned u) { float f; std::memcpy(&f, &u, 4); return f; }
 inline float __int_as_float(int u) { float f; std::memcpy(&f, &u, 4); return f; }
+inline double __longlong_as_double(long long u) { double f; std::memcpy(&f, &u, 8); return f; }
+inline long long __double_as_longlong(double f) { long long u; std::memcpy(&u, &f, 8); return u; }
 // IEEE round-to-nearest, one operation each (built with -ffp-contract=off)
 inline float __fadd_rn(float a, float b) { volatile float r = a + b; return r; }
 inline float __fmul_rn(float a, float b) { volatile float r = a * b; return r; }
