@@ -296,6 +296,31 @@ void *refo_imp_create(void *hp, const uint64_t *phased, unsigned nthreads, int s
 
 void refo_imp_destroy(void *ip) { delete (ImpHandle*)ip; }
 
+/* New phased target haplotypes against the imputer's existing reference
+ * PBWT: the match part of PBWTImputer::prepareImputation
+ * (PBWTImputer.cpp:117-157) with the reference's own TargetImp, OpenMP
+ * dynamic,1 over the haplotypes as there.  The PBWT is built once per
+ * imputer; this times what each further set of targets costs. */
+void refo_imp_retarget(void *ip, const uint64_t *phased, unsigned nthreads) {
+    ImpHandle *ih = (ImpHandle*)ip;
+    VCFData &v = ih->h->vd;
+    PBWTImputer *imp = ih->imp;
+    size_t cap = capBytes(v.M);
+    memcpy(ih->pdata, phased, 2 * v.Ntarget * cap);
+    std::vector<size_t> nsites = {0, v.Mref, 0};
+    imp->targets.clear();
+    imp->targets.reserve(imp->nTargetHap);
+    for (size_t nhap = 0; nhap < imp->nTargetHap; nhap++)
+        imp->targets.emplace_back(nhap, v, *imp->pbwt, ih->phased[v.getHaploidsTgtMap()[nhap]], imp->num_blocks,
+                                  imp->setmaxerrors, imp->imputeCalls, imp->debug);
+    omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (size_t nhap = 0; nhap < imp->nTargetHap; nhap++) {
+        imp->targets[nhap].calcSMMatches();
+        imp->targets[nhap].prepareBlocks(nsites);
+    }
+}
+
 size_t refo_imp_nmatches(void *ip, size_t hap) {
     ImpHandle *ih = (ImpHandle*)ip;
     return ih->imp->targets[hap].sm_matches.size();

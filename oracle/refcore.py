@@ -57,6 +57,7 @@ def lib():
         L.refo_imp_create.restype = C.c_void_p
         L.refo_imp_create.argtypes = [C.c_void_p, _u64p, C.c_uint, C.c_int, C.c_int]
         L.refo_imp_destroy.argtypes = [C.c_void_p]
+        L.refo_imp_retarget.argtypes = [C.c_void_p, _u64p, C.c_uint]
         L.refo_imp_nmatches.restype = C.c_size_t
         L.refo_imp_nmatches.argtypes = [C.c_void_p, C.c_size_t]
         L.refo_imp_matches.argtypes = [C.c_void_p, C.c_size_t, _i64p]
@@ -267,6 +268,13 @@ class RefImputer:
             self.close()
         except Exception:
             pass
+
+    def retarget(self, phased: np.ndarray, nthreads: int = 1):
+        """Matches of new phased haplotypes of the same targets against the
+        PBWT already built (the match part of prepareImputation)."""
+        phased = np.ascontiguousarray(phased, dtype=np.uint64)
+        assert phased.shape == (2 * self.core.ntarget, W(self.core.M))
+        lib().refo_imp_retarget(self.h, phased, nthreads)
 
     def matches(self, hap: int) -> np.ndarray:
         n = lib().refo_imp_nmatches(self.h, hap)
