@@ -602,23 +602,39 @@ __device__ __forceinline__ float dos_f64_to_f32(double q) {
 // one covered site's share of a match: the shortcut adds height x single to
 // the sum (and to the score where the alternative allele is the major one),
 // otherwise single per reference of the match (n of them in this chunk,
-// cnt of them with the alternative allele)
-struct DosSite {
+// cnt of them with the alternative allele).  With fewer than 131,071 typed
+// sites single = (k-start+1)(end-k) <= ((M+1)/2)^2 fits 32 bits and every
+// term is one 32 x 32 -> 64-bit multiply-add (WIDE: 64-bit single).
+template <bool WIDE> struct DosSite {
     int k, hthr;
     bool imp, altmajor;
     uint64_t score, sum;
     __device__ __forceinline__ void add(int st, int en, int h, int cnt, int n, bool first) {
         if (!imp || st > k || k >= en) return;
-        const uint64_t single = (uint64_t)(k - st + 1) * (uint64_t)(en - k);
-        if (h >= hthr) {
-            if (first) {
-                const uint64_t t = (uint64_t)h * single;
-                sum += t;
-                if (altmajor) score += t;
+        if (WIDE) {
+            const uint64_t single = (uint64_t)(k - st + 1) * (uint64_t)(en - k);
+            if (h >= hthr) {
+                if (first) {
+                    const uint64_t t = (uint64_t)h * single;
+                    sum += t;
+                    if (altmajor) score += t;
+                }
+            } else {
+                score += single * (uint64_t)cnt;
+                sum += single * (uint64_t)n;
             }
         } else {
-            score += single * (uint64_t)cnt;
-            sum += single * (uint64_t)n;
+            const uint32_t single = (uint32_t)(k - st + 1) * (uint32_t)(en - k);
+            if (h >= hthr) {
+                if (first) {
+                    const uint64_t t = (uint64_t)(uint32_t)h * single;
+                    sum += t;
+                    if (altmajor) score += t;
+                }
+            } else {
+                score += (uint64_t)single * (uint32_t)cnt;
+                sum += (uint64_t)single * (uint32_t)n;
+            }
         }
     }
     __device__ __forceinline__ float dosage(int &bit) const {
@@ -637,7 +653,8 @@ __device__ __forceinline__ void dos_word(const uint64_t *__restrict__ hr, int w0
     hi = (uint32_t)(x >> 32);
 }
 
-__global__ void __launch_bounds__(256) dosage_kernel(
+template <bool WIDE>
+__global__ void __launch_bounds__(256, 4) dosage_kernel(
     const int4 *__restrict__ matches, int cap, const int *__restrict__ nmatch,
     const int32_t *__restrict__ absperm, int K, const uint64_t *__restrict__ hapmajor_full, int wMref,
     const int2 *__restrict__ sinfo, const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt,
@@ -685,7 +702,7 @@ __global__ void __launch_bounds__(256) dosage_kernel(
             win = wb + lane < n ? mt[wb + lane] : NONE;
             if (nd < 32) break;
         }
-        DosSite S0, S1;
+        DosSite<WIDE> S0, S1;
         const int s0 = base + lane, s1 = base + 32 + lane;
         const bool valid0 = s0 < end, valid1 = s1 < end;
         {
@@ -887,9 +904,9 @@ cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const
     const long ntiles = (nsites + 63) / 64;
     long warps = (long)nhaps * ((ntiles + DOS_SPAN - 1) / DOS_SPAN);
     long blocks = (warps + 7) / 8;
-    dosage_kernel<<<(unsigned)blocks, 256, 0, st>>>(matches, cap, nmatch, absperm, K, hapmajor_full, wMref, sinfo,
-                                                    phased, wM, gt, M, nhaps, mref_begin, nsites, imputeCalls, dos,
-                                                    ldd, bits, ldb);
+    auto kern = M < 131071 ? dosage_kernel<false> : dosage_kernel<true>;
+    kern<<<(unsigned)blocks, 256, 0, st>>>(matches, cap, nmatch, absperm, K, hapmajor_full, wMref, sinfo, phased, wM,
+                                           gt, M, nhaps, mref_begin, nsites, imputeCalls, dos, ldd, bits, ldb);
     return cudaGetLastError();
 }
 

@@ -82,7 +82,7 @@ int main(int argc, char **argv) {
                 blockIdx.x = (unsigned)gw;
                 blockDim.x = 32;
                 emu_warp = &warp;
-                eimp::dosage_kernel(matches.data(), cap, nmatch.data(), absperm.data(), K, hapfull.data(), wMref,
+                (M < 131071 ? eimp::dosage_kernel<false> : eimp::dosage_kernel<true>)(matches.data(), cap, nmatch.data(), absperm.data(), K, hapfull.data(), wMref,
                                     sinfo.data(), phased.data(), wM, gt.data(), M, nhaps, mref_begin, nsites, impcalls,
                                     dos.data(), nsites, bits.data(), ldb);
             });
