@@ -53,6 +53,10 @@ _PROTOS = [
     ("eimp_gpu_block_size", _sz, [_vp]),
     ("eimp_gpu_run_cref_pbwt", _i32, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("eimp_phase_set_reference", _i32, [_vp, _sz, _sz, _vp, _vp, _vp]),
+    ("eimp_phase_set_haploid_ref", _i32, [_vp, _sz, _vp]),
+    ("eimp_phase_haploid_targets", _i32, [_vp, _sz, _vp]),
+    ("eimp_imp_set_haploid_ref", _i32, [_vp, _sz, _vp]),
+    ("eimp_imp_haploid_targets", _i32, [_vp, _sz, _vp]),
     ("eimp_phase_prep", _i32, [_vp, C.POINTER(EimpPhaseParams), _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("eimp_phase_cref_pbwt", _i32, [_vp, C.POINTER(EimpPhaseParams), _sz, _vp, C.POINTER(_sz), _vp, _vp, _vp, _vp]),
     ("eimp_phase_targets", _i32, [_vp, C.POINTER(EimpPhaseParams), _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

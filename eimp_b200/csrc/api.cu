@@ -68,14 +68,28 @@ struct eimp_ctx {
     // start phases of the targets of the next phasing calls (chunk carry)
     DBuf startph;
     size_t startph_n = 0;
+    // ploidy: haploid samples of the phasing reference (count, device flags)
+    // and haploid targets of the next phasing calls
+    size_t p_nhaploid = 0;
+    DBuf p_haploid;
+    DBuf tgthap;
+    size_t tgthap_n = 0;
     DBuf p_hapmajor, p_sitemajor, p_cm;
     // phasing batch scratch
     DBuf b_gt, b_nerr, b_bh, b_flags, b_monos, b_splits, b_calls, b_cmd, b_nsplits, b_ncalls, b_rowoff, b_cref,
         b_count0, b_pbwt, b_arena, b_out_mat, b_out_pat, b_out_dm, b_out_dp, b_out_tc, b_out_nc;
     size_t b_rows = 0;
 
-    // imputation reference
-    size_t i_Mref = 0, i_nhaps = 0, i_M = 0;
+    // imputation reference; with haploid panel samples the PBWT holds i_K <
+    // i_nhaps haplotypes, i_refmap their panel columns, i_sitetyped_c the
+    // typed rows reduced to them
+    size_t i_Mref = 0, i_nhaps = 0, i_M = 0, i_K = 0;
+    size_t i_refhap_samples = 0, i_refK = 0;
+    DBuf i_refmap, i_sitetyped_c;
+    // haploid targets of the imputation: i_hapmap = row of each existing
+    // target haplotype (i_ntgthaps of them) for i_tgthap_n targets
+    size_t i_tgthap_n = 0, i_ntgthaps = 0;
+    DBuf i_hapmap;
     DBuf i_hapfull, i_sitefull_tmp, i_af, i_typed, i_segm, i_common, i_sinfo, i_sitetyped_tmp, i_compr,
         i_absperm, i_count0;
     // prepared targets
@@ -134,6 +148,7 @@ int check_status(eimp_ctx *ctx) {
         CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(uint32_t), ctx->stream));
         if (st & EIMP_ERR_BEAM_EMPTY) return fail(ctx, EIMP_E_BEAM_EMPTY, "Beam is empty. No paths left.");
         if (st & EIMP_ERR_QREF_TRUNCATED) return fail(ctx, EIMP_E_ARG, "Truncated runlength sequence!");
+        if (st & EIMP_ERR_HAPLOID_HET) return fail(ctx, EIMP_E_ARG, "Found heterozygous genotype in haploid target.");
         char b[160];
         snprintf(b, sizeof b, "device structure capacity exceeded (status 0x%x)", st);
         return fail(ctx, EIMP_E_CAPACITY, b);
@@ -145,8 +160,10 @@ int check_status(eimp_ctx *ctx) {
 // all of the panel, or all but its own two in iterations after the first
 // (PBWTPhaser.cpp:408-476: localK = min(K, localNrefhapsCorr))
 size_t phase_K(const eimp_ctx *ctx, const eimp_phase_params *p) {
-    const size_t nh = ctx->p_nhaps;
-    const size_t corr = ctx->self0 >= 0 && nh >= 2 ? nh - 2 : nh;
+    // PBWTPhaser.cpp:159, 210: one haplotype less per haploid sample of the
+    // panel, and the target's own two in iterations after the first
+    size_t corr = ctx->p_nhaps - ctx->p_nhaploid;
+    if (ctx->self0 >= 0) corr = corr >= 2 ? corr - 2 : 0;
     return (size_t)p->K < corr ? (size_t)p->K : corr;
 }
 
@@ -277,8 +294,13 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
     CK(cudaEventRecord(ctx->main_mark, ctx->stream));
     CK(cudaStreamWaitEvent(ctx->side, ctx->main_mark, 0));
     cudaStream_t st = ctx->side;
-    const size_t wN = eimp_W(nhaps), wMref = eimp_W(Mref), kw = eimp_kw(nhaps);
-    ctx->i_Mref = Mref; ctx->i_nhaps = nhaps; ctx->i_M = M;
+    if (ctx->i_refhap_samples && 2 * ctx->i_refhap_samples != nhaps)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_set_reference: haploid flags were set for a different panel");
+    // the PBWT's haplotypes: all, or without the haploid samples'
+    // placeholder columns (PBWTImputer.cpp:31-34, 67-114)
+    const size_t K = ctx->i_refhap_samples ? ctx->i_refK : nhaps;
+    const size_t wN = eimp_W(nhaps), wMref = eimp_W(Mref), kw = eimp_kw(K);
+    ctx->i_Mref = Mref; ctx->i_nhaps = nhaps; ctx->i_M = M; ctx->i_K = K;
     CK(ctx->i_hapfull.reserve(nhaps * wMref * 8));
     CK(ctx->i_af.reserve(Mref * 4));
     CK(ctx->i_typed.reserve(M * 8));
@@ -286,7 +308,7 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
     CK(ctx->i_common.reserve(Mref));
     CK(ctx->i_sinfo.reserve(Mref * sizeof(int2)));
     CK(ctx->i_compr.reserve(M * kw * 4));
-    CK(ctx->i_absperm.reserve((M + 1) * nhaps * 4));
+    CK(ctx->i_absperm.reserve((M + 1) * K * 4));
     CK(ctx->i_count0.reserve(M * 4));
     CK(cudaMemcpyAsync(ctx->i_af.p, d_af_full, Mref * 4, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(ctx->i_typed.p, d_typed, M * 8, cudaMemcpyDeviceToDevice, st));
@@ -294,9 +316,67 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
     LAUNCH(launch_transpose(d_sitemajor_full, Mref, wN, ctx->i_hapfull.as<uint64_t>(), nhaps, wMref, st));
     LAUNCH(launch_segmap(ctx->i_typed.as<int64_t>(), (int)M, (int)Mref, ctx->i_af.as<float>(), (int)nhaps,
                          ctx->i_segm.as<int32_t>(), ctx->i_common.as<uint8_t>(), ctx->i_sinfo.as<int2>(), st));
-    LAUNCH(launch_refpbwt(d_sitemajor_typed, (int)M, (int)nhaps, (int)wN, ctx->i_compr.as<uint32_t>(),
+    const uint64_t *typed_rows = d_sitemajor_typed;
+    size_t wK = wN;
+    if (ctx->i_refhap_samples) {
+        wK = eimp_W(K);
+        CK(ctx->i_sitetyped_c.reserve(M * wK * 8));
+        LAUNCH(launch_compact_cols(d_sitemajor_typed, (int)M, (int)wN, ctx->i_refmap.as<int32_t>(), (int)K,
+                                   ctx->i_sitetyped_c.as<uint64_t>(), (int)wK, st));
+        typed_rows = ctx->i_sitetyped_c.as<uint64_t>();
+    }
+    LAUNCH(launch_refpbwt(typed_rows, (int)M, (int)K, (int)wK, ctx->i_compr.as<uint32_t>(),
                           ctx->i_absperm.as<int32_t>(), ctx->i_count0.as<int32_t>(), st));
     CK(cudaEventRecord(ctx->ref_ready, st));
+    return 0;
+}
+
+int eimp_imp_set_haploid_ref(eimp_ctx *ctx, size_t nsamples, const uint8_t *haploid) {
+    if (!ctx) return EIMP_E_ARG;
+    if (int r = use_device(ctx)) return r;
+    size_t n = 0;
+    for (size_t i = 0; haploid && i < nsamples; i++) n += haploid[i] != 0;
+    if (!n) {   // all diploid: the PBWT over every column
+        ctx->i_refhap_samples = 0;
+        return 0;
+    }
+    // the existing haplotypes' panel columns, in panel order (VCFData.cpp:2191-2193)
+    std::vector<int32_t> map;
+    map.reserve(2 * nsamples - n);
+    for (size_t i = 0; i < nsamples; i++) {
+        map.push_back((int32_t)(2 * i));
+        if (!haploid[i]) map.push_back((int32_t)(2 * i + 1));
+    }
+    CK(cudaStreamSynchronize(ctx->side));   // the map may be in use by a reference build
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(ctx->i_refmap.reserve(map.size() * 4));
+    CK(cudaMemcpy(ctx->i_refmap.p, map.data(), map.size() * 4, cudaMemcpyHostToDevice));
+    ctx->i_refhap_samples = nsamples;
+    ctx->i_refK = map.size();
+    return 0;
+}
+
+int eimp_imp_haploid_targets(eimp_ctx *ctx, size_t ntgt, const uint8_t *haploid) {
+    if (!ctx) return EIMP_E_ARG;
+    if (int r = use_device(ctx)) return r;
+    size_t n = 0;
+    for (size_t i = 0; haploid && i < ntgt; i++) n += haploid[i] != 0;
+    if (!n) {
+        ctx->i_tgthap_n = 0;
+        return 0;
+    }
+    // the rows of the existing target haplotypes (VCFData.cpp:1340-1348)
+    std::vector<int32_t> map;
+    map.reserve(2 * ntgt - n);
+    for (size_t i = 0; i < ntgt; i++) {
+        map.push_back((int32_t)(2 * i));
+        if (!haploid[i]) map.push_back((int32_t)(2 * i + 1));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));   // the map may be in use by queued imputation work
+    CK(ctx->i_hapmap.reserve(map.size() * 4));
+    CK(cudaMemcpy(ctx->i_hapmap.p, map.data(), map.size() * 4, cudaMemcpyHostToDevice));
+    ctx->i_tgthap_n = ntgt;
+    ctx->i_ntgthaps = map.size();
     return 0;
 }
 
@@ -336,16 +416,22 @@ int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phase
     ctx->i_cap = cap;
     CK(ctx->i_phased.reserve(nh * wM * 8));
     CK(ctx->i_gt.reserve(ntargets * M));
+    if (ctx->i_tgthap_n && ctx->i_tgthap_n != ntargets)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_prepare: haploid targets were set for a different number of targets");
     CK(ctx->i_matches.reserve(nh * cap * sizeof(int4)));
     CK(ctx->i_nmatch.reserve(nh * sizeof(int)));
     if (d_phased != ctx->i_phased.as<uint64_t>())
         CK(cudaMemcpyAsync(ctx->i_phased.p, d_phased, nh * wM * 8, cudaMemcpyDeviceToDevice, ctx->stream));
     if (d_gt != ctx->i_gt.as<uint8_t>())
         CK(cudaMemcpyAsync(ctx->i_gt.p, d_gt, ntargets * M, cudaMemcpyDeviceToDevice, ctx->stream));
-    LAUNCH(launch_smm(ctx->i_compr.as<uint32_t>(), ctx->i_count0.as<int32_t>(), (int)M, (int)ctx->i_nhaps,
-                      ctx->i_phased.as<uint64_t>(), (int)wM, ctx->i_gt.as<uint8_t>(), (int)nh, setmaxerrors,
-                      ctx->i_matches.as<int4>(), (int)cap, ctx->i_nmatch.as<int>(), ctx->status.as<uint32_t>(),
-                      ctx->stream));
+    // haploid targets: only their first haplotype is searched (PBWTImputer.cpp:31, 130)
+    const int32_t *hapmap = ctx->i_tgthap_n ? ctx->i_hapmap.as<int32_t>() : nullptr;
+    const size_t nsearch = ctx->i_tgthap_n ? ctx->i_ntgthaps : nh;
+    if (hapmap) CK(cudaMemsetAsync(ctx->i_nmatch.p, 0, nh * sizeof(int), ctx->stream));
+    LAUNCH(launch_smm(ctx->i_compr.as<uint32_t>(), ctx->i_count0.as<int32_t>(), (int)M, (int)ctx->i_K,
+                      ctx->i_phased.as<uint64_t>(), (int)wM, ctx->i_gt.as<uint8_t>(), (int)nsearch, hapmap,
+                      setmaxerrors, ctx->i_matches.as<int4>(), (int)cap, ctx->i_nmatch.as<int>(),
+                      ctx->status.as<uint32_t>(), ctx->stream));
     ctx->launches++;   // launch_smm launches twice: the small node pool, then the retry pass
     return 0;
 }
@@ -374,10 +460,13 @@ int eimp_imp_bunch_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t
     if (int r = use_device(ctx)) return r;
     const size_t M = ctx->i_M;
     CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
+    const int32_t *hapmap = ctx->i_tgthap_n ? ctx->i_hapmap.as<int32_t>() : nullptr;
+    const size_t nimp = ctx->i_tgthap_n ? ctx->i_ntgthaps : 2 * ctx->i_ntargets;
     LAUNCH(launch_dosage(ctx->i_matches.as<int4>(), (int)ctx->i_cap, ctx->i_nmatch.as<int>(),
-                         ctx->i_absperm.as<int32_t>(), (int)ctx->i_nhaps, ctx->i_hapfull.as<uint64_t>(),
+                         ctx->i_absperm.as<int32_t>(), (int)ctx->i_K,
+                         ctx->i_refhap_samples ? ctx->i_refmap.as<int32_t>() : nullptr, ctx->i_hapfull.as<uint64_t>(),
                          (int)eimp_W(ctx->i_Mref), ctx->i_sinfo.as<int2>(), ctx->i_phased.as<uint64_t>(), (int)eimp_W(M),
-                         ctx->i_gt.as<uint8_t>(), (int)M, (int)(2 * ctx->i_ntargets), (int)mref_begin, (int)nsites,
+                         ctx->i_gt.as<uint8_t>(), (int)M, (int)nimp, hapmap, (int)mref_begin, (int)nsites,
                          ctx->i_imputeCalls, d_dos, (int)ldd, d_bits, (int)ldb_words, ctx->stream));
     return 0;
 }
@@ -390,6 +479,8 @@ int eimp_imp_bunch(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t *bi
     CK(ctx->i_bits.reserve(nh * wb * 8));
     CK(ctx->i_dos.reserve(nh * nsites * 4));
     CK(cudaMemsetAsync(ctx->i_bits.p, 0, nh * wb * 8, ctx->stream));
+    // rows of haploid targets' second haplotype are not imputed: zero
+    if (ctx->i_tgthap_n) CK(cudaMemsetAsync(ctx->i_dos.p, 0, nh * nsites * 4, ctx->stream));
     int r = eimp_imp_bunch_dev(ctx, mref_begin, nsites, ctx->i_bits.as<uint64_t>(), wb, ctx->i_dos.as<float>(), nsites);
     if (r) return r;
     CK(cudaMemcpyAsync(bits, ctx->i_bits.p, nh * wb * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -419,6 +510,8 @@ int eimp_imp_site_stats_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, con
                             float *d_r2, float *d_af, float *d_maf, int32_t *d_ac, int32_t *d_an, uint8_t *d_pass,
                             uint64_t *d_conflicts) {
     if (!ctx || !ctx->i_ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: imputation not prepared");
+    if (ctx->i_tgthap_n)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: haploid targets are not supported by the output statistics");
     if (!opts || !d_bits || !d_dos || !d_ads || !d_gtbits || !d_r2 || !d_af || !d_maf || !d_ac || !d_an || !d_pass ||
         !d_conflicts)
         return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: NULL argument");
@@ -516,6 +609,41 @@ int eimp_phase_start_phases(eimp_ctx *ctx, size_t ntgt, const uint8_t *phases) {
     return 0;
 }
 
+int eimp_phase_set_haploid_ref(eimp_ctx *ctx, size_t nsamples, const uint8_t *haploid) {
+    if (!ctx) return EIMP_E_ARG;
+    if (!ctx->p_M) return fail(ctx, EIMP_E_ARG, "eimp_phase_set_haploid_ref: phasing reference not set");
+    if (haploid && 2 * nsamples != ctx->p_nhaps)
+        return fail(ctx, EIMP_E_ARG, "eimp_phase_set_haploid_ref: one flag per sample of the phasing reference");
+    if (int r = use_device(ctx)) return r;
+    size_t n = 0;
+    for (size_t i = 0; haploid && i < nsamples; i++) n += haploid[i] != 0;
+    if (n) {
+        CK(cudaStreamSynchronize(ctx->stream));   // the flags may be in use by queued phasing work
+        CK(ctx->p_haploid.reserve(nsamples));
+        std::vector<uint8_t> f(haploid, haploid + nsamples);
+        for (auto &x : f) x = x != 0;
+        CK(cudaMemcpy(ctx->p_haploid.p, f.data(), nsamples, cudaMemcpyHostToDevice));
+    }
+    ctx->p_nhaploid = n;
+    return 0;
+}
+
+int eimp_phase_haploid_targets(eimp_ctx *ctx, size_t ntgt, const uint8_t *haploid) {
+    if (!ctx || (ntgt && !haploid)) return fail(ctx, EIMP_E_ARG, "eimp_phase_haploid_targets: NULL argument");
+    if (int r = use_device(ctx)) return r;
+    size_t n = 0;
+    for (size_t i = 0; i < ntgt; i++) n += haploid[i] != 0;
+    if (n) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(ctx->tgthap.reserve(ntgt));
+        std::vector<uint8_t> f(haploid, haploid + ntgt);
+        for (auto &x : f) x = x != 0;
+        CK(cudaMemcpy(ctx->tgthap.p, f.data(), ntgt, cudaMemcpyHostToDevice));
+    }
+    ctx->tgthap_n = n ? ntgt : 0;
+    return 0;
+}
+
 int eimp_qref_index(const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref, int64_t *offsets) {
     if ((!section && nbytes) || (!offsets && Mref)) return EIMP_E_ARG;
     const size_t raw = eimp_W(2 * Nref) * 8;   // hapcapacity: 2*Nref bits in 512-bit units
@@ -599,7 +727,7 @@ int eimp_imp_matches(eimp_ctx *ctx, size_t hap, int32_t *out, size_t cap, size_t
 int eimp_imp_refpbwt(eimp_ctx *ctx, uint32_t *compr, int32_t *absperm) {
     if (!ctx || !ctx->i_Mref) return fail(ctx, EIMP_E_ARG, "eimp_imp_refpbwt: no reference set");
     if (int r = use_device(ctx)) return r;
-    const size_t M = ctx->i_M, K = ctx->i_nhaps;
+    const size_t M = ctx->i_M, K = ctx->i_K;
     CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
     if (compr) CK(cudaMemcpyAsync(compr, ctx->i_compr.p, M * eimp_kw(K) * 4, cudaMemcpyDeviceToHost, ctx->stream));
     if (absperm) CK(cudaMemcpyAsync(absperm, ctx->i_absperm.p, (M + 1) * K * 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -616,6 +744,7 @@ int eimp_phase_set_reference(eimp_ctx *ctx, size_t M, size_t nhaps, const uint64
     if (int r = use_device(ctx)) return r;
     const size_t wM = eimp_W(M), wN = eimp_W(nhaps);
     ctx->p_M = M; ctx->p_nhaps = nhaps;
+    ctx->p_nhaploid = 0;   // a new panel: all samples diploid until eimp_phase_set_haploid_ref
     CK(ctx->p_hapmajor.reserve(nhaps * wM * 8));
     CK(ctx->p_sitemajor.reserve(M * wN * 8));
     CK(ctx->p_cm.reserve(M * 4));
@@ -644,13 +773,18 @@ int run_prep(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint8
     CK(ctx->b_cmd.reserve(ntgt * (M + 1) * 4));
     CK(ctx->b_nsplits.reserve(ntgt * 4));
     CK(ctx->b_ncalls.reserve(ntgt * 4));
+    if (ctx->tgthap_n && ctx->tgthap_n != ntgt)
+        return fail(ctx, EIMP_E_ARG, "haploid targets were set for a different number of targets");
+    const uint8_t *refhap = ctx->p_nhaploid ? ctx->p_haploid.as<uint8_t>() : nullptr;
+    const uint8_t *tgthap = ctx->tgthap_n ? ctx->tgthap.as<uint8_t>() : nullptr;
     LAUNCH(launch_besthaps(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)nh, (int)wM, (int)K,
                            ctx->b_nerr.as<uint32_t>(), ctx->b_bh.as<int32_t>(), ctx->b_flags.as<uint64_t>(), (int)wN,
-                           (int)ctx->self0, st));
+                           (int)ctx->self0, refhap, st));
     LAUNCH(launch_monos_calls(d_gt, (int)ntgt, (int)M, ctx->p_hapmajor.as<uint64_t>(), (int)wM,
                               ctx->b_bh.as<int32_t>(), (int)K, ctx->p_cm.as<float>(), p->cMmaxsplit,
                               ctx->b_monos.as<uint64_t>(), ctx->b_splits.as<int32_t>(), ctx->b_calls.as<int32_t>(),
-                              ctx->b_cmd.as<float>(), ctx->b_nsplits.as<int32_t>(), ctx->b_ncalls.as<int32_t>(), st));
+                              ctx->b_cmd.as<float>(), ctx->b_nsplits.as<int32_t>(), ctx->b_ncalls.as<int32_t>(),
+                              tgthap, st));
     return 0;
 }
 
@@ -814,6 +948,9 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
                        ctx->b_cmd.as<float>(), ctx->b_pbwt.as<uint32_t>(), ctx->b_count0.as<int32_t>(),
                        ctx->b_rowoff.as<int64_t>(), ctx->b_arena.p, ab, d_mats, d_pats, d_dm, d_dp, d_tc, d_nc,
                        ctx->status.as<uint32_t>(), ctx->cur_skip, ctx->stream));
+    if (ctx->tgthap_n)   // haploid targets are not phased (Target.cpp:166-203)
+        LAUNCH(launch_haploid_phase(d_gt, (int)ntgt, (int)M, (int)eimp_W(M), ctx->tgthap.as<uint8_t>(), d_mats,
+                                    d_pats, d_dm, d_dp, d_tc, d_nc, ctx->status.as<uint32_t>(), ctx->stream));
     tmark(ctx, 5);
     ctx->tvalid = ctx->timing;
     return 0;

@@ -59,4 +59,5 @@ enum : uint32_t {
     EIMP_ERR_BEAM_CAPACITY  = 1u << 4,   // beam/happath pool exhausted
     EIMP_ERR_ROWS_OVERFLOW  = 1u << 5,   // condensed reference rows exceed the buffer
     EIMP_ERR_QREF_TRUNCATED = 1u << 6,   // "Truncated runlength sequence!" (utils.h:222-240)
+    EIMP_ERR_HAPLOID_HET    = 1u << 7,   // "Found heterozygous genotype in haploid target." (Target.cpp:196-199)
 };

@@ -198,12 +198,13 @@ template <int NODES, int WARPS, bool RETRY>
 __global__ void __launch_bounds__(WARPS * 32) smm_kernel(
     const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
     const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
-    int setmaxerrors, int4 *__restrict__ matches, int cap, int *__restrict__ nmatch,
-    uint32_t *__restrict__ status) {
+    const int32_t *__restrict__ hapmap, int setmaxerrors, int4 *__restrict__ matches, int cap,
+    int *__restrict__ nmatch, uint32_t *__restrict__ status) {
     extern __shared__ uint8_t smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int hap = blockIdx.x * WARPS + wid;
-    if (hap >= nhaps) return;
+    const int hi = blockIdx.x * WARPS + wid;
+    if (hi >= nhaps) return;
+    const int hap = hapmap ? hapmap[hi] : hi;   // the haplotypes that exist (PBWTImputer.cpp:130)
     if (RETRY && nmatch[hap] != SMM_RETRY) return;
     SmmWarpSmem<NODES> &S = reinterpret_cast<SmmWarpSmem<NODES> *>(smem_raw)[wid];
     const uint8_t *g = gt + (size_t)(hap >> 1) * M;
@@ -388,12 +389,13 @@ template <int NODES, int WARPS, bool RETRY>
 __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
     const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
     const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
-    int setmaxerrors, int4 *__restrict__ matches, int cap, int *__restrict__ nmatch,
-    uint32_t *__restrict__ status) {
+    const int32_t *__restrict__ hapmap, int setmaxerrors, int4 *__restrict__ matches, int cap,
+    int *__restrict__ nmatch, uint32_t *__restrict__ status) {
     extern __shared__ uint8_t smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int hap = blockIdx.x * WARPS + wid;
-    if (hap >= nhaps) return;
+    const int hi = blockIdx.x * WARPS + wid;
+    if (hi >= nhaps) return;
+    const int hap = hapmap ? hapmap[hi] : hi;   // the haplotypes that exist (PBWTImputer.cpp:130)
     if (RETRY && nmatch[hap] != SMM_RETRY) return;
     SmmWarpSmemC<NODES> &S = reinterpret_cast<SmmWarpSmemC<NODES> *>(smem_raw)[wid];
     SmmTree<NODES> *A = &S.A, *B = &S.B;   // the tree and the one being built; swapped when a site merges nothing
@@ -653,20 +655,26 @@ __device__ __forceinline__ void dos_word(const uint64_t *__restrict__ hr, int w0
     hi = (uint32_t)(x >> 32);
 }
 
+// hapmap (null: identity): the target haplotype row of each of the nhaps
+// haplotypes imputed (PBWTImputer.cpp:130, 202); refmap (null: identity):
+// the panel haplotype of each haplotype of the reduced reference PBWT whose
+// prefix arrays absperm holds (TargetImp.cpp:536, haploidsRefMap)
 template <bool WIDE>
 __global__ void __launch_bounds__(256, 4) dosage_kernel(
     const int4 *__restrict__ matches, int cap, const int *__restrict__ nmatch,
-    const int32_t *__restrict__ absperm, int K, const uint64_t *__restrict__ hapmajor_full, int wMref,
-    const int2 *__restrict__ sinfo, const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt,
-    int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *__restrict__ dos, int ldd,
+    const int32_t *__restrict__ absperm, int K, const int32_t *__restrict__ refmap,
+    const uint64_t *__restrict__ hapmajor_full, int wMref, const int2 *__restrict__ sinfo,
+    const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int M, int nhaps,
+    const int32_t *__restrict__ hapmap, int mref_begin, int nsites, int imputeCalls, float *__restrict__ dos, int ldd,
     uint64_t *__restrict__ bits, int ldb) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const long gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int ntiles = (nsites + 63) / 64;
     const int nspans = (ntiles + DOS_SPAN - 1) / DOS_SPAN;
-    const int hap = (int)(gw / nspans);
-    if (hap >= nhaps) return;
+    const int hi = (int)(gw / nspans);
+    if (hi >= nhaps) return;
+    const int hap = hapmap ? hapmap[hi] : hi;
     const int t0 = (int)(gw % nspans) * DOS_SPAN, t1 = min(ntiles, t0 + DOS_SPAN);
     const int end = mref_begin + nsites;
     const uint8_t *g = gt + (size_t)(hap >> 1) * M;
@@ -731,6 +739,7 @@ __global__ void __launch_bounds__(256, 4) dosage_kernel(
             const int my = __shfl_sync(FULL, win.y, mi), mz = __shfl_sync(FULL, win.z, mi);
             const int mo = __shfl_sync(FULL, off, mi);
             sref = lane < total ? absperm[(size_t)my * K + mz + (lane - mo)] : -1;
+            if (refmap && sref >= 0) sref = refmap[sref];
             cwb = wb;
             cncov = ncov;
         }
@@ -771,9 +780,11 @@ __global__ void __launch_bounds__(256, 4) dosage_kernel(
                     const int my = __shfl_sync(FULL, pw.y, mi), mz = __shfl_sync(FULL, pw.z, mi);
                     const int mo = __shfl_sync(FULL, po, mi);
                     uint32_t xlo = 0u, xhi = 0u;
-                    if (s < ptot)
-                        dos_word(hapmajor_full + (size_t)absperm[(size_t)my * K + mz + (s - mo)] * wMref, w0, o0,
-                                 wMref, xlo, xhi);
+                    if (s < ptot) {
+                        int ref = absperm[(size_t)my * K + mz + (s - mo)];
+                        if (refmap) ref = refmap[ref];
+                        dos_word(hapmajor_full + (size_t)ref * wMref, w0, o0, wMref, xlo, xhi);
+                    }
                     const int cend = min(ptot, c + 32);
                     for (int i = 0; i < pn; i++) {
                         const int oi = __shfl_sync(FULL, po, i), hi = __shfl_sync(FULL, ph, i);
@@ -865,48 +876,52 @@ cudaError_t launch_transpose(const uint64_t *src, size_t rows, size_t srcw, uint
 
 template <class Smem, class Kern>
 static cudaError_t smm_launch(Kern kern, int warps, const uint32_t *compr, const int32_t *count0, int M, int K,
-                              const uint64_t *phased, int wM, const uint8_t *gt, int nhaps, int setmaxerrors,
-                              int4 *matches, int cap, int *nmatch, uint32_t *status, cudaStream_t st) {
+                              const uint64_t *phased, int wM, const uint8_t *gt, int nhaps, const int32_t *hapmap,
+                              int setmaxerrors, int4 *matches, int cap, int *nmatch, uint32_t *status,
+                              cudaStream_t st) {
     const size_t sm = sizeof(Smem) * warps;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     const int blocks = (nhaps + warps - 1) / warps;
-    kern<<<blocks, warps * 32, sm, st>>>(compr, count0, M, K, phased, wM, gt, nhaps, setmaxerrors, matches, cap,
-                                        nmatch, status);
+    kern<<<blocks, warps * 32, sm, st>>>(compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches,
+                                        cap, nmatch, status);
     return cudaGetLastError();
 }
 
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
-                       const uint8_t *gt, int nhaps, int setmaxerrors, int4 *matches, int cap, int *nmatch,
-                       uint32_t *status, cudaStream_t st) {
+                       const uint8_t *gt, int nhaps, const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap,
+                       int *nmatch, uint32_t *status, cudaStream_t st) {
     cudaError_t e;
     if (M < 65536) {   // depths fit the compact tree
         e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false>, SMMC_WARPS,
-                                                compr, count0, M, K, phased, wM, gt, nhaps, setmaxerrors, matches,
-                                                cap, nmatch, status, st);
+                                                compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
+                                                matches, cap, nmatch, status, st);
         if (e != cudaSuccess) return e;
         return smm_launch<SmmWarpSmemC<SMM_NODES_RETRY>>(smm_compact_kernel<SMM_NODES_RETRY, 1, true>, 1, compr,
-                                                         count0, M, K, phased, wM, gt, nhaps, setmaxerrors,
+                                                         count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
                                                          matches, cap, nmatch, status, st);
     }
     e = smm_launch<SmmWarpSmem<SMM_NODES>>(smm_kernel<SMM_NODES, SMM_WARPS, false>, SMM_WARPS, compr, count0, M, K,
-                                           phased, wM, gt, nhaps, setmaxerrors, matches, cap, nmatch, status, st);
+                                           phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status,
+                                           st);
     if (e != cudaSuccess) return e;
     return smm_launch<SmmWarpSmem<SMM_NODES_RETRY>>(smm_kernel<SMM_NODES_RETRY, 1, true>, 1, compr, count0, M, K,
-                                                    phased, wM, gt, nhaps, setmaxerrors, matches, cap, nmatch,
+                                                    phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
                                                     status, st);
 }
 
 cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,
-                          const uint64_t *hapmajor_full, int wMref, const int2 *sinfo, const uint64_t *phased, int wM,
-                          const uint8_t *gt, int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *dos,
-                          int ldd, uint64_t *bits, int ldb, cudaStream_t st) {
+                          const int32_t *refmap, const uint64_t *hapmajor_full, int wMref, const int2 *sinfo,
+                          const uint64_t *phased, int wM, const uint8_t *gt, int M, int nhaps, const int32_t *hapmap,
+                          int mref_begin, int nsites, int imputeCalls, float *dos, int ldd, uint64_t *bits, int ldb,
+                          cudaStream_t st) {
     const long ntiles = (nsites + 63) / 64;
     long warps = (long)nhaps * ((ntiles + DOS_SPAN - 1) / DOS_SPAN);
     long blocks = (warps + 7) / 8;
     auto kern = M < 131071 ? dosage_kernel<false> : dosage_kernel<true>;
-    kern<<<(unsigned)blocks, 256, 0, st>>>(matches, cap, nmatch, absperm, K, hapmajor_full, wMref, sinfo, phased, wM,
-                                           gt, M, nhaps, mref_begin, nsites, imputeCalls, dos, ldd, bits, ldb);
+    kern<<<(unsigned)blocks, 256, 0, st>>>(matches, cap, nmatch, absperm, K, refmap, hapmajor_full, wMref, sinfo,
+                                           phased, wM, gt, M, nhaps, hapmap, mref_begin, nsites, imputeCalls, dos, ldd,
+                                           bits, ldb);
     return cudaGetLastError();
 }
 

@@ -23,13 +23,18 @@ cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint
                            int32_t *count0, cudaStream_t st);
 cudaError_t launch_transpose(const uint64_t *src, size_t rows, size_t srcw, uint64_t *dst, size_t cols, size_t dstw,
                              cudaStream_t st);
+// hapmap (null: identity): the target haplotype (row of phased, matches,
+// outputs; its target = row / 2) of each of the nhaps haplotypes searched
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
-                       const uint8_t *gt, int nhaps, int setmaxerrors, int4 *matches, int cap, int *nmatch,
-                       uint32_t *status, cudaStream_t st);
+                       const uint8_t *gt, int nhaps, const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap,
+                       int *nmatch, uint32_t *status, cudaStream_t st);
+// refmap (null: identity): panel haplotype of each PBWT haplotype (the
+// reduced reference without the haploid samples' placeholder columns)
 cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,
-                          const uint64_t *hapmajor_full, int wMref, const int2 *sinfo, const uint64_t *phased, int wM,
-                          const uint8_t *gt, int M, int nhaps, int mref_begin, int nsites, int imputeCalls, float *dos,
-                          int ldd, uint64_t *bits, int ldb, cudaStream_t st);
+                          const int32_t *refmap, const uint64_t *hapmajor_full, int wMref, const int2 *sinfo,
+                          const uint64_t *phased, int wM, const uint8_t *gt, int M, int nhaps, const int32_t *hapmap,
+                          int mref_begin, int nsites, int imputeCalls, float *dos, int ldd, uint64_t *bits, int ldb,
+                          cudaStream_t st);
 // segment map of the typed sites over the reference sites, plus the dosage
 // kernel's per-site pair (segment | typed << 31, shortcut height | af>0.5 << 31)
 cudaError_t launch_segmap(const int64_t *typed, int M, int Mref, const float *af, int nrefhaps_total, int32_t *segm,
@@ -61,13 +66,23 @@ cudaError_t launch_qref_decode(const uint8_t *sec, const int64_t *offs, int Mref
                                size_t ldw, uint32_t *status, cudaStream_t st);
 
 // ---- phasing preparation, condensed reference, PBWT (phase_prep.cu)
+// haploid: per reference sample, 1 = haploid (its second column is never
+// chosen); null: all diploid
 cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int nhaps, int wM, int K,
                             uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, int self0,
-                            cudaStream_t st);
+                            const uint8_t *haploid, cudaStream_t st);
+// tgt_haploid: per target, 1 = haploid (no split sites); null: all diploid
 cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM,
                                const int32_t *besthaps, int K, const float *cm, float cMmaxsplit, uint64_t *monos,
                                int32_t *splits, int32_t *calls, float *cmdiffs, int32_t *nsplits, int32_t *ncalls,
-                               cudaStream_t st);
+                               const uint8_t *tgt_haploid, cudaStream_t st);
+// outputs of the haploid targets of a batch (written after the beam)
+cudaError_t launch_haploid_phase(const uint8_t *gt, int ntgt, int M, int wM, const uint8_t *tgt_haploid,
+                                 uint64_t *mats, uint64_t *pats, float *dmat, float *dpat, float *totalconf,
+                                 int32_t *ncallsites, uint32_t *status, cudaStream_t st);
+// dst row r bit j = src row r bit map[j], j < ncols
+cudaError_t launch_compact_cols(const uint64_t *src, int rows, int srcw, const int32_t *map, int ncols, uint64_t *dst,
+                                int dstw, cudaStream_t st);
 // condensed reference from the haplotype-major reference (nhaps x wM words)
 cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM, int nhaps,
                         const int32_t *besthaps, int K, const int32_t *splits, const int32_t *nsplits,

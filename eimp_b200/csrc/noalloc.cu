@@ -67,7 +67,7 @@ extern "C" int eimp_besthaps_noalloc(void *stream, size_t ntgt, size_t M, const 
     if (int r = nerr_address(&nerr)) return r;
     const size_t Kc = K < nhaps ? K : nhaps;
     cudaError_t e = eimp::launch_besthaps(d_gt, (int)ntgt, (int)M, d_hapmajor, (int)nhaps, (int)eimp_W(M), (int)Kc,
-                                          nerr, d_besthaps, d_flags, (int)eimp_W(nhaps), -1,
+                                          nerr, d_besthaps, d_flags, (int)eimp_W(nhaps), -1, nullptr,
                                           static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? EIMP_OK : EIMP_E_CUDA;
 }

@@ -42,11 +42,14 @@ __device__ __forceinline__ int block_exscan_bit(int pred, int *buf, int *total) 
 }
 
 // ---------------------------------------------------------------------------
+// haploid: per reference sample, 1 = haploid (null: all diploid).  The
+// second column of a haploid sample is never chosen (Target.cpp:800-806,
+// 830-838), nor are the target's own two in iterations after the first.
 __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict__ gt, int M,
                                                       const uint64_t *__restrict__ hapmajor, int nhaps, int wM,
                                                       int K, uint32_t *__restrict__ nerr_scratch,
                                                       int32_t *__restrict__ besthaps, uint64_t *__restrict__ flags,
-                                                      int wN, int self0) {
+                                                      int wN, int self0, const uint8_t *__restrict__ haploid) {
     extern __shared__ uint64_t sm[];
     uint64_t *is0 = sm, *is2 = sm + wM;
     __shared__ int buf[32];
@@ -72,7 +75,29 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
     // phasing iterations after the first: the panel ends with the phased
     // targets and a target ignores its own two haplotypes (Target.cpp:791-796)
     const int ign = self0 >= 0 ? 2 * (self0 + t) : -2;
-    if (ign >= 0 && K >= nhaps - 2) {   // all but the target's own (Target.cpp:798-811)
+    if (haploid) {
+        // with haploid samples: all existing haplotypes when K covers them
+        // (Target.cpp:798-811), else the K best of them (below)
+        int avail = 0;
+        for (int h = tid; h < nhaps; h += nt)
+            avail += !(h == ign || h == ign + 1 || ((h & 1) && haploid[h >> 1]));
+        avail = block_sum_int(avail, buf);
+        if (K >= avail) {
+            int carry = 0;
+            for (int h0 = 0; h0 < nhaps; h0 += nt) {
+                const int h = h0 + tid;
+                const int sel = h < nhaps && !(h == ign || h == ign + 1 || ((h & 1) && haploid[h >> 1]));
+                int tot;
+                const int pos = block_exscan_bit(sel, buf, &tot) + carry;
+                if (sel && pos < K) bh[pos] = h;
+                const unsigned bal = __ballot_sync(0xffffffffu, sel);
+                if ((tid & 31) == 0 && h < nhaps) reinterpret_cast<uint32_t *>(fl)[h >> 5] = bal;
+                carry += tot;
+                __syncthreads();
+            }
+            return;
+        }
+    } else if (ign >= 0 && K >= nhaps - 2) {   // all but the target's own (Target.cpp:798-811)
         for (int h = tid; h < nhaps; h += nt)
             if (h != ign && h != ign + 1) bh[h < ign ? h : h - 2] = h;
         __syncthreads();
@@ -85,7 +110,7 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
         }
         return;
     }
-    if (K >= nhaps) {
+    if (!haploid && K >= nhaps) {
         for (int h = tid; h < nhaps; h += nt) bh[h] = h;
         __syncthreads();
         for (int w = tid; w < wN; w += nt) {
@@ -98,7 +123,8 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
         const uint64_t *row = hapmajor + (size_t)h * wM;
         uint32_t e = 0;
         for (int w = 0; w < wM; w++) e += __popcll((is0[w] & row[w]) | (is2[w] & ~row[w]));
-        nerr[h] = (h == ign || h == ign + 1) ? 0xffffffffu : e;   // never selected
+        const bool excl = h == ign || h == ign + 1 || (haploid && (h & 1) && haploid[h >> 1]);
+        nerr[h] = excl ? 0xffffffffu : e;   // never selected
     }
     __syncthreads();
     // smallest threshold thr with #(nerr <= thr) >= K
@@ -139,13 +165,14 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
 
 cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int nhaps, int wM, int K,
                             uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, int self0,
-                            cudaStream_t st) {
+                            const uint8_t *haploid, cudaStream_t st) {
     size_t sm = (size_t)2 * wM * sizeof(uint64_t);
     if (sm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(besthaps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
-    besthaps_kernel<<<ntgt, 512, sm, st>>>(gt, M, hapmajor, nhaps, wM, K, nerr_scratch, besthaps, flags, wN, self0);
+    besthaps_kernel<<<ntgt, 512, sm, st>>>(gt, M, hapmajor, nhaps, wM, K, nerr_scratch, besthaps, flags, wN, self0,
+                                           haploid);
     return cudaGetLastError();
 }
 
@@ -154,10 +181,15 @@ __global__ void __launch_bounds__(256) monos_calls_kernel(
     const uint8_t *__restrict__ gt, int M, const uint64_t *__restrict__ hapmajor, int wM,
     const int32_t *__restrict__ besthaps, int K, const float *__restrict__ cm, float cMmaxsplit,
     uint64_t *__restrict__ monos, int32_t *__restrict__ splits, int32_t *__restrict__ calls,
-    float *__restrict__ cmdiffs, int32_t *__restrict__ nsplits, int32_t *__restrict__ ncalls) {
+    float *__restrict__ cmdiffs, int32_t *__restrict__ nsplits, int32_t *__restrict__ ncalls,
+    const uint8_t *__restrict__ tgt_haploid) {
     extern __shared__ unsigned long long smo[];
     unsigned long long *sand = smo, *sor = smo + wM;
     const int t = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    if (tgt_haploid && tgt_haploid[t]) {   // not phased (Target.cpp:166-203): no split sites
+        if (tid == 0) { nsplits[t] = 0; ncalls[t] = 0; }
+        return;
+    }
     const int32_t *bh = besthaps + (size_t)t * K;
     for (int w = tid; w < wM; w += nt) { sand[w] = ~0ull; sor[w] = 0ull; }
     __syncthreads();
@@ -217,14 +249,91 @@ __global__ void __launch_bounds__(256) monos_calls_kernel(
 cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM,
                                const int32_t *besthaps, int K, const float *cm, float cMmaxsplit, uint64_t *monos,
                                int32_t *splits, int32_t *calls, float *cmdiffs, int32_t *nsplits, int32_t *ncalls,
-                               cudaStream_t st) {
+                               const uint8_t *tgt_haploid, cudaStream_t st) {
     size_t sm = (size_t)2 * wM * sizeof(uint64_t);
     if (sm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(monos_calls_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
     monos_calls_kernel<<<ntgt, 256, sm, st>>>(gt, M, hapmajor, wM, besthaps, K, cm, cMmaxsplit, monos, splits, calls,
-                                              cmdiffs, nsplits, ncalls);
+                                              cmdiffs, nsplits, ncalls, tgt_haploid);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Haploid targets (Target.cpp:166-203, with missing genotypes left missing,
+// the default without --impMissing): no phasing; the maternal haplotype and
+// dosage are the genotypes (HomAlt -> 1), the paternal outputs are zero, the
+// confidence and the call sites count the non-missing sites.  A heterozygous
+// genotype is an error.  One CTA per target; diploid targets return at once.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) haploid_phase_kernel(
+    const uint8_t *__restrict__ gt, int M, int wM, const uint8_t *__restrict__ tgt_haploid,
+    uint64_t *__restrict__ mats, uint64_t *__restrict__ pats, float *__restrict__ dmat, float *__restrict__ dpat,
+    float *__restrict__ totalconf, int32_t *__restrict__ ncallsites, uint32_t *__restrict__ status) {
+    __shared__ int buf[32];
+    const int t = blockIdx.x, tid = threadIdx.x;
+    if (!tgt_haploid[t]) return;
+    const uint8_t *g = gt + (size_t)t * M;
+    int miss = 0, het = 0;
+    for (int m = tid; m < M; m += blockDim.x) {
+        const uint8_t c = g[m];
+        miss += c == 3;
+        het |= c == 1;
+        dmat[(size_t)t * M + m] = c == 2 ? 1.0f : 0.0f;
+        dpat[(size_t)t * M + m] = 0.0f;
+    }
+    for (int w = tid; w < wM; w += blockDim.x) {
+        uint64_t x = 0;
+        for (int j = 0; j < 64; j++) {
+            const int m = w * 64 + j;
+            if (m < M && g[m] == 2) x |= 1ull << j;
+        }
+        mats[(size_t)t * wM + w] = x;
+        pats[(size_t)t * wM + w] = 0ull;
+    }
+    if (__syncthreads_or(het) && tid == 0) atomicOr(status, (uint32_t)EIMP_ERR_HAPLOID_HET);
+    miss = block_sum_int(miss, buf);
+    if (tid == 0) {
+        totalconf[t] = (float)(M - miss);
+        ncallsites[t] = M - miss;
+    }
+}
+
+cudaError_t launch_haploid_phase(const uint8_t *gt, int ntgt, int M, int wM, const uint8_t *tgt_haploid,
+                                 uint64_t *mats, uint64_t *pats, float *dmat, float *dpat, float *totalconf,
+                                 int32_t *ncallsites, uint32_t *status, cudaStream_t st) {
+    haploid_phase_kernel<<<ntgt, 256, 0, st>>>(gt, M, wM, tgt_haploid, mats, pats, dmat, dpat, totalconf, ncallsites,
+                                               status);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Columns of a bit matrix gathered by a map: dst row r bit j = src row r bit
+// map[j] (j < ncols; the padding words are zero).  The imputation reference
+// without the placeholder column of its haploid samples (PBWTImputer.cpp:67-114).
+// ---------------------------------------------------------------------------
+__global__ void compact_cols_kernel(const uint64_t *__restrict__ src, int rows, int srcw,
+                                    const int32_t *__restrict__ map, int ncols, uint64_t *__restrict__ dst, int dstw) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)rows * dstw) return;
+    const int r = (int)(i / dstw), w = (int)(i % dstw);
+    const uint64_t *s = src + (size_t)r * srcw;
+    uint64_t o = 0;
+    for (int j = 0; j < 64; j++) {
+        const int c = w * 64 + j;
+        if (c < ncols) {
+            const int col = map[c];
+            o |= ((s[col >> 6] >> (col & 63)) & 1ull) << j;
+        }
+    }
+    dst[i] = o;
+}
+
+cudaError_t launch_compact_cols(const uint64_t *src, int rows, int srcw, const int32_t *map, int ncols, uint64_t *dst,
+                                int dstw, cudaStream_t st) {
+    const long n = (long)rows * dstw;
+    compact_cols_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, rows, srcw, map, ncols, dst, dstw);
     return cudaGetLastError();
 }
 

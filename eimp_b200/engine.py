@@ -143,6 +143,7 @@ class Phaser:
         ctx.check(ctx.L.eimp_phase_exclude_self(ctx.h, -1))
         ctx.check(ctx.L.eimp_phase_set_reference(ctx.h, self.M, self.nhaps, ptr(_c(hapmajor, np.uint64)),
                                                  ptr(_c(sitemajor, np.uint64)), ptr(_c(cm, np.float32))))
+        self.nhaploid = 0
 
     def excludeSelf(self, first_sample: int):
         """Phasing iterations after the first: target t is sample
@@ -150,6 +151,27 @@ class Phaser:
         of its best haplotypes (Target.cpp:791-811); -1 turns it off."""
         self.ctx.check(self.ctx.L.eimp_phase_exclude_self(self.ctx.h, int(first_sample)))
         self.self0 = int(first_sample)
+
+    def setHaploidRef(self, haploid):
+        """Haploid samples of this reference (nhaps/2 flags; None: all
+        diploid): their second haplotype is never chosen and K is clamped to
+        the haplotypes that exist (Target.cpp:798-838, PBWTPhaser.cpp:210)."""
+        if haploid is None:
+            self.ctx.check(self.ctx.L.eimp_phase_set_haploid_ref(self.ctx.h, 0, None))
+            self.nhaploid = 0
+            return
+        f = _c(haploid, np.uint8)
+        self.ctx.check(self.ctx.L.eimp_phase_set_haploid_ref(self.ctx.h, f.size, ptr(f)))
+        self.nhaploid = int((f != 0).sum())
+
+    def setHaploidTargets(self, haploid):
+        """Haploid targets of the next phase() calls (one flag per target;
+        None: all diploid): they are not phased (Target.cpp:166-203)."""
+        if haploid is None:
+            self.ctx.check(self.ctx.L.eimp_phase_haploid_targets(self.ctx.h, 0, None))
+            return
+        f = _c(haploid, np.uint8)
+        self.ctx.check(self.ctx.L.eimp_phase_haploid_targets(self.ctx.h, f.size, ptr(f)))
 
     def setStartPhases(self, phases):
         """The maternal phase of every target's first heterozygous site carried
@@ -163,7 +185,8 @@ class Phaser:
         self.ctx.check(self.ctx.L.eimp_phase_start_phases(self.ctx.h, ph.size, ptr(ph)))
 
     def _K(self, params: PhaseParams) -> int:
-        return min(params.K, self.nhaps - 2 if self.self0 >= 0 else self.nhaps)
+        corr = self.nhaps - getattr(self, "nhaploid", 0)
+        return min(params.K, corr - 2 if self.self0 >= 0 else corr)
 
     def prep(self, params: PhaseParams, gt: np.ndarray):
         gt = _c(gt, np.uint8)
@@ -243,18 +266,24 @@ def _transpose_bits(rows: np.ndarray, ncols: int) -> np.ndarray:
 
 
 def phase_iterations(ctx: Context, hapmajor: np.ndarray, sitemajor: np.ndarray, cm: np.ndarray,
-                     params: PhaseParams, gt: np.ndarray, iters: int):
+                     params: PhaseParams, gt: np.ndarray, iters: int, haploid_ref=None, haploid_tgt=None):
     """PBWTPhaser's phasing iterations (PBWTPhaser.cpp:406-476, --phaseIters):
     iteration 1 phases the targets against the reference; every further
     iteration phases them again against the reference followed by the phased
     targets of the previous iteration, each target leaving its own
     haplotypes out; reverse phasing and the call confidences only in the last
-    iteration.  Returns the last iteration's (mats, pats, dm, dp, tc, nc)."""
+    iteration.  Haploid reference samples and targets (flags or None) stay
+    haploid in the grown panel (VCFData.cpp:1926-1931).  Returns the last
+    iteration's (mats, pats, dm, dp, tc, nc)."""
     import dataclasses
     gt = _c(gt, np.uint8)
     n, M = gt.shape
     nh = hapmajor.shape[0]
+    hr = np.zeros(nh // 2, np.uint8) if haploid_ref is None else _c(haploid_ref, np.uint8)
+    ht = np.zeros(n, np.uint8) if haploid_tgt is None else _c(haploid_tgt, np.uint8)
     ph = Phaser(ctx, hapmajor, sitemajor, cm)
+    ph.setHaploidRef(hr if hr.any() else None)
+    ph.setHaploidTargets(ht if ht.any() else None)
     out = None
     for it in range(1, iters + 1):
         p = dataclasses.replace(params, doRevPhasing=params.doRevPhasing and it == iters)
@@ -264,9 +293,13 @@ def phase_iterations(ctx: Context, hapmajor: np.ndarray, sitemajor: np.ndarray, 
             tgt[0::2], tgt[1::2] = mats, pats
             aug = np.concatenate([_c(hapmajor, np.uint64), tgt])
             ph = Phaser(ctx, aug, _transpose_bits(aug, M), cm)
+            hf = np.concatenate([hr, ht])
+            ph.setHaploidRef(hf if hf.any() else None)
+            ph.setHaploidTargets(ht if ht.any() else None)
             ph.excludeSelf(nh // 2)
         out = ph.phase(p, gt)
     ph.excludeSelf(-1)
+    ph.setHaploidTargets(None)
     return out
 
 
@@ -279,13 +312,18 @@ class PBWTImputer:
     """
 
     def __init__(self, ctx: Context, sitemajor_full: np.ndarray, af_full: np.ndarray, typed: np.ndarray,
-                 sitemajor_typed: np.ndarray, nhaps: int, setmaxerrors: int = 0, imputeCalls: bool = False):
+                 sitemajor_typed: np.ndarray, nhaps: int, setmaxerrors: int = 0, imputeCalls: bool = False,
+                 haploid_ref=None):
         self.ctx = ctx
         self.Mref = sitemajor_full.shape[0]
         self.M = len(typed)
         self.nhaps = nhaps
         self.setmaxerrors = setmaxerrors
         self.imputeCalls = imputeCalls
+        # haploid panel samples: the PBWT without their placeholder columns
+        hr = None if haploid_ref is None else _c(haploid_ref, np.uint8)
+        self.K = nhaps - (0 if hr is None else int((hr != 0).sum()))
+        ctx.check(ctx.L.eimp_imp_set_haploid_ref(ctx.h, 0 if hr is None else hr.size, None if hr is None else ptr(hr)))
         ctx.check(ctx.L.eimp_imp_set_reference(ctx.h, self.Mref, nhaps, ptr(_c(sitemajor_full, np.uint64)),
                                                ptr(_c(af_full, np.float32)), self.M, ptr(_c(typed, np.int64)),
                                                ptr(_c(sitemajor_typed, np.uint64))))
@@ -293,11 +331,16 @@ class PBWTImputer:
         self.block_pos = {}
 
     def prepareImputation(self, phasedTargets: np.ndarray, gt: np.ndarray, num_sites_per_block=None,
-                          match_cap: int = 0):
+                          match_cap: int = 0, haploid_targets=None):
+        """haploid_targets: one flag per target (None: all diploid); only the
+        first haplotype of a haploid target is imputed (PBWTImputer.cpp:130)."""
         phased = _c(phasedTargets, np.uint64)
         gt = _c(gt, np.uint8)
         self.ntargets = gt.shape[0]
         assert phased.shape == (2 * self.ntargets, W(self.M))
+        ht = None if haploid_targets is None else _c(haploid_targets, np.uint8)
+        self.ctx.check(self.ctx.L.eimp_imp_haploid_targets(self.ctx.h, 0 if ht is None else ht.size,
+                                                           None if ht is None else ptr(ht)))
         self.ctx.check(self.ctx.L.eimp_imp_prepare(self.ctx.h, self.ntargets, ptr(phased), ptr(gt),
                                                    self.setmaxerrors, int(self.imputeCalls), match_cap))
         self.block_pos = {}
@@ -371,9 +414,9 @@ class PBWTImputer:
         return out
 
     def refpbwt(self):
-        kw = 2 * ((self.nhaps + 31) // 32)
+        kw = 2 * ((self.K + 31) // 32)
         compr = np.zeros((self.M, kw), np.uint32)
-        ap = np.zeros((self.M + 1, self.nhaps), np.int32)
+        ap = np.zeros((self.M + 1, self.K), np.int32)
         self.ctx.check(self.ctx.L.eimp_imp_refpbwt(self.ctx.h, ptr(compr), ptr(ap)))
         return compr, ap
 

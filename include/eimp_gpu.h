@@ -178,6 +178,30 @@ int eimp_phase_exclude_self(eimp_ctx *ctx, int64_t first_sample);
  * ntgt = 0 goes back to Ref for all (the first chunk). */
 int eimp_phase_start_phases(eimp_ctx *ctx, size_t ntgt, const uint8_t *phases);
 
+/* Haploid samples of the phasing reference (chrX males and other haploid
+ * regions; VCFData::getHaploidsRef, read with the Qref, VCFData.cpp:2157-2209):
+ * nsamples = Nrefhaps/2 flags, 1 = haploid.  A haploid sample's second
+ * haplotype column is a placeholder (a homozygous copy) that no target
+ * chooses (Target.cpp:800-806, 830-838), and K is clamped to the haplotypes
+ * that exist: Nrefhaps less one per haploid sample, less the target's own two
+ * in iterations after the first (PBWTPhaser.cpp:159, 210).  In iterations
+ * after the first the flags cover the reference followed by the phased
+ * targets, haploid targets flagged as the reference does (VCFData.cpp:1926-1931).
+ * Call after eimp_phase_set_reference, which resets all samples to diploid;
+ * haploid = NULL (or no flag set) means all diploid. */
+int eimp_phase_set_haploid_ref(eimp_ctx *ctx, size_t nsamples, const uint8_t *haploid);
+
+/* Haploid targets of the next phasing calls (VCFData::getHaploidsTgt): ntgt
+ * flags, 1 = haploid; the calls must then phase exactly ntgt targets.  A
+ * haploid target is not phased (Target.cpp:166-203): its genotypes (0, 2, 3 =
+ * missing) become the maternal haplotype and dosage, missing sites stay Ref
+ * with dosage 0 (the reference's default without --impMissing), the
+ * confidence and the number of call sites are its non-missing sites, and its
+ * paternal haplotype and dosages are zero.  A heterozygous genotype in a
+ * haploid target returns EIMP_E_ARG ("Found heterozygous genotype in haploid
+ * target.").  ntgt = 0 goes back to all diploid. */
+int eimp_phase_haploid_targets(eimp_ctx *ctx, size_t ntgt, const uint8_t *haploid);
+
 /* Capacity mode for phasing (no counterpart in the reference): reserves the
  * batch buffers for up to max_targets targets and max_rows condensed rows
  * (sum over the targets of 2*S_t+1).  Afterwards the row offsets are computed
@@ -211,6 +235,23 @@ int eimp_imp_set_reference(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint6
  * VCFData::tgtmiss).  match_cap = matches stored per haplotype (0: M/4+64). */
 int eimp_imp_prepare(eimp_ctx *ctx, size_t ntargets, const uint64_t *phased, const uint8_t *gt,
                      int setmaxerrors, int imputeCalls, size_t match_cap);
+
+/* Haploid samples of the imputation reference (PBWTImputer.cpp:31-34,
+ * 67-114): nsamples = nhaps/2 flags, 1 = haploid.  The reference PBWT and
+ * its prefix arrays then hold K = nhaps - (haploid samples) haplotypes, the
+ * first column of every sample and the second of the diploid ones, and the
+ * dosages read the panel through that column map (VCFData::getHaploidsRefMap,
+ * TargetImp.cpp:536).  Applies to the next eimp_imp_set_reference[_dev],
+ * which must then have nhaps = 2 * nsamples; NULL = all diploid. */
+int eimp_imp_set_haploid_ref(eimp_ctx *ctx, size_t nsamples, const uint8_t *haploid);
+
+/* Haploid targets of the next eimp_imp_prepare[_dev] (ntgt must equal its
+ * ntargets): only the first haplotype of a haploid target is searched and
+ * imputed (PBWTImputer.cpp:31, 130, 202); its second row of matches is empty
+ * and its second row of dosages and alleles is zero in eimp_imp_bunch and
+ * left unwritten by eimp_imp_bunch_dev.  The output statistics do not support
+ * haploid targets (EIMP_E_ARG).  ntgt = 0 or NULL: all diploid. */
+int eimp_imp_haploid_targets(eimp_ctx *ctx, size_t ntgt, const uint8_t *haploid);
 
 /* PBWTImputer::imputeBunch (PBWTImputer.cpp:187-204) for the window of nsites
  * reference sites starting at mref_begin: bits 2*ntargets x W(nsites) words,

@@ -61,9 +61,14 @@ size_t capBytes(size_t nbits) { return roundToMultiple(nbits, UNITWORDS * sizeof
 struct Handle {
     VCFData vd;
     bool lastIter = true;
-    // NrefhapsCorrected of PBWTPhaser (PBWTPhaser.cpp:408-476): all
-    // haplotypes, or all but the target's own two in iterations after the first
-    size_t ncorr() const { return vd.NrefhapsOrig ? vd.Nrefhaps - 2 : vd.Nrefhaps; }
+    // NrefhapsCorrected of PBWTPhaser (PBWTPhaser.cpp:408-476, 630, 681): all
+    // haplotypes less one per haploid sample of the panel, and less the
+    // target's own two in iterations after the first
+    size_t ncorr() const {
+        size_t n = vd.Nrefhaps - vd.nHaploidsRef;
+        if (vd.NrefhapsOrig) n -= vd.nHaploidsTgt + 2;
+        return n;
+    }
     std::vector<uint64_t*> bufs;
     ~Handle() { for (auto p : bufs) free(p); }
     uint64_t *alloc(size_t bytes) {
@@ -156,6 +161,40 @@ void *refo_create(size_t nhaps, size_t M, size_t Mref,
 }
 
 void refo_destroy(void *hp) { delete (Handle*)hp; }
+
+/* Ploidy of the panel's samples (nhaps/2 bytes) and of the targets (ntarget
+ * bytes), 1 = haploid; NULL = all diploid.  Sets what VCFData holds after
+ * reading a Qref and the targets (VCFData.cpp:1900-1935, 2157-2209, 1340-1348):
+ * haploidsRef/haploidsTgt, their counts, and the index maps of the haplotypes
+ * that exist (2i, and 2i+1 for a diploid sample).  In phasing iterations
+ * after the first the panel's trailing samples are the targets: their flags
+ * come in ref (as the reference sets haploidsRef[Nref+i]) and count as target
+ * haploids, not reference ones. */
+void refo_set_haploids(void *hp, const uint8_t *ref, const uint8_t *tgt) {
+    Handle *h = (Handle*)hp;
+    VCFData &v = h->vd;
+    const size_t ns = v.Nrefhaps / 2, nref = (v.NrefhapsOrig ? v.NrefhapsOrig : v.Nrefhaps) / 2;
+    v.haploidsRef.assign(ns, false);
+    v.haploidsRefMap.clear();
+    v.nHaploidsRef = 0;
+    for (size_t i = 0; i < ns; i++) {
+        const bool hap = ref && ref[i];
+        v.haploidsRef[i] = hap;
+        if (hap && i < nref) v.nHaploidsRef++;
+        v.haploidsRefMap.push_back(2 * i);
+        if (!hap) v.haploidsRefMap.push_back(2 * i + 1);
+    }
+    v.haploidsTgt.assign(v.Ntarget, false);
+    v.haploidsTgtMap.clear();
+    v.nHaploidsTgt = 0;
+    for (size_t i = 0; i < v.Ntarget; i++) {
+        const bool hap = tgt && tgt[i];
+        v.haploidsTgt[i] = hap;
+        if (hap) v.nHaploidsTgt++;
+        v.haploidsTgtMap.push_back(2 * i);
+        if (!hap) v.haploidsTgtMap.push_back(2 * i + 1);
+    }
+}
 
 /* Start phases of the targets (VCFData::chunkStartPhase, carried over from
  * the previous chunk, VCFData.cpp:2802-2816): ntarget bytes, 0 = Ref. */
@@ -250,6 +289,9 @@ int refo_phase(void *hp, size_t t, size_t K, float expectIBDcM, float hist, floa
         *ncallsites = tg.getNCallSites();
     }
     memcpy(mat, md, cap); memcpy(pat, pd, cap);
+    // a haploid target (Target.cpp:166-203) fills only the maternal dosages
+    dm.resize(v.M, 0.0f);
+    dp.resize(v.M, 0.0f);
     memcpy(dos_mat, dm.data(), v.M * sizeof(float));
     memcpy(dos_pat, dp.data(), v.M * sizeof(float));
     free(md); free(pd);
@@ -321,6 +363,13 @@ void refo_imp_retarget(void *ip, const uint64_t *phased, unsigned nthreads) {
     }
 }
 
+/* haplotypes of the imputation PBWT (PBWTImputer.cpp:31-34: the panel's
+ * haplotypes less one per haploid sample) and target haplotypes imputed */
+size_t refo_imp_K(void *ip) { return ((ImpHandle*)ip)->imp->pbwt->K; }
+size_t refo_imp_ntargethaps(void *ip) { return ((ImpHandle*)ip)->imp->nTargetHap; }
+
+/* matches of the imputer's target haplotype `hap` (0..ntargethaps-1: the
+ * haplotypes that exist, in the order of VCFData::getHaploidsTgtMap) */
 size_t refo_imp_nmatches(void *ip, size_t hap) {
     ImpHandle *ih = (ImpHandle*)ip;
     return ih->imp->targets[hap].sm_matches.size();

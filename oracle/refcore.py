@@ -41,6 +41,11 @@ def lib():
                                   _f32p, _f32p, _f32p, C.c_size_t, _u8p]
         L.refo_destroy.argtypes = [C.c_void_p]
         L.refo_set_iteration.argtypes = [C.c_void_p, C.c_size_t, C.c_int]
+        L.refo_set_haploids.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.refo_imp_K.restype = C.c_size_t
+        L.refo_imp_K.argtypes = [C.c_void_p]
+        L.refo_imp_ntargethaps.restype = C.c_size_t
+        L.refo_imp_ntargethaps.argtypes = [C.c_void_p]
         L.refo_set_start_phases.argtypes = [C.c_void_p, _u8p]
         L.refo_set_params.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int]
         L.refo_prep.restype = C.c_long
@@ -171,8 +176,21 @@ class RefCore:
 
     @property
     def ncorr(self) -> int:
-        """Haplotypes a target chooses its K best from (PBWTPhaser.cpp:408-476)."""
-        return self.nhaps - 2 if getattr(self, "nhaps_orig", 0) else self.nhaps
+        """Haplotypes a target chooses its K best from (PBWTPhaser.cpp:408-476):
+        the panel less one per haploid sample, less the target's own two in
+        iterations after the first."""
+        n = self.nhaps - getattr(self, "nhaploid_ref", 0)
+        return n - 2 if getattr(self, "nhaps_orig", 0) else n
+
+    def set_haploids(self, ref=None, tgt=None):
+        """Ploidy of the panel's samples (nhaps/2 flags) and of the targets
+        (ntarget flags), 1 = haploid; None = all diploid.  Call after
+        set_iteration in iterations after the first."""
+        self._hr = None if ref is None else np.ascontiguousarray(ref, np.uint8)
+        self._ht = None if tgt is None else np.ascontiguousarray(tgt, np.uint8)
+        lib().refo_set_haploids(self.h, None if self._hr is None else self._hr.ctypes.data,
+                                None if self._ht is None else self._ht.ctypes.data)
+        self.nhaploid_ref = 0 if self._hr is None else int(self._hr.sum())
 
     def set_start_phases(self, phases):
         """VCFData::chunkStartPhase of every target (0 = Ref)."""
@@ -283,8 +301,17 @@ class RefImputer:
             lib().refo_imp_matches(self.h, hap, out)
         return out
 
+    @property
+    def K(self) -> int:
+        """haplotypes of the imputation PBWT (one per haploid panel sample)"""
+        return int(lib().refo_imp_K(self.h))
+
+    @property
+    def ntargethaps(self) -> int:
+        return int(lib().refo_imp_ntargethaps(self.h))
+
     def refpbwt(self):
-        M, K = self.core.M, self.core.nhaps
+        M, K = self.core.M, self.K
         kw = 2 * ((K + 31) // 32)
         compr = np.zeros((M, kw), np.uint32)
         absperm = np.zeros((M + 1, K), np.int32)

@@ -13,10 +13,22 @@ inputs and outputs as compressed .npz files:
                       for K=64 also the imputation: reference PBWT + prefix
                       arrays, set-maximal matches and imputed bits/dosages.
 
+  golden_haploid.npz -- the same panel with every fourth reference sample
+                      haploid (stored as a homozygous diploid pair, its
+                      second column a copy of the first) and 8 targets of
+                      which 3 are haploid (genotypes 0/2/missing): for K in
+                      {64, 200} (200 takes every existing haplotype, 175)
+                      the best haplotypes, phased haplotypes, dosages and
+                      confidences, and for K=64 the imputation over the
+                      reduced reference (PBWTImputer.cpp:31-34, 67-114):
+                      its PBWT and prefix arrays, the matches of the 13
+                      target haplotypes and the imputed bits/dosages.
+
 K=50 is not a multiple of 32, K=200 equals the number of haplotypes (the
 reference's copy-all path, Target.cpp:969-974).  Usage:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # both fixtures
+    python tests/golden/make_golden.py haploid    # golden_haploid.npz only
 """
 from __future__ import annotations
 
@@ -119,5 +131,77 @@ def main():
     print(path, os.path.getsize(path), "bytes")
 
 
+def haploid_case():
+    """The tiny panel with every fourth reference sample haploid and targets
+    1, 3 and 6 haploid (the inputs of golden_haploid.npz)."""
+    from eimp_b200.bits import pack_rows, transpose_bits
+    panel, groups = synth.generate("tiny")
+    tg = make_targets(groups)
+    nh, Mref = panel.nhaps, panel.nsites
+    ref_hap = (np.arange(nh // 2) % 4 == 0).astype(np.uint8)
+    dense = unpack_rows(panel.hapmajor, Mref)
+    for s in np.flatnonzero(ref_hap):
+        dense[2 * s + 1] = dense[2 * s]
+    hm = pack_rows(dense, W(Mref))
+    sm = transpose_bits(hm, nh, Mref)
+    af = (dense.sum(axis=0) / nh).astype(np.float32)
+    panel = synth.Panel(nh, Mref, panel.pos, panel.cm, af, hm, sm)
+    tgt_hap = np.zeros(tg.gt.shape[0], np.uint8)
+    tgt_hap[[1, 3, 6]] = 1
+    gt = tg.gt.copy()
+    truth = tg.truth.copy()
+    for t in np.flatnonzero(tgt_hap):
+        miss = gt[t] == 3
+        gt[t] = 2 * truth[2 * t]
+        gt[t][miss] = 3
+        truth[2 * t + 1] = truth[2 * t]
+    return panel, synth.Targets(tg.typed, gt, truth), ref_hap, tgt_hap
+
+
+def main_haploid():
+    panel, tg, ref_hap, tgt_hap = haploid_case()
+    rc = RefCore(panel, tg)
+    rc.set_haploids(ref_hap, tgt_hap)
+    nt = tg.gt.shape[0]
+    out = dict(nhaps=panel.nhaps, Mref=panel.nsites, M=len(tg.typed), typed=tg.typed, gt=tg.gt,
+               sitemajor_full=panel.sitemajor, af_full=panel.af, hapmajor_typed=rc.hapmajor_typed,
+               sitemajor_typed=rc.sitemajor_typed, cm_typed=rc.cm_typed, ref_haploid=ref_hap,
+               tgt_haploid=tgt_hap)
+    for K in (64, 200):
+        rc.set_params(PhaseParams(K=K, beamwidth=16))
+        pre = f"K{K}_"
+        dip = np.flatnonzero(tgt_hap == 0)
+        out[pre + "besthaps"] = np.stack([rc.prep(int(t))["besthaps"] for t in dip])
+        res = [rc.phase(t) for t in range(nt)]
+        out[pre + "mat"] = np.stack([r[0] for r in res])
+        out[pre + "pat"] = np.stack([r[1] for r in res])
+        out[pre + "dos_mat"] = np.stack([r[2] for r in res])
+        out[pre + "dos_pat"] = np.stack([r[3] for r in res])
+        out[pre + "totalconf"] = np.array([r[4] for r in res], np.float32)
+        out[pre + "ncallsites"] = np.array([r[5] for r in res], np.int64)
+        if K == 64:
+            ph = np.zeros((2 * nt, W(rc.M)), np.uint64)
+            ph[0::2] = out[pre + "mat"]
+            ph[1::2] = out[pre + "pat"]
+            imp = rc.imputer(ph, 1)
+            compr, absperm = imp.refpbwt()
+            out["imp_phased"] = ph
+            out["imp_K"] = imp.K
+            out["imp_compr"] = compr
+            out["imp_absperm"] = absperm
+            ms = [imp.matches(h) for h in range(imp.ntargethaps)]
+            out["imp_nmatches"] = np.array([len(m) for m in ms], np.int64)
+            out["imp_matches"] = np.concatenate(ms) if ms else np.zeros((0, 4), np.int64)
+            bits, dos = imp.bunch(rc.Mref, 1)
+            out["imp_bits"] = bits
+            out["imp_dos"] = dos
+            imp.close()
+    path = os.path.join(HERE, "golden_haploid.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] != ["haploid"]:
+        main()
+    main_haploid()

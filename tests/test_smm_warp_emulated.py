@@ -37,7 +37,7 @@ def emu_exe(tmp_path_factory):
     src = open(os.path.join(CSRC, "imp_kernels.cu")).read()
     # the match section only: the other kernels use block-wide barriers
     i = src.index("struct SNode {")
-    j = src.index("// dosages.")
+    j = src.index("// dosages (TargetImp::imputeBunch")
     j = src.rindex("// ----", 0, j)
     body = src[i:j]
     decl = "extern __shared__ uint8_t smem_raw[];"

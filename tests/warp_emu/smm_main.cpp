@@ -82,8 +82,8 @@ int main(int argc, char **argv) {
                                               : eimp::smm_compact_kernel<SMM_NODES, 1, false>)
                                       : (pass ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true>
                                               : eimp::smm_kernel<SMM_NODES, 1, false>);
-                    kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, sme, matches.data(),
-                         cap, nmatch.data(), &status);
+                    kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
+                         matches.data(), cap, nmatch.data(), &status);
                 });
             for (auto &x : lanes) x.join();
             free(smem);
