@@ -80,7 +80,9 @@ cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_
 cudaError_t launch_haploid_phase(const uint8_t *gt, int ntgt, int M, int wM, const uint8_t *tgt_haploid,
                                  uint64_t *mats, uint64_t *pats, float *dmat, float *dpat, float *totalconf,
                                  int32_t *ncallsites, uint32_t *status, cudaStream_t st);
-// dst row r bit j = src row r bit map[j], j < ncols
+// dst row r bit j = src row r bit map[j], j < ncols; a second haplotype (odd
+// map value) at a word's first column is zero, as the reference's
+// setPairWithPreInit leaves it
 cudaError_t launch_compact_cols(const uint64_t *src, int rows, int srcw, const int32_t *map, int ncols, uint64_t *dst,
                                 int dstw, cudaStream_t st);
 // condensed reference from the haplotype-major reference (nhaps x wM words)

@@ -312,6 +312,15 @@ cudaError_t launch_haploid_phase(const uint8_t *gt, int ntgt, int M, int wM, con
 // Columns of a bit matrix gathered by a map: dst row r bit j = src row r bit
 // map[j] (j < ncols; the padding words are zero).  The imputation reference
 // without the placeholder column of its haploid samples (PBWTImputer.cpp:67-114).
+//
+// The reference writes a diploid sample's two columns with one call that
+// sets bits pos and pos+1 inside the word of pos (BooleanVector::
+// setPairWithPreInit, Datatypes.h:190-197, meant for even pos).  After a
+// haploid sample pos can be odd; at pos % 64 == 63 the second bit (2 << 63)
+// falls off the word, so that sample's second haplotype reads as all zeros in
+// the PBWT.  The kernel reproduces it: a second haplotype (odd panel column)
+// whose compacted column starts a word is left zero.  Only the PBWT sees it;
+// the dosages read the panel itself (TargetImp.cpp:536).
 // ---------------------------------------------------------------------------
 __global__ void compact_cols_kernel(const uint64_t *__restrict__ src, int rows, int srcw,
                                     const int32_t *__restrict__ map, int ncols, uint64_t *__restrict__ dst, int dstw) {
@@ -324,6 +333,7 @@ __global__ void compact_cols_kernel(const uint64_t *__restrict__ src, int rows, 
         const int c = w * 64 + j;
         if (c < ncols) {
             const int col = map[c];
+            if (j == 0 && (col & 1)) continue;   // lost off the previous word (see above)
             o |= ((s[col >> 6] >> (col & 63)) & 1ull) << j;
         }
     }
