@@ -13,7 +13,7 @@ from eimp_b200.bits import W
 pytestmark = pytest.mark.gpu
 
 
-def reference_iterations(hm, sm, cm, gt, af_common, K, beam, iters):
+def reference_iterations(hm, sm, cm, gt, af_common, K, beam, iters, ref_hap=None, tgt_hap=None):
     from eimp_b200.engine import _transpose_bits
     from oracle import refcore
     n, M = gt.shape
@@ -30,6 +30,10 @@ def reference_iterations(hm, sm, cm, gt, af_common, K, beam, iters):
             panel = (aug, _transpose_bits(aug, M))
         rc = refcore.RefCore.typed_only(panel[0], panel[1], cm, gt, af_common)
         rc.set_iteration(nh if it > 1 else 0, last)
+        if ref_hap is not None:
+            # iterations after the first: the phased targets join the panel
+            # with their ploidy (VCFData.cpp:1926-1931)
+            rc.set_haploids(ref_hap if it == 1 else np.concatenate([ref_hap, tgt_hap]), tgt_hap)
         rc.set_params(refcore.PhaseParams(K=K, beamwidth=beam, doRevPhasing=last))
         res = [rc.phase(t) for t in range(n)]
         rc.close()
@@ -77,3 +81,19 @@ def test_best_haps_leave_own_sample_out(ctx):
         assert not own & set(got[t].tolist())
         np.testing.assert_array_equal(got[t], rc.prep(t)["besthaps"])
     rc.close()
+
+
+@pytest.mark.parametrize("K", [64, 400])
+def test_phasing_iterations_haploid_vs_reference(ctx, K):
+    """Two iterations over a panel with haploid samples and haploid targets
+    (golden_haploid.npz): the grown panel carries the targets' ploidy, K is
+    clamped to the haplotypes that exist (PBWTPhaser.cpp:159)."""
+    from eimp_b200.engine import PhaseParams, phase_iterations
+    g = np.load(golden_path("golden_haploid.npz"))
+    hm, sm, cm, gt = g["hapmajor_typed"], g["sitemajor_typed"], g["cm_typed"], g["gt"]
+    af_common = g["af_full"][g["typed"]]
+    rh, th = g["ref_haploid"], g["tgt_haploid"]
+    got = phase_iterations(ctx, hm, sm, cm, PhaseParams(K=K, beamwidth=16), gt, 2, haploid_ref=rh, haploid_tgt=th)
+    want = reference_iterations(hm, sm, cm, gt, af_common, K, 16, 2, rh, th)
+    for name, a, b in zip(("mats", "pats", "dm", "dp", "totalconf", "ncallsites"), got, want):
+        np.testing.assert_array_equal(np.asarray(a), np.asarray(b).astype(np.asarray(a).dtype), err_msg=name)
