@@ -53,9 +53,10 @@ CPU_SAMPLE = {"cfg2": 200, "cfg3": 32}
 # haplotypes of each CPU sample whose dosages are also checked against the
 # FP64 dosage oracle (score/sum in double, not rounded to float)
 PARITY_FP64_HAPS = 32
-# device memory per density group for the condensed references, PBWTs and
-# beam arenas of one phasing batch
-PHASE_BATCH_BYTES = 24e9
+# device memory per density group for the condensed references and PBWTs of
+# one phasing batch (the beam arenas belong to the resident warps, not to
+# the targets)
+PHASE_BATCH_BYTES = 36e9
 
 
 def parse():
@@ -437,9 +438,10 @@ def profile_stages(groups, cfg, flush, stream_main):
 def auto_batch(M, K, nt):
     """Targets per phasing batch within PHASE_BATCH_BYTES: about 0.25*M
     condensed rows per target (S ~ 0.12 M split sites at ~11 % heterozygous
-    sites) of W(K) words plus two PBWT directions, and a beam arena."""
+    sites) of W(K) words plus two PBWT directions, and the per-target prep
+    vectors."""
     kw = 2 * ((K + 31) // 32)
-    per = 0.25 * M * (W(K) * 8 + 2 * kw * 4 + 8) + 3.0e6
+    per = 0.25 * M * (W(K) * 8 + 2 * kw * 4 + 8) + 20.0 * M
     return int(max(64, min(nt, PHASE_BATCH_BYTES // per)))
 
 

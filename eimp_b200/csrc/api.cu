@@ -77,7 +77,8 @@ struct eimp_ctx {
     DBuf p_hapmajor, p_sitemajor, p_cm;
     // phasing batch scratch
     DBuf b_gt, b_nerr, b_bh, b_flags, b_monos, b_splits, b_calls, b_cmd, b_nsplits, b_ncalls, b_rowoff, b_cref,
-        b_count0, b_pbwt, b_arena, b_out_mat, b_out_pat, b_out_dm, b_out_dp, b_out_tc, b_out_nc;
+        b_count0, b_pbwt, b_arena, b_out_mat, b_out_pat, b_out_dm, b_out_dp, b_out_tc, b_out_nc, b_order,
+        b_workq;
     size_t b_rows = 0;
 
     // imputation reference; with haploid panel samples the PBWT holds i_K <
@@ -941,13 +942,18 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
     std::vector<int64_t> ro;
     if (int r = run_cref_pbwt(ctx, K, ntgt, d_gt, ro)) return r;
     const size_t ab = beam_arena_bytes(bp, (int)M);
-    CK(ctx->b_arena.reserve(ntgt * ab));
+    const int slots = beam_slots(bp, (int)M, (int)ntgt);
+    if (slots < 1) return fail(ctx, EIMP_E_CUDA, "beam launch shape: occupancy query failed");
+    CK(ctx->b_arena.reserve((size_t)slots * ab));
+    CK(ctx->b_order.reserve(ntgt * sizeof(int32_t)));
+    CK(ctx->b_workq.reserve(sizeof(int)));
     tmark(ctx, 4);
     LAUNCH(launch_beam(bp, (int)ntgt, (int)M, d_gt, ctx->b_monos.as<uint64_t>(), ctx->b_splits.as<int32_t>(),
                        ctx->b_nsplits.as<int32_t>(), ctx->b_calls.as<int32_t>(), ctx->b_ncalls.as<int32_t>(),
                        ctx->b_cmd.as<float>(), ctx->b_pbwt.as<uint32_t>(), ctx->b_count0.as<int32_t>(),
-                       ctx->b_rowoff.as<int64_t>(), ctx->b_arena.p, ab, d_mats, d_pats, d_dm, d_dp, d_tc, d_nc,
-                       ctx->status.as<uint32_t>(), ctx->cur_skip, ctx->stream));
+                       ctx->b_rowoff.as<int64_t>(), ctx->b_arena.p, ab, slots, ctx->b_order.as<int32_t>(),
+                       ctx->b_workq.as<int>(), d_mats, d_pats, d_dm, d_dp, d_tc, d_nc, ctx->status.as<uint32_t>(),
+                       ctx->cur_skip, ctx->stream));
     if (ctx->tgthap_n)   // haploid targets are not phased (Target.cpp:166-203)
         LAUNCH(launch_haploid_phase(d_gt, (int)ntgt, (int)M, (int)eimp_W(M), ctx->tgthap.as<uint8_t>(), d_mats,
                                     d_pats, d_dm, d_dp, d_tc, d_nc, ctx->status.as<uint32_t>(), ctx->stream));
@@ -988,7 +994,11 @@ int eimp_phase_reserve(eimp_ctx *ctx, const eimp_phase_params *p, size_t max_tar
     CK(ctx->b_cref.reserve(max_rows * eimp_W(K) * 8));
     CK(ctx->b_count0.reserve(max_rows * 4));
     CK(ctx->b_pbwt.reserve(2 * max_rows * eimp_kw(K) * 4));
-    CK(ctx->b_arena.reserve(n * beam_arena_bytes(bp, (int)M)));
+    const int slots = beam_slots(bp, (int)M, (int)n);
+    if (slots < 1) return fail(ctx, EIMP_E_CUDA, "beam launch shape: occupancy query failed");
+    CK(ctx->b_arena.reserve((size_t)slots * beam_arena_bytes(bp, (int)M)));
+    CK(ctx->b_order.reserve(n * sizeof(int32_t)));
+    CK(ctx->b_workq.reserve(sizeof(int)));
     CK(ctx->skipbuf.reserve(sizeof(int)));
     ctx->rows_cap = (int64_t)max_rows;
     return 0;

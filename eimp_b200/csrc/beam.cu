@@ -1205,7 +1205,29 @@ __host__ __device__ __forceinline__ size_t beam_canon_bytes(int NH) { return (((
 __device__ __forceinline__ void setbit_(uint64_t *v, int i) { v[i >> 6] |= 1ull << (i & 63); }
 __device__ __forceinline__ void clrbit_(uint64_t *v, int i) { v[i >> 6] &= ~(1ull << (i & 63)); }
 
-// One warp per target: Target::phaseExtPBWT (Target.cpp:291-777)
+// Targets in longest-first order: order[rank] = target, ranked by split sites
+// descending, ties by index.  One CTA; the persistent beam below takes the
+// targets in this order, so the longest walks start first and the short ones
+// fill the end of the launch.
+__global__ void lpt_order_kernel(const int32_t *__restrict__ nsplits, int ntgt, int32_t *__restrict__ order,
+                                 const int *__restrict__ skip) {
+    if (skip && *skip) return;
+    for (int i = threadIdx.x; i < ntgt; i += blockDim.x) {
+        const int si = nsplits[i];
+        int rank = 0;
+        for (int j = 0; j < ntgt; j++) {
+            const int sj = nsplits[j];
+            rank += sj > si || (sj == si && j < i);
+        }
+        order[rank] = i;
+    }
+}
+
+// Target::phaseExtPBWT (Target.cpp:291-777), one warp per target.  The grid
+// is persistent (as many CTAs as are resident at once): every warp takes the
+// next target from a device counter, in the order given (longest first), and
+// phases it with the beam arena of its slot, so the arenas number the
+// resident warps, not the targets.
 __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
     const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
@@ -1213,13 +1235,19 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     const int32_t *__restrict__ count0, const int64_t *__restrict__ rowoff, uint8_t *__restrict__ arena,
     size_t arena_bytes, uint64_t *__restrict__ mats, uint64_t *__restrict__ pats, float *__restrict__ dmat,
     float *__restrict__ dpat, float *__restrict__ totalconf, int32_t *__restrict__ ncallsites,
-    uint32_t *__restrict__ status, const int *__restrict__ skip) {
+    uint32_t *__restrict__ status, const int *__restrict__ skip, const int32_t *__restrict__ order,
+    int *__restrict__ workq) {
     if (skip && *skip) return;   // the batch exceeds the reserved rows
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int t = blockIdx.x * BEAM_WARPS + wid;
-    if (t >= ntgt) return;
     WS &w = reinterpret_cast<WS *>(smem_raw)[wid];
+    uint8_t *const ab = arena + (size_t)(blockIdx.x * BEAM_WARPS + wid) * arena_bytes;
+    for (;;) {
+    int qi = 0;
+    if (lane == 0) qi = atomicAdd(workq, 1);
+    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if (qi >= ntgt) break;
+    const int t = order[qi];
     const int wM = (int)eimp_W(M);
     const uint8_t *g = gt + (size_t)t * M;
     const uint64_t *mo = monos + (size_t)t * wM;
@@ -1242,7 +1270,6 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
                                             (size_t)wid * beam_canon_bytes(al.NH));
     }
     Ctx c;
-    uint8_t *ab = arena + (size_t)t * arena_bytes;
     c.hp = reinterpret_cast<HPh *>(ab + al.hp);
     c.ph = reinterpret_cast<float *>(ab + al.ph);
     c.ivpool = reinterpret_cast<uint32_t *>(ab + al.ivpool);
@@ -1448,22 +1475,45 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
         ncallsites[t] = nc;
         if (err) atomicOr(status, w.err ? w.err : (uint32_t)EIMP_ERR_BEAM_EMPTY);
     }
+    __syncwarp();
+    }
+}
+
+static size_t beam_smem(const BeamParams &p, const ArenaLayout &al) {
+    return (sizeof(WS) + beam_rows_bytes(p.K) + beam_canon_bytes(al.NH)) * BEAM_WARPS;
+}
+
+int beam_slots(const BeamParams &p, int M, int ntgt) {
+    const ArenaLayout al = arena_layout(p, M);
+    const size_t sm = beam_smem(p, al);
+    int dev = 0, nsm = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return -1;
+    if (cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, beam_kernel, 32 * BEAM_WARPS, sm) != cudaSuccess || per < 1)
+        return -1;
+    const int ctas = per * nsm;
+    const int need = (ntgt + BEAM_WARPS - 1) / BEAM_WARPS;
+    return (need < ctas ? need : ctas) * BEAM_WARPS;
 }
 
 cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt, const uint64_t *monos,
                         const int32_t *splits, const int32_t *nsplits, const int32_t *calls, const int32_t *ncalls,
                         const float *cmdiffs, const uint32_t *pbwt, const int32_t *count0, const int64_t *rowoff,
-                        void *arena, size_t arena_bytes, uint64_t *mats, uint64_t *pats, float *dmat, float *dpat,
-                        float *totalconf, int32_t *ncallsites, uint32_t *status, const int *skip, cudaStream_t st) {
+                        void *arena, size_t arena_bytes, int slots, int32_t *order, int *workq, uint64_t *mats,
+                        uint64_t *pats, float *dmat, float *dpat, float *totalconf, int32_t *ncallsites,
+                        uint32_t *status, const int *skip, cudaStream_t st) {
     ArenaLayout al = arena_layout(p, M);
-    if (arena_bytes < al.total) return cudaErrorInvalidValue;
-    const size_t sm = (sizeof(WS) + beam_rows_bytes(p.K) + beam_canon_bytes(al.NH)) * BEAM_WARPS;
+    if (arena_bytes < al.total || slots < BEAM_WARPS || slots % BEAM_WARPS) return cudaErrorInvalidValue;
+    const size_t sm = beam_smem(p, al);
     cudaError_t e = cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    int blocks = (ntgt + BEAM_WARPS - 1) / BEAM_WARPS;
-    beam_kernel<<<blocks, 32 * BEAM_WARPS, sm, st>>>(p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls,
-                                                     cmdiffs, pbwt, count0, rowoff, (uint8_t *)arena, arena_bytes,
-                                                     mats, pats, dmat, dpat, totalconf, ncallsites, status, skip);
+    lpt_order_kernel<<<1, 1024, 0, st>>>(nsplits, ntgt, order, skip);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(workq, 0, sizeof(int), st)) != cudaSuccess) return e;
+    beam_kernel<<<slots / BEAM_WARPS, 32 * BEAM_WARPS, sm, st>>>(
+        p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls, cmdiffs, pbwt, count0, rowoff, (uint8_t *)arena,
+        arena_bytes, mats, pats, dmat, dpat, totalconf, ncallsites, status, skip, order, workq);
     return cudaGetLastError();
 }
 

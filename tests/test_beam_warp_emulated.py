@@ -37,7 +37,7 @@ def emu_exe(tmp_path_factory):
     (d / "kernels.h").write_text(kh.replace("#define BEAM_WARPS 4", "#define BEAM_WARPS 1"))
     src = open(os.path.join(CSRC, "beam.cu")).read()
     # the launcher (triple-chevron launch, runtime attributes) is device-only
-    i, j = src.index("cudaError_t launch_beam("), src.rindex("}  // namespace eimp")
+    i, j = src.index("static size_t beam_smem("), src.rindex("}  // namespace eimp")
     src = src[:i] + src[j:]
     decl = "extern __shared__ __align__(16) uint8_t smem_raw[];"
     assert decl in src
@@ -73,8 +73,8 @@ def write_inputs(d, gt, monos, splits, calls, cmd, pbwt, count0, rows, K, P, pre
         np.ascontiguousarray(a).tofile(os.path.join(d, name + ".bin"))
 
 
-def run_emu(exe, d, nt, M):
-    r = subprocess.run([exe, str(d)], capture_output=True, text=True, timeout=900)
+def run_emu(exe, d, nt, M, queue=False):
+    r = subprocess.run([exe, str(d)] + (["queue"] if queue else []), capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
     wM = ((M + 511) // 512) * 8
     rd = lambda n, dt, shape: np.fromfile(os.path.join(d, n), dt).reshape(shape)
@@ -98,6 +98,24 @@ def test_beam_emulated_matches_reference_golden(emu_exe, tmp_path):
     write_inputs(tmp_path, K=K, P=16, prephase=False, **golden_inputs(g, K))
     nt, M = g["gt"].shape
     mats, pats, dm, dp, tc, nc, st = run_emu(emu_exe, tmp_path, nt, M)
+    assert not st.any()
+    np.testing.assert_array_equal(mats, g["K64_mat"])
+    np.testing.assert_array_equal(pats, g["K64_pat"])
+    np.testing.assert_array_equal(dm, g["K64_dos_mat"])
+    np.testing.assert_array_equal(dp, g["K64_dos_pat"])
+    np.testing.assert_array_equal(tc, g["K64_totalconf"])
+    np.testing.assert_array_equal(nc, g["K64_ncallsites"])
+
+
+def test_beam_emulated_persistent_queue(emu_exe, tmp_path):
+    """The persistent form: one warp takes all eight targets from the queue in
+    longest-first order and reuses one arena (filled with a pattern first);
+    every target's outputs must equal the reference's."""
+    g = np.load(golden_path("golden_tiny.npz"))
+    K = 64
+    write_inputs(tmp_path, K=K, P=16, prephase=False, **golden_inputs(g, K))
+    nt, M = g["gt"].shape
+    mats, pats, dm, dp, tc, nc, st = run_emu(emu_exe, tmp_path, nt, M, queue=True)
     assert not st.any()
     np.testing.assert_array_equal(mats, g["K64_mat"])
     np.testing.assert_array_equal(pats, g["K64_pat"])

@@ -1,7 +1,10 @@
 // Runs beam_kernel (generated host copy of eimp_b200/csrc/beam.cu) one
 // target at a time under the warp emulator.
 //
-//   beam_emu <dir> [t0 t1]
+//   beam_emu <dir> [t0 t1]     one target per kernel call, each with a fresh arena
+//   beam_emu <dir> queue       all targets through one call of one warp: the
+//                              persistent loop takes them from the queue in
+//                              longest-first order and reuses one arena
 //
 // <dir> holds the kernel inputs as raw little-endian arrays (params_i.bin,
 // params_f.bin, gt.bin, monos.bin, splits.bin, nsplits.bin, calls.bin,
@@ -46,10 +49,11 @@ template <class T> static void wr(const std::string &d, const char *name, const 
 int main(int argc, char **argv) {
     if (argc < 2) { fprintf(stderr, "usage: %s <dir> [t0 t1]\n", argv[0]); return 1; }
     const std::string d = argv[1];
+    const bool queue = argc > 2 && std::string(argv[2]) == "queue";
     const auto pi = rd<int32_t>(d, "params_i.bin");
     const auto pf = rd<float>(d, "params_f.bin");
     const int ntgt = pi[0], M = pi[1];
-    int t0 = argc > 2 ? atoi(argv[2]) : 0, t1 = argc > 3 ? atoi(argv[3]) : ntgt;
+    int t0 = argc > 2 && !queue ? atoi(argv[2]) : 0, t1 = argc > 3 ? atoi(argv[3]) : ntgt;
     if (t1 > ntgt) t1 = ntgt;
     eimp::BeamParams p;   // start phases: all Ref unless startph.bin is given
     p.K = pi[2]; p.H = pi[3]; p.P = pi[4]; p.Delta = pi[5]; p.Hf = pi[6]; p.Pf = pi[7]; p.Deltaf = pi[8];
@@ -77,7 +81,42 @@ int main(int argc, char **argv) {
     std::vector<float> dm((size_t)ntgt * M), dp((size_t)ntgt * M), tc(ntgt);
     std::vector<int32_t> nc(ntgt);
     std::vector<uint32_t> st(ntgt);
-    for (int t = t0; t < t1; t++) {
+    if (queue) {
+        std::vector<int32_t> order(ntgt, -1);
+        threadIdx.x = 0;
+        blockDim.x = 1;
+        eimp::lpt_order_kernel(nsplits.data(), ntgt, order.data(), nullptr);
+        for (int i = 1; i < ntgt; i++)   // longest first, ties by index
+            if (nsplits[order[i - 1]] < nsplits[order[i]] ||
+                (nsplits[order[i - 1]] == nsplits[order[i]] && order[i - 1] > order[i])) { fprintf(stderr, "order\n"); return 4; }
+        uint8_t *arena = (uint8_t *)malloc(al.total);
+        memset(arena, 0xA5, al.total);
+        uint8_t *smem = (uint8_t *)aligned_alloc(16, (smb + 15) / 16 * 16);
+        memset(smem, 0x5A, smb);
+        int workq = 0;
+        uint32_t status = 0;
+        EmuWarp warp;
+        std::vector<std::thread> lanes;
+        for (int l = 0; l < 32; l++)
+            lanes.emplace_back([&, l] {
+                threadIdx.x = l;
+                blockIdx.x = 0;
+                blockDim.x = 32;
+                emu_warp = &warp;
+                emu_smem_ptr = smem;
+                eimp::BeamParams pt = p;
+                pt.startph = startph.empty() ? nullptr : startph.data();
+                eimp::beam_kernel(pt, al, ntgt, M, gt.data(), monos.data(), splits.data(), nsplits.data(),
+                                  calls.data(), ncalls.data(), cmd.data(), pbwt.data(), count0.data(), rowoff.data(),
+                                  arena, al.total, mats.data(), pats.data(), dm.data(), dp.data(), tc.data(),
+                                  nc.data(), &status, nullptr, order.data(), &workq);
+            });
+        for (auto &x : lanes) x.join();
+        for (int t = 0; t < ntgt; t++) st[t] = status;
+        free(arena);
+        free(smem);
+    }
+    for (int t = t0; t < t1 && !queue; t++) {
         // fill patterns instead of zeros: the kernel must not read what it has not written
         uint8_t *arena = (uint8_t *)malloc(al.total);
         memset(arena, 0xA5, al.total);
@@ -86,12 +125,15 @@ int main(int argc, char **argv) {
         const int64_t r0 = rowoff[t];
         const int64_t zero = 0;
         uint32_t status = 0;
+        const int32_t first = 0;
+        int workq = 0;
         EmuWarp warp;
         std::vector<std::thread> lanes;
         for (int l = 0; l < 32; l++)
             lanes.emplace_back([&, l] {
                 threadIdx.x = l;
                 blockIdx.x = 0;
+                blockDim.x = 32;
                 emu_warp = &warp;
                 emu_smem_ptr = smem;
                 eimp::BeamParams pt = p;
@@ -101,7 +143,7 @@ int main(int argc, char **argv) {
                                   ncalls.data() + t, cmd.data() + (size_t)t * (M + 1), pbwt.data() + 2 * r0 * kw,
                                   count0.data() + r0, &zero, arena, al.total, mats.data() + (size_t)t * wM,
                                   pats.data() + (size_t)t * wM, dm.data() + (size_t)t * M, dp.data() + (size_t)t * M,
-                                  tc.data() + t, nc.data() + t, &status, nullptr);
+                                  tc.data() + t, nc.data() + t, &status, nullptr, &first, &workq);
             });
         for (auto &x : lanes) x.join();
         st[t] = status;
