@@ -70,8 +70,11 @@ def parse():
     ap.add_argument("--batch-targets", type=int, default=0, help="phasing batch size (0: from the memory budget)")
     ap.add_argument("--plain-targets", type=int, default=4,
                     help="targets per group timed one per call for the plain-form comparison (0: skip)")
-    ap.add_argument("--serving-requests", type=int, default=40, help="requests of the serving run (0: skip)")
-    ap.add_argument("--serving-rate", type=float, default=40.0, help="mean request arrivals per second")
+    ap.add_argument("--serving-requests", type=int, default=24, help="requests of the serving run (0: skip)")
+    ap.add_argument("--serving-rate", type=float, default=40.0, help="mean request arrivals per second (cfg2)")
+    ap.add_argument("--serving-rate-windows", type=float, default=3.0,
+                    help="mean request arrivals per second of the window requests on the cfg3 panel")
+    ap.add_argument("--serving-slots", type=int, default=3, help="slots of the window-request server")
     ap.add_argument("--graph-steps", type=int, default=3, help="replays timed in the CUDA-graph form (0: skip)")
     ap.add_argument("--qref-steps", type=int, default=5,
                     help="timed decodes of the panel's Qref haplotype section (0: skip)")
@@ -518,6 +521,8 @@ def main():
         tot_ms = float(t.item())
         dist.barrier()
     dos_per_step = sum(g.imputed() for g in groups)
+    batches_info = [len(g.batches) for g in groups]
+    targets_total = sum(g.nt for g in groups)
     value = world * dos_per_step * args.steps / (tot_ms / 1e3)
     ms_per_step = tot_ms / args.steps
 
@@ -557,6 +562,8 @@ def main():
                          "achieved_gbs": step_bytes / (ms_per_step / 1e3) / 1e9,
                          "frac": step_bytes / (ms_per_step / 1e3) / 1e9 / peak},
                 "stages": stages}
+
+    serving = None
 
     # ---- the CUDA-graph form: each group's step captured once (phasing in
     # capacity mode) and replayed, the groups' graphs concurrently; the
@@ -616,34 +623,6 @@ def main():
         plain = {"value": pl_value, "unit": UNIT, "targets": npl_all, "ms_per_target": pl_ms / npl_all,
                  "batched_over_plain": (value / world) / pl_value,
                  "form": "one target per call: eimp_phase_targets_dev, eimp_imp_prepare_dev, eimp_imp_bunch_dev"}
-
-    # ---- serving: continuous batching of requests of 1..256 targets of the
-    # first group arriving as a Poisson stream, two slots (contexts) on this
-    # device; host buffers in and out; latency from submission to result
-    serving = None
-    if rank == 0 and args.serving_requests > 0 and len(groups) == 1:
-        from eimp_b200.serving import GpuSlot, Server, device_bytes_per_target, load_test
-        tg = tgroups[0]
-        nt, M = tg.gt.shape
-        hm, sm, cm = synth.typed_views(panel, tg.typed)
-        srng = np.random.default_rng(cfg.seed + 7)
-        sizes = np.exp(srng.uniform(0.0, np.log(256.0), size=args.serving_requests)).astype(int).clip(1, 256)
-        reqs, o = [], 0
-        for sz in sizes:
-            idx = (o + np.arange(sz)) % nt
-            reqs.append(np.ascontiguousarray(tg.gt[idx]))
-            o += sz
-        slots = [GpuSlot(local, hm, sm, cm, panel.sitemajor, panel.af.astype(np.float32), tg.typed, nh_ref, params)
-                 for _ in range(2)]
-        bpt = device_bytes_per_target(M, Mref, min(cfg.K, nh_ref), P=cfg.beam)
-        free_b, _tot = torch.cuda.mem_get_info(dev)
-        srv = Server(slots, max_batch_targets=512, mem_budget=0.5 * free_b, bytes_per_target=bpt)
-        srv.warmup(tg.gt[np.arange(512) % nt])   # buffers at their working size
-        cnt = lambda gg: int(2 * ((Mref - M) * gg.shape[0] + (gg == 3).sum()))  # noqa: E731
-        serving = load_test(srv, reqs, args.serving_rate, seed=cfg.seed, count=cnt)
-        srv.close()
-        serving.update({"unit": UNIT, "slots": 2, "max_batch_targets": 512,
-                        "request_sizes": "log-uniform 1..256 targets", "arrivals": "Poisson"})
 
     # ---- the panel's Qref haplotype section (qref_spec.md section I)
     # decoded on the device into site-major rows, on the panel's first
@@ -768,6 +747,79 @@ def main():
                "form": "host API per group in turn: eimp_phase_targets per batch, eimp_imp_prepare, eimp_imp_bunch"}
         del gt_pin, ph_pin, mats_pin, pats_pin, pdm_pin, pdp_pin, dos_pin, bits_pin
 
+    # ---- serving: continuous batching of requests of 1..256 targets of the
+    # first group arriving as a Poisson stream, two slots (contexts) on this
+    # device; host buffers in and out; latency from submission to result
+    if rank == 0 and args.serving_requests > 0 and len(groups) == 1:
+        from eimp_b200.serving import GpuSlot, Server, device_bytes_per_target, load_test
+        tg = tgroups[0]
+        nt, M = tg.gt.shape
+        hm, sm, cm = synth.typed_views(panel, tg.typed)
+        srng = np.random.default_rng(cfg.seed + 7)
+        sizes = np.exp(srng.uniform(0.0, np.log(256.0), size=args.serving_requests)).astype(int).clip(1, 256)
+        reqs, o = [], 0
+        for sz in sizes:
+            idx = (o + np.arange(sz)) % nt
+            reqs.append(np.ascontiguousarray(tg.gt[idx]))
+            o += sz
+        slots = [GpuSlot(local, hm, sm, cm, panel.sitemajor, panel.af.astype(np.float32), tg.typed, nh_ref, params)
+                 for _ in range(2)]
+        bpt = device_bytes_per_target(M, Mref, min(cfg.K, nh_ref), P=cfg.beam)
+        free_b, _tot = torch.cuda.mem_get_info(dev)
+        srv = Server(slots, max_batch_targets=512, mem_budget=0.5 * free_b, bytes_per_target=bpt)
+        srv.warmup(tg.gt[np.arange(512) % nt])   # buffers at their working size
+        cnt = lambda gg: int(2 * ((Mref - M) * gg.shape[0] + (gg == 3).sum()))  # noqa: E731
+        serving = load_test(srv, reqs, args.serving_rate, seed=cfg.seed, count=cnt)
+        srv.close()
+        serving.update({"unit": UNIT, "slots": 2, "max_batch_targets": 512,
+                        "request_sizes": "log-uniform 1..256 targets", "arrivals": "Poisson"})
+
+    # ---- serving on the resident cfg3 panel (the cfg5 workload): requests of
+    # log-uniform 1..5,000 targets, typed density 1-8 %, each in a random
+    # 2-10 Mb window, Poisson arrivals; every request has its own typed sites,
+    # so its references are built on the device from the resident panel and
+    # requests overlap on the slots (admitted by device memory); the same
+    # requests one at a time on one slot beside it
+    if rank == 0 and args.serving_requests > 0 and len(groups) > 1:
+        from eimp_b200.serving import Server, WindowSlot, load_test, window_request_bytes
+        for g in groups:   # the batch's device buffers are not needed any more
+            g.close()
+        groups = []
+        torch.cuda.empty_cache()
+        reqs = synth.window_requests(cfg, panel, args.serving_requests, seed=cfg.seed + 11)
+        nb = lambda r: window_request_bytes(r, nh_ref, cfg.K, cfg.beam)  # noqa: E731
+        cnt = lambda r: int(2 * ((r.hi - r.lo - len(r.typed)) * r.n + (r.gt == 3).sum()))  # noqa: E731
+        slots = [WindowSlot(local, d_full, d_af, panel.cm, nh_ref, params) for _ in range(args.serving_slots)]
+        big = max(reqs, key=nb)
+        for sl in slots:     # buffers at their working size
+            sl.run(big)
+        torch.cuda.synchronize()
+        free_b, _tot = torch.cuda.mem_get_info(dev)
+        srv = Server(slots, merge=False, mem_budget=0.8 * free_b, request_bytes=nb)
+        served = load_test(srv, reqs, args.serving_rate_windows, seed=cfg.seed + 12, count=cnt)
+        srv.close()
+        solo = WindowSlot(local, d_full, d_af, panel.cm, nh_ref, params)
+        solo.run(big)
+        lat1 = []
+        t0 = time.perf_counter()
+        for r in reqs:
+            a = time.perf_counter()
+            solo.run(r)
+            lat1.append(time.perf_counter() - a)
+        t1 = time.perf_counter() - t0
+        solo.close()
+        lat1 = np.array(lat1) * 1e3
+        units = sum(cnt(r) for r in reqs)
+        served.update({"unit": UNIT, "workload": "cfg5: requests on the resident cfg3 panel",
+                       "slots": args.serving_slots, "arrivals": "Poisson",
+                       "request_sizes": "log-uniform 1..5000 targets, typed density U(1 %, 8 %), windows U(2, 10) Mb",
+                       "request_targets": [int(r.n) for r in reqs],
+                       "one_at_a_time": {"p50_ms": float(np.percentile(lat1, 50)),
+                                         "p99_ms": float(np.percentile(lat1, 99)), "total_s": t1,
+                                         "throughput": units / t1, "unit": UNIT,
+                                         "form": "the same requests back to back on one slot"}})
+        serving = served
+
     # ---- the reference's own CPU path on each group's sample, and parity of
     # the GPU step against it
     cpu = None
@@ -790,10 +842,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64/f32",
                 "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
-                "config": config_block(cfg, panel, tgroups, [len(g.batches) for g in groups]),
+                "config": config_block(cfg, panel, tgroups, batches_info),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-                "gpu_launches": int(launches), "phased_samples_per_sec": world * sum(g.nt for g in groups) / (
-                    ms_per_step / 1e3),
+                "gpu_launches": int(launches), "phased_samples_per_sec": world * targets_total / (ms_per_step / 1e3),
                 "plain": plain, "serving": serving, "graph": graph, "qref_decode": qref, "parity": parity}
         print(json.dumps(line), flush=True)
     for g in groups:

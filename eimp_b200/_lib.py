@@ -53,6 +53,7 @@ _PROTOS = [
     ("eimp_gpu_block_size", _sz, [_vp]),
     ("eimp_gpu_run_cref_pbwt", _i32, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("eimp_phase_set_reference", _i32, [_vp, _sz, _sz, _vp, _vp, _vp]),
+    ("eimp_phase_set_reference_dev", _i32, [_vp, _sz, _sz, _vp, _sz, _vp, _vp]),
     ("eimp_phase_set_haploid_ref", _i32, [_vp, _sz, _vp]),
     ("eimp_phase_haploid_targets", _i32, [_vp, _sz, _vp]),
     ("eimp_imp_set_haploid_ref", _i32, [_vp, _sz, _vp]),

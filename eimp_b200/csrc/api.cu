@@ -318,11 +318,17 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
     LAUNCH(launch_segmap(ctx->i_typed.as<int64_t>(), (int)M, (int)Mref, ctx->i_af.as<float>(), (int)nhaps,
                          ctx->i_segm.as<int32_t>(), ctx->i_common.as<uint8_t>(), ctx->i_sinfo.as<int2>(), st));
     const uint64_t *typed_rows = d_sitemajor_typed;
+    if (!typed_rows) {   // the typed sites' rows from the panel itself
+        CK(ctx->i_sitetyped_tmp.reserve(M * wN * 8));
+        LAUNCH(launch_gather_rows(d_sitemajor_full, wN, ctx->i_typed.as<int64_t>(), (int)M, (int)wN,
+                                  ctx->i_sitetyped_tmp.as<uint64_t>(), st));
+        typed_rows = ctx->i_sitetyped_tmp.as<uint64_t>();
+    }
     size_t wK = wN;
     if (ctx->i_refhap_samples) {
         wK = eimp_W(K);
         CK(ctx->i_sitetyped_c.reserve(M * wK * 8));
-        LAUNCH(launch_compact_cols(d_sitemajor_typed, (int)M, (int)wN, ctx->i_refmap.as<int32_t>(), (int)K,
+        LAUNCH(launch_compact_cols(typed_rows, (int)M, (int)wN, ctx->i_refmap.as<int32_t>(), (int)K,
                                    ctx->i_sitetyped_c.as<uint64_t>(), (int)wK, st));
         typed_rows = ctx->i_sitetyped_c.as<uint64_t>();
     }
@@ -753,6 +759,27 @@ int eimp_phase_set_reference(eimp_ctx *ctx, size_t M, size_t nhaps, const uint64
     CK(cudaMemcpyAsync(ctx->p_sitemajor.p, sitemajor, M * wN * 8, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->p_cm.p, cM, M * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int eimp_phase_set_reference_dev(eimp_ctx *ctx, size_t M, size_t nhaps, const uint64_t *d_sitemajor_full,
+                                 size_t ldw_words, const int64_t *d_typed, const float *d_cM) {
+    if (!ctx || !M || !nhaps || !d_sitemajor_full || !d_typed || !d_cM)
+        return fail(ctx, EIMP_E_ARG, "eimp_phase_set_reference_dev: bad argument");
+    const size_t wM = eimp_W(M), wN = eimp_W(nhaps);
+    if (ldw_words < wN) return fail(ctx, EIMP_E_ARG, "eimp_phase_set_reference_dev: leading dimension too small");
+    if (int r = use_device(ctx)) return r;
+    cudaStream_t st = ctx->stream;
+    ctx->p_M = M; ctx->p_nhaps = nhaps;
+    ctx->p_nhaploid = 0;
+    CK(ctx->p_hapmajor.reserve(nhaps * wM * 8));
+    CK(ctx->p_sitemajor.reserve(M * wN * 8));
+    CK(ctx->p_cm.reserve(M * 4));
+    LAUNCH(launch_gather_rows(d_sitemajor_full, ldw_words, d_typed, (int)M, (int)wN, ctx->p_sitemajor.as<uint64_t>(),
+                              st));
+    CK(cudaMemsetAsync(ctx->p_hapmajor.p, 0, nhaps * wM * 8, st));
+    LAUNCH(launch_transpose(ctx->p_sitemajor.as<uint64_t>(), M, wN, ctx->p_hapmajor.as<uint64_t>(), nhaps, wM, st));
+    CK(cudaMemcpyAsync(ctx->p_cm.p, d_cM, M * 4, cudaMemcpyDeviceToDevice, st));
     return 0;
 }
 

@@ -850,6 +850,15 @@ __global__ void segmap_kernel(const int64_t *__restrict__ typed, int M, int Mref
     sinfo[mref] = make_int2(k | (cm << 31), h | ((afv > 0.5f ? 1 : 0) << 31));
 }
 
+// rows of a bit matrix gathered by index: dst[i] = src[idx[i]] (w words each)
+__global__ void gather_rows_kernel(const uint64_t *__restrict__ src, size_t ldsrc, const int64_t *__restrict__ idx,
+                                   int n, int w, uint64_t *__restrict__ dst) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)n * w) return;
+    const int r = (int)(i / w), c = (int)(i % w);
+    dst[i] = src[(size_t)idx[r] * ldsrc + c];
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -864,6 +873,14 @@ cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint
     cudaError_t e = cudaFuncSetAttribute(refpbwt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     refpbwt_kernel<<<1, 1024, sm, st>>>(sitemajor, M, K, wN, compr, absperm, count0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const uint64_t *src, size_t ldsrc, const int64_t *idx, int n, int w, uint64_t *dst,
+                               cudaStream_t st) {
+    const long tot = (long)n * w;
+    if (tot == 0) return cudaSuccess;
+    gather_rows_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(src, ldsrc, idx, n, w, dst);
     return cudaGetLastError();
 }
 

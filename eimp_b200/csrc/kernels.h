@@ -23,6 +23,9 @@ cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint
                            int32_t *count0, cudaStream_t st);
 cudaError_t launch_transpose(const uint64_t *src, size_t rows, size_t srcw, uint64_t *dst, size_t cols, size_t dstw,
                              cudaStream_t st);
+// dst row i (w words) = src row idx[i] (rows ldsrc words apart)
+cudaError_t launch_gather_rows(const uint64_t *src, size_t ldsrc, const int64_t *idx, int n, int w, uint64_t *dst,
+                               cudaStream_t st);
 // hapmap (null: identity): the target haplotype (row of phased, matches,
 // outputs; its target = row / 2) of each of the nhaps haplotypes searched
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,

@@ -29,6 +29,7 @@ phased haplotypes and imputed dosages.
 from __future__ import annotations
 
 import collections
+import ctypes as C
 import threading
 import time
 from concurrent.futures import Future
@@ -54,13 +55,13 @@ class Result:
 
 @dataclass
 class _Request:
-    gt: np.ndarray
+    gt: object                 # genotype array, or a request object for slots that take one
     future: Future
     t_submit: float
     n: int = field(init=False)
 
     def __post_init__(self):
-        self.n = self.gt.shape[0]
+        self.n = self.gt.shape[0] if isinstance(self.gt, np.ndarray) else int(self.gt.n)
 
 
 class GpuSlot:
@@ -113,13 +114,19 @@ class Server:
     ``run(gt) -> (mats, pats, bits, dosages)`` and ``close()``)."""
 
     def __init__(self, slots, max_batch_targets: int = 256, mem_budget: float = float("inf"),
-                 bytes_per_target: float = 0.0):
+                 bytes_per_target: float = 0.0, merge: bool = True, request_bytes=None):
+        """merge: requests share launches (they must share the typed sites);
+        with merge=False every launch serves one request, and the requests in
+        flight overlap on the slots.  request_bytes(req) overrides the
+        per-target device-memory estimate."""
         if not slots:
             raise ValueError("a server needs at least one slot")
         self.slots = list(slots)
         self.max_batch = int(max_batch_targets)
         self.mem_budget = float(mem_budget)
         self.bytes_per_target = float(bytes_per_target)
+        self.merge = bool(merge)
+        self.request_bytes = request_bytes
         self._q: collections.deque[_Request] = collections.deque()
         self._cv = threading.Condition()
         self._reserved = 0.0
@@ -131,16 +138,20 @@ class Server:
             t.start()
 
     # ------------------------------------------------------------ client side
-    def submit(self, gt: np.ndarray) -> Future:
-        gt = np.ascontiguousarray(gt, dtype=np.uint8)
+    def _bytes(self, req: _Request) -> float:
+        return float(self.request_bytes(req.gt)) if self.request_bytes else self.bytes_per_target * req.n
+
+    def submit(self, gt) -> Future:
         fut: Future = Future()
-        if gt.ndim != 2 or gt.shape[0] == 0:
-            fut.set_exception(ValueError("a request is a non-empty (targets x typed sites) genotype array"))
-            return fut
-        if self.bytes_per_target * gt.shape[0] > self.mem_budget:
+        if isinstance(gt, np.ndarray) or not hasattr(gt, "n"):
+            gt = np.ascontiguousarray(gt, dtype=np.uint8)
+            if gt.ndim != 2 or gt.shape[0] == 0:
+                fut.set_exception(ValueError("a request is a non-empty (targets x typed sites) genotype array"))
+                return fut
+        need = self._bytes(_Request(gt, fut, 0.0))
+        if need > self.mem_budget:
             fut.set_exception(MemoryError(
-                f"request of {gt.shape[0]} targets needs ~{self.bytes_per_target * gt.shape[0]:.3g} B of device "
-                f"memory, more than the budget {self.mem_budget:.3g} B"))
+                f"request needs ~{need:.3g} B of device memory, more than the budget {self.mem_budget:.3g} B"))
             return fut
         with self._cv:
             if self._stop:
@@ -182,17 +193,18 @@ class Server:
         """Requests for the next launch (called with the lock held): arrival
         order, up to max_batch targets (a larger single request goes alone),
         within the memory left; None when nothing can start now."""
-        batch, n = [], 0
+        batch, n, need = [], 0, 0.0
         while self._q:
             r = self._q[0]
-            if batch and n + r.n > self.max_batch:
+            if batch and (not self.merge or n + r.n > self.max_batch):
                 break
-            need = self.bytes_per_target * (n + r.n)
-            if self._reserved + need > self.mem_budget:
+            more = self._bytes(r)
+            if self._reserved + need + more > self.mem_budget:
                 break
             batch.append(self._q.popleft())
             n += r.n
-        return (batch, n) if batch else None
+            need += more
+        return (batch, n, need) if batch else None
 
     def _work(self, slot):
         while True:
@@ -205,12 +217,13 @@ class Server:
                     self._cv.wait()
                 if got is None:
                     return
-                batch, n = got
-                reserve = self.bytes_per_target * n
+                batch, n, reserve = got
                 self._reserved += reserve
             try:
                 gt = batch[0].gt if len(batch) == 1 else np.concatenate([r.gt for r in batch])
                 mats, pats, bits, dos = slot.run(gt)
+                if not isinstance(mats, np.ndarray):   # a slot that keeps the result on the device
+                    mats, pats, bits, dos = (np.asarray(x) for x in (mats, pats, bits, dos))
                 t_done = time.perf_counter()
                 off = 0
                 for r in batch:
@@ -229,6 +242,72 @@ class Server:
                     self._reserved -= reserve
                     self._batches.append(n)
                     self._cv.notify_all()
+
+
+class WindowSlot:
+    """A slot for requests with their own typed sites in a window of a panel
+    resident on the device (the panel is shared by all slots): per request it
+    builds the phasing reference (the typed rows gathered and transposed on
+    the device), phases the targets, builds the imputation reference of the
+    window (haplotype-major window, segment map, reference PBWT of the typed
+    sites) and imputes every site of the window."""
+
+    def __init__(self, device: int, d_sitemajor_full, d_af, cm: np.ndarray, nhaps: int, params):
+        import torch
+        from .engine import Context
+        self.ctx = Context(device)
+        self.dev = torch.device("cuda", device)
+        self.d_full, self.d_af = d_sitemajor_full, d_af
+        self.wN = int(d_sitemajor_full.shape[1])
+        self.cm = np.asarray(cm)
+        self.nhaps = nhaps
+        self.params = params
+        self._pin = GpuSlot._pinned.__get__(self)
+        self._bufs, self._keep = {}, {}
+
+    def run(self, req):
+        import torch
+        from ._lib import ptr
+        L, h = self.ctx.L, self.ctx.h
+        lo, hi, M, n = req.lo, req.hi, len(req.typed), req.n
+        Mw = hi - lo
+        typed_abs = torch.from_numpy(lo + req.typed).to(self.dev)
+        typed_rel = torch.from_numpy(np.ascontiguousarray(req.typed)).to(self.dev)
+        cm_t = torch.from_numpy(self.cm[lo + req.typed].astype(np.float32)).to(self.dev)
+        self._keep["req"] = (typed_abs, typed_rel, cm_t)   # in use until the calls below have run
+        self.ctx.check(L.eimp_phase_set_reference_dev(h, M, self.nhaps, self.d_full.data_ptr(), self.wN,
+                                                      typed_abs.data_ptr(), cm_t.data_ptr()))
+        gt = np.ascontiguousarray(req.gt, np.uint8)
+        mats = self._pin("mats", n, W(M), np.uint64)
+        pats = self._pin("pats", n, W(M), np.uint64)
+        dm = self._pin("dm", n, M, np.float32)
+        dp = self._pin("dp", n, M, np.float32)
+        tc = self._pin("tc", n, 1, np.float32)
+        nc = self._pin("nc", n, 1, np.int32)
+        p = self.params.c()
+        self.ctx.check(L.eimp_phase_targets(h, C.byref(p), n, ptr(gt), ptr(mats), ptr(pats), ptr(dm), ptr(dp),
+                                            ptr(tc), ptr(nc)))
+        phased = self._pin("phased", 2 * n, W(M), np.uint64)
+        phased[0::2], phased[1::2] = mats, pats
+        self.ctx.check(L.eimp_imp_set_reference_dev(h, Mw, self.nhaps, self.d_full.data_ptr() + lo * self.wN * 8,
+                                                    self.d_af.data_ptr() + lo * 4, M, typed_rel.data_ptr(), None))
+        self.ctx.check(L.eimp_imp_prepare(h, n, ptr(phased), ptr(gt), 0, 0, 0))
+        bits = self._pin("bits", 2 * n, W(Mw), np.uint64)
+        dos = self._pin("dos", 2 * n, Mw, np.float32)
+        self.ctx.check(L.eimp_imp_bunch(h, 0, Mw, ptr(bits), ptr(dos)))
+        return mats.copy(), pats.copy(), bits.copy(), dos.copy()
+
+    def close(self):
+        self.ctx.close()
+
+
+def window_request_bytes(req, nhaps: int, K: int, P: int = 128) -> float:
+    """Device memory of one window request: its references (typed rows both
+    ways, the window's haplotype-major copy, prefix arrays) and its targets
+    (device_bytes_per_target over the window)."""
+    M, Mw = len(req.typed), req.hi - req.lo
+    refs = 2 * M * W(nhaps) * 8 + nhaps * W(Mw) * 8 + 4 * (M + 1) * nhaps + Mw * 16
+    return refs + req.n * device_bytes_per_target(M, Mw, min(K, nhaps), P=P)
 
 
 def device_bytes_per_target(M: int, Mref: int, K: int, P: int = 128, H: int = 100, split_fraction: float = 0.25):
@@ -270,8 +349,9 @@ def load_test(server: Server, requests, rate_per_s: float, seed: int = 0, count=
     res = [f.result() for f in futs]
     makespan = time.perf_counter() - t0
     lat = np.array([r.latency_s for r in res]) * 1e3
-    units = sum(count(g) for g in requests) if count else sum(g.shape[0] for g in requests)
-    return {"requests": len(requests), "targets": int(sum(g.shape[0] for g in requests)),
+    nt = lambda g: int(g.n) if hasattr(g, "n") else int(g.shape[0])  # noqa: E731
+    units = sum(count(g) for g in requests) if count else sum(nt(g) for g in requests)
+    return {"requests": len(requests), "targets": int(sum(nt(g) for g in requests)),
             "rate_per_s": rate_per_s, "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
             "max_ms": float(lat.max()), "makespan_s": makespan, "throughput": units / makespan,
             "mean_batch_targets": float(np.mean([r.batch_targets for r in res]))}

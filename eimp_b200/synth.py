@@ -89,6 +89,7 @@ class Panel:
     af: np.ndarray             # float32 (Mref,) alt allele frequency in the panel
     hapmajor: np.ndarray       # uint64 (nhaps, W(Mref))  one row per haplotype
     sitemajor: np.ndarray      # uint64 (Mref, W(nhaps))  one row per site (referenceFullT)
+    founders: np.ndarray | None = None   # uint64 (F, W(Mref)) the founders (for more targets)
 
 
 @dataclass
@@ -165,7 +166,7 @@ def _cache_dir() -> str:
 
 
 # version of the generator's drawing order (part of the cache key)
-GENERATOR = 2
+GENERATOR = 3
 
 
 def generate(cfg: SynthConfig | str, cache: bool = True):
@@ -175,7 +176,8 @@ def generate(cfg: SynthConfig | str, cache: bool = True):
     path = os.path.join(_cache_dir(), f"{cfg.name}-g{GENERATOR}-{cfg.key()}.npz")
     if cache and os.path.exists(path):
         z = np.load(path)
-        panel = Panel(cfg.nhaps, cfg.nsites, z["pos"], z["cm"], z["af"], z["hapmajor"], z["sitemajor"])
+        panel = Panel(cfg.nhaps, cfg.nsites, z["pos"], z["cm"], z["af"], z["hapmajor"], z["sitemajor"],
+                      z["founders"])
         groups = [Targets(z[f"typed{g}"], np.ascontiguousarray(z[f"gt{g}"]), np.ascontiguousarray(z[f"truth{g}"]))
                   for g in range(len(cfg.groups))]
         return panel, groups
@@ -202,7 +204,7 @@ def generate(cfg: SynthConfig | str, cache: bool = True):
     sitemajor = transpose_bits(hapmajor, nh, n)
     ac = np.bitwise_count(sitemajor).sum(axis=1, dtype=np.int64)
     af = (ac / float(nh)).astype(np.float32)
-    panel = Panel(nh, n, pos.astype(np.int64), cm, af, hapmajor, sitemajor)
+    panel = Panel(nh, n, pos.astype(np.int64), cm, af, hapmajor, sitemajor, Fw)
 
     groups = []
     for g in cfg.groups:
@@ -221,7 +223,8 @@ def generate(cfg: SynthConfig | str, cache: bool = True):
         groups.append(Targets(typed, np.ascontiguousarray(gt), np.ascontiguousarray(th)))
 
     if cache:
-        kw = dict(pos=panel.pos, cm=panel.cm, af=panel.af, hapmajor=panel.hapmajor, sitemajor=panel.sitemajor)
+        kw = dict(pos=panel.pos, cm=panel.cm, af=panel.af, hapmajor=panel.hapmajor, sitemajor=panel.sitemajor,
+                  founders=Fw)
         for i, t in enumerate(groups):
             kw[f"typed{i}"] = t.typed
             kw[f"gt{i}"] = t.gt
@@ -230,6 +233,53 @@ def generate(cfg: SynthConfig | str, cache: bool = True):
         np.savez(tmp, **kw)
         os.replace(tmp, path)
     return panel, groups
+
+
+@dataclass
+class WindowRequest:
+    """A serving request: targets genotyped at their own typed sites inside a
+    window [lo, hi) of the panel's sites.  typed holds window-relative site
+    indices (ascending); gt is (n, len(typed)) with 3 = missing."""
+    lo: int
+    hi: int
+    typed: np.ndarray
+    gt: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return self.gt.shape[0]
+
+
+def window_requests(cfg: SynthConfig, panel: Panel, nreq: int, seed: int, max_targets: int = 5000,
+                    density=(0.01, 0.08), window_mb=(2.0, 10.0), miss=(0.0, 0.05)):
+    """Seeded serving requests over a resident panel: log-uniform 1..max_targets
+    targets, a typed density uniform in ``density``, a window of uniform length
+    in ``window_mb`` Mb at a uniform position, per-target missingness uniform in
+    ``miss``.  Targets are held-out mosaics of the panel's founders, like the
+    configurations' targets."""
+    if panel.founders is None:
+        raise ValueError("the panel was generated without its founders")
+    rng = np.random.default_rng(seed)
+    span = float(panel.pos[-1] - panel.pos[0])
+    out = []
+    for _ in range(nreq):
+        n = int(np.clip(np.exp(rng.uniform(0.0, np.log(max_targets))), 1, max_targets))
+        d = rng.uniform(*density)
+        wl = min(span, rng.uniform(*window_mb) * 1e6)
+        start = panel.pos[0] + rng.uniform(0.0, span - wl)
+        lo, hi = (int(x) for x in np.searchsorted(panel.pos, [start, start + wl]))
+        m = max(2, int(round(d * (hi - lo))))
+        typed = np.sort(rng.choice(hi - lo, m, replace=False)).astype(np.int64)
+        th = np.zeros((2 * n, m), np.uint8)
+        for a in range(0, 2 * n, 1024):
+            b = min(2 * n, a + 1024)
+            th[a:b] = gather_bits(_mosaic_words(rng, panel.founders, panel.cm, b - a, cfg.mean_segment_cm,
+                                                cfg.copy_err), lo + typed)
+        gt = (th[0::2] + th[1::2]).astype(np.uint8)
+        rates = rng.uniform(*miss, n)
+        gt[rng.random(gt.shape) < rates[:, None]] = 3
+        out.append(WindowRequest(lo, hi, typed, np.ascontiguousarray(gt)))
+    return out
 
 
 def typed_views(panel: Panel, typed: np.ndarray):

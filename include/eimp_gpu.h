@@ -138,6 +138,15 @@ int eimp_gpu_run_cref_pbwt(eimp_ctx *ctx, size_t ntgt, const uint64_t *const *tg
 int eimp_phase_set_reference(eimp_ctx *ctx, size_t M, size_t nhaps, const uint64_t *hapmajor,
                              const uint64_t *sitemajor, const float *cM);
 
+/* The same from a panel already in device memory (no counterpart in the
+ * reference, whose VCFData builds reference/referenceT while reading): the
+ * rows d_typed[0..M-1] of the site-major panel d_sitemajor_full (rows of
+ * ldw_words >= W(nhaps) words) are the typed sites; their haplotype-major
+ * transpose is built on the device.  d_cM: M genetic positions.  Enqueued on
+ * the context's stream; the device buffers must stay valid until it ran. */
+int eimp_phase_set_reference_dev(eimp_ctx *ctx, size_t M, size_t nhaps, const uint64_t *d_sitemajor_full,
+                                 size_t ldw_words, const int64_t *d_typed, const float *d_cM);
+
 /* Target::prepPhase (Target.cpp:95-163) for a batch of targets, on the device:
  * best haplotypes (K ascending indices per target), best-haplotype flags
  * (W(nhaps) words), monomorphic sites (W(M) words), split sites and call
@@ -332,6 +341,8 @@ int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phase
                          int setmaxerrors, int imputeCalls, size_t match_cap);
 int eimp_imp_bunch_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t *d_bits, size_t ldb_words,
                        float *d_dos, size_t ldd);
+/* d_sitemajor_typed may be NULL: the typed rows are then gathered from
+ * d_sitemajor_full at d_typed on the device. */
 int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint64_t *d_sitemajor_full,
                                const float *d_af_full, size_t M, const int64_t *d_typed,
                                const uint64_t *d_sitemajor_typed);
