@@ -795,29 +795,34 @@ def main():
             sl.run(big)
         torch.cuda.synchronize()
         free_b, _tot = torch.cuda.mem_get_info(dev)
-        srv = Server(slots, merge=False, mem_budget=0.8 * free_b, request_bytes=nb)
-        served = load_test(srv, reqs, args.serving_rate_windows, seed=cfg.seed + 12, count=cnt)
-        srv.close()
-        solo = WindowSlot(local, d_full, d_af, panel.cm, nh_ref, params)
-        solo.run(big)
-        lat1 = []
-        t0 = time.perf_counter()
-        for r in reqs:
-            a = time.perf_counter()
-            solo.run(r)
-            lat1.append(time.perf_counter() - a)
-        t1 = time.perf_counter() - t0
-        solo.close()
-        lat1 = np.array(lat1) * 1e3
-        units = sum(cnt(r) for r in reqs)
+
+        def serve(sl, rate):
+            srv = Server(sl, merge=False, mem_budget=0.8 * free_b, request_bytes=nb)
+            out = load_test(srv, reqs, rate, seed=cfg.seed + 12, count=cnt)
+            srv.shutdown()
+            return out
+
+        # continuous batching over the slots, then the same requests one at a
+        # time (one slot, first come first served), under the same Poisson
+        # arrivals; and both saturated (all requests at once) for throughput
+        served = serve(slots, args.serving_rate_windows)
+        fifo = serve(slots[:1], args.serving_rate_windows)
+        sat = serve(slots, 1e9)
+        sat1 = serve(slots[:1], 1e9)
+        for sl in slots:
+            sl.close()
         served.update({"unit": UNIT, "workload": "cfg5: requests on the resident cfg3 panel",
                        "slots": args.serving_slots, "arrivals": "Poisson",
                        "request_sizes": "log-uniform 1..5000 targets, typed density U(1 %, 8 %), windows U(2, 10) Mb",
                        "request_targets": [int(r.n) for r in reqs],
-                       "one_at_a_time": {"p50_ms": float(np.percentile(lat1, 50)),
-                                         "p99_ms": float(np.percentile(lat1, 99)), "total_s": t1,
-                                         "throughput": units / t1, "unit": UNIT,
-                                         "form": "the same requests back to back on one slot"}})
+                       "one_at_a_time": {"p50_ms": fifo["p50_ms"], "p99_ms": fifo["p99_ms"],
+                                         "throughput": fifo["throughput"], "makespan_s": fifo["makespan_s"],
+                                         "unit": UNIT, "form": "the same requests and arrivals, one slot, "
+                                                               "first come first served"},
+                       "saturated": {"throughput": sat["throughput"], "makespan_s": sat["makespan_s"],
+                                     "one_at_a_time_throughput": sat1["throughput"],
+                                     "one_at_a_time_makespan_s": sat1["makespan_s"],
+                                     "form": "all requests submitted at once"}})
         serving = served
 
     # ---- the reference's own CPU path on each group's sample, and parity of

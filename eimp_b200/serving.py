@@ -179,12 +179,16 @@ class Server:
         with self._cv:
             return list(self._batches)
 
-    def close(self):
+    def shutdown(self):
+        """Stops the workers once the queue is served; the slots stay open."""
         with self._cv:
             self._stop = True
             self._cv.notify_all()
         for t in self._workers:
             t.join()
+
+    def close(self):
+        self.shutdown()
         for s in self.slots:
             s.close()
 
@@ -262,8 +266,19 @@ class WindowSlot:
         self.cm = np.asarray(cm)
         self.nhaps = nhaps
         self.params = params
-        self._pin = GpuSlot._pinned.__get__(self)
         self._bufs, self._keep = {}, {}
+
+    def _pin(self, name: str, rows: int, cols: int, dtype):
+        """A (rows, cols) view of a page-locked host buffer reused across
+        requests and grown to the largest request's size (rows and columns
+        change with every request's targets, typed sites and window)."""
+        nbytes = rows * cols * np.dtype(dtype).itemsize
+        t = self._keep.get(name)
+        if t is None or t.numel() < nbytes:
+            import torch
+            t = torch.empty(max(nbytes, 64), dtype=torch.uint8, pin_memory=True)
+            self._keep[name] = t
+        return t.numpy()[:nbytes].view(dtype).reshape(rows, cols)
 
     def run(self, req):
         import torch
