@@ -81,6 +81,7 @@ def parse():
     ap.add_argument("--qref-variants", type=int, default=100000, help="panel variants of the Qref leg")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-sample-targets", type=int, default=0,
                     help="targets per group of the reference's CPU runs (0: the configuration's default)")
     return ap.parse_args()
@@ -485,6 +486,11 @@ def main():
         groups.append(DensityGroup(local, d_full, d_af, nh_ref, tg.typed, hm, sm, cm, tg.gt, params, B))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    # launch shapes tuned on every group's own data (eimp_b200/autotune.py)
+    tuning = None
+    if not args.no_autotune:
+        from eimp_b200.autotune import tune_group
+        tuning = [tune_group(g) for g in groups]
 
     def step_timed(graphs=False):
         e0, e1 = ev(), ev()
@@ -850,7 +856,8 @@ def main():
                 "config": config_block(cfg, panel, tgroups, batches_info),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": int(launches), "phased_samples_per_sec": world * targets_total / (ms_per_step / 1e3),
-                "plain": plain, "serving": serving, "graph": graph, "qref_decode": qref, "parity": parity}
+                "plain": plain, "serving": serving, "graph": graph, "qref_decode": qref, "parity": parity,
+                "autotune": tuning}
         print(json.dumps(line), flush=True)
     for g in groups:
         g.close()

@@ -49,6 +49,8 @@ _PROTOS = [
     ("eimp_capture_end", C.c_int, [_vp]),
     ("eimp_graph_launch", C.c_int, [_vp]),
     ("eimp_phase_reserve", C.c_int, [_vp, C.POINTER(EimpPhaseParams), _sz, _sz]),
+    ("eimp_set_launch_shape", C.c_int, [_vp, C.c_int, C.c_int]),
+    ("eimp_get_launch_shape", C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
     ("eimp_gpu_initialize", _i32, [_vp, _sz, _sz, _sz, _sz, _sz, _sz, _vp]),
     ("eimp_gpu_block_size", _sz, [_vp]),
     ("eimp_gpu_run_cref_pbwt", _i32, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),

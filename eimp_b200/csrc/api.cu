@@ -56,6 +56,8 @@ struct eimp_ctx {
     std::string err;
     uint64_t launches = 0;
     DBuf status;
+    // launch shapes (eimp_set_launch_shape)
+    int shape_dos_span = 8, shape_smm_warps = SMMC_WARPS, shape_beam_pct = 100;
 
     // GPUEngine drop-in
     size_t g_K = 0, g_Kwords = 0, g_M = 0, g_Ncorr = 0, g_NAD = 0, g_refTcap = 0;
@@ -283,6 +285,36 @@ int eimp_graph_launch(eimp_ctx *ctx) {
 
 void *eimp_stream(eimp_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
+int eimp_set_launch_shape(eimp_ctx *ctx, int knob, int value) {
+    if (!ctx) return EIMP_E_ARG;
+    switch (knob) {
+    case EIMP_SHAPE_DOSAGE_SPAN:
+        if (value != 4 && value != 8 && value != 16) return fail(ctx, EIMP_E_ARG, "dosage span: 4, 8 or 16 tiles");
+        ctx->shape_dos_span = value;
+        return 0;
+    case EIMP_SHAPE_SMM_WARPS:
+        if (value != 1 && value != 2 && value != 4) return fail(ctx, EIMP_E_ARG, "match-search warps per CTA: 1, 2 or 4");
+        ctx->shape_smm_warps = value;
+        return 0;
+    case EIMP_SHAPE_BEAM_SLOTS_PCT:
+        if (value < 1 || value > 100) return fail(ctx, EIMP_E_ARG, "beam slots: 1..100 % of the resident warps");
+        ctx->shape_beam_pct = value;
+        return 0;
+    default:
+        return fail(ctx, EIMP_E_ARG, "unknown launch-shape knob");
+    }
+}
+
+int eimp_get_launch_shape(const eimp_ctx *ctx, int knob, int *value) {
+    if (!ctx || !value) return EIMP_E_ARG;
+    switch (knob) {
+    case EIMP_SHAPE_DOSAGE_SPAN: *value = ctx->shape_dos_span; return 0;
+    case EIMP_SHAPE_SMM_WARPS: *value = ctx->shape_smm_warps; return 0;
+    case EIMP_SHAPE_BEAM_SLOTS_PCT: *value = ctx->shape_beam_pct; return 0;
+    default: return EIMP_E_ARG;
+    }
+}
+
 // ------------------------------------------------------------------ imputation
 
 int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const uint64_t *d_sitemajor_full,
@@ -438,7 +470,7 @@ int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phase
     LAUNCH(launch_smm(ctx->i_compr.as<uint32_t>(), ctx->i_count0.as<int32_t>(), (int)M, (int)ctx->i_K,
                       ctx->i_phased.as<uint64_t>(), (int)wM, ctx->i_gt.as<uint8_t>(), (int)nsearch, hapmap,
                       setmaxerrors, ctx->i_matches.as<int4>(), (int)cap, ctx->i_nmatch.as<int>(),
-                      ctx->status.as<uint32_t>(), ctx->stream));
+                      ctx->status.as<uint32_t>(), ctx->shape_smm_warps, ctx->stream));
     ctx->launches++;   // launch_smm launches twice: the small node pool, then the retry pass
     return 0;
 }
@@ -474,7 +506,8 @@ int eimp_imp_bunch_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, uint64_t
                          ctx->i_refhap_samples ? ctx->i_refmap.as<int32_t>() : nullptr, ctx->i_hapfull.as<uint64_t>(),
                          (int)eimp_W(ctx->i_Mref), ctx->i_sinfo.as<int2>(), ctx->i_phased.as<uint64_t>(), (int)eimp_W(M),
                          ctx->i_gt.as<uint8_t>(), (int)M, (int)nimp, hapmap, (int)mref_begin, (int)nsites,
-                         ctx->i_imputeCalls, d_dos, (int)ldd, d_bits, (int)ldb_words, ctx->stream));
+                         ctx->i_imputeCalls, d_dos, (int)ldd, d_bits, (int)ldb_words, ctx->shape_dos_span,
+                         ctx->stream));
     return 0;
 }
 
@@ -969,7 +1002,7 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
     std::vector<int64_t> ro;
     if (int r = run_cref_pbwt(ctx, K, ntgt, d_gt, ro)) return r;
     const size_t ab = beam_arena_bytes(bp, (int)M);
-    const int slots = beam_slots(bp, (int)M, (int)ntgt);
+    const int slots = beam_slots(bp, (int)M, (int)ntgt, ctx->shape_beam_pct);
     if (slots < 1) return fail(ctx, EIMP_E_CUDA, "beam launch shape: occupancy query failed");
     CK(ctx->b_arena.reserve((size_t)slots * ab));
     CK(ctx->b_order.reserve(ntgt * sizeof(int32_t)));
@@ -1021,7 +1054,7 @@ int eimp_phase_reserve(eimp_ctx *ctx, const eimp_phase_params *p, size_t max_tar
     CK(ctx->b_cref.reserve(max_rows * eimp_W(K) * 8));
     CK(ctx->b_count0.reserve(max_rows * 4));
     CK(ctx->b_pbwt.reserve(2 * max_rows * eimp_kw(K) * 4));
-    const int slots = beam_slots(bp, (int)M, (int)n);
+    const int slots = beam_slots(bp, (int)M, (int)n);   // the most any launch shape takes
     if (slots < 1) return fail(ctx, EIMP_E_CUDA, "beam launch shape: occupancy query failed");
     CK(ctx->b_arena.reserve((size_t)slots * beam_arena_bytes(bp, (int)M)));
     CK(ctx->b_order.reserve(n * sizeof(int32_t)));

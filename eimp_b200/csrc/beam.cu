@@ -1483,7 +1483,7 @@ static size_t beam_smem(const BeamParams &p, const ArenaLayout &al) {
     return (sizeof(WS) + beam_rows_bytes(p.K) + beam_canon_bytes(al.NH)) * BEAM_WARPS;
 }
 
-int beam_slots(const BeamParams &p, int M, int ntgt) {
+int beam_slots(const BeamParams &p, int M, int ntgt, int pct) {
     const ArenaLayout al = arena_layout(p, M);
     const size_t sm = beam_smem(p, al);
     int dev = 0, nsm = 0, per = 0;
@@ -1492,7 +1492,8 @@ int beam_slots(const BeamParams &p, int M, int ntgt) {
     if (cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, beam_kernel, 32 * BEAM_WARPS, sm) != cudaSuccess || per < 1)
         return -1;
-    const int ctas = per * nsm;
+    int ctas = (int)((long)per * nsm * (pct < 1 ? 1 : pct > 100 ? 100 : pct) / 100);
+    if (ctas < 1) ctas = 1;
     const int need = (ntgt + BEAM_WARPS - 1) / BEAM_WARPS;
     return (need < ctas ? need : ctas) * BEAM_WARPS;
 }

@@ -580,7 +580,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
 // TargetImp.cpp:522-531 (float maf * Nrefhaps < 0.01 * height, evaluated
 // once per site instead of once per match) | (af > 0.5) << 31.
 // ---------------------------------------------------------------------------
-constexpr int DOS_SPAN = 8;
+constexpr int DOS_SPAN = 8;   // default tiles per warp (eimp_set_launch_shape: 4, 8 or 16)
 
 // uint64 -> double without the conversion unit: exact for x < 2^52 (the bits
 // of 2^52 + x as a double, minus 2^52)
@@ -659,7 +659,7 @@ __device__ __forceinline__ void dos_word(const uint64_t *__restrict__ hr, int w0
 // haplotypes imputed (PBWTImputer.cpp:130, 202); refmap (null: identity):
 // the panel haplotype of each haplotype of the reduced reference PBWT whose
 // prefix arrays absperm holds (TargetImp.cpp:536, haploidsRefMap)
-template <bool WIDE>
+template <bool WIDE, int SPAN>
 __global__ void __launch_bounds__(256, 4) dosage_kernel(
     const int4 *__restrict__ matches, int cap, const int *__restrict__ nmatch,
     const int32_t *__restrict__ absperm, int K, const int32_t *__restrict__ refmap,
@@ -671,11 +671,11 @@ __global__ void __launch_bounds__(256, 4) dosage_kernel(
     const int lane = threadIdx.x & 31;
     const long gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int ntiles = (nsites + 63) / 64;
-    const int nspans = (ntiles + DOS_SPAN - 1) / DOS_SPAN;
+    const int nspans = (ntiles + SPAN - 1) / SPAN;
     const int hi = (int)(gw / nspans);
     if (hi >= nhaps) return;
     const int hap = hapmap ? hapmap[hi] : hi;
-    const int t0 = (int)(gw % nspans) * DOS_SPAN, t1 = min(ntiles, t0 + DOS_SPAN);
+    const int t0 = (int)(gw % nspans) * SPAN, t1 = min(ntiles, t0 + SPAN);
     const int end = mref_begin + nsites;
     const uint8_t *g = gt + (size_t)(hap >> 1) * M;
     const uint64_t *hw = phased + (size_t)hap * wM;
@@ -907,12 +907,21 @@ static cudaError_t smm_launch(Kern kern, int warps, const uint32_t *compr, const
 
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
                        const uint8_t *gt, int nhaps, const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap,
-                       int *nmatch, uint32_t *status, cudaStream_t st) {
+                       int *nmatch, uint32_t *status, int warps, cudaStream_t st) {
     cudaError_t e;
-    if (M < 65536) {   // depths fit the compact tree
-        e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false>, SMMC_WARPS,
-                                                compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
-                                                matches, cap, nmatch, status, st);
+    if (M < 65536) {   // depths fit the compact tree; warps per CTA of the first pass: 1, 2 or 4
+        if (warps == 1)
+            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, 1, false>, 1, compr, count0, M, K,
+                                                    phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
+                                                    status, st);
+        else if (warps == 4)
+            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, 4, false>, 4, compr, count0, M, K,
+                                                    phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
+                                                    status, st);
+        else
+            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false>, SMMC_WARPS,
+                                                    compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
+                                                    matches, cap, nmatch, status, st);
         if (e != cudaSuccess) return e;
         return smm_launch<SmmWarpSmemC<SMM_NODES_RETRY>>(smm_compact_kernel<SMM_NODES_RETRY, 1, true>, 1, compr,
                                                          count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
@@ -927,15 +936,24 @@ cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int 
                                                     status, st);
 }
 
+template <int SPAN>
+static void *dosage_kernel_for(bool wide) {
+    return wide ? (void *)dosage_kernel<true, SPAN> : (void *)dosage_kernel<false, SPAN>;
+}
+
 cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,
                           const int32_t *refmap, const uint64_t *hapmajor_full, int wMref, const int2 *sinfo,
                           const uint64_t *phased, int wM, const uint8_t *gt, int M, int nhaps, const int32_t *hapmap,
                           int mref_begin, int nsites, int imputeCalls, float *dos, int ldd, uint64_t *bits, int ldb,
-                          cudaStream_t st) {
+                          int span, cudaStream_t st) {
+    if (span != 4 && span != 16) span = DOS_SPAN;
     const long ntiles = (nsites + 63) / 64;
-    long warps = (long)nhaps * ((ntiles + DOS_SPAN - 1) / DOS_SPAN);
+    long warps = (long)nhaps * ((ntiles + span - 1) / span);
     long blocks = (warps + 7) / 8;
-    auto kern = M < 131071 ? dosage_kernel<false> : dosage_kernel<true>;
+    const bool wide = M >= 131071;
+    using Kern = decltype(&dosage_kernel<false, DOS_SPAN>);
+    const Kern kern = (Kern)(span == 4 ? dosage_kernel_for<4>(wide)
+                                       : span == 16 ? dosage_kernel_for<16>(wide) : dosage_kernel_for<DOS_SPAN>(wide));
     kern<<<(unsigned)blocks, 256, 0, st>>>(matches, cap, nmatch, absperm, K, refmap, hapmajor_full, wMref, sinfo,
                                            phased, wM, gt, M, nhaps, hapmap, mref_begin, nsites, imputeCalls, dos, ldd,
                                            bits, ldb);

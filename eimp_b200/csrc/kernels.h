@@ -30,14 +30,14 @@ cudaError_t launch_gather_rows(const uint64_t *src, size_t ldsrc, const int64_t 
 // outputs; its target = row / 2) of each of the nhaps haplotypes searched
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
                        const uint8_t *gt, int nhaps, const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap,
-                       int *nmatch, uint32_t *status, cudaStream_t st);
+                       int *nmatch, uint32_t *status, int warps, cudaStream_t st);
 // refmap (null: identity): panel haplotype of each PBWT haplotype (the
 // reduced reference without the haploid samples' placeholder columns)
 cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,
                           const int32_t *refmap, const uint64_t *hapmajor_full, int wMref, const int2 *sinfo,
                           const uint64_t *phased, int wM, const uint8_t *gt, int M, int nhaps, const int32_t *hapmap,
                           int mref_begin, int nsites, int imputeCalls, float *dos, int ldd, uint64_t *bits, int ldb,
-                          cudaStream_t st);
+                          int span, cudaStream_t st);
 // segment map of the typed sites over the reference sites, plus the dosage
 // kernel's per-site pair (segment | typed << 31, shortcut height | af>0.5 << 31)
 cudaError_t launch_segmap(const int64_t *typed, int M, int Mref, const float *af, int nrefhaps_total, int32_t *segm,
@@ -115,7 +115,7 @@ struct BeamParams {
 size_t beam_arena_bytes(const BeamParams &p, int S_max);
 // warps of the persistent beam launch for ntgt targets (a multiple of the
 // warps per CTA; at most the resident ones), -1 on a CUDA error
-int beam_slots(const BeamParams &p, int M, int ntgt);
+int beam_slots(const BeamParams &p, int M, int ntgt, int pct = 100);
 // the persistent beam: slots warps (beam_slots), one arena of arena_bytes per
 // slot; order (ntgt ints) and workq (one int) are scratch: the longest-first
 // order and the queue counter, both filled here

@@ -211,6 +211,17 @@ int eimp_phase_set_haploid_ref(eimp_ctx *ctx, size_t nsamples, const uint8_t *ha
  * target.").  ntgt = 0 goes back to all diploid. */
 int eimp_phase_haploid_targets(eimp_ctx *ctx, size_t ntgt, const uint8_t *haploid);
 
+/* Launch shapes (no counterpart in the reference; the results do not depend
+ * on them), per context, for the autotuner (eimp_b200/autotune.py):
+ *   EIMP_SHAPE_DOSAGE_SPAN     64-site tiles per warp of the dosage kernel: 4, 8 [default] or 16
+ *   EIMP_SHAPE_SMM_WARPS       warps (target haplotypes) per CTA of the match search: 1, 2 [default] or 4
+ *   EIMP_SHAPE_BEAM_SLOTS_PCT  warps of the persistent beam launch, in % of the warps that can be
+ *                              resident at once: 1..100 [default 100]
+ * A value outside these returns EIMP_E_ARG and changes nothing. */
+enum { EIMP_SHAPE_DOSAGE_SPAN = 0, EIMP_SHAPE_SMM_WARPS = 1, EIMP_SHAPE_BEAM_SLOTS_PCT = 2 };
+int eimp_set_launch_shape(eimp_ctx *ctx, int knob, int value);
+int eimp_get_launch_shape(const eimp_ctx *ctx, int knob, int *value);
+
 /* Capacity mode for phasing (no counterpart in the reference): reserves the
  * batch buffers for up to max_targets targets and max_rows condensed rows
  * (sum over the targets of 2*S_t+1).  Afterwards the row offsets are computed

@@ -82,7 +82,7 @@ int main(int argc, char **argv) {
                 blockIdx.x = (unsigned)gw;
                 blockDim.x = 32;
                 emu_warp = &warp;
-                (M < 131071 ? eimp::dosage_kernel<false> : eimp::dosage_kernel<true>)(
+                (M < 131071 ? eimp::dosage_kernel<false, eimp::DOS_SPAN> : eimp::dosage_kernel<true, eimp::DOS_SPAN>)(
                     matches.data(), cap, nmatch.data(), absperm.data(), K, nullptr, hapfull.data(), wMref,
                     sinfo.data(), phased.data(), wM, gt.data(), M, nhaps, nullptr, mref_begin, nsites, impcalls,
                     dos.data(), nsites, bits.data(), ldb);
