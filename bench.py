@@ -557,9 +557,9 @@ def main():
     beam_ms = st_ms["beam"]
     achieved = st_by["beam"] / (beam_ms / 1e3) / 1e9
     # DRAM bytes of the beam kernel from an ncu capture of a 64-target cfg2
-    # launch (158.3 MB read + 13.1 MB written), scaled by condensed rows (the
-    # PBWT rows the kernel streams): 64 targets there had 69,584 rows
-    traffic = 171.3e6 * rows_total / 69584.0
+    # launch (160.9 MB read + 14.5 MB written), scaled by condensed rows (the
+    # PBWT rows the kernel streams): those 64 targets have 71,310 rows
+    traffic = 175.5e6 * rows_total / 71310.0
     roofline = {"kernel": "beam_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": st_by["beam"], "avg_launch_ms": beam_ms,
