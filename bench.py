@@ -489,10 +489,8 @@ def main():
     # launch shapes tuned on every group's own data (eimp_b200/autotune.py)
     tuning = None
     if not args.no_autotune:
-        from eimp_b200.autotune import tune_group, tune_step
-        tuning = {"groups": [tune_group(g) for g in groups]}
-        if len(groups) > 1:   # the beam's share of the SMs with every group running
-            tuning["step_beam_slots_pct"] = tune_step(groups)
+        from eimp_b200.autotune import tune_group
+        tuning = [tune_group(g) for g in groups]
 
     def step_timed(graphs=False):
         e0, e1 = ev(), ev()

@@ -81,34 +81,3 @@ def tune_group(group, reps: int = 2, knobs=("dosage_span", "smm_warps", "beam_sl
     group.enqueue()
     group.ctx.synchronize()
     return out
-
-
-def tune_step(groups, reps: int = 1, values=(100, 75, 50)) -> dict:
-    """Tunes the persistent beam's share of the resident warps over the whole
-    step, all groups running together: a beam that leaves some of every SM
-    free lets the other groups' kernels run beside it, which a group timed
-    alone cannot show.  Sets the fastest value on every group; returns
-    {"chosen": value, "ms": {value: best step ms}}."""
-    import torch
-    from .batch import enqueue_step
-    dev_stream = torch.cuda.current_stream()
-    times = {}
-    for v in values:
-        for g in groups:
-            set_shape(g, "beam_slots_pct", v)
-        best = float("inf")
-        for _ in range(reps):
-            for g in groups:
-                g.ctx.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(dev_stream)
-            for e in enqueue_step(groups, e0):
-                dev_stream.wait_event(e)
-            e1.record(dev_stream)
-            torch.cuda.synchronize()
-            best = min(best, e0.elapsed_time(e1))
-        times[v] = best
-    chosen = min(times, key=times.get)
-    for g in groups:
-        set_shape(g, "beam_slots_pct", chosen)
-    return {"chosen": chosen, "ms": {str(v): round(t, 1) for v, t in times.items()}}

@@ -471,7 +471,7 @@ int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phase
                       ctx->i_phased.as<uint64_t>(), (int)wM, ctx->i_gt.as<uint8_t>(), (int)nsearch, hapmap,
                       setmaxerrors, ctx->i_matches.as<int4>(), (int)cap, ctx->i_nmatch.as<int>(),
                       ctx->status.as<uint32_t>(), ctx->shape_smm_warps, ctx->stream));
-    ctx->launches += 2;   // launch_smm launches three times: the small node pool, then two retry passes
+    ctx->launches++;   // launch_smm launches twice: the small node pool, then the retry pass
     return 0;
 }
 

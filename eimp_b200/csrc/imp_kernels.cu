@@ -184,22 +184,17 @@ __device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x &
 // large pool too is an error (EIMP_ERR_NODE_OVERFLOW).  set-maximal errors
 // make the trees grow: on a 5000-haplotype panel at 2000 sites the largest
 // trees held 148, 718, 1733 and 3093 nodes at 0, 1, 2 and 3 errors.
-// A middle launch with 1024-node pools (two warps per CTA) takes the trees
-// that outgrow the first pool, and only those that outgrow it too go to the
-// last launch with 4096-node pools (one warp per CTA): at 20,000 reference
-// haplotypes and 32,000 typed sites the overflows of the first pool are
-// common enough that redoing all of them at one warp per CTA costs time.
 constexpr int SMM_RETRY = -2;
-__device__ __forceinline__ void smm_finish(int lane, uint32_t err, bool last_pass, int nres, int *nmatch, int hap,
+__device__ __forceinline__ void smm_finish(int lane, uint32_t err, bool retry_pass, int nres, int *nmatch, int hap,
                                            uint32_t *status) {
     if (lane) return;
     if (!err) { nmatch[hap] = nres; return; }
-    if (!last_pass && err == EIMP_ERR_NODE_OVERFLOW) { nmatch[hap] = SMM_RETRY; return; }
+    if (!retry_pass && err == EIMP_ERR_NODE_OVERFLOW) { nmatch[hap] = SMM_RETRY; return; }
     nmatch[hap] = -1;
     atomicOr(status, err);
 }
 
-template <int NODES, int WARPS, bool RETRY, bool LAST>
+template <int NODES, int WARPS, bool RETRY>
 __global__ void __launch_bounds__(WARPS * 32) smm_kernel(
     const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
     const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
@@ -356,7 +351,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_kernel(
         td = md;
     }
     for (int o = 16; o; o >>= 1) err |= __shfl_xor_sync(FULL, err, o);
-    smm_finish(lane, err, LAST, nres, nmatch, hap, status);
+    smm_finish(lane, err, RETRY, nres, nmatch, hap, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -390,7 +385,7 @@ __device__ __forceinline__ unsigned dps_make(int depth, int parent, int side) {
     return (unsigned)depth | ((unsigned)(parent + 1) << 16) | ((unsigned)side << 31);
 }
 
-template <int NODES, int WARPS, bool RETRY, bool LAST>
+template <int NODES, int WARPS, bool RETRY>
 __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
     const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
     const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
@@ -553,7 +548,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
         td = md;
     }
     for (int o = 16; o; o >>= 1) err |= __shfl_xor_sync(FULL, err, o);
-    smm_finish(lane, err, LAST, nres, nmatch, hap, status);
+    smm_finish(lane, err, RETRY, nres, nmatch, hap, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -916,35 +911,27 @@ cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int 
     cudaError_t e;
     if (M < 65536) {   // depths fit the compact tree; warps per CTA of the first pass: 1, 2 or 4
         if (warps == 1)
-            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, 1, false, false>, 1, compr, count0,
-                                                    M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap,
-                                                    nmatch, status, st);
+            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, 1, false>, 1, compr, count0, M, K,
+                                                    phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
+                                                    status, st);
         else if (warps == 4)
-            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, 4, false, false>, 4, compr, count0,
-                                                    M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap,
-                                                    nmatch, status, st);
+            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, 4, false>, 4, compr, count0, M, K,
+                                                    phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
+                                                    status, st);
         else
-            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false, false>,
-                                                    SMMC_WARPS, compr, count0, M, K, phased, wM, gt, nhaps, hapmap,
-                                                    setmaxerrors, matches, cap, nmatch, status, st);
+            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false>, SMMC_WARPS,
+                                                    compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
+                                                    matches, cap, nmatch, status, st);
         if (e != cudaSuccess) return e;
-        e = smm_launch<SmmWarpSmemC<SMM_NODES_MID>>(smm_compact_kernel<SMM_NODES_MID, 2, true, false>, 2, compr,
-                                                    count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches,
-                                                    cap, nmatch, status, st);
-        if (e != cudaSuccess) return e;
-        return smm_launch<SmmWarpSmemC<SMM_NODES_RETRY>>(smm_compact_kernel<SMM_NODES_RETRY, 1, true, true>, 1, compr,
+        return smm_launch<SmmWarpSmemC<SMM_NODES_RETRY>>(smm_compact_kernel<SMM_NODES_RETRY, 1, true>, 1, compr,
                                                          count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
                                                          matches, cap, nmatch, status, st);
     }
-    e = smm_launch<SmmWarpSmem<SMM_NODES>>(smm_kernel<SMM_NODES, SMM_WARPS, false, false>, SMM_WARPS, compr, count0, M,
-                                           K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status,
+    e = smm_launch<SmmWarpSmem<SMM_NODES>>(smm_kernel<SMM_NODES, SMM_WARPS, false>, SMM_WARPS, compr, count0, M, K,
+                                           phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status,
                                            st);
     if (e != cudaSuccess) return e;
-    e = smm_launch<SmmWarpSmem<SMM_NODES_MID>>(smm_kernel<SMM_NODES_MID, 2, true, false>, 2, compr, count0, M, K,
-                                               phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
-                                               status, st);
-    if (e != cudaSuccess) return e;
-    return smm_launch<SmmWarpSmem<SMM_NODES_RETRY>>(smm_kernel<SMM_NODES_RETRY, 1, true, true>, 1, compr, count0, M, K,
+    return smm_launch<SmmWarpSmem<SMM_NODES_RETRY>>(smm_kernel<SMM_NODES_RETRY, 1, true>, 1, compr, count0, M, K,
                                                     phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
                                                     status, st);
 }

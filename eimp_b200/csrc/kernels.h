@@ -11,7 +11,6 @@
 #define SMM_WARPS 4
 #define SMMC_WARPS 2
 #define SMM_NODES 512
-#define SMM_NODES_MID 1024
 #define SMM_NODES_RETRY 4096
 // beam phasing: warps (targets) per CTA
 #define BEAM_WARPS 4

@@ -59,16 +59,14 @@ int main(int argc, char **argv) {
     std::vector<int32_t> nmatch(nhaps, -7);
     uint32_t status = 0;
     int retried = 0;
-    // the launches of launch_smm: the small node pool, then the two retry passes
-    for (int pass = 0; pass < 3; pass++) {
-        const size_t smb = which ? (pass == 2 ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY>)
-                                    : pass == 1 ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_MID>)
-                                                : sizeof(eimp::SmmWarpSmemC<SMM_NODES>))
-                                 : (pass == 2 ? sizeof(eimp::SmmWarpSmem<SMM_NODES_RETRY>)
-                                    : pass == 1 ? sizeof(eimp::SmmWarpSmem<SMM_NODES_MID>)
-                                                : sizeof(eimp::SmmWarpSmem<SMM_NODES>));
+    // the launches of launch_smm: the small node pool, then the retry pass
+    for (int pass = 0; pass < 2; pass++) {
+        const size_t smb = which ? (pass ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY>)
+                                         : sizeof(eimp::SmmWarpSmemC<SMM_NODES>))
+                                 : (pass ? sizeof(eimp::SmmWarpSmem<SMM_NODES_RETRY>)
+                                         : sizeof(eimp::SmmWarpSmem<SMM_NODES>));
         for (int h = 0; h < nhaps; h++) {
-            if (pass == 1) retried += nmatch[h] == eimp::SMM_RETRY;
+            if (pass) retried += nmatch[h] == eimp::SMM_RETRY;
             // a fill pattern instead of zeros: the kernel must not read what it has not written
             uint8_t *smem = (uint8_t *)aligned_alloc(16, (smb + 15) / 16 * 16);
             memset(smem, 0x5A, smb);
@@ -80,12 +78,10 @@ int main(int argc, char **argv) {
                     blockIdx.x = h;
                     emu_warp = &warp;
                     emu_smem_ptr = smem;
-                    auto kern = which ? (pass == 2 ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, true>
-                                         : pass == 1 ? eimp::smm_compact_kernel<SMM_NODES_MID, 1, true, false>
-                                                     : eimp::smm_compact_kernel<SMM_NODES, 1, false, false>)
-                                      : (pass == 2 ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true, true>
-                                         : pass == 1 ? eimp::smm_kernel<SMM_NODES_MID, 1, true, false>
-                                                     : eimp::smm_kernel<SMM_NODES, 1, false, false>);
+                    auto kern = which ? (pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true>
+                                              : eimp::smm_compact_kernel<SMM_NODES, 1, false>)
+                                      : (pass ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true>
+                                              : eimp::smm_kernel<SMM_NODES, 1, false>);
                     kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
                          matches.data(), cap, nmatch.data(), &status);
                 });
