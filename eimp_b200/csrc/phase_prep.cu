@@ -42,32 +42,87 @@ __device__ __forceinline__ int block_exscan_bit(int pred, int *buf, int *total) 
 }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Hamming counts of GenotypeVector::compare_withPreInit (Datatypes.cpp:107-116)
+// for TB targets at once: nerr[t][h] = popc((is0_t & h) | (is2_t & ~h))
+// over the typed-site words.  A warp takes one reference haplotype at a time
+// and its lanes read the haplotype's row word by word (coalesced); every word
+// read serves the CTA's TB targets, whose genotype words sit in shared
+// memory (16 * TB * W(M) bytes), so the panel is read once per TB targets
+// instead of once per target.  TB is 8 where that fits the shared memory,
+// else 4, 2 or 1.  Excluded haplotypes (the target's own in iterations after the
+// first, haploid placeholders) get 0xffffffff: never selected.
+// ---------------------------------------------------------------------------
+constexpr int HAM_WARPS = 8;     // warps per CTA
+constexpr int HAM_HPW = 16;      // haplotypes per warp
+
+template <int HAM_TB>
+__global__ void __launch_bounds__(32 * HAM_WARPS) hamming_kernel(const uint8_t *__restrict__ gt, int ntgt, int M,
+                                                                 const uint64_t *__restrict__ hapmajor, int nhaps,
+                                                                 int wM, uint32_t *__restrict__ nerr, int self0,
+                                                                 const uint8_t *__restrict__ haploid) {
+    extern __shared__ uint64_t shm[];
+    uint64_t *is0 = shm, *is2 = shm + (size_t)HAM_TB * wM;   // [target][word]
+    const int tb = blockIdx.x * HAM_TB;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // genotype bit-planes of the CTA's targets, one 64-site word per warp
+    // step: two coalesced byte loads per lane and four ballots
+    for (int i = warp; i < HAM_TB * wM; i += HAM_WARPS) {
+        const int tt = i / wM, w = i - tt * wM, t = tb + tt;
+        uint32_t a[2], b[2];
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            const int m = w * 64 + half * 32 + lane;
+            const uint8_t c = (t < ntgt && m < M) ? gt[(size_t)t * M + m] : 1;   // 1 sets neither plane
+            a[half] = __ballot_sync(0xffffffffu, c == 0 || c == 3);
+            b[half] = __ballot_sync(0xffffffffu, c == 2 || c == 3);
+        }
+        if (lane == 0) {
+            is0[i] = a[0] | (uint64_t)a[1] << 32;
+            is2[i] = b[0] | (uint64_t)b[1] << 32;
+        }
+    }
+    __syncthreads();
+    const int h0 = (blockIdx.y * HAM_WARPS + warp) * HAM_HPW;
+    for (int k = 0; k < HAM_HPW; k++) {
+        const int h = h0 + k;
+        if (h >= nhaps) break;
+        const uint64_t *row = hapmajor + (size_t)h * wM;
+        uint32_t acc[HAM_TB];
+#pragma unroll
+        for (int q = 0; q < HAM_TB; q++) acc[q] = 0;
+        for (int w = lane; w < wM; w += 32) {
+            const uint64_t x = row[w];
+#pragma unroll
+            for (int q = 0; q < HAM_TB; q++)
+                acc[q] += __popcll((is0[q * wM + w] & x) | (is2[q * wM + w] & ~x));
+        }
+#pragma unroll
+        for (int q = 0; q < HAM_TB; q++)
+            for (int o = 16; o; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        if (lane < HAM_TB && tb + lane < ntgt) {
+            uint32_t v = acc[0];
+#pragma unroll
+            for (int q = 1; q < HAM_TB; q++) if (lane == q) v = acc[q];
+            const int t = tb + lane;
+            const int ign = self0 >= 0 ? 2 * (self0 + t) : -2;
+            const bool excl = h == ign || h == ign + 1 || (haploid && (h & 1) && haploid[h >> 1]);
+            nerr[(size_t)t * nhaps + h] = excl ? 0xffffffffu : v;
+        }
+    }
+}
+
 // haploid: per reference sample, 1 = haploid (null: all diploid).  The
 // second column of a haploid sample is never chosen (Target.cpp:800-806,
 // 830-838), nor are the target's own two in iterations after the first.
+// The error counts come from hamming_kernel.
 __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict__ gt, int M,
                                                       const uint64_t *__restrict__ hapmajor, int nhaps, int wM,
                                                       int K, uint32_t *__restrict__ nerr_scratch,
                                                       int32_t *__restrict__ besthaps, uint64_t *__restrict__ flags,
                                                       int wN, int self0, const uint8_t *__restrict__ haploid) {
-    extern __shared__ uint64_t sm[];
-    uint64_t *is0 = sm, *is2 = sm + wM;
     __shared__ int buf[32];
     const int t = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
-    const uint8_t *g = gt + (size_t)t * M;
-    for (int w = tid; w < wM; w += nt) {
-        uint64_t a = 0, b = 0;
-        for (int j = 0; j < 64; j++) {
-            int m = w * 64 + j;
-            if (m < M) {
-                uint8_t c = g[m];
-                if (c == 0 || c == 3) a |= 1ull << j;
-                if (c == 2 || c == 3) b |= 1ull << j;
-            }
-        }
-        is0[w] = a; is2[w] = b;
-    }
-    __syncthreads();
     uint32_t *nerr = nerr_scratch + (size_t)t * nhaps;
     int32_t *bh = besthaps + (size_t)t * K;
     uint64_t *fl = flags + (size_t)t * wN;
@@ -119,14 +174,6 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
         }
         return;
     }
-    for (int h = tid; h < nhaps; h += nt) {
-        const uint64_t *row = hapmajor + (size_t)h * wM;
-        uint32_t e = 0;
-        for (int w = 0; w < wM; w++) e += __popcll((is0[w] & row[w]) | (is2[w] & ~row[w]));
-        const bool excl = h == ign || h == ign + 1 || (haploid && (h & 1) && haploid[h >> 1]);
-        nerr[h] = excl ? 0xffffffffu : e;   // never selected
-    }
-    __syncthreads();
     // smallest threshold thr with #(nerr <= thr) >= K
     int lo = 0, hi = M;
     while (lo < hi) {
@@ -166,13 +213,28 @@ __global__ void __launch_bounds__(512) besthaps_kernel(const uint8_t *__restrict
 cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int nhaps, int wM, int K,
                             uint32_t *nerr_scratch, int32_t *besthaps, uint64_t *flags, int wN, int self0,
                             const uint8_t *haploid, cudaStream_t st) {
-    size_t sm = (size_t)2 * wM * sizeof(uint64_t);
-    if (sm > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(besthaps_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    // the Hamming counts are needed only when K leaves a choice (the kernel
+    // below takes every existing haplotype otherwise, without them)
+    const int excl = (self0 >= 0 ? 2 : 0);
+    if (haploid || K < nhaps - excl) {
+        int dev = 0, optin = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         if (e != cudaSuccess) return e;
+        const size_t per = (size_t)2 * wM * sizeof(uint64_t);   // one target's genotype words
+        const int tb = per * 8 <= (size_t)optin ? 8 : per * 4 <= (size_t)optin ? 4 : per * 2 <= (size_t)optin ? 2 : 1;
+        const size_t sm = per * tb;
+        auto kern = tb == 8 ? hamming_kernel<8> : tb == 4 ? hamming_kernel<4> : tb == 2 ? hamming_kernel<2>
+                                                                                        : hamming_kernel<1>;
+        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+            return e;
+        dim3 grid((unsigned)((ntgt + tb - 1) / tb),
+                  (unsigned)((nhaps + HAM_WARPS * HAM_HPW - 1) / (HAM_WARPS * HAM_HPW)));
+        kern<<<grid, 32 * HAM_WARPS, sm, st>>>(gt, ntgt, M, hapmajor, nhaps, wM, nerr_scratch, self0, haploid);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    besthaps_kernel<<<ntgt, 512, sm, st>>>(gt, M, hapmajor, nhaps, wM, K, nerr_scratch, besthaps, flags, wN, self0,
-                                           haploid);
+    besthaps_kernel<<<ntgt, 512, 0, st>>>(gt, M, hapmajor, nhaps, wM, K, nerr_scratch, besthaps, flags, wN, self0,
+                                          haploid);
     return cudaGetLastError();
 }
 
