@@ -94,7 +94,7 @@ struct eimp_ctx {
     size_t i_tgthap_n = 0, i_ntgthaps = 0;
     DBuf i_hapmap;
     DBuf i_hapfull, i_sitefull_tmp, i_af, i_typed, i_segm, i_common, i_sinfo, i_sitetyped_tmp, i_compr,
-        i_absperm, i_count0;
+        i_absperm, i_count0, i_rpscratch;
     // prepared targets
     size_t i_ntargets = 0;
     int i_imputeCalls = 0;
@@ -364,8 +364,11 @@ int eimp_imp_set_reference_dev(eimp_ctx *ctx, size_t Mref, size_t nhaps, const u
                                    ctx->i_sitetyped_c.as<uint64_t>(), (int)wK, st));
         typed_rows = ctx->i_sitetyped_c.as<uint64_t>();
     }
+    const size_t rps = refpbwt_scratch_bytes((int)K, (int)wK);
+    if (rps) CK(ctx->i_rpscratch.reserve(rps));
     LAUNCH(launch_refpbwt(typed_rows, (int)M, (int)K, (int)wK, ctx->i_compr.as<uint32_t>(),
-                          ctx->i_absperm.as<int32_t>(), ctx->i_count0.as<int32_t>(), st));
+                          ctx->i_absperm.as<int32_t>(), ctx->i_count0.as<int32_t>(),
+                          rps ? ctx->i_rpscratch.as<int32_t>() : nullptr, st));
     CK(cudaEventRecord(ctx->ref_ready, st));
     return 0;
 }

@@ -53,12 +53,134 @@ __device__ void block_exscan(int *a, int n, int *warpbuf, int *total) {
 }
 
 // ---------------------------------------------------------------------------
-// reference PBWT with prefix arrays.  One CTA sweeps the M sites in order;
-// absperm[m] is the order before site m, absperm[m+1] is written from it.
+// reference PBWT with prefix arrays, in two passes.
+//
+// The order before site m+1 is the order before site m, stably partitioned by
+// the haplotypes' bits at site m; so the order before site m+n is the order
+// before m stably sorted by the n-bit key (b[m+n-1] ... b[m+1] b[m]), the
+// last site most significant.  The checkpoint pass (one CTA) walks the sites
+// RP_BITS at a time with that 32-bucket stable sort and stores only the order
+// before every RP_CK-th site; the fill pass (one CTA per RP_CK sites) starts
+// from its checkpoint and steps site by site, writing every prefix array,
+// compressed row and zero count of its interval.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) refpbwt_kernel(const uint64_t *__restrict__ sitemajor, int M, int K,
-                                                      int wN, uint32_t *__restrict__ compr,
-                                                      int32_t *__restrict__ absperm, int32_t *__restrict__ count0) {
+constexpr int RP_CK = 64;     // sites between checkpoint orders
+constexpr int RP_BITS = 5;    // sites per step of the checkpoint pass: 32 buckets, one per lane
+
+// The orders (cur, nxt) and the step's keys live in shared memory, or in
+// global scratch (2K int32 + K bytes) when 'scratch' is given; the step's
+// site rows are staged in shared memory when 'stage_rows' is set.
+__global__ void __launch_bounds__(1024, 1) refpbwt_ckpt_kernel(const uint64_t *__restrict__ sitemajor, int M, int K,
+                                                               int wN, int32_t *__restrict__ absperm,
+                                                               int32_t *scratch, int stage_rows) {
+    extern __shared__ uint64_t rp_smem[];
+    int *hist = reinterpret_cast<int *>(rp_smem);   // [bucket][warp], 32 x 32
+    int *wsum = hist + 1024;                        // 32
+    uint64_t *rows = rp_smem + (1024 + 32) / 2;     // RP_BITS * wN when staged
+    char *tail = reinterpret_cast<char *>(rows + (stage_rows ? (size_t)RP_BITS * wN : 0));
+    int32_t *cur, *nxt;
+    uint8_t *keys;
+    if (scratch) {
+        cur = scratch; nxt = scratch + K; keys = reinterpret_cast<uint8_t *>(scratch + 2 * (size_t)K);
+    } else {
+        cur = reinterpret_cast<int32_t *>(tail); nxt = cur + K; keys = reinterpret_cast<uint8_t *>(nxt + K);
+    }
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int per = ((K + 1023) / 1024) * 32;   // elements per warp, a multiple of 32
+    const int lo = min(K, w * per), hi = min(K, lo + per);
+    if (M <= 0) {
+        for (int i = tid; i < K; i += 1024) absperm[i] = i;
+        return;
+    }
+    for (int i = tid; i < K; i += 1024) cur[i] = i;
+    __syncthreads();
+    for (int m = 0; m < M;) {
+        const int nb = min(RP_BITS, min(M - m, RP_CK - m % RP_CK));
+        if (m % RP_CK == 0) {
+            int32_t *out = absperm + (size_t)m * K;
+            for (int i = tid; i < K; i += 1024) out[i] = cur[i];
+        }
+        const uint64_t *rw = sitemajor + (size_t)m * wN;   // rows m .. m+nb-1 are contiguous
+        if (stage_rows) {
+            for (int i = tid; i < nb * wN; i += 1024) rows[i] = rw[i];
+            rw = rows;
+            __syncthreads();
+        }
+        // pass 1: keys and the per-warp bucket counts (lane b counts bucket b)
+        int cnt = 0;
+        for (int i0 = lo; i0 < hi; i0 += 32) {
+            const int i = i0 + lane;
+            const bool ok = i < hi;
+            int key = 0;
+            if (ok) {
+                const int h = cur[i];
+                for (int j = 0; j < nb; j++) key |= (int)((rw[(size_t)j * wN + (h >> 6)] >> (h & 63)) & 1) << j;
+                keys[i] = (uint8_t)key;
+            }
+            unsigned mine = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+            for (int j = 0; j < RP_BITS; j++) {
+                const unsigned bj = __ballot_sync(0xffffffffu, (key >> j) & 1);
+                mine &= ((lane >> j) & 1) ? bj : ~bj;
+            }
+            cnt += __popc(mine);
+        }
+        hist[lane * 32 + w] = cnt;
+        __syncthreads();
+        // exclusive scan, bucket-major: the next order holds bucket 0 of
+        // every warp (in warp order) first, then bucket 1, ...
+        {
+            const int v = hist[tid];
+            int x = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) wsum[w] = x;
+            __syncthreads();
+            if (w == 0) {
+                int z = wsum[lane];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, z, o);
+                    if (lane >= o) z += y;
+                }
+                wsum[lane] = z;
+            }
+            __syncthreads();
+            hist[tid] = x - v + (w ? wsum[w - 1] : 0);
+            __syncthreads();
+        }
+        // pass 2: stable scatter; hist[b][w] is warp w's next slot of bucket b
+        for (int i0 = lo; i0 < hi; i0 += 32) {
+            const int i = i0 + lane;
+            const bool ok = i < hi;
+            const int key = ok ? (int)keys[i] : 32 + lane;   // past the end: a bucket of its own
+            const unsigned same = __match_any_sync(0xffffffffu, key);
+            const int rank = __popc(same & ((1u << lane) - 1u));
+            int base = 0;
+            if (ok) {
+                base = hist[key * 32 + w];
+                nxt[base + rank] = cur[i];
+            }
+            __syncwarp();
+            if (ok && rank == 0) hist[key * 32 + w] = base + __popc(same);
+            __syncwarp();
+        }
+        __syncthreads();
+        int32_t *t = cur; cur = nxt; nxt = t;
+        m += nb;
+    }
+}
+
+// Fill pass: CTA c covers sites [c*RP_CK, min(M, (c+1)*RP_CK)); the order
+// before its first site is the checkpoint.  Per site: the bits in prefix
+// order (one ballot per 32 positions), the zeros per 32-position word and
+// their exclusive scan give the compressed row [data, cumulative zeros] and
+// the stable partition into the next order (PBWT.cpp:207-285).
+__global__ void __launch_bounds__(1024) refpbwt_fill_kernel(const uint64_t *__restrict__ sitemajor, int M, int K,
+                                                           int wN, uint32_t *__restrict__ compr,
+                                                           int32_t *__restrict__ absperm,
+                                                           int32_t *__restrict__ count0) {
     extern __shared__ uint8_t smem[];
     const int nwords = (K + 31) / 32;
     uint32_t *row = reinterpret_cast<uint32_t *>(smem);                  // 2*wN u32
@@ -68,10 +190,9 @@ __global__ void __launch_bounds__(1024) refpbwt_kernel(const uint64_t *__restric
     int *tot = warpbuf + 32;                                             // 1
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
     const size_t kw = 2 * (size_t)nwords;
+    const int m0 = blockIdx.x * RP_CK, m1 = min(M, m0 + RP_CK);
 
-    for (int i = tid; i < K; i += blockDim.x) absperm[i] = i;
-    __syncthreads();
-    for (int m = 0; m < M; m++) {
+    for (int m = m0; m < m1; m++) {
         const uint64_t *src = sitemajor + (size_t)m * wN;
         for (int w = tid; w < wN; w += blockDim.x) {
             uint64_t x = src[w];
@@ -81,6 +202,8 @@ __global__ void __launch_bounds__(1024) refpbwt_kernel(const uint64_t *__restric
         __syncthreads();
         const int32_t *perm = absperm + (size_t)m * K;
         int32_t *nperm = absperm + (size_t)(m + 1) * K;
+        // the order before the next checkpoint site exists already
+        const bool put = !((m + 1) % RP_CK == 0 && m + 1 < M);
         // pass 1: bits in prefix order, zeros per 32-position word
         for (int w = wid; w < nwords; w += nwarps) {
             int i = w * 32 + lane;
@@ -101,7 +224,7 @@ __global__ void __launch_bounds__(1024) refpbwt_kernel(const uint64_t *__restric
             int i = w * 32 + lane;
             uint32_t b = data[w];
             int zb = pz[w];
-            if (i < K) {
+            if (i < K && put) {
                 int h = perm[i];
                 uint32_t lt = (1u << lane) - 1u;
                 int dst = ((b >> lane) & 1) ? cnt0 + (w * 32 - zb) + __popc(b & lt) : zb + __popc(~b & lt);
@@ -862,17 +985,49 @@ __global__ void gather_rows_kernel(const uint64_t *__restrict__ src, size_t ldsr
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-size_t refpbwt_smem(int K, int wN) {
+static size_t refpbwt_fill_smem(int K, int wN) {
     int nwords = (K + 31) / 32;
     return (size_t)2 * wN * 4 + (size_t)nwords * 4 + (size_t)(nwords + 1) * 4 + 33 * 4;
 }
 
+// shared memory of the checkpoint pass: counts and scan sums, the staged
+// rows, and (without scratch) the two orders and the keys
+static size_t refpbwt_ckpt_smem(int K, int wN, bool stage_rows, bool in_smem) {
+    return (size_t)(1024 + 32) * 4 + (stage_rows ? (size_t)RP_BITS * wN * 8 : 0) +
+           (in_smem ? (size_t)K * 9 : 0);
+}
+
+static int optin_smem() {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return 0;
+    return v;
+}
+
+size_t refpbwt_scratch_bytes(int K, int wN) {
+    const size_t lim = (size_t)optin_smem();
+    return refpbwt_ckpt_smem(K, wN, true, true) <= lim ? 0 : (size_t)K * 9;
+}
+
 cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint32_t *compr, int32_t *absperm,
-                           int32_t *count0, cudaStream_t st) {
-    size_t sm = refpbwt_smem(K, wN);
-    cudaError_t e = cudaFuncSetAttribute(refpbwt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                           int32_t *count0, int32_t *scratch, cudaStream_t st) {
+    const size_t lim = (size_t)optin_smem();
+    const bool in_smem = refpbwt_ckpt_smem(K, wN, true, true) <= lim;
+    if (!in_smem && !scratch) return cudaErrorInvalidValue;
+    const bool stage = refpbwt_ckpt_smem(K, wN, true, in_smem) <= lim;
+    size_t sm = refpbwt_ckpt_smem(K, wN, stage, in_smem);
+    cudaError_t e = cudaFuncSetAttribute(refpbwt_ckpt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    refpbwt_kernel<<<1, 1024, sm, st>>>(sitemajor, M, K, wN, compr, absperm, count0);
+    refpbwt_ckpt_kernel<<<1, 1024, sm, st>>>(sitemajor, M, K, wN, absperm, in_smem ? nullptr : scratch,
+                                              stage ? 1 : 0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (M <= 0) return cudaSuccess;
+    sm = refpbwt_fill_smem(K, wN);
+    if ((e = cudaFuncSetAttribute(refpbwt_fill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) !=
+        cudaSuccess)
+        return e;
+    refpbwt_fill_kernel<<<(M + RP_CK - 1) / RP_CK, 1024, sm, st>>>(sitemajor, M, K, wN, compr, absperm, count0);
     return cudaGetLastError();
 }
 

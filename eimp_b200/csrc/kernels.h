@@ -18,9 +18,10 @@
 namespace eimp {
 
 // ---- imputation (imp_kernels.cu)
-size_t refpbwt_smem(int K, int wN);
+// global scratch launch_refpbwt needs (0: none) for K haplotypes
+size_t refpbwt_scratch_bytes(int K, int wN);
 cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint32_t *compr, int32_t *absperm,
-                           int32_t *count0, cudaStream_t st);
+                           int32_t *count0, int32_t *scratch, cudaStream_t st);
 cudaError_t launch_transpose(const uint64_t *src, size_t rows, size_t srcw, uint64_t *dst, size_t cols, size_t dstw,
                              cudaStream_t st);
 // dst row i (w words) = src row idx[i] (rows ldsrc words apart)

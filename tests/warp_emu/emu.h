@@ -2,7 +2,7 @@
 //
 // Compiles a kernel's CUDA C++ source as host C++ (with the sanitizers) and
 // runs each warp as 32 host threads.  Every warp collective (__syncwarp,
-// __ballot_sync, __any_sync, __shfl*_sync) meets at a barrier and records the
+// __ballot_sync, __any_sync, __match_any_sync, __shfl*_sync) meets at a barrier and records the
 // source line each lane called it from: lanes that reach different shuffles
 // or ballots (a divergent collective, undefined on the device) are counted in
 // emu_divergence; __syncwarp calls from different lines are reported but
@@ -136,7 +136,16 @@ template <class T> inline T emu_shfl_xor(int site, T v, int m) {
     emu_leave();
     return r;
 }
+inline unsigned emu_match_any(int site, uint64_t v) {
+    emu_enter(site, v, true);
+    unsigned r = 0;
+    const uint64_t mine = emu_warp->vals[emu_lane()];
+    for (int i = 0; i < 32; i++) if (emu_warp->vals[i] == mine) r |= 1u << i;
+    emu_leave();
+    return r;
+}
 #define __syncwarp(...) emu_syncwarp(__LINE__)
+#define __match_any_sync(m, v) emu_match_any(__LINE__, emu_bits(v))
 #define __ballot_sync(m, p) emu_ballot(__LINE__, (p))
 #define __any_sync(m, p) (emu_ballot(__LINE__, (p)) != 0u)
 #define __shfl_sync(m, v, s) emu_shfl(__LINE__, (v), (s))
