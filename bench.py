@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--cpu-sample-targets", type=int, default=0,
                     help="targets per group of the reference's CPU runs (0: the configuration's default)")
+    ap.add_argument("--cfg4-targets", type=int, default=1024,
+                    help="targets of the large-panel (cfg4) leg, one batch of its 50,000 (0: skip)")
+    ap.add_argument("--cfg4-steps", type=int, default=2, help="timed steps of the cfg4 leg")
     return ap.parse_args()
 
 
@@ -436,6 +439,135 @@ def profile_stages(groups, cfg, flush, stream_main):
         ms["smm"] += e[0].elapsed_time(e[1])
         ms["dosage"] += e[1].elapsed_time(e[2])
     return ms, by
+
+
+# ---------------------------------------------------------------- cfg4
+def cfg4_fp64(g, P, typed, nhap_sample=8, frac=0.01, seed=4):
+    """The cfg4 leg's FP32 dosages against the FP64 dosage oracle
+    (oracle/restate.py impute_fp64_sites) on a 1 % sample of the untyped
+    sites, for the first target haplotypes: their matches, the prefix-array
+    slices the covering matches need and the panel rows of the sampled sites
+    come from the device; the 16 GB of prefix arrays stay there."""
+    import torch
+    from oracle import restate as R
+    rng = np.random.default_rng(seed)
+    untyped = np.setdiff1d(np.arange(P.nsites), typed)
+    sites = np.sort(rng.choice(untyped, max(1, int(frac * P.nsites)), replace=False)).astype(np.int64)
+    d_sites = torch.from_numpy(sites).to(P.d_site.device)
+    rows = P.d_site[d_sites].cpu().numpy().view(np.uint64)
+    af = P.d_af.cpu().numpy()
+    nh = min(nhap_sample, 2 * g.nt)
+    dos = g.d_dos[:nh][:, d_sites].cpu().numpy()
+    cache = {}
+
+    def prefix_slice(en, rs, re):
+        k = (en, rs, re)
+        if k not in cache:
+            out = np.empty(re - rs + 1, np.int32)
+            g.ctx.check(g.L.eimp_imp_prefix_slice(g.h, en, rs, re, out.ctypes.data))
+            cache[k] = out.astype(np.int64)
+        return cache[k]
+
+    def site_bits(j, refs):
+        return (rows[j][refs >> 6] >> (refs & 63).astype(np.uint64)) & np.uint64(1)
+
+    err, bad, cov, conf_ok, t0 = 0.0, 0, 0, True, time.perf_counter()
+    for h in range(nh):
+        n = C.c_size_t(0)
+        g.ctx.check(g.L.eimp_imp_matches(g.h, h, None, 0, C.byref(n)))
+        m = np.zeros((n.value, 4), np.int32)
+        if n.value:
+            g.ctx.check(g.L.eimp_imp_matches(g.h, h, m.ctypes.data, n.value, C.byref(n)))
+        d64 = R.impute_fp64_sites(m, sites, typed, af, P.nhaps, prefix_slice, site_bits)
+        c = d64 >= 0
+        conf_ok = conf_ok and bool(np.all(dos[h][~c] == -1.0))
+        if c.any():
+            err = max(err, float(np.max(np.abs(dos[h][c].astype(np.float64) - d64[c]))))
+            bad += int(np.count_nonzero(dos[h][c] != d64[c].astype(np.float32)))
+            cov += int(c.sum())
+    return {"haplotypes": nh, "sites": int(sites.size), "sample": f"{frac:.0%} of the panel sites, untyped, seeded",
+            "covered": cov, "max_abs_err": err, "not_equal_to_rounded_fp64": bad,
+            "uncovered_marked_conflict": conf_ok, "prefix_slices": len(cache),
+            "check_s": round(time.perf_counter() - t0, 2)}
+
+
+def cfg4_leg(args, local, dev):
+    """The large panel (cfg4): 200,000 reference haplotypes x 1,000,000 sites
+    over 60 Mb (5,000 founders, 1/x SFS down to MAF 5e-6) generated and kept
+    on the device, 25 GB site-major; targets typed at 2 % (20,000 sites) with
+    1 % missing, K = 8,192, beam 128.  A step is one batch of the 50,000
+    targets: the imputation reference of the typed sites (the library's
+    haplotype-major copy of the panel, the 20,000 x 200,000 reference PBWT
+    with 16 GB of prefix arrays), phasing, matches and dosages at all
+    1,000,000 sites.  Device-resident (no host copies in the timed region)."""
+    import torch
+    from eimp_b200 import synth, synth_device
+    from eimp_b200.batch import DensityGroup
+    from eimp_b200.engine import Context, PhaseParams
+    cfg = synth.CONFIGS["cfg4"]
+    t0 = time.perf_counter()
+    gctx = Context(local)
+    P = synth_device.generate(cfg, local, gctx)
+    typed, gt = synth_device.targets(P, cfg.groups[0], args.cfg4_targets, seed=cfg.seed + 1)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    params = PhaseParams(K=cfg.K, beamwidth=cfg.beam)
+    g = DensityGroup(local, P.d_site, P.d_af, cfg.nhaps, typed, None, None, P.cm[typed].astype(np.float32), gt,
+                     params, batch_targets=args.cfg4_targets)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    g.enqueue()
+    g.ctx.synchronize()
+    times = []
+    for _ in range(max(1, args.cfg4_steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(g.stream)
+        g.enqueue()
+        e1.record(g.stream)
+        g.ctx.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.mean(times))
+    # a batch with the imputation reference already resident (the reference
+    # PBWT of the typed sites is built once for all 50,000 targets)
+    rtimes = []
+    for _ in range(max(1, args.cfg4_steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(g.stream)
+        g.phase()
+        g.impute()
+        e1.record(g.stream)
+        g.ctx.synchronize()
+        rtimes.append(e0.elapsed_time(e1))
+    ms_res = float(np.mean(rtimes))
+    free_b, tot_b = torch.cuda.mem_get_info(dev)
+    fp = cfg4_fp64(g, P, typed)
+    sms, sby = profile_stages([g], cfg, flush, torch.cuda.current_stream())
+    stages = {k: {"ms": sms[k], "algorithmic_bytes": sby[k], "achieved_gbs": sby[k] / (sms[k] / 1e3) / 1e9}
+              for k in sms if sms[k] > 0}
+    out = {"workload": f"cfg4: {cfg.nhaps} ref haps x {cfg.nsites} sites, {g.nt} of {cfg.groups[0].ntargets} "
+                       f"targets (one batch) at {g.M} typed sites, K={cfg.K}, beam={cfg.beam}",
+           "metric": METRIC, "unit": UNIT, "value": g.imputed() / (ms / 1e3), "ms_per_step": ms,
+           "steps": len(times), "targets": g.nt, "imputed_per_step": g.imputed(),
+           "phased_samples_per_sec": g.nt / (ms / 1e3), "generate_s": round(gen_s, 1),
+           "batch_ms_reference_resident": ms_res}
+    # the whole job: the reference built once, then every batch of the 50,000
+    ntj = cfg.groups[0].ntargets
+    job_s = (sms["refbuild"] + ntj / g.nt * ms_res) / 1e3
+    out.update({
+           "job_estimate": {"targets": ntj, "batches": -(-ntj // g.nt), "seconds": job_s,
+                            "value": g.imputed() / g.nt * ntj / job_s,
+                            "form": "reference build once + batches with the reference resident"},
+           "device_gb_in_use": round((tot_b - free_b) / 1e9, 1), "stages": stages, "fp64": fp,
+           "data": "synthetic, generated on the device (eimp_b200/synth_device.py)",
+           "l2": "flushed between timed steps (256 MiB write)"})
+    g.close()
+    gctx.close()
+    del P, g, flush
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------- our arm
@@ -848,6 +980,16 @@ def main():
             for s in samples:
                 s.close()
 
+    # ---- the large panel (cfg4) on the device, after everything above
+    cfg4 = None
+    if rank == 0 and world == 1 and args.cfg4_targets > 0 and args.config == CONFIG:
+        for g in groups:
+            g.close()
+        groups = []
+        del d_full, d_af
+        torch.cuda.empty_cache()
+        cfg4 = cfg4_leg(args, local, dev)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -857,7 +999,7 @@ def main():
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": int(launches), "phased_samples_per_sec": world * targets_total / (ms_per_step / 1e3),
                 "plain": plain, "serving": serving, "graph": graph, "qref_decode": qref, "parity": parity,
-                "autotune": tuning}
+                "autotune": tuning, "cfg4": cfg4}
         print(json.dumps(line), flush=True)
     for g in groups:
         g.close()

@@ -81,6 +81,8 @@ _PROTOS = [
     ("eimp_imp_site_stats_dev", _i32, [_vp, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _sz,
                                        _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("eimp_imp_refpbwt", _i32, [_vp, _vp, _vp]),
+    ("eimp_imp_prefix_slice", _i32, [_vp, _sz, _sz, _sz, _vp]),
+    ("eimp_transpose_bits_dev", _i32, [_vp, _vp, _sz, _sz, _vp, _sz, _sz]),
     ("eimp_besthaps_noalloc", _i32, [_vp, _sz, _sz, _vp, _vp, _sz, _sz, _vp, _vp]),
 ]
 

@@ -44,9 +44,8 @@ class DensityGroup:
     docstring).  ``d_full``/``d_af`` are the resident panel (site-major rows
     of W(nhaps) words, allele frequencies) shared by all groups."""
 
-    def __init__(self, device: int, d_full, d_af, nhaps: int, typed: np.ndarray, hapmajor_typed: np.ndarray,
-                 sitemajor_typed: np.ndarray, cm_typed: np.ndarray, gt: np.ndarray, params,
-                 batch_targets: int = 1024):
+    def __init__(self, device: int, d_full, d_af, nhaps: int, typed: np.ndarray, hapmajor_typed,
+                 sitemajor_typed, cm_typed: np.ndarray, gt: np.ndarray, params, batch_targets: int = 1024):
         import torch
         from .engine import Context, Phaser
         self.ctx = Context(device)
@@ -65,9 +64,18 @@ class DensityGroup:
         self.gt_host = gt
         self.nt = gt.shape[0]
         self.d_full, self.d_af = d_full, d_af
-        Phaser(self.ctx, hapmajor_typed, sitemajor_typed, cm_typed)   # phasing reference, resident
         self.d_typed = _dev_tensor(self.typed, self.dev)
-        self.d_sitetyped = _dev_tensor(sitemajor_typed, self.dev)
+        if hapmajor_typed is None:
+            # both references of the typed sites built on the device from the
+            # resident panel (no host copy of the typed views)
+            self.d_cm = _dev_tensor(np.asarray(cm_typed, np.float32), self.dev)
+            self.ctx.check(self.L.eimp_phase_set_reference_dev(self.h, self.M, nhaps, d_full.data_ptr(),
+                                                               int(d_full.shape[1]), self.d_typed.data_ptr(),
+                                                               self.d_cm.data_ptr()))
+            self.d_sitetyped = None
+        else:
+            Phaser(self.ctx, hapmajor_typed, sitemajor_typed, cm_typed)   # phasing reference, resident
+            self.d_sitetyped = _dev_tensor(sitemajor_typed, self.dev)
         self.d_gt = _dev_tensor(gt, self.dev)
         nt, wM, M, Mref = self.nt, self.wM, self.M, self.Mref
         i64, f32, i32 = torch.int64, torch.float32, torch.int32
@@ -98,7 +106,7 @@ class DensityGroup:
         context's side stream (overlapping the phasing that follows)."""
         self.ctx.check(self.L.eimp_imp_set_reference_dev(
             self.h, self.Mref, self.nhaps, self.d_full.data_ptr(), self.d_af.data_ptr(), self.M,
-            self.d_typed.data_ptr(), self.d_sitetyped.data_ptr()))
+            self.d_typed.data_ptr(), None if self.d_sitetyped is None else self.d_sitetyped.data_ptr()))
 
     def phase(self):
         import torch

@@ -778,6 +778,27 @@ int eimp_imp_refpbwt(eimp_ctx *ctx, uint32_t *compr, int32_t *absperm) {
     return 0;
 }
 
+int eimp_imp_prefix_slice(eimp_ctx *ctx, size_t site, size_t lo, size_t hi, int32_t *out) {
+    if (!ctx || !ctx->i_Mref) return fail(ctx, EIMP_E_ARG, "eimp_imp_prefix_slice: no reference set");
+    if (!out || site > ctx->i_M || lo > hi || hi >= ctx->i_K)
+        return fail(ctx, EIMP_E_ARG, "eimp_imp_prefix_slice: slice outside the prefix arrays");
+    if (int r = use_device(ctx)) return r;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ref_ready, 0));
+    CK(cudaMemcpyAsync(out, ctx->i_absperm.as<int32_t>() + site * ctx->i_K + lo, (hi - lo + 1) * 4,
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int eimp_transpose_bits_dev(eimp_ctx *ctx, const uint64_t *d_src, size_t rows, size_t src_ld, uint64_t *d_dst,
+                            size_t cols, size_t dst_ld) {
+    if (!ctx || !d_src || !d_dst || src_ld < (cols + 63) / 64 || dst_ld < (rows + 63) / 64 || (cols + 63) / 64 > 65535)
+        return fail(ctx, EIMP_E_ARG, "eimp_transpose_bits_dev: bad sizes");
+    if (int r = use_device(ctx)) return r;
+    LAUNCH(launch_transpose_ld(d_src, rows, src_ld, d_dst, cols, (rows + 63) / 64, dst_ld, ctx->stream));
+    return 0;
+}
+
 // --------------------------------------------------------------------- phasing
 
 int eimp_phase_set_reference(eimp_ctx *ctx, size_t M, size_t nhaps, const uint64_t *hapmajor,

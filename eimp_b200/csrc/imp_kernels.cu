@@ -241,24 +241,26 @@ __global__ void __launch_bounds__(1024) refpbwt_fill_kernel(const uint64_t *__re
 }
 
 // ---------------------------------------------------------------------------
-// bit-matrix transpose: src (rows x srcw words, 'cols' valid bits per row) ->
-// dst (cols x dstw words).  One 64x64 tile per block of 64 threads.
+// bit-matrix transpose: src (rows of src_ld words, 'cols' valid bits per row)
+// -> dst (cols rows of dst_ld words, of which the first dstw are written:
+// word w of dst row c holds bit c of src rows 64w .. 64w+63).  One 64x64 tile
+// per block of 64 threads; grid (ceil(rows/64), ceil(cols/64)).
 // ---------------------------------------------------------------------------
-__global__ void transpose_kernel(const uint64_t *__restrict__ src, size_t rows, size_t srcw,
-                                 uint64_t *__restrict__ dst, size_t cols, size_t dstw) {
+__global__ void transpose_kernel(const uint64_t *__restrict__ src, size_t rows, size_t src_ld,
+                                 uint64_t *__restrict__ dst, size_t cols, size_t dstw, size_t dst_ld) {
     __shared__ uint64_t tile[64];
     const size_t rw = blockIdx.x;      // 64-row block (source rows -> dest word)
     const size_t cw = blockIdx.y;      // source word (-> 64 dest rows)
     const int t = threadIdx.x;
     size_t r = rw * 64 + t;
-    tile[t] = (r < rows && cw < srcw) ? src[r * srcw + cw] : 0ull;
+    tile[t] = r < rows ? src[r * src_ld + cw] : 0ull;
     __syncthreads();
     size_t c = cw * 64 + t;
     if (c < cols && rw < dstw) {
         uint64_t o = 0;
 #pragma unroll 8
         for (int j = 0; j < 64; j++) o |= ((tile[j] >> t) & 1ull) << j;
-        dst[c * dstw + rw] = o;
+        dst[c * dst_ld + rw] = o;
     }
 }
 
@@ -1041,8 +1043,16 @@ cudaError_t launch_gather_rows(const uint64_t *src, size_t ldsrc, const int64_t 
 
 cudaError_t launch_transpose(const uint64_t *src, size_t rows, size_t srcw, uint64_t *dst, size_t cols, size_t dstw,
                              cudaStream_t st) {
-    dim3 grid((unsigned)((rows + 63) / 64), (unsigned)srcw);
-    transpose_kernel<<<grid, 64, 0, st>>>(src, rows, srcw, dst, cols, dstw);
+    return launch_transpose_ld(src, rows, srcw, dst, cols, dstw, dstw, st);
+}
+
+cudaError_t launch_transpose_ld(const uint64_t *src, size_t rows, size_t src_ld, uint64_t *dst, size_t cols,
+                                size_t dstw, size_t dst_ld, cudaStream_t st) {
+    if (!rows || !cols) return cudaSuccess;
+    const size_t gy = (cols + 63) / 64;
+    if (gy > 65535 || gy > src_ld) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)((rows + 63) / 64), (unsigned)gy);
+    transpose_kernel<<<grid, 64, 0, st>>>(src, rows, src_ld, dst, cols, dstw, dst_ld);
     return cudaGetLastError();
 }
 

@@ -24,6 +24,9 @@ cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint
                            int32_t *count0, int32_t *scratch, cudaStream_t st);
 cudaError_t launch_transpose(const uint64_t *src, size_t rows, size_t srcw, uint64_t *dst, size_t cols, size_t dstw,
                              cudaStream_t st);
+// the same with separate row strides; dstw words of each dst row are written
+cudaError_t launch_transpose_ld(const uint64_t *src, size_t rows, size_t src_ld, uint64_t *dst, size_t cols,
+                                size_t dstw, size_t dst_ld, cudaStream_t st);
 // dst row i (w words) = src row idx[i] (rows ldsrc words apart)
 cudaError_t launch_gather_rows(const uint64_t *src, size_t ldsrc, const int64_t *idx, int n, int w, uint64_t *dst,
                                cudaStream_t st);

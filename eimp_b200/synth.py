@@ -76,6 +76,9 @@ CONFIGS = {
     "cfg3": SynthConfig("cfg3", nhaps=20000, nsites=400000, segment_mb=40.0, founders=1000,
                         groups=(TargetGroup(3334, 0.01, 0.0, 0.05), TargetGroup(3333, 0.03, 0.0, 0.05),
                                 TargetGroup(3333, 0.08, 0.0, 0.05)), K=4096, beam=128, seed=1003),
+    # generated on the device only (eimp_b200/synth_device.py): 25 GB bit-packed
+    "cfg4": SynthConfig("cfg4", nhaps=200000, nsites=1000000, segment_mb=60.0, founders=5000,
+                        groups=(TargetGroup(50000, 0.02, 0.01, 0.01),), K=8192, beam=128, maf_min=5e-6, seed=1004),
 }
 
 

@@ -290,6 +290,21 @@ int eimp_imp_matches(eimp_ctx *ctx, size_t hap, int32_t *out, size_t cap, size_t
  * and prefix arrays ((M+1) x nhaps int32, PBWT::getSortOrder, PBWT.h:67). */
 int eimp_imp_refpbwt(eimp_ctx *ctx, uint32_t *compr, int32_t *absperm);
 
+/* gAbsPerm[site][lo..hi] (PBWT.h:67) of the reference PBWT, to the host
+ * (site <= M: the order before typed site 'site').  For checking dosages
+ * against an oracle on a sample without copying all (M+1) x K prefix
+ * entries. */
+int eimp_imp_prefix_slice(eimp_ctx *ctx, size_t site, size_t lo, size_t hi, int32_t *out);
+
+/* Bit-matrix transpose on the device (no counterpart in the reference, whose
+ * VCFData builds referenceT and reference while reading): d_src has 'rows'
+ * rows of src_ld 64-bit words holding 'cols' bits each (LSB first); row c of
+ * d_dst (stride dst_ld words) gets bit c of every source row, the first
+ * ceil(rows/64) words written.  cols <= 65535 * 64.  Enqueued on the
+ * context's stream. */
+int eimp_transpose_bits_dev(eimp_ctx *ctx, const uint64_t *d_src, size_t rows, size_t src_ld, uint64_t *d_dst,
+                            size_t cols, size_t dst_ld);
+
 /* Output statistics of an imputed bunch: the numeric part of
  * VCFData::writeVCFImputedBunch (VCFData.cpp:3068-3446), which main.cpp:454
  * calls after PBWTImputer::imputeBunch for every bunch.  Diploid targets.

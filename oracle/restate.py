@@ -276,3 +276,50 @@ def phase_many(gt, hapmajor, sitemajor, cm, params: PhaseParamsC, nthreads=8):
     if rc:
         raise RuntimeError(f"oracle phasing failed ({rc})")
     return mats, pats, dm, dp
+
+
+def impute_fp64_sites(matches, sites, typed, af_full, nrefhaps_total, prefix_slice, site_bits):
+    """FP64 dosage oracle on a sample of panel sites for one target haplotype:
+    TargetImp::imputeBunch (TargetImp.cpp:474-558; eo_impute in
+    eimp_oracle.c) with score and sum as exact integers and score/sum in
+    double, without the reference's final rounding to float.
+
+    matches: (n, 4) int [start, end, rs, re] in typed-site indices, in the
+    order the match search emits them (ascending end); sites: ascending
+    untyped panel sites; typed: the typed panel sites; af_full: float32 panel
+    allele frequencies; prefix_slice(en, rs, re) -> gAbsPerm[en][rs..re];
+    site_bits(j, refs) -> alleles (0/1) of reference haplotypes refs at
+    sites[j].  Returns float64 (len(sites),), -1 where no match covers the
+    site (DOSAGE_CONFLICT, :26)."""
+    matches = np.asarray(matches, np.int64).reshape(-1, 4)
+    starts, ends = matches[:, 0], matches[:, 1]
+    n = len(matches)
+    # the last typed site at or before each site (0 before the first)
+    currm = np.searchsorted(np.asarray(typed), np.asarray(sites), side="right") - 1
+    currm[currm < 0] = 0
+    out = np.empty(len(sites), np.float64)
+    n32 = np.float32(nrefhaps_total)
+    for j, (s, c) in enumerate(zip(sites, currm)):
+        i = int(np.searchsorted(ends, c, side="right"))     # first match with end > currm (:504-505)
+        if i >= n or starts[i] > c:
+            out[j] = -1.0
+            continue
+        af = np.float32(af_full[s])
+        maf = np.float32(np.float32(1.0) - af) if af > np.float32(0.5) else af
+        score = total = 0
+        while i < n and starts[i] <= c:
+            st, en, rs, re = (int(v) for v in matches[i])
+            single = (int(c) - st + 1) * (en - int(c))
+            height = re - rs + 1
+            # :526: float maf * (float)size_t vs double 0.01 * size_t
+            if float(np.float32(maf * n32)) < 0.01 * float(height):
+                total += height * single
+                if af > np.float32(0.5):
+                    score += height * single
+            else:
+                ones = int(np.count_nonzero(site_bits(j, prefix_slice(en, rs, re))))
+                total += height * single
+                score += ones * single
+            i += 1
+        out[j] = float(score) / float(total)
+    return out
