@@ -66,10 +66,14 @@ __device__ void block_exscan(int *a, int n, int *warpbuf, int *total) {
 // ---------------------------------------------------------------------------
 constexpr int RP_CK = 64;     // sites between checkpoint orders
 constexpr int RP_BITS = 5;    // sites per step of the checkpoint pass: 32 buckets, one per lane
+// rounds of 32 positions whose loads are issued together: 8 with the orders
+// in global memory (their latency overlapped), 1 in shared memory (fewer
+// registers and instructions measured faster there)
 
 // The orders (cur, nxt) and the step's keys live in shared memory, or in
 // global scratch (2K int32 + K bytes) when 'scratch' is given; the step's
 // site rows are staged in shared memory when 'stage_rows' is set.
+template <int RP_U>
 __global__ void __launch_bounds__(1024, 1) refpbwt_ckpt_kernel(const uint64_t *__restrict__ sitemajor, int M, int K,
                                                                int wN, int32_t *__restrict__ absperm,
                                                                int32_t *scratch, int stage_rows) {
@@ -106,24 +110,35 @@ __global__ void __launch_bounds__(1024, 1) refpbwt_ckpt_kernel(const uint64_t *_
             rw = rows;
             __syncthreads();
         }
-        // pass 1: keys and the per-warp bucket counts (lane b counts bucket b)
+        // pass 1: keys and the per-warp bucket counts (lane b counts bucket b);
+        // the orders of RP_U rounds are loaded before any is used, so that
+        // their latencies overlap when the orders are in global memory
         int cnt = 0;
-        for (int i0 = lo; i0 < hi; i0 += 32) {
-            const int i = i0 + lane;
-            const bool ok = i < hi;
-            int key = 0;
-            if (ok) {
-                const int h = cur[i];
-                for (int j = 0; j < nb; j++) key |= (int)((rw[(size_t)j * wN + (h >> 6)] >> (h & 63)) & 1) << j;
-                keys[i] = (uint8_t)key;
-            }
-            unsigned mine = __ballot_sync(0xffffffffu, ok);
+        for (int i00 = lo; i00 < hi; i00 += 32 * RP_U) {
+            int hv[RP_U];
 #pragma unroll
-            for (int j = 0; j < RP_BITS; j++) {
-                const unsigned bj = __ballot_sync(0xffffffffu, (key >> j) & 1);
-                mine &= ((lane >> j) & 1) ? bj : ~bj;
+            for (int u = 0; u < RP_U; u++) {
+                const int i = i00 + u * 32 + lane;
+                hv[u] = i < hi ? cur[i] : 0;
             }
-            cnt += __popc(mine);
+#pragma unroll
+            for (int u = 0; u < RP_U; u++) {
+                const int i = i00 + u * 32 + lane;
+                const bool ok = i < hi;
+                int key = 0;
+                if (ok) {
+                    const int h = hv[u];
+                    for (int j = 0; j < nb; j++) key |= (int)((rw[(size_t)j * wN + (h >> 6)] >> (h & 63)) & 1) << j;
+                    keys[i] = (uint8_t)key;
+                }
+                unsigned mine = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+                for (int j = 0; j < RP_BITS; j++) {
+                    const unsigned bj = __ballot_sync(0xffffffffu, (key >> j) & 1);
+                    mine &= ((lane >> j) & 1) ? bj : ~bj;
+                }
+                cnt += __popc(mine);
+            }
         }
         hist[lane * 32 + w] = cnt;
         __syncthreads();
@@ -150,21 +165,32 @@ __global__ void __launch_bounds__(1024, 1) refpbwt_ckpt_kernel(const uint64_t *_
             hist[tid] = x - v + (w ? wsum[w - 1] : 0);
             __syncthreads();
         }
-        // pass 2: stable scatter; hist[b][w] is warp w's next slot of bucket b
-        for (int i0 = lo; i0 < hi; i0 += 32) {
-            const int i = i0 + lane;
-            const bool ok = i < hi;
-            const int key = ok ? (int)keys[i] : 32 + lane;   // past the end: a bucket of its own
-            const unsigned same = __match_any_sync(0xffffffffu, key);
-            const int rank = __popc(same & ((1u << lane) - 1u));
-            int base = 0;
-            if (ok) {
-                base = hist[key * 32 + w];
-                nxt[base + rank] = cur[i];
+        // pass 2: stable scatter in round order; hist[b][w] is warp w's next
+        // slot of bucket b
+        for (int i00 = lo; i00 < hi; i00 += 32 * RP_U) {
+            int kv[RP_U], hv[RP_U];
+#pragma unroll
+            for (int u = 0; u < RP_U; u++) {
+                const int i = i00 + u * 32 + lane;
+                const bool ok = i < hi;
+                kv[u] = ok ? (int)keys[i] : 32 + lane;   // past the end: a bucket of its own
+                hv[u] = ok ? cur[i] : 0;
             }
-            __syncwarp();
-            if (ok && rank == 0) hist[key * 32 + w] = base + __popc(same);
-            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < RP_U; u++) {
+                const bool ok = i00 + u * 32 + lane < hi;
+                const int key = kv[u];
+                const unsigned same = __match_any_sync(0xffffffffu, key);
+                const int rank = __popc(same & ((1u << lane) - 1u));
+                int base = 0;
+                if (ok) {
+                    base = hist[key * 32 + w];
+                    nxt[base + rank] = hv[u];
+                }
+                __syncwarp();
+                if (ok && rank == 0) hist[key * 32 + w] = base + __popc(same);
+                __syncwarp();
+            }
         }
         __syncthreads();
         int32_t *t = cur; cur = nxt; nxt = t;
@@ -1019,10 +1045,10 @@ cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint
     if (!in_smem && !scratch) return cudaErrorInvalidValue;
     const bool stage = refpbwt_ckpt_smem(K, wN, true, in_smem) <= lim;
     size_t sm = refpbwt_ckpt_smem(K, wN, stage, in_smem);
-    cudaError_t e = cudaFuncSetAttribute(refpbwt_ckpt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    auto ck = in_smem ? refpbwt_ckpt_kernel<1> : refpbwt_ckpt_kernel<8>;
+    cudaError_t e = cudaFuncSetAttribute(ck, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    refpbwt_ckpt_kernel<<<1, 1024, sm, st>>>(sitemajor, M, K, wN, absperm, in_smem ? nullptr : scratch,
-                                              stage ? 1 : 0);
+    ck<<<1, 1024, sm, st>>>(sitemajor, M, K, wN, absperm, in_smem ? nullptr : scratch, stage ? 1 : 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (M <= 0) return cudaSuccess;
     sm = refpbwt_fill_smem(K, wN);

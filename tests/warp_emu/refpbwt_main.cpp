@@ -8,7 +8,9 @@
 // sitemajor.bin (M x wN words).  Outputs: o_compr.bin (M x 2*ceil(K/32)
 // uint32), o_absperm.bin ((M+1) x K int32), o_count0.bin (M int32).  The
 // orders live in the block's shared memory or in a global scratch buffer as
-// the flags say (the launcher picks by the shared-memory size).  Exit status
+// the flags say (the launcher picks by the shared-memory size), with one
+// round of loads in flight in shared memory and eight in global memory, as
+// the launcher runs them.  Exit status
 // 3: a divergent warp collective.
 #include "refpbwt_emu.cpp"
 
@@ -76,7 +78,8 @@ int main(int argc, char **argv) {
     const size_t ck_smem = (size_t)(1024 + 32) * 4 + (stage ? (size_t)eimp::RP_BITS * wN * 8 : 0) +
                            (in_smem ? (size_t)K * 9 : 0);
     run_blocks(1, 1024, ck_smem, [&] {
-        eimp::refpbwt_ckpt_kernel(sm.data(), M, K, wN, absperm.data(), in_smem ? nullptr : scratch.data(), stage);
+        if (in_smem) eimp::refpbwt_ckpt_kernel<1>(sm.data(), M, K, wN, absperm.data(), nullptr, stage);
+        else eimp::refpbwt_ckpt_kernel<8>(sm.data(), M, K, wN, absperm.data(), scratch.data(), stage);
     });
     const size_t fill_smem = (size_t)2 * wN * 4 + (size_t)nwords * 4 + (size_t)(nwords + 1) * 4 + 33 * 4;
     run_blocks((M + eimp::RP_CK - 1) / eimp::RP_CK, 1024, fill_smem, [&] {
