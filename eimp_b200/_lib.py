@@ -76,6 +76,7 @@ _PROTOS = [
     ("eimp_phase_start_phases", _i32, [_vp, _sz, _vp]),
     ("eimp_qref_index", _i32, [_vp, _sz, _sz, _sz, _vp]),
     ("eimp_qref_decode", _i32, [_vp, _vp, _sz, _sz, _sz, _vp, _sz, _vp]),
+    ("eimp_qref_decode_masked", _i32, [_vp, _vp, _sz, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _vp, _sz, _vp]),
     ("eimp_qref_decode_dev", _i32, [_vp, _vp, _vp, _sz, _sz, _vp, _sz]),
     ("eimp_imp_bunch_stats", _i32, [_vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("eimp_imp_site_stats_dev", _i32, [_vp, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _sz,

@@ -105,7 +105,7 @@ struct eimp_ctx {
     // phased dosages (eimp_imp_phased_dosages) and staging of the output statistics
     DBuf i_pdm, i_pdp, s_ads, s_gt, s_ds, s_gp, s_site, s_conf;
     // Qref haplotype section staging
-    DBuf q_sec, q_offs, q_out;
+    DBuf q_sec, q_offs, q_out, q_rows, q_mask, q_maskhap, q_kept, q_af;
     bool i_have_pdos = false;
 };
 
@@ -743,6 +743,79 @@ int eimp_qref_decode(eimp_ctx *ctx, const uint8_t *section, size_t nbytes, size_
             CK(cudaMemcpyAsync(host_out, dst, Mref * nw * 8, cudaMemcpyDeviceToHost, ctx->stream));
         } else {
             CK(cudaMemcpy2DAsync(host_out, nw * 8, dst, ldw_words * 8, nw * 8, Mref, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}
+
+int eimp_qref_decode_masked(eimp_ctx *ctx, const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref,
+                            size_t nmasked, const int64_t *masked, const uint8_t *masked_haploid,
+                            size_t nhaploid_ref, float *af, uint64_t *d_out, size_t ldw_words, uint64_t *host_out) {
+    if (!ctx || (!section && nbytes) || (nmasked && (!masked || !masked_haploid)) || (Mref && !af))
+        return fail(ctx, EIMP_E_ARG, "eimp_qref_decode_masked: NULL argument");
+    if (nmasked >= Nref) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode_masked: every sample masked");
+    size_t mhap = 0;
+    for (size_t i = 0; i < nmasked; i++) {
+        if (masked[i] < 0 || (size_t)masked[i] >= Nref || (i && masked[i] <= masked[i - 1]))
+            return fail(ctx, EIMP_E_ARG, "eimp_qref_decode_masked: masked samples must be ascending sample indices");
+        mhap += masked_haploid[i] != 0;
+    }
+    if (mhap > nhaploid_ref) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode_masked: more haploid samples masked than exist");
+    const size_t nw = eimp_W(2 * Nref), nout = Nref - nmasked, nwo = eimp_W(2 * nout);
+    if (!d_out) ldw_words = nwo;
+    if (ldw_words < nwo) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode_masked: leading dimension too small");
+    if (Mref > (size_t)INT32_MAX || nw > (size_t)INT32_MAX) return fail(ctx, EIMP_E_ARG, "eimp_qref_decode_masked: too large");
+    std::vector<int64_t> offs(Mref);
+    if (eimp_qref_index(section, nbytes, Mref, Nref, offs.data()))
+        return fail(ctx, EIMP_E_ARG, "Failed reading haplotypes from reference.");
+    std::vector<int32_t> kept;
+    kept.reserve(nout);
+    for (size_t sIdx = 0, i = 0; sIdx < Nref; sIdx++) {
+        if (i < nmasked && (size_t)masked[i] == sIdx) { i++; continue; }
+        kept.push_back((int32_t)sIdx);
+    }
+    if (int r = use_device(ctx)) return r;
+    CK(ctx->q_sec.reserve(nbytes + 16));
+    CK(ctx->q_offs.reserve(Mref * 8 + 8));
+    CK(ctx->q_mask.reserve(nmasked * 8 + 8));
+    CK(ctx->q_maskhap.reserve(nmasked + 8));
+    CK(ctx->q_kept.reserve(nout * 4 + 8));
+    CK(ctx->q_af.reserve(Mref * 4 + 8));
+    CK(cudaMemsetAsync(ctx->q_sec.as<uint8_t>() + nbytes, 0, 16, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->q_sec.p, section, nbytes, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->q_offs.p, offs.data(), Mref * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (nmasked) {
+        CK(cudaMemcpyAsync(ctx->q_mask.p, masked, nmasked * 8, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->q_maskhap.p, masked_haploid, nmasked, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaMemcpyAsync(ctx->q_kept.p, kept.data(), nout * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->q_af.p, af, Mref * 4, cudaMemcpyHostToDevice, ctx->stream));
+    uint64_t *dst = d_out;
+    if (!dst) {
+        CK(ctx->q_out.reserve(Mref * nwo * 8 + 8));
+        dst = ctx->q_out.as<uint64_t>();
+    }
+    // the unmasked rows of a chunk of variants, then their masked rows
+    const size_t chunk = std::max<size_t>(1, std::min<size_t>(Mref, (size_t(256) << 20) / (nw * 8)));
+    CK(ctx->q_rows.reserve(chunk * nw * 8));
+    const float an_before = (float)(2 * Nref - nhaploid_ref), an_after = (float)(2 * nout - (nhaploid_ref - mhap));
+    for (size_t v0 = 0; v0 < Mref; v0 += chunk) {
+        const int n = (int)std::min(chunk, Mref - v0);
+        LAUNCH(launch_qref_decode(ctx->q_sec.as<uint8_t>(), ctx->q_offs.as<int64_t>() + v0, n, (int)nw,
+                                  ctx->q_rows.as<uint64_t>(), nw, ctx->status.as<uint32_t>(), ctx->stream));
+        LAUNCH(launch_qref_mask(ctx->q_sec.as<uint8_t>(), ctx->q_offs.as<int64_t>() + v0, n,
+                                ctx->q_rows.as<uint64_t>(), nw, ctx->q_kept.as<int32_t>(), (int)nout, (int)nwo,
+                                ctx->q_mask.as<int64_t>(), (int)nmasked, ctx->q_maskhap.as<uint8_t>(), an_before,
+                                an_after, ctx->q_af.as<float>() + v0, dst + v0 * ldw_words, ldw_words, ctx->stream));
+    }
+    CK(cudaMemcpyAsync(af, ctx->q_af.p, Mref * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (host_out) {
+        if (ldw_words == nwo) {
+            CK(cudaMemcpyAsync(host_out, dst, Mref * nwo * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        } else {
+            CK(cudaMemcpy2DAsync(host_out, nwo * 8, dst, ldw_words * 8, nwo * 8, Mref, cudaMemcpyDeviceToHost,
                                  ctx->stream));
         }
     }

@@ -71,6 +71,10 @@ cudaError_t launch_site_stats(const SiteStatsArgs &a, cudaStream_t st);
 // ---- Qref haplotype section (qref_decode.cu)
 cudaError_t launch_qref_decode(const uint8_t *sec, const int64_t *offs, int Mref, int nwords, uint64_t *out,
                                size_t ldw, uint32_t *status, cudaStream_t st);
+cudaError_t launch_qref_mask(const uint8_t *sec, const int64_t *offs, int nvar, const uint64_t *rows, size_t ldr,
+                             const int32_t *kept, int nkept, int nwout, const int64_t *masked, int nmasked,
+                             const uint8_t *masked_hap, float an_before, float an_after, float *af, uint64_t *out,
+                             size_t ldo, cudaStream_t st);
 
 // ---- phasing preparation, condensed reference, PBWT (phase_prep.cu)
 // haploid: per reference sample, 1 = haploid (its second column is never

@@ -7,6 +7,11 @@
 //                        raw or run-length coded (qref_spec.md section I),
 //                        into its row of the site-major panel
 //                        (referenceFullT).
+//  qref_mask_kernel   -- the same with masked reference samples
+//                        (--excludeRefSamples, VCFData.cpp:2405-2523): the
+//                        decoded row with the masked samples' bit pairs
+//                        removed, and the panel allele frequency corrected
+//                        for the masked variant alleles.
 //
 // The host copies the section as it lies in the file (one transfer) and the
 // byte offset of every variant's <encsize> field (a walk over the size
@@ -117,6 +122,72 @@ __global__ void __launch_bounds__(128) qref_decode_kernel(const uint8_t *__restr
     const bool cut = carry != 0;
     const bool midword = (pos & 63ull) && (pos >> 6) <= max((unsigned long long)nwords - 1, last_start >> 6);
     if (lane == 0 && (cut || midword)) atomicOr(status, EIMP_ERR_QREF_TRUNCATED);
+}
+
+// 32 bits -> the even bits of a 64-bit word
+__device__ __forceinline__ uint64_t spread_even(uint32_t b) {
+    uint64_t x = b;
+    x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+    x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    x = (x | (x << 1)) & 0x5555555555555555ull;
+    return x;
+}
+
+// One warp per variant: rows (the decoded rows, 2 bits per sample) -> out
+// (the kept samples' pairs in order, then zeros, nwout words).  The masked
+// variant alleles are counted by the rule of the variant's storage: a raw
+// vector counts a masked sample once if either bit is set and once more for
+// a diploid 11 (VCFData.cpp:2471-2477); a run-length code counts each set
+// bit of a diploid sample and, for a haploid one, the second bit after a set
+// first bit (utils.h runlengthDecode, the masked-haplotype loop).  af[v] <-
+// (float(an_before) * af - masked) / float(an_after) in float arithmetic
+// (VCFData.cpp:2429-2434, 2517-2521).
+__global__ void __launch_bounds__(128) qref_mask_kernel(
+    const uint8_t *__restrict__ sec, const int64_t *__restrict__ offs, int nvar, const uint64_t *__restrict__ rows,
+    size_t ldr, const int32_t *__restrict__ kept, int nkept, int nwout, const int64_t *__restrict__ masked,
+    int nmasked, const uint8_t *__restrict__ masked_hap, float an_before, float an_after, float *__restrict__ af,
+    uint64_t *__restrict__ out, size_t ldo) {
+    const int lane = threadIdx.x & 31;
+    const int v = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (v >= nvar) return;
+    const uint8_t *p = sec + offs[v];
+    uint64_t encsize = 0;
+    if (lane < 8) encsize = (uint64_t)p[lane] << (8 * lane);
+    for (int o = 4; o; o >>= 1) encsize |= __shfl_xor_sync(0xffffffffu, encsize, o);
+    const bool raw = __shfl_sync(0xffffffffu, encsize, 0) == 0;
+    const uint64_t *row = rows + (size_t)v * ldr;
+    int cnt = 0;
+    for (int i = lane; i < nmasked; i += 32) {
+        const int64_t sm = masked[i];
+        const int pair = (int)((row[sm >> 5] >> ((sm & 31) * 2)) & 3ull);
+        const bool hap = masked_hap[i] != 0;
+        cnt += raw ? (pair != 0) + (pair == 3 && !hap) : (hap ? (pair == 3) : __popc(pair));
+    }
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    uint64_t *orow = out + (size_t)v * ldo;
+    for (int w = 0; w < nwout; w++) {
+        const int k = w * 32 + lane;
+        int pair = 0;
+        if (k < nkept) {
+            const int sk = kept[k];
+            pair = (int)((row[sk >> 5] >> ((sk & 31) * 2)) & 3ull);
+        }
+        const unsigned b0 = __ballot_sync(0xffffffffu, pair & 1), b1 = __ballot_sync(0xffffffffu, pair & 2);
+        if (lane == 0) orow[w] = spread_even(b0) | (spread_even(b1) << 1);
+    }
+    if (lane == 0) af[v] = __fdiv_rn(__fsub_rn(__fmul_rn(an_before, af[v]), (float)cnt), an_after);
+}
+
+cudaError_t launch_qref_mask(const uint8_t *sec, const int64_t *offs, int nvar, const uint64_t *rows, size_t ldr,
+                             const int32_t *kept, int nkept, int nwout, const int64_t *masked, int nmasked,
+                             const uint8_t *masked_hap, float an_before, float an_after, float *af, uint64_t *out,
+                             size_t ldo, cudaStream_t st) {
+    if (nvar <= 0) return cudaSuccess;
+    qref_mask_kernel<<<(nvar + 3) / 4, 128, 0, st>>>(sec, offs, nvar, rows, ldr, kept, nkept, nwout, masked, nmasked,
+                                                     masked_hap, an_before, an_after, af, out, ldo);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_qref_decode(const uint8_t *sec, const int64_t *offs, int Mref, int nwords, uint64_t *out,

@@ -346,7 +346,7 @@ int eimp_imp_bunch_stats(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const 
  * run-length bytes, or by the raw vector of W(2*Nref) words when encsize is
  * 0.  Decoded into Mref rows of W(2*Nref) words (bit 2s mat, 2s+1 pat of
  * sample s; the site-major referenceFullT layout, VCFData.h:211).  Masked
- * reference samples (--excludeRefSamples) are not supported.
+ * reference samples (--excludeRefSamples): eimp_qref_decode_masked below.
  *
  * eimp_qref_index (host only, no device): the byte offset of every variant's
  * <encsize> field; EIMP_E_ARG when the section is shorter than its variants
@@ -359,6 +359,19 @@ int eimp_imp_bunch_stats(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const 
 int eimp_qref_index(const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref, int64_t *offsets);
 int eimp_qref_decode(eimp_ctx *ctx, const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref,
                      uint64_t *d_out, size_t ldw_words, uint64_t *host_out);
+/* The same with masked reference samples (--excludeRefSamples;
+ * VCFData::qRefLoadNextVariant VCFData.cpp:2378-2535, runlengthDecode
+ * utils.h:194-): Nref samples in the section, masked[0..nmasked-1] ascending
+ * sample indices to leave out (masked_haploid: 1 for a haploid sample),
+ * nhaploid_ref haploid samples in the section.  Rows hold the
+ * Nref - nmasked kept samples (W(2*(Nref-nmasked)) words); af (Mref floats,
+ * the panel allele frequencies of the variants) is corrected in place for
+ * the masked variant alleles as the reference does.  A raw vector and a
+ * run-length code count a masked haploid sample stored as 01 or 10
+ * differently, as the reference's two paths do. */
+int eimp_qref_decode_masked(eimp_ctx *ctx, const uint8_t *section, size_t nbytes, size_t Mref, size_t Nref,
+                            size_t nmasked, const int64_t *masked, const uint8_t *masked_haploid,
+                            size_t nhaploid_ref, float *af, uint64_t *d_out, size_t ldw_words, uint64_t *host_out);
 
 /* ------------------------------------------- device-resident variants ----
  * Same operations on device pointers (inputs already in HBM; outputs written to

@@ -428,6 +428,21 @@ void refo_rle_decode(const uint8_t *enc, size_t encsize, uint64_t *dest, size_t 
     runlengthDecode(in, dest, nwords, masked, maskedhap, maskedalleles);
 }
 
+// runlengthDecode with masked reference samples (utils.h:194-, as
+// qRefLoadNextVariant calls it for --excludeRefSamples): the kept haplotypes
+// into nwords words; returns the masked variant alleles it counts.  The
+// sequence must be well-formed (the reference exits on a truncated one).
+size_t refo_rle_decode_masked(const uint8_t *enc, size_t encsize, uint64_t *dest, size_t nwords,
+                              const uint64_t *masked, size_t nmasked, const uint8_t *maskedhap) {
+    vector<char> in((const char *)enc, (const char *)enc + encsize);
+    vector<size_t> m(masked, masked + nmasked);
+    vector<bool> mh(nmasked);
+    for (size_t i = 0; i < nmasked; i++) mh[i] = maskedhap[i] != 0;
+    size_t maskedalleles = 0;
+    runlengthDecode(in, dest, nwords, m, mh, maskedalleles);
+    return maskedalleles;
+}
+
 // the haplotype section of a Qref file decoded variant by variant with the
 // reference's runlengthDecode, as qRefLoadNextVariant does after its reads
 // (VCFData.cpp:2378-2535; no masked samples); returns -2 for a short section

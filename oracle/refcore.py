@@ -71,6 +71,8 @@ def lib():
         L.refo_rle_encode.restype = C.c_long
         L.refo_rle_encode.argtypes = [_u64p, C.c_size_t, _u8p]
         L.refo_rle_decode.argtypes = [_u8p, C.c_size_t, _u64p, C.c_size_t]
+        L.refo_rle_decode_masked.restype = C.c_size_t
+        L.refo_rle_decode_masked.argtypes = [_u8p, C.c_size_t, _u64p, C.c_size_t, _u64p, C.c_size_t, _u8p]
         L.refo_qref_decode.restype = C.c_int
         L.refo_qref_decode.argtypes = [_u8p, C.c_size_t, C.c_size_t, C.c_size_t, _u64p]
         _lib = L
@@ -93,6 +95,21 @@ def rle_decode(enc: np.ndarray, nwords: int) -> np.ndarray:
     out = np.zeros(nwords, np.uint64)
     lib().refo_rle_decode(e if e.size else np.zeros(1, np.uint8), e.size, out, nwords)
     return out
+
+
+def rle_decode_masked(enc: np.ndarray, nwords: int, masked, masked_haploid):
+    """The reference's runlengthDecode with masked samples (utils.h:194-):
+    (the kept haplotypes in nwords words, the masked variant alleles it
+    counts).  masked: ascending sample indices; the sequence must be
+    well-formed."""
+    e = np.ascontiguousarray(enc, np.uint8)
+    out = np.zeros(nwords, np.uint64)
+    m = np.ascontiguousarray(masked, np.uint64)
+    mh = np.ascontiguousarray(masked_haploid, np.uint8)
+    n = lib().refo_rle_decode_masked(e if e.size else np.zeros(1, np.uint8), e.size, out, nwords,
+                                     m if m.size else np.zeros(1, np.uint64), m.size,
+                                     mh if mh.size else np.zeros(1, np.uint8))
+    return out, int(n)
 
 
 def qref_decode(section: np.ndarray, Mref: int, nwords: int):

@@ -323,3 +323,39 @@ def impute_fp64_sites(matches, sites, typed, af_full, nrefhaps_total, prefix_sli
             i += 1
         out[j] = float(score) / float(total)
     return out
+
+
+def qref_mask_row(row, raw, masked, masked_haploid, nsamples, nwords_out):
+    """A decoded Qref haplotype row (2 bits per sample, LSB first) with masked
+    reference samples removed, as VCFData::qRefLoadNextVariant stores it for
+    --excludeRefSamples (VCFData.cpp:2449-2523 for a raw vector,
+    runlengthDecode utils.h:194- for a run-length code): the kept samples'
+    bit pairs in order, then zeros; and the masked variant alleles it
+    counts.  A raw vector counts a masked sample once if either bit is set and
+    twice for a diploid 11; a run-length code counts each set bit of a
+    diploid sample and, for a haploid one (stored as a homozygous pair), the
+    second bit only after a set first bit."""
+    row = np.asarray(row, np.uint64)
+    s = np.arange(nsamples, dtype=np.int64)
+    pairs = ((row[s >> 5] >> ((s & 31) * 2).astype(np.uint64)) & np.uint64(3)).astype(np.int64)
+    mk = np.asarray(masked, np.int64)
+    mh = np.asarray(masked_haploid, np.uint8).astype(bool)
+    mp = pairs[mk]
+    if raw:
+        cnt = int(np.count_nonzero(mp) + np.count_nonzero((mp == 3) & ~mh))
+    else:
+        cnt = int(np.where(mh, mp == 3, (mp & 1) + (mp >> 1)).sum())
+    keep = np.setdiff1d(s, mk)
+    out = np.zeros(nwords_out * 64, np.uint8)
+    kp = pairs[keep]
+    out[0:2 * keep.size:2] = kp & 1
+    out[1:2 * keep.size:2] = kp >> 1
+    return np.packbits(out, bitorder="little").view(np.uint64), cnt
+
+
+def qref_mask_af(af, an_before, an_after, masked_alleles):
+    """The panel allele frequency after masking (VCFData.cpp:2429-2434,
+    2517-2521): float(an_before) * af - masked, over float(an_after), in
+    float arithmetic."""
+    f = np.float32
+    return f(f(f(an_before) * f(af)) - f(masked_alleles)) / f(an_after)
