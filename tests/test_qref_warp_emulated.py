@@ -93,7 +93,8 @@ def emu_exe(tmp_path_factory):
     shutil.copy(os.path.join(CSRC, "common.cuh"), d / "common.cuh")
     shutil.copy(os.path.join(CSRC, "kernels.h"), d / "kernels.h")
     src = open(os.path.join(CSRC, "qref_decode.cu")).read()
-    i, j = src.index("cudaError_t launch_qref_decode("), src.rindex("}  // namespace eimp")
+    # the kernels only: everything from the first host launcher to the namespace's end is cut
+    i, j = src.index("cudaError_t launch_qref_"), src.rindex("}  // namespace eimp")
     (d / "qref_emu.cpp").write_text('#include "emu.h"\n' + src[:i] + src[j:])
     exe = d / "qref_emu"
     cmd = ["g++", "-std=c++20", "-O1", "-g", "-fsanitize=address,undefined", "-fno-sanitize-recover=undefined",
