@@ -79,6 +79,7 @@ _PROTOS = [
     ("eimp_qref_decode_masked", _i32, [_vp, _vp, _sz, _sz, _sz, _sz, _vp, _vp, _sz, _vp, _vp, _sz, _vp]),
     ("eimp_qref_decode_dev", _i32, [_vp, _vp, _vp, _sz, _sz, _vp, _sz]),
     ("eimp_imp_bunch_stats", _i32, [_vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("eimp_imp_improve_stats", _i32, [_vp, _vp, _vp, _i32]),
     ("eimp_imp_site_stats_dev", _i32, [_vp, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _sz,
                                        _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("eimp_imp_refpbwt", _i32, [_vp, _vp, _vp]),

@@ -92,7 +92,7 @@ struct eimp_ctx {
     // haploid targets of the imputation: i_hapmap = row of each existing
     // target haplotype (i_ntgthaps of them) for i_tgthap_n targets
     size_t i_tgthap_n = 0, i_ntgthaps = 0;
-    DBuf i_hapmap;
+    DBuf i_hapmap, i_tgtflag;
     DBuf i_hapfull, i_sitefull_tmp, i_af, i_typed, i_segm, i_common, i_sinfo, i_sitetyped_tmp, i_compr,
         i_absperm, i_count0, i_rpscratch;
     // prepared targets
@@ -104,6 +104,9 @@ struct eimp_ctx {
     DBuf i_bits, i_dos;
     // phased dosages (eimp_imp_phased_dosages) and staging of the output statistics
     DBuf i_pdm, i_pdp, s_ads, s_gt, s_ds, s_gp, s_site, s_conf;
+    // --improveCalls run statistics: 5 counts then 5 double totals, added to
+    // by every output-statistics call (VCFData's improvecnt*/totalimprove*)
+    DBuf s_improve;
     // Qref haplotype section staging
     DBuf q_sec, q_offs, q_out, q_rows, q_mask, q_maskhap, q_kept, q_af;
     bool i_have_pdos = false;
@@ -186,7 +189,8 @@ int eimp_create(int device, eimp_ctx **out) {
         cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ref_ready, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->main_mark, cudaEventDisableTiming) != cudaSuccess ||
-        ctx->status.reserve(sizeof(uint32_t)) != cudaSuccess || cudaMemset(ctx->status.p, 0, sizeof(uint32_t)) != cudaSuccess) {
+        ctx->status.reserve(sizeof(uint32_t)) != cudaSuccess || cudaMemset(ctx->status.p, 0, sizeof(uint32_t)) != cudaSuccess ||
+        ctx->s_improve.reserve(80) != cudaSuccess || cudaMemset(ctx->s_improve.p, 0, 80) != cudaSuccess) {
         if (ctx->main_mark) cudaEventDestroy(ctx->main_mark);
         if (ctx->ref_ready) cudaEventDestroy(ctx->ref_ready);
         if (ctx->side) cudaStreamDestroy(ctx->side);
@@ -417,6 +421,11 @@ int eimp_imp_haploid_targets(eimp_ctx *ctx, size_t ntgt, const uint8_t *haploid)
     CK(cudaStreamSynchronize(ctx->stream));   // the map may be in use by queued imputation work
     CK(ctx->i_hapmap.reserve(map.size() * 4));
     CK(cudaMemcpy(ctx->i_hapmap.p, map.data(), map.size() * 4, cudaMemcpyHostToDevice));
+    // the flags themselves, for the output statistics (VCFData::haploidsTgt)
+    std::vector<uint8_t> f(ntgt);
+    for (size_t i = 0; i < ntgt; i++) f[i] = haploid[i] != 0;
+    CK(ctx->i_tgtflag.reserve(ntgt));
+    CK(cudaMemcpy(ctx->i_tgtflag.p, f.data(), ntgt, cudaMemcpyHostToDevice));
     ctx->i_tgthap_n = ntgt;
     ctx->i_ntgthaps = map.size();
     return 0;
@@ -553,8 +562,6 @@ int eimp_imp_site_stats_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, con
                             float *d_r2, float *d_af, float *d_maf, int32_t *d_ac, int32_t *d_an, uint8_t *d_pass,
                             uint64_t *d_conflicts) {
     if (!ctx || !ctx->i_ntargets) return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: imputation not prepared");
-    if (ctx->i_tgthap_n)
-        return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: haploid targets are not supported by the output statistics");
     if (!opts || !d_bits || !d_dos || !d_ads || !d_gtbits || !d_r2 || !d_af || !d_maf || !d_ac || !d_an || !d_pass ||
         !d_conflicts)
         return fail(ctx, EIMP_E_ARG, "eimp_imp_site_stats: NULL argument");
@@ -581,7 +588,20 @@ int eimp_imp_site_stats_dev(eimp_ctx *ctx, size_t mref_begin, size_t nsites, con
     a.ads = d_ads; a.lda = (int)lda; a.gtbits = d_gtbits; a.ldg = (int)ldg_words; a.ds = d_ds; a.gp = d_gp;
     a.r2 = d_r2; a.af_out = d_af; a.maf = d_maf; a.ac = d_ac; a.an = d_an; a.pass = d_pass;
     a.conflicts = reinterpret_cast<unsigned long long *>(d_conflicts);
+    a.haptgt = ctx->i_tgthap_n ? ctx->i_tgtflag.as<uint8_t>() : nullptr;
+    a.icnt = opts->improveCalls ? ctx->s_improve.as<unsigned long long>() : nullptr;
+    a.itot = opts->improveCalls ? reinterpret_cast<double *>(ctx->s_improve.as<unsigned long long>() + 5) : nullptr;
     LAUNCH(launch_site_stats(a, ctx->stream));
+    return 0;
+}
+
+int eimp_imp_improve_stats(eimp_ctx *ctx, uint64_t *counts, double *totals, int reset) {
+    if (!ctx || !counts || !totals) return fail(ctx, EIMP_E_ARG, "eimp_imp_improve_stats: NULL argument");
+    if (int r = use_device(ctx)) return r;
+    CK(cudaMemcpyAsync(counts, ctx->s_improve.p, 40, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(totals, ctx->s_improve.as<uint8_t>() + 40, 40, cudaMemcpyDeviceToHost, ctx->stream));
+    if (reset) CK(cudaMemsetAsync(ctx->s_improve.p, 0, 80, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return 0;
 }
 

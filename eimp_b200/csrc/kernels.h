@@ -65,6 +65,9 @@ struct SiteStatsArgs {
     int32_t *ac, *an;
     uint8_t *pass;
     unsigned long long *conflicts;            // incremented by the conflicts found
+    const uint8_t *haptgt;                    // per target, 1 = haploid (NULL: all diploid)
+    unsigned long long *icnt;                 // --improveCalls run statistics, added to:
+    double *itot;                             //   5 counts and 5 totals (NULL: not kept)
 };
 cudaError_t launch_site_stats(const SiteStatsArgs &a, cudaStream_t st);
 

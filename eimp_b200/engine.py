@@ -405,6 +405,16 @@ class PBWTImputer:
         out["conflicts"] = int(conf[0])
         return out
 
+    def improveStats(self, reset: bool = False):
+        """The --improveCalls run statistics (VCFData's improvecnt* /
+        totalimprove* counters, VCFData.cpp:3306-3330) summed over the output
+        statistics computed so far: counts and totals in the order no change,
+        het->het, hom->hom, het->hom, hom->het."""
+        counts = np.zeros(5, np.uint64)
+        totals = np.zeros(5, np.float64)
+        self.ctx.check(self.ctx.L.eimp_imp_improve_stats(self.ctx.h, ptr(counts), ptr(totals), int(reset)))
+        return counts.astype(np.int64), totals
+
     def matches(self, hap: int) -> np.ndarray:
         n = C.c_size_t(0)
         self.ctx.check(self.ctx.L.eimp_imp_matches(self.ctx.h, hap, None, 0, C.byref(n)))

@@ -307,7 +307,7 @@ int eimp_transpose_bits_dev(eimp_ctx *ctx, const uint64_t *d_src, size_t rows, s
 
 /* Output statistics of an imputed bunch: the numeric part of
  * VCFData::writeVCFImputedBunch (VCFData.cpp:3068-3446), which main.cpp:454
- * calls after PBWTImputer::imputeBunch for every bunch.  Diploid targets.
+ * calls after PBWTImputer::imputeBunch for every bunch.
  * Per target haplotype and site: the allele dosage written (ADS; an imputation
  * conflict takes the reference panel allele frequency RefPanelAF and the
  * allele RefPanelAF > 0.5; a typed, non-missing call keeps the phased allele
@@ -316,8 +316,17 @@ int eimp_transpose_bits_dev(eimp_ctx *ctx, const uint64_t *d_src, size_t rows, s
  * DS = ADS0 + ADS1 and GP (three floats, VCFData.cpp:3159-3166).  Per site:
  * AF and MAF from the dosages, minimac4's r2, AC, AN and whether the record
  * passes the --imputeR2filter / --imputeMAFfilter thresholds.  `conflicts`
- * receives the number of conflicts (VCFData::conflictcnt).  The per-category
- * counters that --improveCalls adds to the run statistics are not produced. */
+ * receives the number of conflicts (VCFData::conflictcnt).
+ * Haploid targets (eimp_imp_haploid_targets; VCFData.cpp:3192-3226,
+ * 3399-3437) use their first haplotype row: its ADS and allele, the second
+ * row's ADS set to htslib's "vector end" (0x7F800002) and its GT bit 0, DS =
+ * ADS0 and GP = (1 - ADS0, ADS0, vector end).  At a typed, non-missing site
+ * (without overwriteCalls) a haploid target keeps its phased allele with ADS
+ * "missing" (0x7F800001) and adds nothing to AF, r2, AC or AN; the reference
+ * leaves DS and GP unset there (its writer buffers keep an earlier site's
+ * values), and they are written as DS missing and GP (missing, vector end,
+ * vector end).  The --improveCalls run statistics go to the context's
+ * counters (eimp_imp_improve_stats). */
 typedef struct {
     int overwriteCalls;   /* --overwriteCalls (Args.cpp:304) */
     int improveCalls;     /* --improveCalls (Args.cpp:305) */
@@ -339,6 +348,17 @@ int eimp_imp_phased_dosages(eimp_ctx *ctx, const float *dos_mat, const float *do
 int eimp_imp_bunch_stats(eimp_ctx *ctx, size_t mref_begin, size_t nsites, const eimp_site_stats_opts *opts,
                          float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2, float *af, float *maf,
                          int32_t *ac, int32_t *an, uint8_t *pass, uint64_t *conflicts);
+
+/* The --improveCalls run statistics (VCFData's improvecnt* and totalimprove*
+ * members, VCFData.cpp:3306-3330, reported in the run summary): improved calls
+ * counted over every output-statistics call of the context with improveCalls
+ * set, since the context was made or last reset.  counts[5] and totals[5] (the
+ * sums of the calls' improvements) in the order: no allele change, het->het,
+ * hom->hom, het->hom, hom->het.  reset != 0 zeroes them after the read.
+ * Synchronises the context's stream.  The counts are exact; the device adds
+ * the totals in an order of its own, so their last bits can differ from a
+ * sequential sum (the reference's own order depends on its thread count). */
+int eimp_imp_improve_stats(eimp_ctx *ctx, uint64_t *counts, double *totals, int reset);
 
 /* Qref reference panel, haplotype section (qref_spec.md section I; read by
  * VCFData::qRefLoadNextVariant, VCFData.cpp:2378-2535, with runlengthDecode,

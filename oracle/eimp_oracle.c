@@ -476,13 +476,24 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
 static int eo_getbit(const uint64_t *row, size_t i) { return (int)((row[i >> 6] >> (i & 63)) & 1u); }
 static void eo_setbit(uint64_t *row, size_t i, int v) { if (v) row[i >> 6] |= 1ull << (i & 63); }
 
+/* htslib's bit patterns for a missing float and the end of a shorter vector */
+static float eo_bcf_float(uint32_t bits) {
+    float f;
+    memcpy(&f, &bits, 4);
+    return f;
+}
+#define EO_BCF_FLOAT_MISSING 0x7F800001u
+#define EO_BCF_FLOAT_VECTOR_END 0x7F800002u
+
 long eo_site_stats(size_t ntgt, size_t mref_begin, size_t nsites, const uint64_t *bits, size_t wb,
                    const float *dos, const uint64_t *phased, size_t wM, const float *pdm, const float *pdp,
                    const uint8_t *gt, size_t M, const int32_t *typed_idx, const uint8_t *is_typed,
-                   const float *af_full, int overwriteCalls, int improveCalls, float r2filter, float maffilter,
-                   float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2o, float *afo, float *mafo,
-                   int32_t *aco, int32_t *ano, uint8_t *pass) {
+                   const float *af_full, const uint8_t *haploid, int overwriteCalls, int improveCalls,
+                   float r2filter, float maffilter, float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2o,
+                   float *afo, float *mafo, int32_t *aco, int32_t *ano, uint8_t *pass, uint64_t *icnt,
+                   double *itot) {
     long conflictcnt = 0;
+    const float fmissing = eo_bcf_float(EO_BCF_FLOAT_MISSING), fend = eo_bcf_float(EO_BCF_FLOAT_VECTOR_END);
     for (size_t isite = 0; isite < nsites; isite++) {
         const size_t idx = mref_begin + isite;
         const float rpaf = af_full[idx];                       /* :3118 */
@@ -495,6 +506,48 @@ long eo_site_stats(size_t ntgt, size_t mref_begin, size_t nsites, const uint64_t
             int hap0, hap1;
             float ads0, ads1;
             const int missing = !isimputed && gt[i * M + psite] == 3;   /* :3238 */
+            if (haploid && haploid[i]) {
+                /* haploid target, :3192-3226 (imputed) and :3399-3437 (typed):
+                 * only the first haplotype row carries the sample; the second
+                 * ADS and GP2 are "vector end".  A typed, non-missing call
+                 * (without --overwriteCalls) keeps the phased allele with a
+                 * missing ADS and adds nothing to AF, r2, AC or AN; the
+                 * reference then leaves DS and GP unset (its per-thread buffers
+                 * keep an earlier site's values), and this restatement writes
+                 * DS missing and GP (missing, end, end) there. */
+                if (isimputed || missing || overwriteCalls) {
+                    hap0 = eo_getbit(bits + h0 * wb, isite);
+                    ads0 = dos[h0 * nsites + isite];
+                    if (ads0 < 0) { ads0 = rpaf; hap0 = rpaf > 0.5; conflictcnt++; }
+                    ads[h0 * nsites + isite] = ads0;
+                    adsum += ads0;
+                    ad2sum += ads0 * ads0;
+                    if (ds) ds[i * nsites + isite] = ads0;
+                    if (gp) {
+                        double gp0 = (1.0 - ads0);
+                        double gp2 = ads0;
+                        gp[(3 * i) * nsites + isite] = (float)gp0;
+                        gp[(3 * i + 1) * nsites + isite] = (float)gp2;
+                        gp[(3 * i + 2) * nsites + isite] = fend;
+                    }
+                    if (hap0) ac1++;
+                    an++;
+                    nval++;
+                } else {
+                    hap0 = eo_getbit(phased + h0 * wM, psite);
+                    ads[h0 * nsites + isite] = fmissing;
+                    if (ds) ds[i * nsites + isite] = fmissing;
+                    if (gp) {
+                        gp[(3 * i) * nsites + isite] = fmissing;
+                        gp[(3 * i + 1) * nsites + isite] = fend;
+                        gp[(3 * i + 2) * nsites + isite] = fend;
+                    }
+                }
+                ads[h1 * nsites + isite] = fend;
+                eo_setbit(gtbits + h0 * wb, isite, hap0);
+                eo_setbit(gtbits + h1 * wb, isite, 0);
+                continue;
+            }
             if (isimputed || missing || overwriteCalls) {      /* :3126-3152, :3246-3270 */
                 hap0 = eo_getbit(bits + h0 * wb, isite);
                 hap1 = eo_getbit(bits + h1 * wb, isite);
@@ -523,8 +576,19 @@ long eo_site_stats(size_t ntgt, size_t mref_begin, size_t nsites, const uint64_t
                     if (improve0 + improve1 > 0) {
                         if (dos[h0 * nsites + isite] < 0) conflictcnt++;
                         if (dos[h1 * nsites + isite] < 0) conflictcnt++;
-                        hap0 = eo_getbit(bits + h0 * wb, isite);
-                        hap1 = eo_getbit(bits + h1 * wb, isite);
+                        /* :3306-3330, the run statistics of an improved call:
+                         * 0 no allele changes, 1 het->het (both change), 2
+                         * hom->hom (both change), 3 het->hom, 4 hom->het (one
+                         * changes); totals add the float improve0 + improve1 */
+                        const int i0 = eo_getbit(bits + h0 * wb, isite), i1 = eo_getbit(bits + h1 * wb, isite);
+                        int cat;
+                        if (hap0 != i0 && hap1 != i1) cat = hap0 != hap1 ? 1 : 2;
+                        else if (hap0 != i0 || hap1 != i1) cat = hap0 == hap1 ? 4 : 3;
+                        else cat = 0;
+                        if (icnt) icnt[cat]++;
+                        if (itot) itot[cat] += improve0 + improve1;
+                        hap0 = i0;
+                        hap1 = i1;
                         ads0 = hap0 ? 1.0 - idos0 : idos0;
                         ads1 = hap1 ? 1.0 - idos1 : idos1;
                     }

@@ -83,19 +83,21 @@ void eo_impute(const int64_t *matches, size_t nmatches, const int32_t *absperm, 
                uint8_t *imputed, double *dos64);
 
 /* Output statistics of an imputed bunch: the numeric part of
- * VCFData::writeVCFImputedBunch (VCFData.cpp:3068-3446) for diploid targets.
+ * VCFData::writeVCFImputedBunch (VCFData.cpp:3068-3446).
  * Site-major over the bunch's nsites sites (site s = reference site
  * mref_begin + s):
  *   bits   2*ntgt rows of wb words (imputed alleles), dos 2*ntgt x nsites
  *   phased 2*ntgt rows of wM words, pdm/pdp ntgt x M phased dosages
  *   gt     ntgt x M genotype codes (3 = missing), typed_idx / is_typed per
  *          reference site (the typed index of the last typed site <= mref)
+ *   haploid ntgt flags or NULL (haploid targets: row 2i only)
  * Outputs: ads 2*ntgt x nsites, gtbits 2*ntgt rows of wb words (zeroed by the
  * caller), ds ntgt x nsites (optional), gp 3*ntgt x nsites (optional, rows
- * GP0, GP1, GP2 per target), per site r2, af, maf, ac, an, pass; returns the
- * number of imputation conflicts.
- * The reference's writer needs htslib and cannot be compiled here: this
- * restatement is pinned by hand-worked cases in the tests only. */
+ * GP0, GP1, GP2 per target), per site r2, af, maf, ac, an, pass; the
+ * --improveCalls run statistics are added to improve_counts[5] and
+ * improve_totals[5] (optional; VCFData.cpp:3306-3330); returns the number of
+ * imputation conflicts.  Pinned to the reference's own writer
+ * (oracle/_ref/libeimp_refwriter.so) by tests/test_site_stats_reference_writer.py. */
 /* Qref haplotype vectors (qref_spec.md section I).
  * eo_rle_encode: runlengthEncode + addRunlength (utils.h:133-191) of nwords
  * words; returns the encoded length, or -1 where the reference gives up (the
@@ -113,9 +115,10 @@ int eo_qref_decode(const uint8_t *section, size_t nbytes, size_t Mref, size_t nw
 long eo_site_stats(size_t ntgt, size_t mref_begin, size_t nsites, const uint64_t *bits, size_t wb,
                    const float *dos, const uint64_t *phased, size_t wM, const float *pdm, const float *pdp,
                    const uint8_t *gt, size_t M, const int32_t *typed_idx, const uint8_t *is_typed,
-                   const float *af_full, int overwriteCalls, int improveCalls, float r2filter, float maffilter,
-                   float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2, float *af, float *maf,
-                   int32_t *ac, int32_t *an, uint8_t *pass);
+                   const float *af_full, const uint8_t *haploid, int overwriteCalls, int improveCalls,
+                   float r2filter, float maffilter, float *ads, uint64_t *gtbits, float *ds, float *gp, float *r2,
+                   float *af, float *maf, int32_t *ac, int32_t *an, uint8_t *pass, uint64_t *improve_counts,
+                   double *improve_totals);
 
 /* a7: phasing parameters (Args.cpp:274-299 defaults) */
 typedef struct {

@@ -20,6 +20,7 @@ _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 
 
@@ -69,9 +70,9 @@ def lib():
                                 _f32p, _u8p, C.c_void_p]
         L.eo_site_stats.restype = C.c_long
         L.eo_site_stats.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t, _u64p, C.c_size_t, _f32p, _u64p, C.c_size_t,
-                                    _f32p, _f32p, _u8p, C.c_size_t, _i32p, _u8p, _f32p, C.c_int, C.c_int,
-                                    C.c_float, C.c_float, _f32p, _u64p, C.c_void_p, C.c_void_p, _f32p, _f32p,
-                                    _f32p, _i32p, _i32p, _u8p]
+                                    _f32p, _f32p, _u8p, C.c_size_t, _i32p, _u8p, _f32p, C.c_void_p, C.c_int,
+                                    C.c_int, C.c_float, C.c_float, _f32p, _u64p, C.c_void_p, C.c_void_p, _f32p,
+                                    _f32p, _f32p, _i32p, _i32p, _u8p, _u64p, _f64p]
         L.eo_rle_encode.restype = C.c_long
         L.eo_rle_encode.argtypes = [_u64p, C.c_size_t, _u8p]
         L.eo_rle_decode.restype = C.c_int
@@ -211,11 +212,13 @@ def qref_decode(section: np.ndarray, Mref: int, nwords: int):
 
 
 def site_stats(mref_begin, bits, dos, phased, pdm, pdp, gt, typed, Mref, af_full, overwriteCalls=False,
-               improveCalls=False, r2filter=0.0, maffilter=0.0, want_ds=False, want_gp=False):
+               improveCalls=False, r2filter=0.0, maffilter=0.0, want_ds=False, want_gp=False, haploid=None):
     """VCFData::writeVCFImputedBunch's numbers for one bunch (eo_site_stats).
     bits: 2N x wb words, dos: 2N x nsites floats, phased: 2N x wM words,
     pdm/pdp: N x M phased dosages, gt: N x M, typed: ascending typed site
-    indices into the Mref reference sites."""
+    indices into the Mref reference sites, haploid: N flags or None.
+    improve_counts / improve_totals: the --improveCalls run statistics of the
+    bunch (no change, het->het, hom->hom, het->hom, hom->het)."""
     nh, nsites = dos.shape
     N, M = gt.shape
     typed = np.asarray(typed, np.int64)
@@ -234,16 +237,20 @@ def site_stats(mref_begin, bits, dos, phased, pdm, pdp, gt, typed, Mref, af_full
     ac = np.zeros(nsites, np.int32)
     an = np.zeros(nsites, np.int32)
     ps = np.zeros(nsites, np.uint8)
+    icnt = np.zeros(5, np.uint64)
+    itot = np.zeros(5, np.float64)
+    hap = np.ascontiguousarray(np.asarray(haploid, np.uint8)) if haploid is not None else None
     conf = lib().eo_site_stats(N, mref_begin, nsites, np.ascontiguousarray(bits, np.uint64), wb,
                                np.ascontiguousarray(dos, np.float32), np.ascontiguousarray(phased, np.uint64),
                                phased.shape[1], np.ascontiguousarray(pdm, np.float32),
                                np.ascontiguousarray(pdp, np.float32), np.ascontiguousarray(gt, np.uint8), M,
-                               typed_idx, is_typed, np.ascontiguousarray(af_full, np.float32), int(overwriteCalls),
+                               typed_idx, is_typed, np.ascontiguousarray(af_full, np.float32),
+                               hap.ctypes.data if hap is not None else None, int(overwriteCalls),
                                int(improveCalls), r2filter, maffilter, ads, gtbits,
                                ds.ctypes.data if ds is not None else None, gp.ctypes.data if gp is not None else None,
-                               r2, af, maf, ac, an, ps)
+                               r2, af, maf, ac, an, ps, icnt, itot)
     return dict(ads=ads, gtbits=gtbits, ds=ds, gp=gp, r2=r2, af=af, maf=maf, ac=ac, an=an, passed=ps,
-                conflicts=int(conf))
+                conflicts=int(conf), improve_counts=icnt.astype(np.int64), improve_totals=itot)
 
 
 def phase(gt_row, hapmajor, sitemajor, cm, params: PhaseParamsC):

@@ -1,10 +1,10 @@
 """The oracle restatement of the output statistics of an imputed bunch
-(VCFData::writeVCFImputedBunch, VCFData.cpp:3068-3446).  The reference's
-writer needs htslib and cannot be compiled here, so the restatement is pinned
-by a case worked by hand and by a second, element-by-element restatement in
-Python with explicit float32/float64 scalars in the reference's order of
-operations, over random inputs with conflicts, missing calls and the
---overwriteCalls / --improveCalls / filter options."""
+(VCFData::writeVCFImputedBunch, VCFData.cpp:3068-3446), checked by a case
+worked by hand and by a second, element-by-element restatement in Python with
+explicit float32/float64 scalars in the reference's order of operations, over
+random inputs with conflicts, missing calls and the --overwriteCalls /
+--improveCalls / filter options.  The pin against the reference's own writer
+is tests/test_site_stats_reference_writer.py."""
 import numpy as np
 import pytest
 

@@ -201,4 +201,10 @@ inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
 inline unsigned long long atomicAdd(unsigned long long *p, unsigned long long v) {
     return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);
 }
+inline double atomicAdd(double *p, double v) {
+    double o, n;
+    __atomic_load(p, &o, __ATOMIC_SEQ_CST);
+    do { n = o + v; } while (!__atomic_compare_exchange(p, &o, &n, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST));
+    return o;
+}
 inline int atomicOr(int *p, int v) { return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST); }

@@ -8,9 +8,11 @@
 // device buffers: params_i.bin (ntgt, mref_begin, nsites, ldb, ldd, wM, ldp,
 // M, Mref, overwriteCalls, improveCalls), params_f.bin (r2filter,
 // maffilter), bits.bin, dos.bin, phased.bin, pdm.bin, pdp.bin, gt.bin,
-// segm.bin, common.bin, af.bin.  Outputs: o_ads.bin, o_gtbits.bin, o_ds.bin,
-// o_gp.bin, o_site.bin (r2, af, maf as float, ac, an as int32, nsites each),
-// o_pass.bin, o_conf.bin.  Exit status 3: a divergent warp collective.
+// segm.bin, common.bin, af.bin, and haptgt.bin (one byte per target; empty:
+// all diploid).  Outputs: o_ads.bin, o_gtbits.bin, o_ds.bin, o_gp.bin,
+// o_site.bin (r2, af, maf as float, ac, an as int32, nsites each),
+// o_pass.bin, o_conf.bin, o_icnt.bin and o_itot.bin (the --improveCalls
+// counts and totals).  Exit status 3: a divergent warp collective.
 #include "stats_emu.cpp"
 
 #include <string>
@@ -57,6 +59,7 @@ int main(int argc, char **argv) {
     const auto segm = rd<int32_t>(d, "segm.bin");
     const auto common = rd<uint8_t>(d, "common.bin");
     const auto af = rd<float>(d, "af.bin");
+    const auto haptgt = rd<uint8_t>(d, "haptgt.bin");
     eimp::SiteStatsArgs a;
     a.ntgt = pi[0]; a.mref_begin = pi[1]; a.nsites = pi[2]; a.ldb = pi[3]; a.ldd = pi[4]; a.wM = pi[5];
     a.ldp = pi[6]; a.M = pi[7]; a.overwriteCalls = pi[9]; a.improveCalls = pi[10];
@@ -70,7 +73,11 @@ int main(int argc, char **argv) {
     std::vector<float> site_f(3 * ns);
     std::vector<int32_t> site_i(2 * ns);
     std::vector<uint8_t> pass(ns);
-    std::vector<unsigned long long> conf(1, 0);
+    std::vector<unsigned long long> conf(1, 0), icnt(5, 0);
+    std::vector<double> itot(5, 0.0);
+    a.haptgt = haptgt.empty() ? nullptr : haptgt.data();
+    a.icnt = icnt.data();
+    a.itot = itot.data();
     a.ads = ads.data(); a.lda = (int)ns; a.gtbits = gtbits.data(); a.ldg = a.ldb; a.ds = ds.data(); a.gp = gp.data();
     a.r2 = site_f.data(); a.af_out = site_f.data() + ns; a.maf = site_f.data() + 2 * ns;
     a.ac = site_i.data(); a.an = site_i.data() + ns; a.pass = pass.data(); a.conflicts = conf.data();
@@ -88,13 +95,16 @@ int main(int argc, char **argv) {
                 blockDim.x = 32 * nw;
                 emu_warp = &warps[t / 32];
                 emu_block = &block;
-                eimp::site_stats_kernel<true, true>(a);
+                if (a.haptgt) eimp::site_stats_kernel<true, true, true>(a);
+                else eimp::site_stats_kernel<true, true, false>(a);
             });
         for (auto &x : threads) x.join();
     }
     wr(d, "o_ads.bin", ads); wr(d, "o_gtbits.bin", gtbits); wr(d, "o_ds.bin", ds); wr(d, "o_gp.bin", gp);
     wr(d, "o_site_f.bin", site_f); wr(d, "o_site_i.bin", site_i); wr(d, "o_pass.bin", pass);
     wr(d, "o_conf.bin", conf);
+    wr(d, "o_icnt.bin", icnt);
+    wr(d, "o_itot.bin", itot);
     if (emu_divergence.load()) { fprintf(stderr, "divergent warp collectives: %d\n", emu_divergence.load()); return 3; }
     return 0;
 }
