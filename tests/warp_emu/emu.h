@@ -43,6 +43,7 @@ inline int2 make_int2(int x, int y) { return int2{x, y}; }
 inline short2 make_short2(short x, short y) { return short2{x, y}; }
 inline int4 make_int4(int x, int y, int z, int w) { return int4{x, y, z, w}; }
 inline uint4 make_uint4(unsigned x, unsigned y, unsigned z, unsigned w) { return uint4{x, y, z, w}; }
+inline uint2 make_uint2(unsigned x, unsigned y) { return uint2{x, y}; }
 inline float4 make_float4(float x, float y, float z, float w) { return float4{x, y, z, w}; }
 
 extern thread_local dim3 threadIdx, blockIdx, blockDim;
