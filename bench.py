@@ -442,54 +442,14 @@ def profile_stages(groups, cfg, flush, stream_main):
 
 
 # ---------------------------------------------------------------- GPUEngine
-def reference_gpuengine_leg(panel, tg, cfg, device, ntgt=256, reps=3):
-    """The reference's own GPU form of the condensed reference and its
-    PBWTs (GPUEngine::runCrefPBWTKernel: crefTKernel + pbwtPartedKernel,
-    GPUEngine.cu:98-217, compiled from the reference's sources for sm_100a
-    by oracle/Makefile) against this project's drop-in of the same call
-    (eimp_gpu_run_cref_pbwt) on one block of targets of a density group,
-    host buffers in and out as the interface has them; the rows' [data,
-    zeros] words and the zero counts compared word for word."""
-    from eimp_b200.bits import pack_genotypes
-    from eimp_b200.engine import Context, GPUEngine, PhaseParams, Phaser
-    from oracle import refgpu
-    if not refgpu.available():
-        return {"unavailable": "the reference's GPU engine is not built (oracle/Makefile target refgpu)"}
-    hm, sm, cm = synth.typed_views(panel, tg.typed)
-    nh, M = panel.nhaps, len(tg.typed)
-    K = min(cfg.K, nh)
-    gt = tg.gt[:ntgt]
-    ctx = Context(device)
-    pre = Phaser(ctx, hm, sm, cm).prep(PhaseParams(K=K, beamwidth=cfg.beam), gt)
-    ctx.close()
-    ns = pre["nsplits"]
-    tgt, spl, bhf = [], [], []
-    for t in range(gt.shape[0]):
-        tgt.append(pack_genotypes(gt[t]))
-        sw = np.zeros(W(M), np.uint64)
-        sp = pre["splits"][t][:ns[t]].astype(np.int64)
-        np.bitwise_or.at(sw, sp >> 6, np.uint64(1) << (sp & 63).astype(np.uint64))
-        spl.append(sw)
-        bhf.append(np.ascontiguousarray(pre["flags"][t][:W(nh)]))
-    off = np.concatenate([[0], np.cumsum(2 * ns.astype(np.int64) + 1)]).astype(np.uint32)
-    Kw, kw = W(K), 2 * ((K + 31) // 32)
-    res = {}
-    for name, eng in (("reference", refgpu.RefGPUEngine(device)), ("ours", GPUEngine(device))):
-        eng.initialize(K, Kw, M, nh, nh, W(nh) * 8, sm)
-        outs = [np.zeros(2 * (2 * int(n) + 1) * 4 * Kw, np.uint32) for n in ns]
-        c0s = [np.zeros(2 * int(n) + 1, np.int32) for n in ns]
-        eng.runCrefPBWTKernel(tgt, spl, bhf, off, outs, c0s)   # warm-up
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            eng.runCrefPBWTKernel(tgt, spl, bhf, off, outs, c0s)
-        res[name] = ((time.perf_counter() - t0) / reps * 1e3, outs, c0s)
-        eng.free()
-    equal = all(np.array_equal(a.reshape(-1, 4 * Kw)[:, :kw], b.reshape(-1, 4 * Kw)[:, :kw]) and np.array_equal(c, d)
-                for a, b, c, d in zip(res["ours"][1], res["reference"][1], res["ours"][2], res["reference"][2]))
-    return {"targets": int(gt.shape[0]), "typed_sites": M, "K": K, "condensed_rows": int(off[-1]),
-            "reference_ms_per_call": res["reference"][0], "ours_ms_per_call": res["ours"][0],
-            "speedup": res["reference"][0] / res["ours"][0], "outputs_equal": bool(equal),
-            "form": "GPUEngine::runCrefPBWTKernel, host buffers in and out, one block of the densest group"}
+# The reference's own GPU form of this call (GPUEngine::runCrefPBWTKernel:
+# crefTKernel + pbwtPartedKernel) is not run: compiled for sm_100a, it ran
+# for the whole 30-minute limit of a B200 call on the 5-target golden case
+# (K = 64) without finishing, after every other GPU test had passed in
+# seconds, so it is kept off the GPUs of this pool.
+REFERENCE_GPU_ENGINE = {"unavailable": "the reference's GPU engine (crefTKernel + pbwtPartedKernel for sm_100a) "
+                                       "did not finish the 5-target golden case within a 30-minute B200 call; "
+                                       "it is not run on this pool"}
 
 
 # ---------------------------------------------------------------- cfg4
@@ -1031,7 +991,7 @@ def main():
                                    for go, k, tg, s in zip(gpu_out, keeps, tgroups, samples)])
             for s in samples:
                 s.close()
-        gpuengine = reference_gpuengine_leg(panel, tgroups[-1], cfg, local)
+        gpuengine = REFERENCE_GPU_ENGINE
 
     # ---- the large panel (cfg4) on the device, after everything above
     cfg4 = None
