@@ -508,22 +508,17 @@ cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapm
 // ---------------------------------------------------------------------------
 // PBWT::buildComprPBWT (PBWT.cpp:207-285) of each target's condensed
 // reference, forward and backward (rows in sweep order), one CTA per (target,
-// direction).  Warp w owns WPW consecutive 32-position words of the prefix
-// order, lane l position l of each: positions are read and written by
-// consecutive lanes.  Per row, two passes:
-//  1. for each of its words the warp gathers the haplotypes' bits in the
-//     current prefix order (one ballot = the row format's data word, the tail
-//     padded with ones), keeps the haplotypes in registers (two 16-bit ones
-//     per register) and the word in lane j, and counts the zeros; the warps'
-//     totals give every warp its zeros before it and the row's zero count;
-//  2. the warp writes its [data, zeros through the word] pairs (one coalesced
-//     store per lane) and places its haplotypes in the next prefix order: a
-//     zero at position p goes to z (the zeros before p), a one to
-//     count0 + p - z.  The zeros of a word land on consecutive entries, and
-//     so do its ones, so the stores of a warp meet no bank conflicts.
-// The prefix arrays are 16-bit (K <= 65536).  The next row is copied into
-// shared memory asynchronously while the current one is processed.  The
-// forward CTA also writes each row's zero count.
+// direction).  Each thread owns WPT consecutive 32-position words of the
+// prefix order.  Per row: the thread gathers its words' bits in the current
+// prefix order (a word is the row format's data word, the tail padded with
+// ones) and counts their zeros; one block scan gives every word's zeros
+// before it; the thread writes its [data, zeros through the word] pairs and
+// places its haplotypes in the next prefix order (zeros first, stable).  The
+// prefix arrays are 16-bit (K <= 65536) and XOR-swizzled within each 32-entry
+// block, so that the 32 lanes reading position j of their own words hit 32
+// different banks.  The next row is copied into shared memory asynchronously
+// while the current one is processed.  The forward CTA also writes each
+// row's zero count.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -532,34 +527,34 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int WPW>
+// position p of the prefix order -> its slot in the swizzled array
+__device__ __forceinline__ int pswz(int p) { return p ^ ((p >> 5) & 31); }
+
+template <int WPT>
 __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__ cref,
                                                     const int64_t *__restrict__ rowoff, int K,
                                                     uint32_t *__restrict__ pbwt, size_t rowstride, int emit_padded,
                                                     int32_t *__restrict__ count0, const int *__restrict__ skip) {
-    static_assert(WPW % 2 == 0 && WPW <= 64, "two haplotypes per register, at most two words per lane");
     if (skip && *skip) return;   // the batch exceeds the reserved rows
     extern __shared__ __align__(16) uint8_t smem[];
-    const unsigned FULL = 0xffffffffu;
     const int t = blockIdx.x >> 1, dir = blockIdx.x & 1;
     const int wK = (int)eimp_W(K);
     const int nwords = (K + 31) / 32;
     const int nthreads = blockDim.x, nwarps = nthreads >> 5;
     uint64_t *rowbuf = reinterpret_cast<uint64_t *>(smem);                 // 2 x wK
     int *wtot = reinterpret_cast<int *>(rowbuf + 2 * wK);                  // 32
-    uint16_t *perm = reinterpret_cast<uint16_t *>(wtot + 32);              // nwarps * WPW * 32
-    uint16_t *nperm = perm + nwarps * WPW * 32;
+    uint16_t *perm = reinterpret_cast<uint16_t *>(wtot + 32);              // nwords*32, swizzled
+    uint16_t *nperm = perm + nwords * 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const unsigned ltmask = (1u << lane) - 1u;
     const int64_t r0 = rowoff[t];
     const int Mp = (int)(rowoff[t + 1] - r0);
     const uint64_t *rows = cref + (size_t)r0 * wK;
     uint32_t *out = pbwt + (size_t)(2 * r0 + (dir ? Mp : 0)) * rowstride;
-    const int wbase = warp * WPW;                   // the warp's first word
-    const int nchunk = wK / 2;                      // 16-byte pieces of a row
-    // identity order; the padding positions past K hold haplotype 0 (never
-    // written later, never used for a bit)
-    for (int i = tid; i < nwarps * WPW * 32; i += nthreads) perm[i] = nperm[i] = (uint16_t)(i < K ? i : 0);
+    const int w0 = tid * WPT;                      // the thread's first word
+    const int nchunk = wK / 2;                     // 16-byte pieces of a row
+    // identity order; the padding positions past K hold haplotype 0 in both
+    // arrays (never written later, never used for a bit)
+    for (int i = tid; i < nwords * 32; i += nthreads) perm[pswz(i)] = nperm[pswz(i)] = (uint16_t)(i < K ? i : 0);
     if (Mp > 0) {
         const uint64_t *src = rows + (size_t)(dir ? Mp - 1 : 0) * wK;
         for (int c = tid; c < nchunk; c += nthreads) cp_async16(rowbuf + 2 * c, src + 2 * c);
@@ -576,91 +571,83 @@ __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__
             for (int c = tid; c < nchunk; c += nthreads) cp_async16(dst + 2 * c, src + 2 * c);
         }
         cp_async_commit();
-        // pass 1: the warp's words in the current prefix order
-        uint32_t hp[WPW / 2];    // haplotypes of positions (wbase + j) * 32 + lane, two per register
-        uint32_t myw0 = ~0u, myw1 = ~0u;   // word wbase + lane (and wbase + 32 + lane)
-        int zw = 0;
+        // the thread's data words in the current prefix order
+        uint32_t word[WPT];
+        int zsum = 0;
 #pragma unroll
-        for (int j = 0; j < WPW; j++) {
-            const int p = (wbase + j) * 32 + lane;
-            uint32_t h = 0u, bit = 1u;
-            if (p < K) {
-                h = perm[p];
-                bit = (row[h >> 5] >> (h & 31)) & 1u;
-            }
-            if (j & 1) hp[j >> 1] |= h << 16;
-            else hp[j >> 1] = h;
-            const uint32_t b = __ballot_sync(FULL, bit);
-            if (lane == (j & 31)) {
-                if (j < 32) myw0 = b;
-                else myw1 = b;
-            }
-            zw += __popc(~b);
-        }
-        if (lane == 0) wtot[warp] = zw;
-        __syncthreads();
-        int zb = 0, cnt0 = 0;
-        for (int q = 0; q < nwarps; q++) {
-            const int v = wtot[q];
-            cnt0 += v;
-            if (q < warp) zb += v;
-        }
-        // the output pairs: zeros through each word by a scan across the lanes
-        uint32_t *o = out + (size_t)midx * rowstride;
-        {
-            int inc = __popc(~myw0);
-            for (int d = 1; d < 32; d <<= 1) {
-                const int y = __shfl_up_sync(FULL, inc, d);
-                if (lane >= d) inc += y;
-            }
-            const int w = wbase + lane;
-            if (w < nwords) reinterpret_cast<uint2 *>(o)[w] = make_uint2(myw0, (uint32_t)(zb + inc));
-            if (WPW > 32) {
-                int inc1 = __popc(~myw1);
-                for (int d = 1; d < 32; d <<= 1) {
-                    const int y = __shfl_up_sync(FULL, inc1, d);
-                    if (lane >= d) inc1 += y;
+        for (int q = 0; q < WPT; q++) {
+            const int w = w0 + q;
+            uint32_t b = ~0u;
+            if (w < nwords) {
+                const uint16_t *pw = perm + w * 32;
+                const int key = w & 31;
+                b = 0u;
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const int h = pw[j ^ key];
+                    const uint32_t bit = (w * 32 + j < K) ? (row[h >> 5] >> (h & 31)) & 1u : 1u;
+                    b |= bit << j;
                 }
-                const int zb1 = zb + __shfl_sync(FULL, inc, 31);
-                if (w + 32 < nwords) reinterpret_cast<uint2 *>(o)[w + 32] = make_uint2(myw1, (uint32_t)(zb1 + inc1));
+                zsum += __popc(~b);
             }
+            word[q] = b;
         }
-        // pass 2: stable placement in the next prefix order
-        int z = zb;   // zeros before the current word
+        // zeros before the thread's words: warp scan, then the warps' totals
+        int inc = zsum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) wtot[warp] = inc;
+        __syncthreads();
+        int zb = inc - zsum, cnt0 = 0;
+        for (int q = 0; q < nwarps; q++) { const int v = wtot[q]; cnt0 += v; if (q < warp) zb += v; }
+        uint32_t *o = out + (size_t)midx * rowstride;
 #pragma unroll
-        for (int j = 0; j < WPW; j++) {
-            const uint32_t b = __shfl_sync(FULL, j < 32 ? myw0 : myw1, j & 31);
-            const int p = (wbase + j) * 32 + lane;
-            if (p < K) {
-                const int zp = z + __popc(~b & ltmask);   // zeros before position p
-                const int dst = ((b >> lane) & 1u) ? cnt0 + (p - zp) : zp;
-                nperm[dst] = (uint16_t)((j & 1) ? hp[j >> 1] >> 16 : hp[j >> 1] & 0xffffu);
+        for (int q = 0; q < WPT; q++) {
+            const int w = w0 + q;
+            if (w >= nwords) continue;
+            const uint32_t b = word[q];
+            const uint16_t *pw = perm + w * 32;
+            const int key = w & 31;
+            int z = zb;   // zeros before position w*32 + j
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const int p = w * 32 + j;
+                if (p < K) {
+                    const int h = pw[j ^ key];
+                    const int dst = ((b >> j) & 1u) ? cnt0 + (p - z) : z;
+                    nperm[pswz(dst)] = (uint16_t)h;
+                }
+                z += (int)((~b >> j) & 1u);
             }
-            z += __popc(~b);
+            reinterpret_cast<uint2 *>(o)[w] = make_uint2(b, (uint32_t)z);
+            zb = z;
         }
         if (emit_padded)
             for (size_t jj = 2 * (size_t)nwords + tid; jj < rowstride; jj += nthreads) o[jj] = 0u;
-        if (dir == 0 && tid == 0) count0[r0 + m] = cnt0;
+        if (dir == 0 && tid == nthreads - 1) count0[r0 + m] = cnt0;
         uint16_t *tp = perm; perm = nperm; nperm = tp;
     }
     cp_async_wait_all();
 }
 
 // shared memory of a CTA: two rows, the warps' zero totals, two prefix arrays
-static size_t pbwt_smem(int K, int nwarps, int wpw) {
-    return (size_t)2 * eimp_W(K) * 8 + 32 * 4 + (size_t)2 * nwarps * wpw * 32 * 2;
+static size_t pbwt_smem(int K) {
+    const int nwords = (K + 31) / 32;
+    return (size_t)2 * eimp_W(K) * 8 + 32 * 4 + (size_t)2 * nwords * 32 * 2;
 }
 
-template <int WPW>
+template <int WPT>
 static cudaError_t launch_pbwt_w(const uint64_t *cref, int32_t *count0, const int64_t *rowoff, int ntgt, int K,
                                  uint32_t *pbwt, size_t rowstride, int emit_padded, const int *skip,
                                  cudaStream_t st) {
     const int nwords = (K + 31) / 32;
-    const int nwarps = (nwords + WPW - 1) / WPW;
-    const size_t sm = pbwt_smem(K, nwarps, WPW);
-    cudaError_t e = cudaFuncSetAttribute(pbwt_kernel<WPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int nthreads = ((nwords + WPT - 1) / WPT + 31) / 32 * 32;
+    const size_t sm = pbwt_smem(K);
+    cudaError_t e = cudaFuncSetAttribute(pbwt_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    pbwt_kernel<WPW><<<2 * ntgt, nwarps * 32, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0, skip);
+    pbwt_kernel<WPT><<<2 * ntgt, nthreads, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0, skip);
     return cudaGetLastError();
 }
 
@@ -669,9 +656,8 @@ cudaError_t launch_pbwt(const uint64_t *cref, int32_t *count0, const int64_t *ro
     // the 8-byte pair stores need 8-byte aligned rows
     if (K < 1 || K > 65536 || rowstride % 2) return cudaErrorInvalidValue;
     const int nwords = (K + 31) / 32;
-    // 32 words per warp up to 32 warps; beyond K = 32768, 64 words per warp
-    if (nwords <= 1024) return launch_pbwt_w<32>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
-    return launch_pbwt_w<64>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
+    if (nwords <= 1024) return launch_pbwt_w<1>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
+    return launch_pbwt_w<2>(cref, count0, rowoff, ntgt, K, pbwt, rowstride, emit_padded, skip, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -4,8 +4,8 @@ on the CPU under the host warp emulator with the address and
 undefined-behaviour sanitizers: every compressed row ([data, zeros through the
 word] pairs, the tail padded with ones), the row padding and the forward zero
 counts must equal the oracle restatement, for K a multiple of 32 and not, K
-below one word, several warps, 64 words per warp, an empty target and rows of
-all zeros and all ones."""
+below one word, several warps, two words per thread, an empty target and rows
+of all zeros and all ones."""
 import os
 import shutil
 import subprocess
@@ -35,8 +35,8 @@ def emu_exe(tmp_path_factory):
     shutil.copy(os.path.join(CSRC, "common.cuh"), d / "common.cuh")
     shutil.copy(os.path.join(CSRC, "kernels.h"), d / "kernels.h")
     src = open(os.path.join(CSRC, "phase_prep.cu")).read()
-    i = src.index("template <int WPW>\n__global__")
-    j = src.index("template <int WPW>\nstatic cudaError_t launch_pbwt_w(")
+    i = src.index("// position p of the prefix order -> its slot in the swizzled array")
+    j = src.index("template <int WPT>\nstatic cudaError_t launch_pbwt_w(")
     body = src[i:j]
     a = "extern __shared__ __align__(16) uint8_t smem[];"
     assert a in body
@@ -59,16 +59,16 @@ def _rows(rng, n, K):
     return np.packbits(bits, axis=1, bitorder="little").view(np.uint64).reshape(n, wK)
 
 
-@pytest.mark.parametrize("K,wpw,nrows", [(4096, 32, [9, 0, 5]), (1000, 32, [7, 3]), (20, 32, [6]),
-                                         (2200, 64, [4, 5]), (64, 32, [1, 2])])
-def test_pbwt_emulated(emu_exe, tmp_path, K, wpw, nrows):
+@pytest.mark.parametrize("K,wpt,nrows", [(4096, 1, [9, 0, 5]), (1000, 1, [7, 3]), (20, 1, [6]),
+                                         (2200, 2, [4, 5]), (64, 1, [1, 2])])
+def test_pbwt_emulated(emu_exe, tmp_path, K, wpt, nrows):
     from oracle import restate as R
     rng = np.random.default_rng(K * 31 + len(nrows))
     rowoff = np.concatenate([[0], np.cumsum(nrows)]).astype(np.int64)
     cref = _rows(rng, int(rowoff[-1]), K)
     kw = 2 * ((K + 31) // 32)
     rowstride = kw + 6
-    np.array([len(nrows), K, rowstride, 1, wpw], np.int32).tofile(tmp_path / "params_i.bin")
+    np.array([len(nrows), K, rowstride, 1, wpt], np.int32).tofile(tmp_path / "params_i.bin")
     rowoff.tofile(tmp_path / "rowoff.bin")
     cref.tofile(tmp_path / "cref.bin")
     r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)

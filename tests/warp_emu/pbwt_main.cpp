@@ -4,7 +4,7 @@
 //
 //   pbwt_emu <dir>
 //
-// <dir> holds params_i.bin (ntgt, K, rowstride, emit_padded, wpw),
+// <dir> holds params_i.bin (ntgt, K, rowstride, emit_padded, wpt),
 // rowoff.bin (ntgt+1 int64) and cref.bin (rows x W(K) words).  Outputs:
 // o_pbwt.bin (2 * rows x rowstride uint32, forward then backward rows of each
 // target), o_count0.bin (rows int32).  Exit status 3: a divergent warp
@@ -47,12 +47,12 @@ int main(int argc, char **argv) {
     const auto pi = rd<int32_t>(d, "params_i.bin");
     const auto rowoff = rd<int64_t>(d, "rowoff.bin");
     const auto cref = rd<uint64_t>(d, "cref.bin");
-    const int ntgt = pi[0], K = pi[1], rowstride = pi[2], emit_padded = pi[3], wpw = pi[4];
+    const int ntgt = pi[0], K = pi[1], rowstride = pi[2], emit_padded = pi[3], wpt = pi[4];
     const size_t rows = (size_t)rowoff[ntgt];
     std::vector<uint32_t> pbwt(2 * rows * rowstride, 0xdeadbeefu);
     std::vector<int32_t> count0(rows, -7);
-    const int nwords = (K + 31) / 32, nwarps = (nwords + wpw - 1) / wpw, nthreads = nwarps * 32;
-    const size_t smem_bytes = eimp::pbwt_smem(K, nwarps, wpw);
+    const int nwords = (K + 31) / 32, nthreads = ((nwords + wpt - 1) / wpt + 31) / 32 * 32, nwarps = nthreads / 32;
+    const size_t smem_bytes = eimp::pbwt_smem(K);
     for (int b = 0; b < 2 * ntgt; b++) {
         std::vector<uint64_t> smem((smem_bytes + 7) / 8, 0x5a5a5a5a5a5a5a5aull);   // exact size: ASan sees overruns
         std::vector<EmuWarp> warps(nwarps);
@@ -67,11 +67,11 @@ int main(int argc, char **argv) {
                 emu_warp = &warps[t / 32];
                 emu_block = &block;
                 emu_smem_ptr = reinterpret_cast<uint8_t *>(smem.data());
-                if (wpw == 32)
-                    eimp::pbwt_kernel<32>(cref.data(), rowoff.data(), K, pbwt.data(), rowstride, emit_padded,
+                if (wpt == 1)
+                    eimp::pbwt_kernel<1>(cref.data(), rowoff.data(), K, pbwt.data(), rowstride, emit_padded,
                                           count0.data(), nullptr);
                 else
-                    eimp::pbwt_kernel<64>(cref.data(), rowoff.data(), K, pbwt.data(), rowstride, emit_padded,
+                    eimp::pbwt_kernel<2>(cref.data(), rowoff.data(), K, pbwt.data(), rowstride, emit_padded,
                                           count0.data(), nullptr);
             });
         for (auto &x : threads) x.join();
