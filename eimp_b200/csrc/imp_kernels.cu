@@ -517,13 +517,17 @@ __global__ void __launch_bounds__(WARPS * 32) smm_kernel(
 // bookkeeping in the extension-index arrays.  Same algorithm and output as
 // smm_kernel above.
 // ---------------------------------------------------------------------------
-template <int NODES> struct SmmTree {
-    int l[NODES], r[NODES];
+// IV: the interval bounds' type -- 16 bits when the reference PBWT holds at
+// most 65,536 haplotypes (22 bytes per node instead of 30, so more warps fit
+// an SM), else 32 bits.  An empty extension interval stored over a node's own
+// (r = -1) is never read back, so its wrap in 16 bits does no harm.
+template <int NODES, typename IV> struct SmmTree {
+    IV l[NODES], r[NODES];
     unsigned dps[NODES];              // depth | (parent + 1) << 16 | side << 31
     unsigned char e[NODES];           // errors
 };
-template <int NODES> struct SmmWarpSmemC {
-    SmmTree<NODES> A, B;
+template <int NODES, typename IV = int> struct SmmWarpSmemC {
+    SmmTree<NODES, IV> A, B;
     short idx0[NODES];                // extension positions; kept positions in the merge pass
     short idx1[NODES];                // extension positions; run starts in the merge pass
     unsigned cflag[NODES / 16];       // 2 bits per node: which children it has
@@ -536,7 +540,7 @@ __device__ __forceinline__ unsigned dps_make(int depth, int parent, int side) {
     return (unsigned)depth | ((unsigned)(parent + 1) << 16) | ((unsigned)side << 31);
 }
 
-template <int NODES, int WARPS, bool RETRY>
+template <int NODES, int WARPS, bool RETRY, typename IV>
 __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
     const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
     const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
@@ -548,8 +552,8 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
     if (hi >= nhaps) return;
     const int hap = hapmap ? hapmap[hi] : hi;   // the haplotypes that exist (PBWTImputer.cpp:130)
     if (RETRY && nmatch[hap] != SMM_RETRY) return;
-    SmmWarpSmemC<NODES> &S = reinterpret_cast<SmmWarpSmemC<NODES> *>(smem_raw)[wid];
-    SmmTree<NODES> *A = &S.A, *B = &S.B;   // the tree and the one being built; swapped when a site merges nothing
+    SmmWarpSmemC<NODES, IV> &S = reinterpret_cast<SmmWarpSmemC<NODES, IV> *>(smem_raw)[wid];
+    SmmTree<NODES, IV> *A = &S.A, *B = &S.B;   // the tree and the one being built; swapped when a site merges nothing
     const uint8_t *g = gt + (size_t)(hap >> 1) * M;
     const uint64_t *hw = phased + (size_t)hap * wM;
     int4 *out = matches + (size_t)hap * cap;
@@ -564,7 +568,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
 
     uint32_t err = 0;
     int n = 1, nres = 0, td = 0;
-    if (lane == 0) { A->l[0] = 0; A->r[0] = K - 1; A->dps[0] = dps_make(0, -1, 0); A->e[0] = 0; }
+    if (lane == 0) { A->l[0] = 0; A->r[0] = (IV)(K - 1); A->dps[0] = dps_make(0, -1, 0); A->e[0] = 0; }
     __syncwarp();
 
     for (int m = 0; m <= M; m++) {
@@ -595,8 +599,8 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
                 const int p0 = e0 ? 1 + cnt0 + __popc(b0 & lanemask_lt()) : -1;
                 S.idx0[i] = (short)p0;
                 S.idx1[i] = e1 ? (short)(cnt1 + __popc(b1 & lanemask_lt())) : (short)-1;   // offset added below
-                if (p0 >= 0 && p0 < NODES) { B->l[p0] = l0; B->r[p0] = r0; }
-                A->l[i] = l1; A->r[i] = r1;
+                if (p0 >= 0 && p0 < NODES) { B->l[p0] = (IV)l0; B->r[p0] = (IV)r0; }
+                A->l[i] = (IV)l1; A->r[i] = (IV)r1;
             }
             if (dead) {
                 const int pos = nres + newcount + __popc(bd & lanemask_lt());
@@ -633,7 +637,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
                 B->e[q] = (unsigned char)((!curr && !missing) ? ne + 1 : ne);
             }
         }
-        if (lane == 0) { B->l[0] = 0; B->r[0] = K - 1; B->dps[0] = dps_make(0, -1, 0); B->e[0] = 0; }
+        if (lane == 0) { B->l[0] = 0; B->r[0] = (IV)(K - 1); B->dps[0] = dps_make(0, -1, 0); B->e[0] = 0; }
         for (int q = lane; q < (nb + 15) / 16; q += 32) S.cflag[q] = 0u;
         __syncwarp();
         // pass 3: merges (TargetImp.cpp:405-432).  Child flags first.
@@ -689,7 +693,7 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
             }
             A->l[np] = B->l[u]; A->r[np] = B->r[u]; A->dps[np] = x; A->e[np] = B->e[u];
         }
-        if (kept == nb) { SmmTree<NODES> *t = A; A = B; B = t; }
+        if (kept == nb) { SmmTree<NODES, IV> *t = A; A = B; B = t; }
         __syncwarp();
         n = kept;
         for (int o = 16; o; o >>= 1) md = max(md, __shfl_xor_sync(FULL, md, o));
@@ -1096,31 +1100,42 @@ static cudaError_t smm_launch(Kern kern, int warps, const uint32_t *compr, const
     return cudaGetLastError();
 }
 
+template <typename IV>
+static cudaError_t launch_smm_compact(const uint32_t *compr, const int32_t *count0, int M, int K,
+                                      const uint64_t *phased, int wM, const uint8_t *gt, int nhaps,
+                                      const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap, int *nmatch,
+                                      uint32_t *status, int warps, cudaStream_t st) {
+    using Small = SmmWarpSmemC<SMM_NODES, IV>;
+    cudaError_t e;
+    // warps per CTA of the first pass: 1, 2 or 4
+    if (warps == 1)
+        e = smm_launch<Small>(smm_compact_kernel<SMM_NODES, 1, false, IV>, 1, compr, count0, M, K, phased, wM, gt,
+                              nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st);
+    else if (warps == 4)
+        e = smm_launch<Small>(smm_compact_kernel<SMM_NODES, 4, false, IV>, 4, compr, count0, M, K, phased, wM, gt,
+                              nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st);
+    else
+        e = smm_launch<Small>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false, IV>, SMMC_WARPS, compr, count0, M, K,
+                              phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st);
+    if (e != cudaSuccess) return e;
+    return smm_launch<SmmWarpSmemC<SMM_NODES_RETRY, IV>>(smm_compact_kernel<SMM_NODES_RETRY, 1, true, IV>, 1, compr,
+                                                         count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
+                                                         matches, cap, nmatch, status, st);
+}
+
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
                        const uint8_t *gt, int nhaps, const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap,
                        int *nmatch, uint32_t *status, int warps, cudaStream_t st) {
-    cudaError_t e;
-    if (M < 65536) {   // depths fit the compact tree; warps per CTA of the first pass: 1, 2 or 4
-        if (warps == 1)
-            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, 1, false>, 1, compr, count0, M, K,
-                                                    phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
-                                                    status, st);
-        else if (warps == 4)
-            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, 4, false>, 4, compr, count0, M, K,
-                                                    phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,
-                                                    status, st);
-        else
-            e = smm_launch<SmmWarpSmemC<SMM_NODES>>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false>, SMMC_WARPS,
-                                                    compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
-                                                    matches, cap, nmatch, status, st);
-        if (e != cudaSuccess) return e;
-        return smm_launch<SmmWarpSmemC<SMM_NODES_RETRY>>(smm_compact_kernel<SMM_NODES_RETRY, 1, true>, 1, compr,
-                                                         count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
-                                                         matches, cap, nmatch, status, st);
+    if (M < 65536) {   // depths fit the compact tree; interval bounds in 16 bits up to 65,536 haplotypes
+        if (K <= 65536)
+            return launch_smm_compact<uint16_t>(compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
+                                                matches, cap, nmatch, status, warps, st);
+        return launch_smm_compact<int>(compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap,
+                                       nmatch, status, warps, st);
     }
-    e = smm_launch<SmmWarpSmem<SMM_NODES>>(smm_kernel<SMM_NODES, SMM_WARPS, false>, SMM_WARPS, compr, count0, M, K,
-                                           phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status,
-                                           st);
+    cudaError_t e = smm_launch<SmmWarpSmem<SMM_NODES>>(smm_kernel<SMM_NODES, SMM_WARPS, false>, SMM_WARPS, compr,
+                                                       count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
+                                                       matches, cap, nmatch, status, st);
     if (e != cudaSuccess) return e;
     return smm_launch<SmmWarpSmem<SMM_NODES_RETRY>>(smm_kernel<SMM_NODES_RETRY, 1, true>, 1, compr, count0, M, K,
                                                     phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch,

@@ -2,7 +2,8 @@
 // section of eimp_b200/csrc/imp_kernels.cu) one target haplotype at a time
 // under the warp emulator.
 //
-//   smm_emu <dir> <kernel>      kernel 0: smm_kernel, 1: smm_compact_kernel
+//   smm_emu <dir> <kernel>      kernel 0: smm_kernel, 1: smm_compact_kernel (32-bit
+//                               intervals), 2: smm_compact_kernel (16-bit intervals)
 //
 // Both launches of launch_smm run: the small node pool first, then the retry
 // pass with the large pool.  <dir> holds the inputs as raw little-endian arrays in the layout of the
@@ -61,10 +62,12 @@ int main(int argc, char **argv) {
     int retried = 0;
     // the launches of launch_smm: the small node pool, then the retry pass
     for (int pass = 0; pass < 2; pass++) {
-        const size_t smb = which ? (pass ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY>)
-                                         : sizeof(eimp::SmmWarpSmemC<SMM_NODES>))
-                                 : (pass ? sizeof(eimp::SmmWarpSmem<SMM_NODES_RETRY>)
-                                         : sizeof(eimp::SmmWarpSmem<SMM_NODES>));
+        const size_t smb = which == 2 ? (pass ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY, uint16_t>)
+                                              : sizeof(eimp::SmmWarpSmemC<SMM_NODES, uint16_t>))
+                           : which ? (pass ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY>)
+                                           : sizeof(eimp::SmmWarpSmemC<SMM_NODES>))
+                                   : (pass ? sizeof(eimp::SmmWarpSmem<SMM_NODES_RETRY>)
+                                           : sizeof(eimp::SmmWarpSmem<SMM_NODES>));
         for (int h = 0; h < nhaps; h++) {
             if (pass) retried += nmatch[h] == eimp::SMM_RETRY;
             // a fill pattern instead of zeros: the kernel must not read what it has not written
@@ -78,10 +81,12 @@ int main(int argc, char **argv) {
                     blockIdx.x = h;
                     emu_warp = &warp;
                     emu_smem_ptr = smem;
-                    auto kern = which ? (pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true>
-                                              : eimp::smm_compact_kernel<SMM_NODES, 1, false>)
-                                      : (pass ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true>
-                                              : eimp::smm_kernel<SMM_NODES, 1, false>);
+                    auto kern = which == 2 ? (pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, uint16_t>
+                                                   : eimp::smm_compact_kernel<SMM_NODES, 1, false, uint16_t>)
+                                : which ? (pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, int>
+                                                : eimp::smm_compact_kernel<SMM_NODES, 1, false, int>)
+                                        : (pass ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true>
+                                                : eimp::smm_kernel<SMM_NODES, 1, false>);
                     kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
                          matches.data(), cap, nmatch.data(), &status);
                 });
