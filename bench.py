@@ -53,10 +53,9 @@ CPU_SAMPLE = {"cfg2": 200, "cfg3": 32}
 # haplotypes of each CPU sample whose dosages are also checked against the
 # FP64 dosage oracle (score/sum in double, not rounded to float)
 PARITY_FP64_HAPS = 32
-# device memory per density group for the condensed references and PBWTs of
-# one phasing batch (the beam arenas belong to the resident warps, not to
-# the targets)
-PHASE_BATCH_BYTES = 36e9
+# device memory kept free beside the groups' buffers (the library's own
+# staging, the graph form, allocator slack)
+DEVICE_RESERVE_BYTES = 24e9
 
 
 def parse():
@@ -582,14 +581,28 @@ def cfg4_leg(args, local, dev):
 
 
 # ---------------------------------------------------------------- our arm
-def auto_batch(M, K, nt):
-    """Targets per phasing batch within PHASE_BATCH_BYTES: about 0.25*M
-    condensed rows per target (S ~ 0.12 M split sites at ~11 % heterozygous
-    sites) of W(K) words plus two PBWT directions, and the per-target prep
-    vectors."""
+def phase_batch_targets(cfg, tgroups, Mref, nh, free_bytes):
+    """Targets per phasing batch of each density group.  A batch's condensed
+    references and PBWTs take about 0.25*M condensed rows per target (S ~
+    0.12 M split sites at ~11 % heterozygous sites) of W(K) words plus two PBWT
+    directions, and the per-target prep vectors.  Every group phases all its
+    targets in one batch when those rows fit the device memory left after the
+    groups' fixed buffers (dosages and imputed alleles of all sites, the
+    imputation reference, the beam arenas of the resident warps); otherwise
+    each group gets a share of it in proportion to its need."""
+    K = min(cfg.K, nh)
     kw = 2 * ((K + 31) // 32)
-    per = 0.25 * M * (W(K) * 8 + 2 * kw * 4 + 8) + 20.0 * M
-    return int(max(64, min(nt, PHASE_BATCH_BYTES // per)))
+    ldb = (Mref + 63) // 64
+    need, fixed = [], 0.0
+    for tg in tgroups:
+        nt, M = tg.gt.shape
+        need.append(nt * (0.25 * M * (W(K) * 8 + 2 * kw * 4 + 8) + 20.0 * M))
+        fixed += 2 * nt * (Mref * 4 + ldb * 8)                                  # dosages, alleles
+        fixed += nh * ldb * 8 + 4.0 * (M + 1) * nh + M * 2 * ((nh + 31) // 32) * 4   # imputation reference
+        fixed += 2.5e9                                                          # beam arenas, prep vectors
+    budget = max(0.0, free_bytes - fixed - DEVICE_RESERVE_BYTES)
+    scale = min(1.0, budget / max(1.0, sum(need)))
+    return [int(max(64, min(tg.gt.shape[0], tg.gt.shape[0] * scale))) for tg in tgroups]
 
 
 def main():
@@ -623,17 +636,21 @@ def main():
     d_af = todev(panel.af.astype(np.float32))
     params = PhaseParams(K=cfg.K, beamwidth=cfg.beam)
     groups = []
-    for tg in tgroups:
+    free_b, _tot = torch.cuda.mem_get_info(dev)
+    bsizes = phase_batch_targets(cfg, tgroups, Mref, nh_ref, free_b)
+    for tg, bauto in zip(tgroups, bsizes):
         hm, sm, cm = synth.typed_views(panel, tg.typed)
-        B = args.batch_targets or auto_batch(len(tg.typed), min(cfg.K, nh_ref), tg.gt.shape[0])
+        B = args.batch_targets or bauto
         groups.append(DensityGroup(local, d_full, d_af, nh_ref, tg.typed, hm, sm, cm, tg.gt, params, B))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     # launch shapes tuned on every group's own data (eimp_b200/autotune.py)
     tuning = None
     if not args.no_autotune:
-        from eimp_b200.autotune import tune_group
-        tuning = [tune_group(g) for g in groups]
+        from eimp_b200.autotune import tune_group, tune_step_shares
+        tuning = {"groups": [tune_group(g) for g in groups]}
+        if len(groups) > 1:
+            tuning["step_beam_shares"] = tune_step_shares(groups)
 
     def step_timed(graphs=False):
         e0, e1 = ev(), ev()

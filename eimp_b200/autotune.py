@@ -14,6 +14,12 @@ context.  Knobs (eimp_set_launch_shape, include/eimp_gpu.h):
 
 Timing is on the device (CUDA events on the group's stream), best of
 ``reps`` runs; the phasing knob is timed over all of the group's batches.
+
+Alone, every group wants all of the SMs for its beam.  In a step the groups
+run side by side and the densest group's chain of kernels is the critical
+path, so :func:`tune_step_shares` then times whole steps with the lighter
+groups' beams held to smaller shares of the resident warps (their kernels
+still overlap the dense group's) and keeps the fastest.
 """
 from __future__ import annotations
 
@@ -81,3 +87,43 @@ def tune_group(group, reps: int = 2, knobs=("dosage_span", "smm_warps", "beam_sl
     group.enqueue()
     group.ctx.synchronize()
     return out
+
+
+def tune_step_shares(groups, reps: int = 1) -> dict:
+    """Step-level choice of the beam shares: the groups with the most
+    condensed rows keep their own choice, the lighter ones get each candidate
+    share set in turn (uniform 100, 75 or 50 %, or graded from 50 % for the
+    lightest up to 75 %); whole steps are timed on the device and the fastest
+    set stays on the groups.  Returns {"chosen": [...], "ms": {label: ms}}."""
+    import torch
+    from .batch import enqueue_step, step_order
+    order = step_order(groups)            # heaviest first
+    light = order[1:]
+    if not light:
+        return {"chosen": [get(g, "beam_slots_pct") for g in groups], "ms": {}}
+    graded = {i: (50 if r == len(light) - 1 else 75) for r, i in enumerate(light)}
+    cands = {"own": {i: get(groups[i], "beam_slots_pct") for i in light},
+             "75": {i: 75 for i in light}, "50": {i: 50 for i in light}, "graded": graded}
+    dev = groups[0].dev
+    main = torch.cuda.current_stream(dev)
+    times = {}
+    for label, shares in cands.items():
+        for i, v in shares.items():
+            set_shape(groups[i], "beam_slots_pct", v)
+        best = float("inf")
+        for _ in range(reps):
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(main)
+            for e in enqueue_step(groups, e0):
+                main.wait_event(e)
+            e1.record(main)
+            torch.cuda.synchronize(dev)
+            for g in groups:
+                g.ctx.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        times[label] = round(best, 3)
+    label = min(times, key=times.get)
+    for i, v in cands[label].items():
+        set_shape(groups[i], "beam_slots_pct", v)
+    return {"chosen": [get(g, "beam_slots_pct") for g in groups], "label": label, "ms": times}

@@ -153,13 +153,22 @@ class DensityGroup:
         self.ctx.close()
 
 
+def step_order(groups):
+    """The order in which a step enqueues its groups: most condensed rows
+    (phasing work) first, so that the longest chain of kernels -- the densest
+    group's -- takes the SMs first and the lighter groups fill in beside it."""
+    return sorted(range(len(groups)), key=lambda i: -sum(groups[i].rows))
+
+
 def enqueue_step(groups, start_event=None, capture_graphs=False):
     """One step of every group: each group's stream waits for start_event
     (when given), the groups run concurrently, and the returned events (one
-    per group, recorded at the end of its step) mark their ends."""
+    per group, in the order of ``groups``, recorded at the end of its step)
+    mark their ends."""
     import torch
-    ends = []
-    for g in groups:
+    ends = [None] * len(groups)
+    for i in step_order(groups):
+        g = groups[i]
         if start_event is not None:
             g.stream.wait_event(start_event)
         if capture_graphs:
@@ -168,5 +177,5 @@ def enqueue_step(groups, start_event=None, capture_graphs=False):
             g.enqueue()
         e = torch.cuda.Event()
         e.record(g.stream)
-        ends.append(e)
+        ends[i] = e
     return ends
