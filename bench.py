@@ -858,8 +858,11 @@ def main():
 
     # ---- end to end through the host API: pinned genotypes in, phased
     # haplotypes back to the host, phased haplotypes in again for the
-    # imputation, dosages and alleles out; the groups one after the other,
-    # through one set of pinned buffers sized for the largest group
+    # imputation, dosages and alleles out.  Every group's chain of host calls
+    # runs in its own host thread with its own pinned buffers (the library's
+    # calls release the interpreter lock and each group has its own context
+    # and streams), so the groups overlap on the device as in the step and a
+    # group's copies overlap the others' kernels
     e2e = None
     if args.e2e_steps > 0:
         # the step's device outputs are no longer needed (parity uses the
@@ -867,51 +870,59 @@ def main():
         for g in groups:
             g.d_dos = g.d_bits = None
         torch.cuda.empty_cache()
-        nmax = max(g.nt for g in groups)
-        wMmax = max(g.wM for g in groups)
-        Mmax = max(g.M for g in groups)
         pin = lambda *shape, dt=torch.int64: torch.empty(shape, dtype=dt).pin_memory()  # noqa: E731
-        gt_pin = pin(nmax * Mmax, dt=torch.uint8)
-        ph_pin = pin(2 * nmax * wMmax)
-        mats_pin, pats_pin = pin(nmax * wMmax), pin(nmax * wMmax)
-        pdm_pin, pdp_pin = pin(nmax * Mmax, dt=torch.float32), pin(nmax * Mmax, dt=torch.float32)
-        tc_pin, nc_pin = pin(nmax, dt=torch.float32), pin(nmax, dt=torch.int32)
-        dos_pin = pin(2 * nmax * Mref, dt=torch.float32)
-        bits_pin = pin(2 * nmax * W(Mref))
+        bufs = []
         h2d = d2h = 0
         for g in groups:
+            bufs.append({"gt": pin(g.nt, g.M, dt=torch.uint8), "ph": pin(g.nt, 2, g.wM), "mats": pin(g.nt, g.wM),
+                         "pats": pin(g.nt, g.wM), "pdm": pin(g.nt, g.M, dt=torch.float32),
+                         "pdp": pin(g.nt, g.M, dt=torch.float32), "tc": pin(g.nt, dt=torch.float32),
+                         "nc": pin(g.nt, dt=torch.int32), "dos": pin(2 * g.nt, Mref, dt=torch.float32),
+                         "bits": pin(2 * g.nt, W(Mref))})
             h2d += 2 * g.nt * g.M + 2 * g.nt * g.wM * 8
             d2h += 2 * g.nt * g.wM * 8 + 2 * g.nt * g.M * 4 + g.nt * 8 + 2 * g.nt * Mref * 4 + 2 * g.nt * W(Mref) * 8
 
-        def e2e_group(g):
+        def e2e_group(g, b):
             L, h = g.L, g.h
-            gv = gt_pin[:g.nt * g.M].view(g.nt, g.M)
-            gv.copy_(torch.from_numpy(g.gt_host))
-            mv, pv = mats_pin[:g.nt * g.wM].view(g.nt, g.wM), pats_pin[:g.nt * g.wM].view(g.nt, g.wM)
-            dmv, dpv = pdm_pin[:g.nt * g.M].view(g.nt, g.M), pdp_pin[:g.nt * g.M].view(g.nt, g.M)
+            b["gt"].copy_(torch.from_numpy(g.gt_host))
             g.set_reference()
             for b0, b1 in g.batches:
-                g.ctx.check(L.eimp_phase_targets(h, C.byref(g.pc), b1 - b0, gv[b0:b1].data_ptr(),
-                                                 mv[b0:b1].data_ptr(), pv[b0:b1].data_ptr(), dmv[b0:b1].data_ptr(),
-                                                 dpv[b0:b1].data_ptr(), tc_pin[b0:b1].data_ptr(),
-                                                 nc_pin[b0:b1].data_ptr()))
-            phv = ph_pin[:2 * g.nt * g.wM].view(g.nt, 2, g.wM)
-            phv[:, 0].copy_(mv)
-            phv[:, 1].copy_(pv)
-            g.ctx.check(L.eimp_imp_prepare(h, g.nt, phv.data_ptr(), gv.data_ptr(), 0, 0, 0))
-            g.ctx.check(L.eimp_imp_bunch(h, 0, Mref, bits_pin.data_ptr(), dos_pin.data_ptr()))
+                g.ctx.check(L.eimp_phase_targets(h, C.byref(g.pc), b1 - b0, b["gt"][b0:b1].data_ptr(),
+                                                 b["mats"][b0:b1].data_ptr(), b["pats"][b0:b1].data_ptr(),
+                                                 b["pdm"][b0:b1].data_ptr(), b["pdp"][b0:b1].data_ptr(),
+                                                 b["tc"][b0:b1].data_ptr(), b["nc"][b0:b1].data_ptr()))
+            b["ph"][:, 0].copy_(b["mats"])
+            b["ph"][:, 1].copy_(b["pats"])
+            g.ctx.check(L.eimp_imp_prepare(h, g.nt, b["ph"].data_ptr(), b["gt"].data_ptr(), 0, 0, 0))
+            g.ctx.check(L.eimp_imp_bunch(h, 0, Mref, b["bits"].data_ptr(), b["dos"].data_ptr()))
 
-        for g in groups:
-            e2e_group(g)
+        def e2e_step():
+            from eimp_b200.batch import step_order
+            errs = []
+
+            def run(i):
+                try:
+                    e2e_group(groups[i], bufs[i])
+                except Exception as ex:   # re-raised below
+                    errs.append(ex)
+            ths = [threading.Thread(target=run, args=(i,)) for i in step_order(groups)]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
+            if errs:
+                raise errs[0]
+
+        e2e_step()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            for g in groups:
-                e2e_group(g)
+            e2e_step()
         dt = (time.perf_counter() - t0) / args.e2e_steps
         e2e = {"value": world * dos_per_step / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
-               "form": "host API per group in turn: eimp_phase_targets per batch, eimp_imp_prepare, eimp_imp_bunch"}
-        del gt_pin, ph_pin, mats_pin, pats_pin, pdm_pin, pdp_pin, dos_pin, bits_pin
+               "form": "host API, one host thread per group (eimp_phase_targets per batch, eimp_imp_prepare, "
+                       "eimp_imp_bunch) with its own pinned buffers, the groups overlapping on the device"}
+        del bufs
 
     # ---- serving: continuous batching of requests of 1..256 targets of the
     # first group arriving as a Poisson stream, two slots (contexts) on this
