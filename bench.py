@@ -918,8 +918,20 @@ def main():
         for _ in range(args.e2e_steps):
             e2e_step()
         dt = (time.perf_counter() - t0) / args.e2e_steps
+        # the copy bandwidth the dosages meet: one pinned 1 GiB device-to-host copy
+        src = torch.empty(1 << 30, dtype=torch.uint8, device=dev)
+        dst = torch.empty(1 << 30, dtype=torch.uint8).pin_memory()
+        dst.copy_(src)
+        c0, c1 = ev(), ev()
+        c0.record(main_stream)
+        dst.copy_(src, non_blocking=True)
+        c1.record(main_stream)
+        torch.cuda.synchronize()
+        d2h_gbs = (1 << 30) / (c0.elapsed_time(c1) / 1e3) / 1e9
+        del src, dst
         e2e = {"value": world * dos_per_step / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
+               "d2h_copy_gbs": round(d2h_gbs, 1), "d2h_copy_ms_per_step": round(d2h / d2h_gbs / 1e6, 1),
                "form": "host API, one host thread per group (eimp_phase_targets per batch, eimp_imp_prepare, "
                        "eimp_imp_bunch) with its own pinned buffers, the groups overlapping on the device"}
         del bufs
