@@ -100,6 +100,8 @@ struct eimp_ctx {
     int i_imputeCalls = 0;
     size_t i_cap = 0;
     DBuf i_phased, i_gt, i_matches, i_nmatch;
+    // global tree pools of the match search (trees that outgrow shared memory) and their counter
+    DBuf i_gpool, i_gnext;
     // host <-> device staging for bunches
     DBuf i_bits, i_dos;
     // phased dosages (eimp_imp_phased_dosages) and staging of the output statistics
@@ -479,10 +481,17 @@ int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phase
     const int32_t *hapmap = ctx->i_tgthap_n ? ctx->i_hapmap.as<int32_t>() : nullptr;
     const size_t nsearch = ctx->i_tgthap_n ? ctx->i_ntgthaps : nh;
     if (hapmap) CK(cudaMemsetAsync(ctx->i_nmatch.p, 0, nh * sizeof(int), ctx->stream));
+    // up to 2048 haplotypes per launch move a large tree to a global pool
+    // instead of being redone by the retry launch
+    const int gslots = (int)std::min<size_t>(nsearch, 2048);
+    CK(ctx->i_gpool.reserve((size_t)gslots * smm_gpool_slot_bytes((int)ctx->i_K)));
+    CK(ctx->i_gnext.reserve(sizeof(int)));
+    CK(cudaMemsetAsync(ctx->i_gnext.p, 0, sizeof(int), ctx->stream));
     LAUNCH(launch_smm(ctx->i_compr.as<uint32_t>(), ctx->i_count0.as<int32_t>(), (int)M, (int)ctx->i_K,
                       ctx->i_phased.as<uint64_t>(), (int)wM, ctx->i_gt.as<uint8_t>(), (int)nsearch, hapmap,
                       setmaxerrors, ctx->i_matches.as<int4>(), (int)cap, ctx->i_nmatch.as<int>(),
-                      ctx->status.as<uint32_t>(), ctx->shape_smm_warps, ctx->stream));
+                      ctx->status.as<uint32_t>(), ctx->shape_smm_warps, ctx->i_gpool.p, gslots,
+                      ctx->i_gnext.as<int>(), ctx->stream));
     ctx->launches++;   // launch_smm launches twice: the small node pool, then the retry pass
     return 0;
 }

@@ -540,39 +540,25 @@ __device__ __forceinline__ unsigned dps_make(int depth, int parent, int side) {
     return (unsigned)depth | ((unsigned)(parent + 1) << 16) | ((unsigned)side << 31);
 }
 
-template <int NODES, int WARPS, bool RETRY, typename IV>
-__global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
-    const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
-    const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
-    const int32_t *__restrict__ hapmap, int setmaxerrors, int4 *__restrict__ matches, int cap,
-    int *__restrict__ nmatch, uint32_t *__restrict__ status) {
-    extern __shared__ uint8_t smem_raw[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int hi = blockIdx.x * WARPS + wid;
-    if (hi >= nhaps) return;
-    const int hap = hapmap ? hapmap[hi] : hi;   // the haplotypes that exist (PBWTImputer.cpp:130)
-    if (RETRY && nmatch[hap] != SMM_RETRY) return;
-    SmmWarpSmemC<NODES, IV> &S = reinterpret_cast<SmmWarpSmemC<NODES, IV> *>(smem_raw)[wid];
-    SmmTree<NODES, IV> *A = &S.A, *B = &S.B;   // the tree and the one being built; swapped when a site merges nothing
-    const uint8_t *g = gt + (size_t)(hap >> 1) * M;
-    const uint64_t *hw = phased + (size_t)hap * wM;
-    int4 *out = matches + (size_t)hap * cap;
-    const size_t kw = eimp_kw(K);
+// The sites [m0, M] of one haplotype's match search on a tree pool of NODES
+// nodes (S, in shared or in global memory); A is the tree, B the one being
+// built.  Returns M + 1 when the haplotype is done (or its tree outgrew the
+// pool: err), or -- with can_switch -- the first site whose pass could
+// outgrow the pool, before touching the tree, so that the caller can move it
+// to a larger pool and go on from that site.
+template <int NODES, typename IV>
+__device__ int smm_compact_sites(SmmWarpSmemC<NODES, IV> &S, SmmTree<NODES, IV> *&A, SmmTree<NODES, IV> *&B,
+                                 int m0, bool can_switch, const uint32_t *__restrict__ compr,
+                                 const int32_t *__restrict__ count0, int M, int K, size_t kw, const uint8_t *g,
+                                 const uint64_t *hw, int setmaxerrors, int4 *out, int cap, int &n, int &nres, int &td,
+                                 uint32_t &err) {
+    const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
-
-    // missingness > 50 %: no matches (TargetImp.cpp:79-80)
-    int nmiss = 0;
-    for (int m = lane; m < M; m += 32) nmiss += g[m] == 3;
-    for (int o = 16; o; o >>= 1) nmiss += __shfl_xor_sync(FULL, nmiss, o);
-    if (nmiss > M / 2) { if (lane == 0) nmatch[hap] = 0; return; }
-
-    uint32_t err = 0;
-    int n = 1, nres = 0, td = 0;
-    if (lane == 0) { A->l[0] = 0; A->r[0] = (IV)(K - 1); A->dps[0] = dps_make(0, -1, 0); A->e[0] = 0; }
-    __syncwarp();
-
-    for (int m = 0; m <= M; m++) {
+    for (int m = m0; m <= M; m++) {
         const bool final = (m == M);   // TargetImp.cpp:144: erase pass, every node reports
+        // a site can at most double the tree (plus the new root): hand over to
+        // the larger pool before the pass that could outgrow this one
+        if (can_switch && !final && 2 * n + 1 > NODES) return m;
         const int curr = final ? 0 : bit_at(hw, m);
         const int missing = final ? 0 : (g[m] == 3);
         const uint32_t *crow = compr + (size_t)(final ? 0 : m) * kw;
@@ -612,10 +598,10 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
         __syncwarp();
         if (final) {
             if (nres + newcount <= cap) nres += newcount;
-            break;
+            return M + 1;
         }
         const int nb = 1 + cnt0 + cnt1;
-        if (nb > NODES) { err |= EIMP_ERR_NODE_OVERFLOW; break; }
+        if (nb > NODES) { err |= EIMP_ERR_NODE_OVERFLOW; return M + 1; }
         // pass 2: the rest of B = [new root] ++ 0-tree ++ 1-tree.  The largest
         // depth of B is the largest after the merges too: a merged node has a
         // child, which is deeper
@@ -701,6 +687,70 @@ __global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
         // longer path is still alive
         if (newcount && td >= md && nres + newcount <= cap) nres += newcount;
         td = md;
+    }
+    return M + 1;
+}
+
+// The first launch gives each warp a shared-memory pool of NODES nodes.  A
+// tree that could outgrow it moves, between two sites, to a pool of
+// SMM_NODES_RETRY nodes in global memory (gpool, one slot per such warp, as
+// many as gpool_slots) and the warp goes on from that site; only when no slot
+// is left does the haplotype end with the retry mark for the retry launch
+// (RETRY: shared pools of SMM_NODES_RETRY nodes, one warp per CTA), which
+// redoes it from its first site.
+template <int NODES, int WARPS, bool RETRY, typename IV>
+__global__ void __launch_bounds__(WARPS * 32) smm_compact_kernel(
+    const uint32_t *__restrict__ compr, const int32_t *__restrict__ count0, int M, int K,
+    const uint64_t *__restrict__ phased, int wM, const uint8_t *__restrict__ gt, int nhaps,
+    const int32_t *__restrict__ hapmap, int setmaxerrors, int4 *__restrict__ matches, int cap,
+    int *__restrict__ nmatch, uint32_t *__restrict__ status, SmmWarpSmemC<SMM_NODES_RETRY, IV> *__restrict__ gpool,
+    int gpool_slots, int *__restrict__ gpool_next) {
+    extern __shared__ uint8_t smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int hi = blockIdx.x * WARPS + wid;
+    if (hi >= nhaps) return;
+    const int hap = hapmap ? hapmap[hi] : hi;   // the haplotypes that exist (PBWTImputer.cpp:130)
+    if (RETRY && nmatch[hap] != SMM_RETRY) return;
+    SmmWarpSmemC<NODES, IV> &S = reinterpret_cast<SmmWarpSmemC<NODES, IV> *>(smem_raw)[wid];
+    SmmTree<NODES, IV> *A = &S.A, *B = &S.B;   // the tree and the one being built; swapped when a site merges nothing
+    const uint8_t *g = gt + (size_t)(hap >> 1) * M;
+    const uint64_t *hw = phased + (size_t)hap * wM;
+    int4 *out = matches + (size_t)hap * cap;
+    const size_t kw = eimp_kw(K);
+    const unsigned FULL = 0xffffffffu;
+
+    // missingness > 50 %: no matches (TargetImp.cpp:79-80)
+    int nmiss = 0;
+    for (int m = lane; m < M; m += 32) nmiss += g[m] == 3;
+    for (int o = 16; o; o >>= 1) nmiss += __shfl_xor_sync(FULL, nmiss, o);
+    if (nmiss > M / 2) { if (lane == 0) nmatch[hap] = 0; return; }
+
+    uint32_t err = 0;
+    int n = 1, nres = 0, td = 0;
+    if (lane == 0) { A->l[0] = 0; A->r[0] = (IV)(K - 1); A->dps[0] = dps_make(0, -1, 0); A->e[0] = 0; }
+    __syncwarp();
+    const bool big = !RETRY && gpool != nullptr && NODES < SMM_NODES_RETRY;
+    int m = smm_compact_sites<NODES, IV>(S, A, B, 0, big, compr, count0, M, K, kw, g, hw, setmaxerrors, out, cap, n,
+                                         nres, td, err);
+    if (m <= M) {
+        int slot = 0;
+        if (lane == 0) slot = atomicAdd(gpool_next, 1);
+        slot = __shfl_sync(FULL, slot, 0);
+        if (slot < gpool_slots) {
+            // the tree (n <= NODES / 2 nodes) into the global pool, then on from site m
+            SmmWarpSmemC<SMM_NODES_RETRY, IV> &G = gpool[slot];
+            for (int i = lane; i < n; i += 32) {
+                G.A.l[i] = A->l[i]; G.A.r[i] = A->r[i]; G.A.dps[i] = A->dps[i]; G.A.e[i] = A->e[i];
+            }
+            __syncwarp();
+            SmmTree<SMM_NODES_RETRY, IV> *GA = &G.A, *GB = &G.B;
+            smm_compact_sites<SMM_NODES_RETRY, IV>(G, GA, GB, m, false, compr, count0, M, K, kw, g, hw, setmaxerrors,
+                                                  out, cap, n, nres, td, err);
+        } else {
+            // no slot left: on in shared memory; a tree that outgrows it is retried
+            smm_compact_sites<NODES, IV>(S, A, B, m, false, compr, count0, M, K, kw, g, hw, setmaxerrors, out, cap, n,
+                                         nres, td, err);
+        }
     }
     for (int o = 16; o; o >>= 1) err |= __shfl_xor_sync(FULL, err, o);
     smm_finish(lane, err, RETRY, nres, nmatch, hap, status);
@@ -1086,52 +1136,64 @@ cudaError_t launch_transpose_ld(const uint64_t *src, size_t rows, size_t src_ld,
     return cudaGetLastError();
 }
 
-template <class Smem, class Kern>
+template <class Smem, class Kern, class... Extra>
 static cudaError_t smm_launch(Kern kern, int warps, const uint32_t *compr, const int32_t *count0, int M, int K,
                               const uint64_t *phased, int wM, const uint8_t *gt, int nhaps, const int32_t *hapmap,
                               int setmaxerrors, int4 *matches, int cap, int *nmatch, uint32_t *status,
-                              cudaStream_t st) {
+                              cudaStream_t st, Extra... extra) {
     const size_t sm = sizeof(Smem) * warps;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     const int blocks = (nhaps + warps - 1) / warps;
     kern<<<blocks, warps * 32, sm, st>>>(compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches,
-                                        cap, nmatch, status);
+                                        cap, nmatch, status, extra...);
     return cudaGetLastError();
+}
+
+size_t smm_gpool_slot_bytes(int K) {
+    return K <= 65536 ? sizeof(SmmWarpSmemC<SMM_NODES_RETRY, uint16_t>) : sizeof(SmmWarpSmemC<SMM_NODES_RETRY, int>);
 }
 
 template <typename IV>
 static cudaError_t launch_smm_compact(const uint32_t *compr, const int32_t *count0, int M, int K,
                                       const uint64_t *phased, int wM, const uint8_t *gt, int nhaps,
                                       const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap, int *nmatch,
-                                      uint32_t *status, int warps, cudaStream_t st) {
+                                      uint32_t *status, int warps, void *gpool, int gpool_slots, int *gpool_next,
+                                      cudaStream_t st) {
     using Small = SmmWarpSmemC<SMM_NODES, IV>;
+    using Big = SmmWarpSmemC<SMM_NODES_RETRY, IV>;
+    Big *gp = static_cast<Big *>(gpool);
     cudaError_t e;
     // warps per CTA of the first pass: 1, 2 or 4
     if (warps == 1)
         e = smm_launch<Small>(smm_compact_kernel<SMM_NODES, 1, false, IV>, 1, compr, count0, M, K, phased, wM, gt,
-                              nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st);
+                              nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st, gp, gpool_slots,
+                              gpool_next);
     else if (warps == 4)
         e = smm_launch<Small>(smm_compact_kernel<SMM_NODES, 4, false, IV>, 4, compr, count0, M, K, phased, wM, gt,
-                              nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st);
+                              nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st, gp, gpool_slots,
+                              gpool_next);
     else
         e = smm_launch<Small>(smm_compact_kernel<SMM_NODES, SMMC_WARPS, false, IV>, SMMC_WARPS, compr, count0, M, K,
-                              phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st);
+                              phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st, gp,
+                              gpool_slots, gpool_next);
     if (e != cudaSuccess) return e;
-    return smm_launch<SmmWarpSmemC<SMM_NODES_RETRY, IV>>(smm_compact_kernel<SMM_NODES_RETRY, 1, true, IV>, 1, compr,
-                                                         count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
-                                                         matches, cap, nmatch, status, st);
+    return smm_launch<Big>(smm_compact_kernel<SMM_NODES_RETRY, 1, true, IV>, 1, compr, count0, M, K, phased, wM, gt,
+                           nhaps, hapmap, setmaxerrors, matches, cap, nmatch, status, st, (Big *)nullptr, 0,
+                           (int *)nullptr);
 }
 
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
                        const uint8_t *gt, int nhaps, const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap,
-                       int *nmatch, uint32_t *status, int warps, cudaStream_t st) {
+                       int *nmatch, uint32_t *status, int warps, void *gpool, int gpool_slots, int *gpool_next,
+                       cudaStream_t st) {
     if (M < 65536) {   // depths fit the compact tree; interval bounds in 16 bits up to 65,536 haplotypes
         if (K <= 65536)
             return launch_smm_compact<uint16_t>(compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,
-                                                matches, cap, nmatch, status, warps, st);
+                                                matches, cap, nmatch, status, warps, gpool, gpool_slots, gpool_next,
+                                                st);
         return launch_smm_compact<int>(compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches, cap,
-                                       nmatch, status, warps, st);
+                                       nmatch, status, warps, gpool, gpool_slots, gpool_next, st);
     }
     cudaError_t e = smm_launch<SmmWarpSmem<SMM_NODES>>(smm_kernel<SMM_NODES, SMM_WARPS, false>, SMM_WARPS, compr,
                                                        count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors,

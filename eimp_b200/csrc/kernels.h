@@ -32,9 +32,14 @@ cudaError_t launch_gather_rows(const uint64_t *src, size_t ldsrc, const int64_t 
                                cudaStream_t st);
 // hapmap (null: identity): the target haplotype (row of phased, matches,
 // outputs; its target = row / 2) of each of the nhaps haplotypes searched
+// gpool: gpool_slots global tree pools of smm_gpool_slot_bytes(K) bytes for
+// the compact kernel's trees that outgrow shared memory, handed out through
+// *gpool_next (zero before the launch); NULL: none (such trees are retried)
 cudaError_t launch_smm(const uint32_t *compr, const int32_t *count0, int M, int K, const uint64_t *phased, int wM,
                        const uint8_t *gt, int nhaps, const int32_t *hapmap, int setmaxerrors, int4 *matches, int cap,
-                       int *nmatch, uint32_t *status, int warps, cudaStream_t st);
+                       int *nmatch, uint32_t *status, int warps, void *gpool, int gpool_slots, int *gpool_next,
+                       cudaStream_t st);
+size_t smm_gpool_slot_bytes(int K);
 // refmap (null: identity): panel haplotype of each PBWT haplotype (the
 // reduced reference without the haploid samples' placeholder columns)
 cudaError_t launch_dosage(const int4 *matches, int cap, const int *nmatch, const int32_t *absperm, int K,

@@ -53,7 +53,7 @@ def emu_exe(tmp_path_factory):
     return str(exe)
 
 
-def run_kernel(exe, d, which, compr, count0, phased, gt, K, setmaxerrors=0, cap=None):
+def run_kernel(exe, d, which, compr, count0, phased, gt, K, setmaxerrors=0, cap=None, pool=0):
     nh = phased.shape[0]
     M = gt.shape[1]
     cap = cap or M // 4 + 64
@@ -62,12 +62,13 @@ def run_kernel(exe, d, which, compr, count0, phased, gt, K, setmaxerrors=0, cap=
                     ("compr", compr.astype(np.uint32)), ("count0", count0.astype(np.int32)),
                     ("phased", phased.astype(np.uint64)), ("gt", gt.astype(np.uint8))]:
         np.ascontiguousarray(a).tofile(os.path.join(d, name + ".bin"))
-    r = subprocess.run([exe, str(d), str(which)], capture_output=True, text=True, timeout=900)
+    r = subprocess.run([exe, str(d), str(which), str(pool)], capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
     m = np.fromfile(os.path.join(d, "o_matches.bin"), np.int32).reshape(nh, cap, 4)
     n = np.fromfile(os.path.join(d, "o_nmatch.bin"), np.int32)
     st = int(np.fromfile(os.path.join(d, "o_status.bin"), np.uint32)[0])
-    retried = int(np.fromfile(os.path.join(d, "o_retried.bin"), np.int32)[0])
+    retried, moved = (int(x) for x in np.fromfile(os.path.join(d, "o_retried.bin"), np.int32))
+    run_kernel.moved = moved
     return [m[h, :n[h]].astype(np.int64) if n[h] >= 0 else None for h in range(nh)], n, st, retried
 
 
@@ -86,14 +87,17 @@ def test_matches_golden(emu_exe, tmp_path, which):
         np.testing.assert_array_equal(got[h], g["imp_matches"][off[h]:off[h + 1]])
 
 
-@pytest.mark.parametrize("which", [0, 1, 2], ids=["wide", "compact", "compact16"])
+@pytest.mark.parametrize("which,pool", [(0, 0), (1, 0), (2, 0), (1, 4), (2, 4), (2, 1)],
+                         ids=["wide", "compact", "compact16", "compact-pool", "compact16-pool", "compact16-pool1"])
 @pytest.mark.parametrize("setmaxerrors", [0, 1])
-def test_matches_vs_oracle_cfg1(emu_exe, tmp_path, which, setmaxerrors):
+def test_matches_vs_oracle_cfg1(emu_exe, tmp_path, which, pool, setmaxerrors):
     """cfg1 panel (5000 haplotypes, 2000 typed sites), 12 target haplotypes
     from the true haplotypes with their missing genotypes, one target with
     more than half of its sites missing (no matches).  With one set-maximal
     error the trees outgrow the first launch's node pool (up to 718 nodes):
-    those haplotypes come from the retry pass."""
+    without global pools those haplotypes come from the retry pass; with
+    them, the first pass moves their trees to a global pool and goes on, and
+    with fewer pools than such haplotypes the rest are retried."""
     from eimp_b200 import synth
     from eimp_b200.synth import typed_views
     from oracle import restate as R
@@ -107,9 +111,14 @@ def test_matches_vs_oracle_cfg1(emu_exe, tmp_path, which, setmaxerrors):
     phased = pack_rows(tg.truth[:2 * nt], W(M))
     compr, c0, _ = R.pbwt(sm, panel.nhaps)
     got, n, st, retried = run_kernel(emu_exe, tmp_path / "k", which, compr, c0, phased, gt, panel.nhaps,
-                                     setmaxerrors, cap=M + 64)
+                                     setmaxerrors, cap=M + 64, pool=pool)
+    moved = run_kernel.moved
     assert st == 0
-    assert (retried > 0) == (setmaxerrors > 0)
+    if pool == 0:
+        assert (retried > 0) == (setmaxerrors > 0) and moved == 0
+    elif setmaxerrors:
+        assert moved > 0
+        assert (retried > 0) == (moved > pool)
     assert n[2 * nt - 2] == 0 and n[2 * nt - 1] == 0
     for h in range(2 * nt):
         miss = np.where(gt[h // 2] == 3)[0].astype(np.int64)

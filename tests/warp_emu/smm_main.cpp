@@ -2,8 +2,10 @@
 // section of eimp_b200/csrc/imp_kernels.cu) one target haplotype at a time
 // under the warp emulator.
 //
-//   smm_emu <dir> <kernel>      kernel 0: smm_kernel, 1: smm_compact_kernel (32-bit
-//                               intervals), 2: smm_compact_kernel (16-bit intervals)
+//   smm_emu <dir> <kernel> [pool]   kernel 0: smm_kernel, 1: smm_compact_kernel
+//                                   (32-bit intervals), 2: smm_compact_kernel (16-bit
+//                                   intervals); pool: global tree pools of the
+//                                   compact kernels' first pass (slots, default 0)
 //
 // Both launches of launch_smm run: the small node pool first, then the retry
 // pass with the large pool.  <dir> holds the inputs as raw little-endian arrays in the layout of the
@@ -49,6 +51,7 @@ int main(int argc, char **argv) {
     if (argc < 3) { fprintf(stderr, "usage: %s <dir> <kernel>\n", argv[0]); return 1; }
     const std::string d = argv[1];
     const int which = atoi(argv[2]);
+    const int pool_slots = argc > 3 ? atoi(argv[3]) : 0;
     const auto pi = rd<int32_t>(d, "params_i.bin");
     const int nhaps = pi[0], M = pi[1], K = pi[2], sme = pi[3], cap = pi[4];
     const auto compr = rd<uint32_t>(d, "compr.bin");
@@ -60,6 +63,13 @@ int main(int argc, char **argv) {
     std::vector<int32_t> nmatch(nhaps, -7);
     uint32_t status = 0;
     int retried = 0;
+    // global tree pools of the first pass (exact size: the address sanitizer
+    // sees any access past the slots handed out) and their counter
+    const size_t slot_bytes = which == 2 ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY, uint16_t>)
+                                         : sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY, int>);
+    std::vector<uint64_t> gpool(pool_slots ? (pool_slots * slot_bytes + 7) / 8 : 0, 0x5a5a5a5a5a5a5a5aull);
+    int gnext = 0;
+    void *gp = pool_slots ? (void *)gpool.data() : nullptr;
     // the launches of launch_smm: the small node pool, then the retry pass
     for (int pass = 0; pass < 2; pass++) {
         const size_t smb = which == 2 ? (pass ? sizeof(eimp::SmmWarpSmemC<SMM_NODES_RETRY, uint16_t>)
@@ -81,20 +91,31 @@ int main(int argc, char **argv) {
                     blockIdx.x = h;
                     emu_warp = &warp;
                     emu_smem_ptr = smem;
-                    auto kern = which == 2 ? (pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, uint16_t>
-                                                   : eimp::smm_compact_kernel<SMM_NODES, 1, false, uint16_t>)
-                                : which ? (pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, int>
-                                                : eimp::smm_compact_kernel<SMM_NODES, 1, false, int>)
-                                        : (pass ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true>
-                                                : eimp::smm_kernel<SMM_NODES, 1, false>);
-                    kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
-                         matches.data(), cap, nmatch.data(), &status);
+                    using Big16 = eimp::SmmWarpSmemC<SMM_NODES_RETRY, uint16_t>;
+                    using Big32 = eimp::SmmWarpSmemC<SMM_NODES_RETRY, int>;
+                    if (which == 2) {
+                        auto kern = pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, uint16_t>
+                                         : eimp::smm_compact_kernel<SMM_NODES, 1, false, uint16_t>;
+                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
+                             matches.data(), cap, nmatch.data(), &status, pass ? nullptr : (Big16 *)gp,
+                             pass ? 0 : pool_slots, pass ? nullptr : &gnext);
+                    } else if (which == 1) {
+                        auto kern = pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, int>
+                                         : eimp::smm_compact_kernel<SMM_NODES, 1, false, int>;
+                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
+                             matches.data(), cap, nmatch.data(), &status, pass ? nullptr : (Big32 *)gp,
+                             pass ? 0 : pool_slots, pass ? nullptr : &gnext);
+                    } else {
+                        auto kern = pass ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true> : eimp::smm_kernel<SMM_NODES, 1, false>;
+                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
+                             matches.data(), cap, nmatch.data(), &status);
+                    }
                 });
             for (auto &x : lanes) x.join();
             free(smem);
         }
     }
-    wr(d, "o_retried.bin", std::vector<int32_t>{retried});
+    wr(d, "o_retried.bin", std::vector<int32_t>{retried, gnext});
     wr(d, "o_matches.bin", matches);
     wr(d, "o_nmatch.bin", nmatch);
     wr(d, "o_status.bin", std::vector<uint32_t>{status});
