@@ -11,6 +11,8 @@ context.  Knobs (eimp_set_launch_shape, include/eimp_gpu.h):
   dosage_span     64-site tiles per warp of the dosage kernel       4, 8, 16
   smm_warps       target haplotypes per CTA of the match search     1, 2, 4
   beam_slots_pct  warps of the persistent beam, % of the resident   100, 75, 50
+  smm_tree_pools  large match trees go on in global pools (1) or    1, 0
+                  are redone by the retry launch (0)
 
 Timing is on the device (CUDA events on the group's stream), best of
 ``reps`` runs; the phasing knob is timed over all of the group's batches.
@@ -29,6 +31,7 @@ KNOBS = {
     "dosage_span": (0, (4, 8, 16)),
     "smm_warps": (1, (1, 2, 4)),
     "beam_slots_pct": (2, (100, 75, 50)),
+    "smm_tree_pools": (3, (1, 0)),
 }
 
 
@@ -56,7 +59,8 @@ def _time(group, fn, reps: int) -> float:
     return best
 
 
-def tune_group(group, reps: int = 2, knobs=("dosage_span", "smm_warps", "beam_slots_pct")) -> dict:
+def tune_group(group, reps: int = 2,
+               knobs=("dosage_span", "smm_warps", "smm_tree_pools", "beam_slots_pct")) -> dict:
     """Tunes the knobs of one DensityGroup (eimp_b200/batch.py) on its data;
     returns {knob: {"chosen": value, "ms": {value: best ms}}}."""
     group.enqueue()   # a full step first: the phased haplotypes and the reference exist
@@ -66,6 +70,8 @@ def tune_group(group, reps: int = 2, knobs=("dosage_span", "smm_warps", "beam_sl
                                                           group.d_dos.data_ptr(), group.Mref),
         "smm_warps": lambda: group.L.eimp_imp_prepare_dev(group.h, group.nt, group.d_ph.data_ptr(),
                                                           group.d_gt.data_ptr(), 0, 0, 0),
+        "smm_tree_pools": lambda: group.L.eimp_imp_prepare_dev(group.h, group.nt, group.d_ph.data_ptr(),
+                                                               group.d_gt.data_ptr(), 0, 0, 0),
         "beam_slots_pct": group.phase,
     }
     out = {}

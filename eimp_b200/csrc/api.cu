@@ -57,7 +57,7 @@ struct eimp_ctx {
     uint64_t launches = 0;
     DBuf status;
     // launch shapes (eimp_set_launch_shape)
-    int shape_dos_span = 8, shape_smm_warps = SMMC_WARPS, shape_beam_pct = 100;
+    int shape_dos_span = 8, shape_smm_warps = SMMC_WARPS, shape_beam_pct = 100, shape_smm_pools = 1;
 
     // GPUEngine drop-in
     size_t g_K = 0, g_Kwords = 0, g_M = 0, g_Ncorr = 0, g_NAD = 0, g_refTcap = 0;
@@ -306,6 +306,10 @@ int eimp_set_launch_shape(eimp_ctx *ctx, int knob, int value) {
         if (value < 1 || value > 100) return fail(ctx, EIMP_E_ARG, "beam slots: 1..100 % of the resident warps");
         ctx->shape_beam_pct = value;
         return 0;
+    case EIMP_SHAPE_SMM_TREE_POOLS:
+        if (value != 0 && value != 1) return fail(ctx, EIMP_E_ARG, "match-search tree pools: 0 or 1");
+        ctx->shape_smm_pools = value;
+        return 0;
     default:
         return fail(ctx, EIMP_E_ARG, "unknown launch-shape knob");
     }
@@ -317,6 +321,7 @@ int eimp_get_launch_shape(const eimp_ctx *ctx, int knob, int *value) {
     case EIMP_SHAPE_DOSAGE_SPAN: *value = ctx->shape_dos_span; return 0;
     case EIMP_SHAPE_SMM_WARPS: *value = ctx->shape_smm_warps; return 0;
     case EIMP_SHAPE_BEAM_SLOTS_PCT: *value = ctx->shape_beam_pct; return 0;
+    case EIMP_SHAPE_SMM_TREE_POOLS: *value = ctx->shape_smm_pools; return 0;
     default: return EIMP_E_ARG;
     }
 }
@@ -483,14 +488,14 @@ int eimp_imp_prepare_dev(eimp_ctx *ctx, size_t ntargets, const uint64_t *d_phase
     if (hapmap) CK(cudaMemsetAsync(ctx->i_nmatch.p, 0, nh * sizeof(int), ctx->stream));
     // up to 2048 haplotypes per launch move a large tree to a global pool
     // instead of being redone by the retry launch
-    const int gslots = (int)std::min<size_t>(nsearch, 2048);
+    const int gslots = ctx->shape_smm_pools ? (int)std::min<size_t>(nsearch, 2048) : 0;
     CK(ctx->i_gpool.reserve((size_t)gslots * smm_gpool_slot_bytes((int)ctx->i_K)));
     CK(ctx->i_gnext.reserve(sizeof(int)));
     CK(cudaMemsetAsync(ctx->i_gnext.p, 0, sizeof(int), ctx->stream));
     LAUNCH(launch_smm(ctx->i_compr.as<uint32_t>(), ctx->i_count0.as<int32_t>(), (int)M, (int)ctx->i_K,
                       ctx->i_phased.as<uint64_t>(), (int)wM, ctx->i_gt.as<uint8_t>(), (int)nsearch, hapmap,
                       setmaxerrors, ctx->i_matches.as<int4>(), (int)cap, ctx->i_nmatch.as<int>(),
-                      ctx->status.as<uint32_t>(), ctx->shape_smm_warps, ctx->i_gpool.p, gslots,
+                      ctx->status.as<uint32_t>(), ctx->shape_smm_warps, gslots ? ctx->i_gpool.p : nullptr, gslots,
                       ctx->i_gnext.as<int>(), ctx->stream));
     ctx->launches++;   // launch_smm launches twice: the small node pool, then the retry pass
     return 0;
