@@ -48,8 +48,7 @@ struct Cons { int type, refidx; };
 constexpr int PHMAX = 128;   // History<fp_type> ring (power of two >= H, H <= 128)
 constexpr int PMAX = 128;    // largest beam width
 constexpr int BPMAX = PMAX;  // beam paths held between two prunes (<= P)
-constexpr int HTS_BITS = 8;
-constexpr int HTS = 1 << HTS_BITS;   // merge hash table entries (load <= 1/2)
+constexpr int HTS = 512;     // merge hash table entries (load <= 1/4)
 static_assert(BPMAX < HTS, "the merge table must never fill");
 
 struct HPh {   // HaplotypePath
@@ -82,7 +81,7 @@ struct Hel { float key; int a; int b; };
 struct __align__(16) WS {   // per-warp state in shared memory
     float prec[PHMAX];
     float cdv[PHMAX];
-    Hel *heap;                    // the pruning's fallback heap: PMAX + 2 entries in the arena
+    Hel heap[PMAX + 2];
     int2 ht[HTS];                 // merge keys: (key, surviving beam path), x = -1 when free
     BPh bp[2][BPMAX];             // the beam in list order (two buffers)
     float acc0[BPMAX], acc1[BPMAX];
@@ -958,7 +957,7 @@ __device__ void beam_merge(const Ctx &c, WS &w) {
         const int mr = w.canon[bp[it].mat], pr = w.canon[bp[it].pat];
         const int k0 = mr < pr ? mr : pr, k1 = mr < pr ? pr : mr;
         const int key = (k0 << 16) | k1;
-        int slot = (int)(((unsigned)key * 2654435761u) >> (32 - HTS_BITS)) & (HTS - 1);
+        int slot = (int)(((unsigned)key * 2654435761u) >> 23) & (HTS - 1);
         // linear probing; the table holds at most BPMAX < HTS keys, so a
         // free or matching slot exists within HTS probes
         for (int probe = 0; probe < HTS; probe++) {
@@ -1164,7 +1163,7 @@ __host__ __device__ __forceinline__ size_t align256(size_t x) { return (x + 255)
 
 // arena layout per target (bytes)
 struct ArenaLayout {
-    size_t hp, ph, ivpool, ivfree, happ, happ_old, hapmap, fstack, copies, heap, cons, rcons, probs, confs, tg, total;
+    size_t hp, ph, ivpool, ivfree, happ, happ_old, hapmap, fstack, copies, cons, rcons, probs, confs, tg, total;
     int NH, HMAX;
 };
 
@@ -1187,7 +1186,6 @@ static ArenaLayout arena_layout(const BeamParams &p, int M) {
     a.hapmap = o; o = align256(o + sizeof(int2) * a.NH);
     a.fstack = o; o = align256(o + sizeof(int) * a.NH);
     a.copies = o; o = align256(o + sizeof(int) * 3 * a.NH);
-    a.heap = o; o = align256(o + sizeof(Hel) * (PMAX + 2));
     a.cons = o; o = align256(o + sizeof(Cons) * (size_t)(M + 1));
     a.rcons = o; o = align256(o + sizeof(Cons) * (size_t)(M + 1));
     a.probs = o; o = align256(o + sizeof(float) * (size_t)(M + 1));
@@ -1230,7 +1228,7 @@ __global__ void lpt_order_kernel(const int32_t *__restrict__ nsplits, int ntgt, 
 // next target from a device counter, in the order given (longest first), and
 // phases it with the beam arena of its slot, so the arenas number the
 // resident warps, not the targets.
-__global__ void __maxnreg__(BEAM_MAX_REGS) beam_kernel(
+__global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
     const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
     const int32_t *__restrict__ ncalls, const float *__restrict__ cmdiffs, const uint32_t *__restrict__ pbwt,
@@ -1270,7 +1268,6 @@ __global__ void __maxnreg__(BEAM_MAX_REGS) beam_kernel(
         w.rowref = w.rowinc + kw;
         w.canon = reinterpret_cast<short *>(base + (size_t)BEAM_WARPS * beam_rows_bytes(K) +
                                             (size_t)wid * beam_canon_bytes(al.NH));
-        w.heap = reinterpret_cast<Hel *>(ab + al.heap);
     }
     Ctx c;
     c.hp = reinterpret_cast<HPh *>(ab + al.hp);

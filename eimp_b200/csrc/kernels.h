@@ -13,10 +13,7 @@
 #define SMM_NODES 512
 #define SMM_NODES_RETRY 4096
 // beam phasing: warps (targets) per CTA
-#define BEAM_WARPS 2
-// registers per thread the beam kernel is held to: 10 warps' worth of
-// registers and of its shared memory fit an SM (198 used, no spills)
-#define BEAM_MAX_REGS 200
+#define BEAM_WARPS 4
 
 namespace eimp {
 

@@ -32,9 +32,9 @@ def emu_exe(tmp_path_factory):
     d = tmp_path_factory.mktemp("beam_emu")
     shutil.copy(os.path.join(CSRC, "common.cuh"), d / "common.cuh")
     kh = open(os.path.join(CSRC, "kernels.h")).read()
-    assert "#define BEAM_WARPS 2" in kh
+    assert "#define BEAM_WARPS 4" in kh
     # one warp per block: each warp's shared memory is its own allocation
-    (d / "kernels.h").write_text(kh.replace("#define BEAM_WARPS 2", "#define BEAM_WARPS 1"))
+    (d / "kernels.h").write_text(kh.replace("#define BEAM_WARPS 4", "#define BEAM_WARPS 1"))
     src = open(os.path.join(CSRC, "beam.cu")).read()
     # the launcher (triple-chevron launch, runtime attributes) is device-only
     i, j = src.index("static size_t beam_smem("), src.rindex("}  // namespace eimp")
