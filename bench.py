@@ -581,6 +581,18 @@ def cfg4_leg(args, local, dev):
 
 
 # ---------------------------------------------------------------- our arm
+def max_over_ranks(x, world, dev):
+    """The largest value of x over the ranks (every rank calls this at the
+    same point); x itself on one GPU."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def phase_batch_targets(cfg, tgroups, Mref, nh, free_bytes):
     """Targets per phasing batch of each density group.  A batch's condensed
     references and PBWTs take about 0.25*M condensed rows per target (S ~
@@ -750,7 +762,7 @@ def main():
         torch.cuda.synchronize()
         for g in groups:
             g.ctx.synchronize()
-        g_ms = float(np.mean([a.elapsed_time(b) for a, b in gms]))
+        g_ms = max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in gms])), world, dev)
         same = all(torch.equal(a, b) for g, r in zip(groups, ref_out)
                    for a, b in zip(r, (g.d_dos, g.d_bits, g.d_mats, g.d_pats)))
         graph = {"value": world * dos_per_step / (g_ms / 1e3), "unit": UNIT, "ms_per_step": g_ms,
@@ -917,7 +929,7 @@ def main():
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             e2e_step()
-        dt = (time.perf_counter() - t0) / args.e2e_steps
+        dt = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, world, dev)
         # the copy bandwidth the dosages meet: one pinned 1 GiB device-to-host copy
         src = torch.empty(1 << 30, dtype=torch.uint8, device=dev)
         dst = torch.empty(1 << 30, dtype=torch.uint8).pin_memory()
