@@ -48,7 +48,8 @@ struct Cons { int type, refidx; };
 constexpr int PHMAX = 128;   // History<fp_type> ring (power of two >= H, H <= 128)
 constexpr int PMAX = 128;    // largest beam width
 constexpr int BPMAX = PMAX;  // beam paths held between two prunes (<= P)
-constexpr int HTS = 512;     // merge hash table entries (load <= 1/4)
+constexpr int HTS_BITS = 8;
+constexpr int HTS = 1 << HTS_BITS;   // merge hash table entries (load <= 1/2)
 static_assert(BPMAX < HTS, "the merge table must never fill");
 
 struct HPh {   // HaplotypePath
@@ -81,7 +82,7 @@ struct Hel { float key; int a; int b; };
 struct __align__(16) WS {   // per-warp state in shared memory
     float prec[PHMAX];
     float cdv[PHMAX];
-    Hel heap[PMAX + 2];
+    Hel *heap;                    // the pruning's fallback heap: PMAX + 2 entries in the arena
     int2 ht[HTS];                 // merge keys: (key, surviving beam path), x = -1 when free
     BPh bp[2][BPMAX];             // the beam in list order (two buffers)
     float acc0[BPMAX], acc1[BPMAX];
@@ -957,7 +958,7 @@ __device__ void beam_merge(const Ctx &c, WS &w) {
         const int mr = w.canon[bp[it].mat], pr = w.canon[bp[it].pat];
         const int k0 = mr < pr ? mr : pr, k1 = mr < pr ? pr : mr;
         const int key = (k0 << 16) | k1;
-        int slot = (int)(((unsigned)key * 2654435761u) >> 23) & (HTS - 1);
+        int slot = (int)(((unsigned)key * 2654435761u) >> (32 - HTS_BITS)) & (HTS - 1);
         // linear probing; the table holds at most BPMAX < HTS keys, so a
         // free or matching slot exists within HTS probes
         for (int probe = 0; probe < HTS; probe++) {
@@ -1163,7 +1164,7 @@ __host__ __device__ __forceinline__ size_t align256(size_t x) { return (x + 255)
 
 // arena layout per target (bytes)
 struct ArenaLayout {
-    size_t hp, ph, ivpool, ivfree, happ, happ_old, hapmap, fstack, copies, cons, rcons, probs, confs, tg, total;
+    size_t hp, ph, ivpool, ivfree, happ, happ_old, hapmap, fstack, copies, heap, cons, rcons, probs, confs, tg, total;
     int NH, HMAX;
 };
 
@@ -1186,6 +1187,7 @@ static ArenaLayout arena_layout(const BeamParams &p, int M) {
     a.hapmap = o; o = align256(o + sizeof(int2) * a.NH);
     a.fstack = o; o = align256(o + sizeof(int) * a.NH);
     a.copies = o; o = align256(o + sizeof(int) * 3 * a.NH);
+    a.heap = o; o = align256(o + sizeof(Hel) * (PMAX + 2));
     a.cons = o; o = align256(o + sizeof(Cons) * (size_t)(M + 1));
     a.rcons = o; o = align256(o + sizeof(Cons) * (size_t)(M + 1));
     a.probs = o; o = align256(o + sizeof(float) * (size_t)(M + 1));
@@ -1228,8 +1230,11 @@ __global__ void lpt_order_kernel(const int32_t *__restrict__ nsplits, int ntgt, 
 // next target from a device counter, in the order given (longest first), and
 // phases it with the beam arena of its slot, so the arenas number the
 // resident warps, not the targets.
-__global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
-    BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
+// The persistent beam, WARPS targets (warps) per CTA; launched through the
+// two kernels below, which differ only in their register budgets.
+template <int WARPS>
+__device__ __forceinline__ void beam_run(
+    const BeamParams &p, const ArenaLayout &al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
     const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
     const int32_t *__restrict__ ncalls, const float *__restrict__ cmdiffs, const uint32_t *__restrict__ pbwt,
     const int32_t *__restrict__ count0, const int64_t *__restrict__ rowoff, uint8_t *__restrict__ arena,
@@ -1241,7 +1246,7 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     extern __shared__ __align__(16) uint8_t smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WS &w = reinterpret_cast<WS *>(smem_raw)[wid];
-    uint8_t *const ab = arena + (size_t)(blockIdx.x * BEAM_WARPS + wid) * arena_bytes;
+    uint8_t *const ab = arena + (size_t)(blockIdx.x * WARPS + wid) * arena_bytes;
     for (;;) {
     int qi = 0;
     if (lane == 0) qi = atomicAdd(workq, 1);
@@ -1263,11 +1268,12 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     const int K = p.K;
     const size_t kw = eimp_kw(K);
     if (lane == 0) {   // the warp's PBWT row pair and merge keys after the WS array
-        uint8_t *base = smem_raw + sizeof(WS) * BEAM_WARPS;
+        uint8_t *base = smem_raw + sizeof(WS) * WARPS;
         w.rowinc = reinterpret_cast<uint32_t *>(base + (size_t)wid * beam_rows_bytes(K));
         w.rowref = w.rowinc + kw;
-        w.canon = reinterpret_cast<short *>(base + (size_t)BEAM_WARPS * beam_rows_bytes(K) +
+        w.canon = reinterpret_cast<short *>(base + (size_t)WARPS * beam_rows_bytes(K) +
                                             (size_t)wid * beam_canon_bytes(al.NH));
+        w.heap = reinterpret_cast<Hel *>(ab + al.heap);
     }
     Ctx c;
     c.hp = reinterpret_cast<HPh *>(ab + al.hp);
@@ -1479,23 +1485,66 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     }
 }
 
-static size_t beam_smem(const BeamParams &p, const ArenaLayout &al) {
-    return (sizeof(WS) + beam_rows_bytes(p.K) + beam_canon_bytes(al.NH)) * BEAM_WARPS;
+// variant 0: four warps per CTA, the registers the code takes
+__global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
+    BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
+    const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
+    const int32_t *__restrict__ ncalls, const float *__restrict__ cmdiffs, const uint32_t *__restrict__ pbwt,
+    const int32_t *__restrict__ count0, const int64_t *__restrict__ rowoff, uint8_t *__restrict__ arena,
+    size_t arena_bytes, uint64_t *__restrict__ mats, uint64_t *__restrict__ pats, float *__restrict__ dmat,
+    float *__restrict__ dpat, float *__restrict__ totalconf, int32_t *__restrict__ ncallsites,
+    uint32_t *__restrict__ status, const int *__restrict__ skip, const int32_t *__restrict__ order,
+    int *__restrict__ workq) {
+    beam_run<BEAM_WARPS>(p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls, cmdiffs, pbwt, count0, rowoff, arena, arena_bytes, mats,
+                      pats, dmat, dpat, totalconf, ncallsites, status, skip, order, workq);
 }
 
-int beam_slots(const BeamParams &p, int M, int ntgt, int pct) {
+// variant 1: two warps per CTA, at most 200 registers
+__global__ void __maxnreg__(200) beam_kernel_r200(
+    BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
+    const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
+    const int32_t *__restrict__ ncalls, const float *__restrict__ cmdiffs, const uint32_t *__restrict__ pbwt,
+    const int32_t *__restrict__ count0, const int64_t *__restrict__ rowoff, uint8_t *__restrict__ arena,
+    size_t arena_bytes, uint64_t *__restrict__ mats, uint64_t *__restrict__ pats, float *__restrict__ dmat,
+    float *__restrict__ dpat, float *__restrict__ totalconf, int32_t *__restrict__ ncallsites,
+    uint32_t *__restrict__ status, const int *__restrict__ skip, const int32_t *__restrict__ order,
+    int *__restrict__ workq) {
+    beam_run<2>(p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls, cmdiffs, pbwt, count0, rowoff, arena, arena_bytes, mats,
+                      pats, dmat, dpat, totalconf, ncallsites, status, skip, order, workq);
+}
+
+static size_t beam_smem(const BeamParams &p, const ArenaLayout &al, int warps) {
+    return (sizeof(WS) + beam_rows_bytes(p.K) + beam_canon_bytes(al.NH)) * warps;
+}
+
+// The beam's two launch variants: 0 -- four warps per CTA and the registers
+// the code takes (234), eight warps per SM; 1 -- two warps per CTA held to
+// 200 registers (198 used, no spills), ten warps per SM.  The second keeps
+// more targets in flight but runs each a little slower: it pays on short
+// targets (few typed sites) and large K, not on long ones.
+struct BeamVariant {
+    int warps;
+    const void *kern;
+};
+static BeamVariant beam_variant(int v) {
+    if (v == 1) return {2, (const void *)beam_kernel_r200};
+    return {BEAM_WARPS, (const void *)beam_kernel};
+}
+
+int beam_slots(const BeamParams &p, int M, int ntgt, int pct, int variant) {
+    const BeamVariant bv = beam_variant(variant);
     const ArenaLayout al = arena_layout(p, M);
-    const size_t sm = beam_smem(p, al);
+    const size_t sm = beam_smem(p, al, bv.warps);
     int dev = 0, nsm = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return -1;
-    if (cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, beam_kernel, 32 * BEAM_WARPS, sm) != cudaSuccess || per < 1)
+    if (cudaFuncSetAttribute(bv.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bv.kern, 32 * bv.warps, sm) != cudaSuccess || per < 1)
         return -1;
     int ctas = (int)((long)per * nsm * (pct < 1 ? 1 : pct > 100 ? 100 : pct) / 100);
     if (ctas < 1) ctas = 1;
-    const int need = (ntgt + BEAM_WARPS - 1) / BEAM_WARPS;
-    return (need < ctas ? need : ctas) * BEAM_WARPS;
+    const int need = (ntgt + bv.warps - 1) / bv.warps;
+    return (need < ctas ? need : ctas) * bv.warps;
 }
 
 cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt, const uint64_t *monos,
@@ -1503,18 +1552,21 @@ cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt,
                         const float *cmdiffs, const uint32_t *pbwt, const int32_t *count0, const int64_t *rowoff,
                         void *arena, size_t arena_bytes, int slots, int32_t *order, int *workq, uint64_t *mats,
                         uint64_t *pats, float *dmat, float *dpat, float *totalconf, int32_t *ncallsites,
-                        uint32_t *status, const int *skip, cudaStream_t st) {
+                        uint32_t *status, const int *skip, int variant, cudaStream_t st) {
+    const BeamVariant bv = beam_variant(variant);
     ArenaLayout al = arena_layout(p, M);
-    if (arena_bytes < al.total || slots < BEAM_WARPS || slots % BEAM_WARPS) return cudaErrorInvalidValue;
-    const size_t sm = beam_smem(p, al);
-    cudaError_t e = cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (arena_bytes < al.total || slots < bv.warps || slots % bv.warps) return cudaErrorInvalidValue;
+    const size_t sm = beam_smem(p, al, bv.warps);
+    cudaError_t e = cudaFuncSetAttribute(bv.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     lpt_order_kernel<<<1, 1024, 0, st>>>(nsplits, ntgt, order, skip);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(workq, 0, sizeof(int), st)) != cudaSuccess) return e;
-    beam_kernel<<<slots / BEAM_WARPS, 32 * BEAM_WARPS, sm, st>>>(
-        p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls, cmdiffs, pbwt, count0, rowoff, (uint8_t *)arena,
-        arena_bytes, mats, pats, dmat, dpat, totalconf, ncallsites, status, skip, order, workq);
+    auto kern = variant == 1 ? beam_kernel_r200 : beam_kernel;
+    kern<<<slots / bv.warps, 32 * bv.warps, sm, st>>>(p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls,
+                                                      cmdiffs, pbwt, count0, rowoff, (uint8_t *)arena, arena_bytes,
+                                                      mats, pats, dmat, dpat, totalconf, ncallsites, status, skip,
+                                                      order, workq);
     return cudaGetLastError();
 }
 
