@@ -13,8 +13,6 @@ context.  Knobs (eimp_set_launch_shape, include/eimp_gpu.h):
   beam_slots_pct  warps of the persistent beam, % of the resident   100, 75, 50
   smm_tree_pools  large match trees go on in global pools (1) or    1, 0
                   are redone by the retry launch (0)
-  beam_variant    the beam with all the registers its code takes    0, 1
-                  (0, 8 warps per SM) or held to 200 (1, 10 warps)
 
 Timing is on the device (CUDA events on the group's stream), best of
 ``reps`` runs; the phasing knob is timed over all of the group's batches.
@@ -34,7 +32,6 @@ KNOBS = {
     "smm_warps": (1, (1, 2, 4)),
     "beam_slots_pct": (2, (100, 75, 50)),
     "smm_tree_pools": (3, (1, 0)),
-    "beam_variant": (4, (0, 1)),
 }
 
 
@@ -63,7 +60,7 @@ def _time(group, fn, reps: int) -> float:
 
 
 def tune_group(group, reps: int = 2,
-               knobs=("dosage_span", "smm_warps", "smm_tree_pools", "beam_variant", "beam_slots_pct")) -> dict:
+               knobs=("dosage_span", "smm_warps", "smm_tree_pools", "beam_slots_pct")) -> dict:
     """Tunes the knobs of one DensityGroup (eimp_b200/batch.py) on its data;
     returns {knob: {"chosen": value, "ms": {value: best ms}}}."""
     group.enqueue()   # a full step first: the phased haplotypes and the reference exist
@@ -75,7 +72,6 @@ def tune_group(group, reps: int = 2,
                                                           group.d_gt.data_ptr(), 0, 0, 0),
         "smm_tree_pools": lambda: group.L.eimp_imp_prepare_dev(group.h, group.nt, group.d_ph.data_ptr(),
                                                                group.d_gt.data_ptr(), 0, 0, 0),
-        "beam_variant": group.phase,
         "beam_slots_pct": group.phase,
     }
     out = {}

@@ -57,8 +57,7 @@ struct eimp_ctx {
     uint64_t launches = 0;
     DBuf status;
     // launch shapes (eimp_set_launch_shape)
-    int shape_dos_span = 8, shape_smm_warps = SMMC_WARPS, shape_beam_pct = 100, shape_smm_pools = 1,
-        shape_beam_variant = 0;
+    int shape_dos_span = 8, shape_smm_warps = SMMC_WARPS, shape_beam_pct = 100, shape_smm_pools = 1;
 
     // GPUEngine drop-in
     size_t g_K = 0, g_Kwords = 0, g_M = 0, g_Ncorr = 0, g_NAD = 0, g_refTcap = 0;
@@ -311,10 +310,6 @@ int eimp_set_launch_shape(eimp_ctx *ctx, int knob, int value) {
         if (value != 0 && value != 1) return fail(ctx, EIMP_E_ARG, "match-search tree pools: 0 or 1");
         ctx->shape_smm_pools = value;
         return 0;
-    case EIMP_SHAPE_BEAM_VARIANT:
-        if (value != 0 && value != 1) return fail(ctx, EIMP_E_ARG, "beam launch variant: 0 or 1");
-        ctx->shape_beam_variant = value;
-        return 0;
     default:
         return fail(ctx, EIMP_E_ARG, "unknown launch-shape knob");
     }
@@ -327,7 +322,6 @@ int eimp_get_launch_shape(const eimp_ctx *ctx, int knob, int *value) {
     case EIMP_SHAPE_SMM_WARPS: *value = ctx->shape_smm_warps; return 0;
     case EIMP_SHAPE_BEAM_SLOTS_PCT: *value = ctx->shape_beam_pct; return 0;
     case EIMP_SHAPE_SMM_TREE_POOLS: *value = ctx->shape_smm_pools; return 0;
-    case EIMP_SHAPE_BEAM_VARIANT: *value = ctx->shape_beam_variant; return 0;
     default: return EIMP_E_ARG;
     }
 }
@@ -1139,7 +1133,7 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
     std::vector<int64_t> ro;
     if (int r = run_cref_pbwt(ctx, K, ntgt, d_gt, ro)) return r;
     const size_t ab = beam_arena_bytes(bp, (int)M);
-    const int slots = beam_slots(bp, (int)M, (int)ntgt, ctx->shape_beam_pct, ctx->shape_beam_variant);
+    const int slots = beam_slots(bp, (int)M, (int)ntgt, ctx->shape_beam_pct);
     if (slots < 1) return fail(ctx, EIMP_E_CUDA, "beam launch shape: occupancy query failed");
     CK(ctx->b_arena.reserve((size_t)slots * ab));
     CK(ctx->b_order.reserve(ntgt * sizeof(int32_t)));
@@ -1150,7 +1144,7 @@ int run_phase(eimp_ctx *ctx, const eimp_phase_params *p, size_t ntgt, const uint
                        ctx->b_cmd.as<float>(), ctx->b_pbwt.as<uint32_t>(), ctx->b_count0.as<int32_t>(),
                        ctx->b_rowoff.as<int64_t>(), ctx->b_arena.p, ab, slots, ctx->b_order.as<int32_t>(),
                        ctx->b_workq.as<int>(), d_mats, d_pats, d_dm, d_dp, d_tc, d_nc, ctx->status.as<uint32_t>(),
-                       ctx->cur_skip, ctx->shape_beam_variant, ctx->stream));
+                       ctx->cur_skip, ctx->stream));
     if (ctx->tgthap_n)   // haploid targets are not phased (Target.cpp:166-203)
         LAUNCH(launch_haploid_phase(d_gt, (int)ntgt, (int)M, (int)eimp_W(M), ctx->tgthap.as<uint8_t>(), d_mats,
                                     d_pats, d_dm, d_dp, d_tc, d_nc, ctx->status.as<uint32_t>(), ctx->stream));
@@ -1191,8 +1185,7 @@ int eimp_phase_reserve(eimp_ctx *ctx, const eimp_phase_params *p, size_t max_tar
     CK(ctx->b_cref.reserve(max_rows * eimp_W(K) * 8));
     CK(ctx->b_count0.reserve(max_rows * 4));
     CK(ctx->b_pbwt.reserve(2 * max_rows * eimp_kw(K) * 4));
-    // the most any launch shape takes
-    const int slots = std::max(beam_slots(bp, (int)M, (int)n, 100, 0), beam_slots(bp, (int)M, (int)n, 100, 1));
+    const int slots = beam_slots(bp, (int)M, (int)n);   // the most any launch shape takes
     if (slots < 1) return fail(ctx, EIMP_E_CUDA, "beam launch shape: occupancy query failed");
     CK(ctx->b_arena.reserve((size_t)slots * beam_arena_bytes(bp, (int)M)));
     CK(ctx->b_order.reserve(n * sizeof(int32_t)));

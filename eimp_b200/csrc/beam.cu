@@ -1230,8 +1230,7 @@ __global__ void lpt_order_kernel(const int32_t *__restrict__ nsplits, int ntgt, 
 // next target from a device counter, in the order given (longest first), and
 // phases it with the beam arena of its slot, so the arenas number the
 // resident warps, not the targets.
-// The persistent beam, WARPS targets (warps) per CTA; launched through the
-// two kernels below, which differ only in their register budgets.
+// The persistent beam, WARPS targets (warps) per CTA (the kernel below).
 template <int WARPS>
 __device__ __forceinline__ void beam_run(
     const BeamParams &p, const ArenaLayout &al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
@@ -1485,7 +1484,6 @@ __device__ __forceinline__ void beam_run(
     }
 }
 
-// variant 0: four warps per CTA, the registers the code takes
 __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
     BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
     const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
@@ -1499,52 +1497,23 @@ __global__ void __launch_bounds__(32 * BEAM_WARPS, 1) beam_kernel(
                       pats, dmat, dpat, totalconf, ncallsites, status, skip, order, workq);
 }
 
-// variant 1: two warps per CTA, at most 200 registers
-__global__ void __maxnreg__(200) beam_kernel_r200(
-    BeamParams p, ArenaLayout al, int ntgt, int M, const uint8_t *__restrict__ gt, const uint64_t *__restrict__ monos,
-    const int32_t *__restrict__ splits, const int32_t *__restrict__ nsplits, const int32_t *__restrict__ calls,
-    const int32_t *__restrict__ ncalls, const float *__restrict__ cmdiffs, const uint32_t *__restrict__ pbwt,
-    const int32_t *__restrict__ count0, const int64_t *__restrict__ rowoff, uint8_t *__restrict__ arena,
-    size_t arena_bytes, uint64_t *__restrict__ mats, uint64_t *__restrict__ pats, float *__restrict__ dmat,
-    float *__restrict__ dpat, float *__restrict__ totalconf, int32_t *__restrict__ ncallsites,
-    uint32_t *__restrict__ status, const int *__restrict__ skip, const int32_t *__restrict__ order,
-    int *__restrict__ workq) {
-    beam_run<2>(p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls, cmdiffs, pbwt, count0, rowoff, arena, arena_bytes, mats,
-                      pats, dmat, dpat, totalconf, ncallsites, status, skip, order, workq);
-}
-
 static size_t beam_smem(const BeamParams &p, const ArenaLayout &al, int warps) {
     return (sizeof(WS) + beam_rows_bytes(p.K) + beam_canon_bytes(al.NH)) * warps;
 }
 
-// The beam's two launch variants: 0 -- four warps per CTA and the registers
-// the code takes (234), eight warps per SM; 1 -- two warps per CTA held to
-// 200 registers (198 used, no spills), ten warps per SM.  The second keeps
-// more targets in flight but runs each a little slower: it pays on short
-// targets (few typed sites) and large K, not on long ones.
-struct BeamVariant {
-    int warps;
-    const void *kern;
-};
-static BeamVariant beam_variant(int v) {
-    if (v == 1) return {2, (const void *)beam_kernel_r200};
-    return {BEAM_WARPS, (const void *)beam_kernel};
-}
-
-int beam_slots(const BeamParams &p, int M, int ntgt, int pct, int variant) {
-    const BeamVariant bv = beam_variant(variant);
+int beam_slots(const BeamParams &p, int M, int ntgt, int pct) {
     const ArenaLayout al = arena_layout(p, M);
-    const size_t sm = beam_smem(p, al, bv.warps);
+    const size_t sm = beam_smem(p, al, BEAM_WARPS);
     int dev = 0, nsm = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return -1;
-    if (cudaFuncSetAttribute(bv.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bv.kern, 32 * bv.warps, sm) != cudaSuccess || per < 1)
+    if (cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, beam_kernel, 32 * BEAM_WARPS, sm) != cudaSuccess || per < 1)
         return -1;
     int ctas = (int)((long)per * nsm * (pct < 1 ? 1 : pct > 100 ? 100 : pct) / 100);
     if (ctas < 1) ctas = 1;
-    const int need = (ntgt + bv.warps - 1) / bv.warps;
-    return (need < ctas ? need : ctas) * bv.warps;
+    const int need = (ntgt + BEAM_WARPS - 1) / BEAM_WARPS;
+    return (need < ctas ? need : ctas) * BEAM_WARPS;
 }
 
 cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt, const uint64_t *monos,
@@ -1552,21 +1521,19 @@ cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt,
                         const float *cmdiffs, const uint32_t *pbwt, const int32_t *count0, const int64_t *rowoff,
                         void *arena, size_t arena_bytes, int slots, int32_t *order, int *workq, uint64_t *mats,
                         uint64_t *pats, float *dmat, float *dpat, float *totalconf, int32_t *ncallsites,
-                        uint32_t *status, const int *skip, int variant, cudaStream_t st) {
-    const BeamVariant bv = beam_variant(variant);
+                        uint32_t *status, const int *skip, cudaStream_t st) {
     ArenaLayout al = arena_layout(p, M);
-    if (arena_bytes < al.total || slots < bv.warps || slots % bv.warps) return cudaErrorInvalidValue;
-    const size_t sm = beam_smem(p, al, bv.warps);
-    cudaError_t e = cudaFuncSetAttribute(bv.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (arena_bytes < al.total || slots < BEAM_WARPS || slots % BEAM_WARPS) return cudaErrorInvalidValue;
+    const size_t sm = beam_smem(p, al, BEAM_WARPS);
+    cudaError_t e = cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     lpt_order_kernel<<<1, 1024, 0, st>>>(nsplits, ntgt, order, skip);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(workq, 0, sizeof(int), st)) != cudaSuccess) return e;
-    auto kern = variant == 1 ? beam_kernel_r200 : beam_kernel;
-    kern<<<slots / bv.warps, 32 * bv.warps, sm, st>>>(p, al, ntgt, M, gt, monos, splits, nsplits, calls, ncalls,
-                                                      cmdiffs, pbwt, count0, rowoff, (uint8_t *)arena, arena_bytes,
-                                                      mats, pats, dmat, dpat, totalconf, ncallsites, status, skip,
-                                                      order, workq);
+    beam_kernel<<<slots / BEAM_WARPS, 32 * BEAM_WARPS, sm, st>>>(p, al, ntgt, M, gt, monos, splits, nsplits, calls,
+                                                                ncalls, cmdiffs, pbwt, count0, rowoff,
+                                                                (uint8_t *)arena, arena_bytes, mats, pats, dmat, dpat,
+                                                                totalconf, ncallsites, status, skip, order, workq);
     return cudaGetLastError();
 }
 

@@ -13,7 +13,7 @@
 #define SMM_NODES 512
 #define SMM_NODES_RETRY 4096
 // beam phasing: warps (targets) per CTA
-#define BEAM_WARPS 4   // of launch variant 0; variant 1 has two
+#define BEAM_WARPS 4
 
 namespace eimp {
 
@@ -131,7 +131,7 @@ struct BeamParams {
 size_t beam_arena_bytes(const BeamParams &p, int S_max);
 // warps of the persistent beam launch for ntgt targets (a multiple of the
 // warps per CTA; at most the resident ones), -1 on a CUDA error
-int beam_slots(const BeamParams &p, int M, int ntgt, int pct = 100, int variant = 0);
+int beam_slots(const BeamParams &p, int M, int ntgt, int pct = 100);
 // the persistent beam: slots warps (beam_slots), one arena of arena_bytes per
 // slot; order (ntgt ints) and workq (one int) are scratch: the longest-first
 // order and the queue counter, both filled here
@@ -140,6 +140,6 @@ cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt,
                         const float *cmdiffs, const uint32_t *pbwt, const int32_t *count0, const int64_t *rowoff,
                         void *arena, size_t arena_bytes, int slots, int32_t *order, int *workq, uint64_t *mats,
                         uint64_t *pats, float *dmat, float *dpat, float *totalconf, int32_t *ncallsites,
-                        uint32_t *status, const int *skip, int variant, cudaStream_t st);
+                        uint32_t *status, const int *skip, cudaStream_t st);
 
 }  // namespace eimp

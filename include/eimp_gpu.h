@@ -220,11 +220,9 @@ int eimp_phase_haploid_targets(eimp_ctx *ctx, size_t ntgt, const uint8_t *haploi
  *   EIMP_SHAPE_SMM_TREE_POOLS  1 [default]: a match tree that could outgrow its shared-memory pool
  *                              moves to a global-memory pool and its warp goes on; 0: such a
  *                              haplotype is redone from its first site by the retry launch
- *   EIMP_SHAPE_BEAM_VARIANT    0 [default]: the beam with the registers its code takes (8 warps per
- *                              SM on a B200); 1: held to 200 registers, 10 warps per SM
  * A value outside these returns EIMP_E_ARG and changes nothing. */
 enum { EIMP_SHAPE_DOSAGE_SPAN = 0, EIMP_SHAPE_SMM_WARPS = 1, EIMP_SHAPE_BEAM_SLOTS_PCT = 2,
-       EIMP_SHAPE_SMM_TREE_POOLS = 3, EIMP_SHAPE_BEAM_VARIANT = 4 };
+       EIMP_SHAPE_SMM_TREE_POOLS = 3 };
 int eimp_set_launch_shape(eimp_ctx *ctx, int knob, int value);
 int eimp_get_launch_shape(const eimp_ctx *ctx, int knob, int *value);
 

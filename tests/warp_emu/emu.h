@@ -25,7 +25,6 @@
 #define __forceinline__ inline
 #define __noinline__
 #define __launch_bounds__(...)
-#define __maxnreg__(...)
 #define __align__(n) __attribute__((aligned(n)))
 #define __restrict__ __restrict
 
