@@ -66,16 +66,17 @@ struct HPh {   // HaplotypePath
     unsigned char active0, active1, toext0, toext1;
 };
 
-struct BPh {   // BeamPath
-    int mat, pat;
+struct BPh {   // BeamPath, 48 bytes
+    unsigned short mat, pat;     // haplotype-path ids (< 4P + 8)
     float prob, weight;
     int nErr;
     float pErrPath, pErrPathp1;
     float extp[4];
     unsigned char active[4];
-    int actidx;
-    int extgeno;
+    signed char actidx;          // -2..3
+    unsigned char extgeno;       // 0..3
 };
+static_assert(sizeof(BPh) == 48, "beam paths stay 48 bytes");
 
 struct Hel { float key; int a; int b; };
 
