@@ -3,6 +3,8 @@
 // Target::prepPhase/phase and PBWTImputer interfaces.
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1263,6 +1265,20 @@ size_t eimp_gpu_block_size(const eimp_ctx *ctx) { (void)ctx; return 1024; }
 }  // extern "C"
 
 namespace eimp {
+cudaError_t ensure_dynamic_smem(const void *kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> limit;   // per device and kernel
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &cur = limit[{dev, kernel}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 // unpack the reference GPU path's per-target inputs into genotype bytes,
 // split lists and best-haplotype lists (one CTA per target)
 __global__ void unpack_gpu_inputs(const uint64_t *__restrict__ gtw, const uint64_t *__restrict__ splitw,

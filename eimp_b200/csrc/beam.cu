@@ -1508,7 +1508,7 @@ int beam_slots(const BeamParams &p, int M, int ntgt, int pct) {
     int dev = 0, nsm = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return -1;
-    if (cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+    if (ensure_dynamic_smem((const void *)beam_kernel, sm) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, beam_kernel, 32 * BEAM_WARPS, sm) != cudaSuccess || per < 1)
         return -1;
     int ctas = (int)((long)per * nsm * (pct < 1 ? 1 : pct > 100 ? 100 : pct) / 100);
@@ -1526,7 +1526,7 @@ cudaError_t launch_beam(const BeamParams &p, int ntgt, int M, const uint8_t *gt,
     ArenaLayout al = arena_layout(p, M);
     if (arena_bytes < al.total || slots < BEAM_WARPS || slots % BEAM_WARPS) return cudaErrorInvalidValue;
     const size_t sm = beam_smem(p, al, BEAM_WARPS);
-    cudaError_t e = cudaFuncSetAttribute(beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = ensure_dynamic_smem((const void *)beam_kernel, sm);
     if (e != cudaSuccess) return e;
     lpt_order_kernel<<<1, 1024, 0, st>>>(nsplits, ntgt, order, skip);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

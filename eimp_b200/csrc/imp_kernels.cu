@@ -1100,13 +1100,13 @@ cudaError_t launch_refpbwt(const uint64_t *sitemajor, int M, int K, int wN, uint
     const bool stage = refpbwt_ckpt_smem(K, wN, true, in_smem) <= lim;
     size_t sm = refpbwt_ckpt_smem(K, wN, stage, in_smem);
     auto ck = in_smem ? refpbwt_ckpt_kernel<1> : refpbwt_ckpt_kernel<8>;
-    cudaError_t e = cudaFuncSetAttribute(ck, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = ensure_dynamic_smem((const void *)ck, sm);
     if (e != cudaSuccess) return e;
     ck<<<1, 1024, sm, st>>>(sitemajor, M, K, wN, absperm, in_smem ? nullptr : scratch, stage ? 1 : 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (M <= 0) return cudaSuccess;
     sm = refpbwt_fill_smem(K, wN);
-    if ((e = cudaFuncSetAttribute(refpbwt_fill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) !=
+    if ((e = ensure_dynamic_smem((const void *)refpbwt_fill_kernel, sm)) !=
         cudaSuccess)
         return e;
     refpbwt_fill_kernel<<<(M + RP_CK - 1) / RP_CK, 1024, sm, st>>>(sitemajor, M, K, wN, compr, absperm, count0);
@@ -1142,7 +1142,7 @@ static cudaError_t smm_launch(Kern kern, int warps, const uint32_t *compr, const
                               int setmaxerrors, int4 *matches, int cap, int *nmatch, uint32_t *status,
                               cudaStream_t st, Extra... extra) {
     const size_t sm = sizeof(Smem) * warps;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = ensure_dynamic_smem((const void *)kern, sm);
     if (e != cudaSuccess) return e;
     const int blocks = (nhaps + warps - 1) / warps;
     kern<<<blocks, warps * 32, sm, st>>>(compr, count0, M, K, phased, wM, gt, nhaps, hapmap, setmaxerrors, matches,

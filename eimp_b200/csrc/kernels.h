@@ -17,6 +17,13 @@
 
 namespace eimp {
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`; never
+// lowers it.  The limit is a property of the kernel, shared by every host
+// thread: launchers that set it to exactly their own size could lower it
+// between another thread's setting and its launch.
+cudaError_t ensure_dynamic_smem(const void *kernel, size_t bytes);
+
+
 // ---- imputation (imp_kernels.cu)
 // global scratch launch_refpbwt needs (0: none) for K haplotypes
 size_t refpbwt_scratch_bytes(int K, int wN);

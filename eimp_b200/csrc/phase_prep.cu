@@ -226,7 +226,7 @@ cudaError_t launch_besthaps(const uint8_t *gt, int ntgt, int M, const uint64_t *
         const size_t sm = per * tb;
         auto kern = tb == 8 ? hamming_kernel<8> : tb == 4 ? hamming_kernel<4> : tb == 2 ? hamming_kernel<2>
                                                                                         : hamming_kernel<1>;
-        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+        if ((e = ensure_dynamic_smem((const void *)kern, sm)) != cudaSuccess)
             return e;
         dim3 grid((unsigned)((ntgt + tb - 1) / tb),
                   (unsigned)((nhaps + HAM_WARPS * HAM_HPW - 1) / (HAM_WARPS * HAM_HPW)));
@@ -314,7 +314,7 @@ cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_
                                const uint8_t *tgt_haploid, cudaStream_t st) {
     size_t sm = (size_t)2 * wM * sizeof(uint64_t);
     if (sm > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(monos_calls_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = ensure_dynamic_smem((const void *)monos_calls_kernel, sm);
         if (e != cudaSuccess) return e;
     }
     monos_calls_kernel<<<ntgt, 256, sm, st>>>(gt, M, hapmajor, wM, besthaps, K, cm, cMmaxsplit, monos, splits, calls,
@@ -495,7 +495,7 @@ cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapm
                         const int64_t *rowoff, uint64_t *cref, const int *skip, cudaStream_t st) {
     const size_t sm = (size_t)3 * wM * sizeof(uint64_t);
     if (sm > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(cref_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = ensure_dynamic_smem((const void *)cref_kernel, sm);
         if (e != cudaSuccess) return e;
     }
     const int wK = (int)eimp_W(K);
@@ -645,7 +645,7 @@ static cudaError_t launch_pbwt_w(const uint64_t *cref, int32_t *count0, const in
     const int nwords = (K + 31) / 32;
     const int nthreads = ((nwords + WPT - 1) / WPT + 31) / 32 * 32;
     const size_t sm = pbwt_smem(K);
-    cudaError_t e = cudaFuncSetAttribute(pbwt_kernel<WPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = ensure_dynamic_smem((const void *)pbwt_kernel<WPT>, sm);
     if (e != cudaSuccess) return e;
     pbwt_kernel<WPT><<<2 * ntgt, nthreads, sm, st>>>(cref, rowoff, K, pbwt, rowstride, emit_padded, count0, skip);
     return cudaGetLastError();
