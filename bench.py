@@ -12,8 +12,11 @@ phase+impute configuration instead (10,000 x 100,000, 1,000 targets typed at
 5 % with 2 % missing).  Synthetic seeded data of these shapes (the
 reference's panels are not available here).
 
-One step = the hot path over every target of the batch.  Per density group,
-on the group's own CUDA streams (the groups overlap on the device):
+One step = the hot path over every target of the batch, timed as the
+batched form runs it: each group's step captured once into a CUDA graph and
+replayed, the groups' graphs concurrently (the eager step, every launch
+enqueued from the host, is reported beside it).  Per density group, on the
+group's own CUDA streams (the groups overlap on the device):
   * the imputation reference of its typed sites (haplotype-major panel,
     segment map, reference PBWT with prefix arrays);
   * phasing of its targets in batches (best haplotypes, condensed reference,
@@ -74,7 +77,8 @@ def parse():
     ap.add_argument("--serving-rate-windows", type=float, default=3.0,
                     help="mean request arrivals per second of the window requests on the cfg3 panel")
     ap.add_argument("--serving-slots", type=int, default=3, help="slots of the window-request server")
-    ap.add_argument("--graph-steps", type=int, default=3, help="replays timed in the CUDA-graph form (0: skip)")
+    ap.add_argument("--graph-steps", type=int, default=1,
+                    help="time the step as CUDA-graph replays (default); 0: the eager step is the timed value")
     ap.add_argument("--qref-steps", type=int, default=5,
                     help="timed decodes of the panel's Qref haplotype section (0: skip)")
     ap.add_argument("--qref-variants", type=int, default=100000, help="panel variants of the Qref leg")
@@ -662,7 +666,7 @@ def main():
         from eimp_b200.autotune import tune_group, tune_step_shares
         tuning = {"groups": [tune_group(g) for g in groups]}
         if len(groups) > 1:
-            tuning["step_beam_shares"] = tune_step_shares(groups)
+            tuning["step_beam_shares"] = tune_step_shares(groups, reps=2)
 
     def step_timed(graphs=False):
         e0, e1 = ev(), ev()
@@ -672,6 +676,27 @@ def main():
         e1.record(main_stream)
         return e0, e1
 
+    def timed(graphs, steps):
+        """steps timed steps (L2 flushed before each); the sum of their device
+        times, the largest over the ranks"""
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            evs.append(step_timed(graphs))
+        torch.cuda.synchronize()
+        for g in groups:
+            g.ctx.synchronize()   # status check (capacity errors would surface here)
+        tot = float(np.sum([a.elapsed_time(b) for a, b in evs]))
+        if world > 1:
+            t = torch.tensor([tot], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot = float(t.item())
+            dist.barrier()
+        return tot
+
+    # the eager step (every launch enqueued from the host), then the step as
+    # the batched form runs it: each group's step captured once into a CUDA
+    # graph and replayed, the groups' graphs concurrently -- the timed value
     for _ in range(args.warmup):
         enqueue_step(groups)
     for g in groups:
@@ -679,30 +704,41 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    launches0 = sum(g.ctx.launches for g in groups)
+    eager_ms = timed(False, args.steps)
+    launches = sum(g.ctx.launches for g in groups) - launches0
+    use_graphs = args.graph_steps > 0
+    graph = None
+    if use_graphs:
+        ref_out = [(g.d_dos.clone(), g.d_bits.clone(), g.d_mats.clone(), g.d_pats.clone()) for g in groups]
+        for g in groups:
+            g.ctx.synchronize()
+            g.capture()
+        for _ in range(args.warmup):
+            enqueue_step(groups, capture_graphs=True)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    launches0 = sum(g.ctx.launches for g in groups)
-    evs = []
-    for _ in range(args.steps):
-        flush.zero_()
-        evs.append(step_timed())
-    torch.cuda.synchronize()
-    for g in groups:
-        g.ctx.synchronize()   # status check (capacity errors would surface here)
-    launches = sum(g.ctx.launches for g in groups) - launches0
+    tot_ms = timed(True, args.steps) if use_graphs else eager_ms
     clocks = sampler.stop()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    tot_ms = float(np.sum(step_ms))
-    if world > 1:
-        t = torch.tensor([tot_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
-        dist.barrier()
+    if use_graphs:
+        same = all(torch.equal(a, b) for g, r in zip(groups, ref_out)
+                   for a, b in zip(r, (g.d_dos, g.d_bits, g.d_mats, g.d_pats)))
+        del ref_out
     dos_per_step = sum(g.imputed() for g in groups)
     batches_info = [len(g.batches) for g in groups]
     targets_total = sum(g.nt for g in groups)
     value = world * dos_per_step * args.steps / (tot_ms / 1e3)
     ms_per_step = tot_ms / args.steps
+    eager = {"value": world * dos_per_step * args.steps / (eager_ms / 1e3), "unit": UNIT,
+             "ms_per_step": eager_ms / args.steps, "steps": args.steps,
+             "form": "every launch enqueued from the host, the groups on their own streams"}
+    if use_graphs:
+        graph = {"value": value, "unit": UNIT, "ms_per_step": ms_per_step, "steps": args.steps,
+                 "equal_to_eager": bool(same), "graphs": len(groups), "rows_reserved": [max(g.rows) for g in groups],
+                 "form": "the timed step: one CUDA graph per group (capacity-mode phasing), replayed concurrently"}
 
     # the last timed step's outputs for each group's CPU sample (compared with
     # the reference's own outputs once the CPU runs are done)
@@ -743,32 +779,6 @@ def main():
 
     serving = None
 
-    # ---- the CUDA-graph form: each group's step captured once (phasing in
-    # capacity mode) and replayed, the groups' graphs concurrently; the
-    # outputs must equal the eager step's
-    graph = None
-    if args.graph_steps > 0:
-        ref_out = [(g.d_dos.clone(), g.d_bits.clone(), g.d_mats.clone(), g.d_pats.clone()) for g in groups]
-        for g in groups:
-            g.ctx.synchronize()
-            g.capture()
-        for _ in range(args.warmup):
-            enqueue_step(groups, capture_graphs=True)
-        torch.cuda.synchronize()
-        gms = []
-        for _ in range(args.graph_steps):
-            flush.zero_()
-            gms.append(step_timed(graphs=True))
-        torch.cuda.synchronize()
-        for g in groups:
-            g.ctx.synchronize()
-        g_ms = max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in gms])), world, dev)
-        same = all(torch.equal(a, b) for g, r in zip(groups, ref_out)
-                   for a, b in zip(r, (g.d_dos, g.d_bits, g.d_mats, g.d_pats)))
-        graph = {"value": world * dos_per_step / (g_ms / 1e3), "unit": UNIT, "ms_per_step": g_ms,
-                 "steps": args.graph_steps, "equal_to_eager": bool(same), "graphs": len(groups),
-                 "rows_reserved": [max(g.rows) for g in groups]}
-        del ref_out
 
     # ---- the plain drop-in form: one target per call (phase, matches,
     # dosages), device-resident inputs, a few targets of every group
@@ -1060,10 +1070,13 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64/f32",
                 "data": "synthetic (seeded Li-Stephens mosaics of the configuration's shape)",
-                "config": config_block(cfg, panel, tgroups, batches_info),
+                "config": dict(config_block(cfg, panel, tgroups, batches_info),
+                               step_form="one CUDA graph per density group, replayed concurrently" if use_graphs
+                               else "eager launches"),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": int(launches), "phased_samples_per_sec": world * targets_total / (ms_per_step / 1e3),
-                "plain": plain, "serving": serving, "graph": graph, "qref_decode": qref, "parity": parity,
+                "plain": plain, "serving": serving, "graph": graph, "eager": eager, "qref_decode": qref,
+                "parity": parity,
                 "autotune": tuning, "cfg4": cfg4, "reference_gpu_engine": gpuengine}
         print(json.dumps(line), flush=True)
     for g in groups:
