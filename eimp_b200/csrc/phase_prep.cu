@@ -422,7 +422,9 @@ cudaError_t launch_compact_cols(const uint64_t *src, int rows, int srcw, const i
 // haplotype-major reference word by word, once: the split sites of the
 // target are a bit mask, so within a word every split closes the running
 // segment (its inconsistency row, then the split site's allele row) and the
-// rest of the word opens the next one.  The warp's ballot is the 32-bit word
+// rest of the word opens the next one.  One 64-bit addition per word gives
+// the inconsistency of every segment the word closes (a carry per segment,
+// below), so a split costs two ballots.  The warp's ballot is the 32-bit word
 // of an output row.  Grid: (target, 8 output words of 32 columns per CTA);
 // the columns past K are written as zero padding up to W(K) words.
 // ---------------------------------------------------------------------------
@@ -463,31 +465,41 @@ __global__ void __launch_bounds__(32 * CREF_WARPS) cref_kernel(
     const uint64_t *hm = hapmajor + (size_t)h * wM;
     const size_t rstride = 2 * (size_t)wK;   // 32-bit words per row
     uint32_t *out = reinterpret_cast<uint32_t *>(cref + (size_t)rowoff[t] * wK) + col32;
-    bool any = false;   // inconsistency of the open segment
-    int row = 0;
+    unsigned open = 0u;   // inconsistency of the open segment (0 or 1)
+    uint32_t *o = out;    // the next row pair
     uint64_t hw = valid ? hm[0] : 0ull;
     for (int q = 0; q < wM; q++) {
         const uint64_t a = hw;
         if (q + 1 < wM) hw = valid ? hm[q + 1] : 0ull;   // next word in flight
+        const uint64_t s = ssp[q];
         const uint64_t x = (a & is0[q]) | (~a & is2[q]);
-        uint64_t bnd = ssp[q];
-        int start = 0;
-        while (bnd) {
-            const int b = __ffsll((long long)bnd) - 1;
-            const uint64_t seg = b > start ? (x >> start) & (~0ull >> (64 - (b - start))) : 0ull;
-            any = any || seg != 0ull;
-            const unsigned wi = __ballot_sync(0xffffffffu, valid && any);
-            const unsigned ws = __ballot_sync(0xffffffffu, valid && ((a >> b) & 1ull));
-            if (lane == 0) { out[(size_t)row * rstride] = wi; out[(size_t)(row + 1) * rstride] = ws; }
-            row += 2;
-            any = false;
-            start = b + 1;
-            bnd &= bnd - 1;
+        // One addition closes every segment of the word: ~s has ones at the
+        // positions that are not split sites, so adding the inconsistencies
+        // there (and the open segment's state at bit 0) carries out of each
+        // segment that holds one into the split site that closes it, and no
+        // carry crosses a split site.  The carry out of the word is the state
+        // of the segment left open after the word's last split.
+        const uint64_t ns = ~s;
+        const uint64_t t = ns + (x & ns);
+        const uint64_t r = t + (uint64_t)open;
+        open = (t < ns || r < t) ? 1u : 0u;
+        const uint64_t marks = valid ? r & s : 0ull;
+#pragma unroll
+        for (int hf = 0; hf < 2; hf++) {
+            uint32_t bnd = (uint32_t)(s >> (32 * hf));
+            const uint32_t mk = (uint32_t)(marks >> (32 * hf)), al = (uint32_t)(a >> (32 * hf));
+            while (bnd) {
+                const int b = __ffs((int)bnd) - 1;
+                const unsigned wi = __ballot_sync(0xffffffffu, (mk >> b) & 1u);
+                const unsigned ws = __ballot_sync(0xffffffffu, (al >> b) & 1u);
+                if (lane == 0) { o[0] = wi; o[rstride] = ws; }
+                o += 2 * rstride;
+                bnd &= bnd - 1;
+            }
         }
-        if (start < 64) any = any || (x >> start) != 0ull;
     }
-    const unsigned wi = __ballot_sync(0xffffffffu, valid && any);
-    if (lane == 0) out[(size_t)row * rstride] = wi;
+    const unsigned wi = __ballot_sync(0xffffffffu, valid && open);
+    if (lane == 0) o[0] = wi;
 }
 
 cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM, int nhaps,
@@ -515,8 +527,10 @@ cudaError_t launch_cref(const uint8_t *gt, int ntgt, int M, const uint64_t *hapm
 // before it; the thread writes its [data, zeros through the word] pairs and
 // places its haplotypes in the next prefix order (zeros first, stable).  The
 // prefix arrays are 16-bit (K <= 65536) and XOR-swizzled within each 32-entry
-// block, so that the 32 lanes reading position j of their own words hit 32
-// different banks.  The next row is copied into shared memory asynchronously
+// block, so that the 32 lanes reading the same pair of positions of their own
+// words hit 32 different banks.  A thread reads its words' haplotypes once
+// per row, sixteen 32-bit pairs per word, and keeps them in registers from
+// the gather to the placement.  The next row is copied into shared memory asynchronously
 // while the current one is processed.  The forward CTA also writes each
 // row's zero count.
 // ---------------------------------------------------------------------------
@@ -529,6 +543,49 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // position p of the prefix order -> its slot in the swizzled array
 __device__ __forceinline__ int pswz(int p) { return p ^ ((p >> 5) & 31); }
+
+// The data word of one 32-position block of the prefix order (key = block &
+// 31, the block's swizzle): positions 2i and 2i+1 sit in the 32-bit pair
+// i ^ (key >> 1) of the block, swapped when key is odd, so sixteen 32-bit
+// loads (the 32 lanes of a warp on 32 different banks) fetch the block.  The
+// pairs go to hp in position order; the bits are pushed from position 31
+// down to 0.
+__device__ __forceinline__ uint32_t pbwt_gather(const uint32_t *__restrict__ pw, int key,
+                                                const uint32_t *__restrict__ row, uint32_t hp[16]) {
+    const int k2 = key >> 1;
+    const unsigned rot = (unsigned)(key & 1) << 4;
+    uint32_t b = 0u;
+#pragma unroll
+    for (int i = 15; i >= 0; i--) {
+        const uint32_t v = pw[i ^ k2];
+        const uint32_t x = __funnelshift_r(v, v, rot);
+        hp[i] = x;
+        const uint32_t h0 = x & 0xffffu, h1 = x >> 16;
+        const uint32_t r1 = row[h1 >> 5], r0 = row[h0 >> 5];
+        b = (b << 1) | (__funnelshift_r(r1, r1, h1) & 1u);
+        b = (b << 1) | (__funnelshift_r(r0, r0, h0) & 1u);
+    }
+    return b;
+}
+
+// Places the haplotypes of one block (hp, data word b) in the next prefix
+// order: a zero at the next zero place dz, a one at the next one place d1
+// (stable).  CHECK: only the first nv positions exist (the block holding K).
+template <bool CHECK>
+__device__ __forceinline__ void pbwt_place(uint16_t *__restrict__ nperm, const uint32_t hp[16], uint32_t b, int nv,
+                                           int &dz, int &d1) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        if (!CHECK || j < nv) {
+            const uint32_t x = hp[j >> 1];
+            const uint16_t h = (uint16_t)((j & 1) ? x >> 16 : x & 0xffffu);
+            const int one = (int)((b >> j) & 1u);
+            nperm[pswz(one ? d1 : dz)] = h;
+            d1 += one;
+            dz += 1 - one;
+        }
+    }
+}
 
 template <int WPT>
 __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__ cref,
@@ -571,23 +628,20 @@ __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__
             for (int c = tid; c < nchunk; c += nthreads) cp_async16(dst + 2 * c, src + 2 * c);
         }
         cp_async_commit();
-        // the thread's data words in the current prefix order
+        // the thread's data words in the current prefix order, and the
+        // haplotypes of their positions (two per register, in position order)
+        // kept for the placement
         uint32_t word[WPT];
+        uint32_t hp[WPT][16];
         int zsum = 0;
 #pragma unroll
         for (int q = 0; q < WPT; q++) {
             const int w = w0 + q;
             uint32_t b = ~0u;
             if (w < nwords) {
-                const uint16_t *pw = perm + w * 32;
-                const int key = w & 31;
-                b = 0u;
-#pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    const int h = pw[j ^ key];
-                    const uint32_t bit = (w * 32 + j < K) ? (row[h >> 5] >> (h & 31)) & 1u : 1u;
-                    b |= bit << j;
-                }
+                b = pbwt_gather(reinterpret_cast<const uint32_t *>(perm + w * 32), w & 31, row, hp[q]);
+                const int past = K - w * 32;   // positions past K read as 1 (the row format's padding)
+                if (past < 32) b |= ~0u << past;
                 zsum += __popc(~b);
             }
             word[q] = b;
@@ -608,21 +662,13 @@ __global__ void __launch_bounds__(1024) pbwt_kernel(const uint64_t *__restrict__
             const int w = w0 + q;
             if (w >= nwords) continue;
             const uint32_t b = word[q];
-            const uint16_t *pw = perm + w * 32;
-            const int key = w & 31;
-            int z = zb;   // zeros before position w*32 + j
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-                const int p = w * 32 + j;
-                if (p < K) {
-                    const int h = pw[j ^ key];
-                    const int dst = ((b >> j) & 1u) ? cnt0 + (p - z) : z;
-                    nperm[pswz(dst)] = (uint16_t)h;
-                }
-                z += (int)((~b >> j) & 1u);
-            }
-            reinterpret_cast<uint2 *>(o)[w] = make_uint2(b, (uint32_t)z);
-            zb = z;
+            // the next zero's place (zeros so far) and the next one's (cnt0 +
+            // ones so far)
+            int dz = zb, d1 = cnt0 + w * 32 - zb;
+            if (w * 32 + 32 <= K) pbwt_place<false>(nperm, hp[q], b, 32, dz, d1);
+            else pbwt_place<true>(nperm, hp[q], b, K - w * 32, dz, d1);
+            reinterpret_cast<uint2 *>(o)[w] = make_uint2(b, (uint32_t)dz);
+            zb = dz;
         }
         if (emit_padded)
             for (size_t jj = 2 * (size_t)nwords + tid; jj < rowstride; jj += nthreads) o[jj] = 0u;
