@@ -54,7 +54,28 @@ __device__ __forceinline__ int block_exscan_bit(int pred, int *buf, int *total) 
 // first, haploid placeholders) get 0xffffffff: never selected.
 // ---------------------------------------------------------------------------
 constexpr int HAM_WARPS = 8;     // warps per CTA
-constexpr int HAM_HPW = 16;      // haplotypes per warp
+constexpr int HAM_HPW = 64;      // haplotypes per warp (a CTA builds its targets' genotype words once for 512)
+constexpr int HAM_HU = 4;        // haplotypes per pass over the typed-site words
+
+// Reduce-scatter of N (a power of two <= 32) per-lane counts: afterwards v[0]
+// of lane l holds the warp's total of count l % N.  Each step halves the
+// counts a lane keeps, swapping the other half with the lane that keeps them
+// (31 shuffles for N = 32 instead of 32 x 5 for separate reductions).
+template <int N>
+__device__ __forceinline__ void warp_reduce_scatter(uint32_t (&v)[N], int lane) {
+#pragma unroll
+    for (int half = N / 2; half >= 1; half >>= 1) {
+        const bool up = (lane & half) != 0;
+#pragma unroll
+        for (int i = 0; i < half; i++) {
+            const uint32_t keep = up ? v[half + i] : v[i];
+            const uint32_t give = up ? v[i] : v[half + i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, give, half);
+        }
+    }
+#pragma unroll
+    for (int o = N; o < 32; o <<= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+}
 
 template <int HAM_TB>
 __global__ void __launch_bounds__(32 * HAM_WARPS) hamming_kernel(const uint8_t *__restrict__ gt, int ntgt, int M,
@@ -83,31 +104,37 @@ __global__ void __launch_bounds__(32 * HAM_WARPS) hamming_kernel(const uint8_t *
         }
     }
     __syncthreads();
+    // HAM_HU haplotypes at a time: their rows' words are independent loads
+    // in flight together, and each genotype word read from shared memory
+    // serves all of them
+    constexpr int NV = HAM_HU * HAM_TB;
     const int h0 = (blockIdx.y * HAM_WARPS + warp) * HAM_HPW;
-    for (int k = 0; k < HAM_HPW; k++) {
-        const int h = h0 + k;
-        if (h >= nhaps) break;
-        const uint64_t *row = hapmajor + (size_t)h * wM;
-        uint32_t acc[HAM_TB];
+    for (int k = 0; k < HAM_HPW; k += HAM_HU) {
+        const int hb = h0 + k;
+        if (hb >= nhaps) break;
+        uint32_t acc[NV];
 #pragma unroll
-        for (int q = 0; q < HAM_TB; q++) acc[q] = 0;
+        for (int i = 0; i < NV; i++) acc[i] = 0;
         for (int w = lane; w < wM; w += 32) {
-            const uint64_t x = row[w];
+            uint64_t x[HAM_HU];
 #pragma unroll
-            for (int q = 0; q < HAM_TB; q++)
-                acc[q] += __popcll((is0[q * wM + w] & x) | (is2[q * wM + w] & ~x));
+            for (int u = 0; u < HAM_HU; u++) x[u] = hb + u < nhaps ? hapmajor[(size_t)(hb + u) * wM + w] : 0ull;
+#pragma unroll
+            for (int q = 0; q < HAM_TB; q++) {
+                const uint64_t a = is0[q * wM + w], b = is2[q * wM + w];
+#pragma unroll
+                for (int u = 0; u < HAM_HU; u++) acc[u * HAM_TB + q] += __popcll((a & x[u]) | (b & ~x[u]));
+            }
         }
-#pragma unroll
-        for (int q = 0; q < HAM_TB; q++)
-            for (int o = 16; o; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-        if (lane < HAM_TB && tb + lane < ntgt) {
-            uint32_t v = acc[0];
-#pragma unroll
-            for (int q = 1; q < HAM_TB; q++) if (lane == q) v = acc[q];
-            const int t = tb + lane;
+        // lane l ends with the warp total of count l % NV: haplotype hb + u,
+        // target tb + q for l = u * HAM_TB + q
+        warp_reduce_scatter<NV>(acc, lane);
+        const int u = (lane % NV) / HAM_TB, q = lane % HAM_TB;
+        const int h = hb + u, t = tb + q;
+        if (lane < NV && h < nhaps && t < ntgt) {
             const int ign = self0 >= 0 ? 2 * (self0 + t) : -2;
             const bool excl = h == ign || h == ign + 1 || (haploid && (h & 1) && haploid[h >> 1]);
-            nerr[(size_t)t * nhaps + h] = excl ? 0xffffffffu : v;
+            nerr[(size_t)t * nhaps + h] = excl ? 0xffffffffu : acc[0];
         }
     }
 }
@@ -281,31 +308,68 @@ __global__ void __launch_bounds__(256) monos_calls_kernel(
         mo[w] = v;
     }
     __syncthreads();
-    if (tid != 0) return;
-    // Target.cpp:900-950 (sequential scan)
+    if (tid >= 32) return;
+    // Target.cpp:900-950, by one warp over 32 sites at a time.  From the
+    // first heterozygous site on, a site that is not monomorphic and not
+    // missing splits when it is heterozygous (a call) or when it lies more
+    // than cMmaxsplit after the previous split.  Heterozygous splits need no
+    // order; a homozygous one depends on the split before it, so within the
+    // chunk the first homozygous site that passes against the splits known so
+    // far is a split, and the sites after it are tested again (such splits
+    // are rare: one pass per chunk usually finds none).
+    const unsigned FULL = 0xffffffffu;
+    const int lane = tid;
+    const unsigned lt = (1u << lane) - 1u;
     const uint8_t *g = gt + (size_t)t * M;
     int32_t *sp = splits + (size_t)t * M, *cl = calls + (size_t)t * M;
     float *cd = cmdiffs + (size_t)t * (M + 1);
     int S = 0, C = 0;
     float last = cm[0];
-    int m = 0;
-    for (; m < M; m++) if (g[m] == 1) break;
-    for (; m < M; m++) {
-        uint8_t c = g[m];
-        bool mono = (sand[m >> 6] >> (m & 63)) & 1ull;
-        if (!mono && c != 3 && (c == 1 || __fsub_rn(cm[m], last) > cMmaxsplit)) {
-            if (c == 1) cl[C++] = S;
-            sp[S++] = m;
-            last = cm[m];
-        }
+    int m0 = M;   // the first heterozygous site (Target.cpp:905)
+    for (int b = 0; b < M; b += 32) {
+        const unsigned f = __ballot_sync(FULL, b + lane < M && g[b + lane] == 1);
+        if (f) { m0 = b + __ffs((int)f) - 1; break; }
     }
-    if (S == 0 || C == 0) { nsplits[t] = 0; ncalls[t] = 0; return; }   // Target.cpp:923-932
+    for (int b = m0; b < M; b += 32) {
+        const int m = b + lane;
+        const uint8_t c = m < M ? g[m] : 3;
+        const bool mono = m < M && ((sand[m >> 6] >> (m & 63)) & 1ull);
+        const float cmv = m < M ? cm[m] : 0.0f;
+        const bool het = !mono && c == 1, hom = !mono && c != 1 && c != 3;
+        const unsigned hets = __ballot_sync(FULL, het);
+        unsigned spl = hets;   // the chunk's splits known so far
+        int front = -1;        // sites up to here are settled
+        for (;;) {
+            const unsigned before = spl & lt;
+            const int src = before ? 31 - __clz((int)before) : 0;
+            const float prev = __shfl_sync(FULL, cmv, src);
+            const float lastv = before ? prev : last;
+            const bool pass = hom && lane > front && __fsub_rn(cmv, lastv) > cMmaxsplit;
+            const unsigned pm = __ballot_sync(FULL, pass);
+            if (!pm) break;
+            front = __ffs((int)pm) - 1;
+            spl |= 1u << front;
+        }
+        const bool isspl = (spl >> lane) & 1u;
+        const int si = S + __popc(spl & lt);
+        if (isspl) sp[si] = m;
+        if (het) cl[C + __popc(hets & lt)] = si;
+        if (spl) last = __shfl_sync(FULL, cmv, 31 - __clz((int)spl));
+        S += __popc(spl);
+        C += __popc(hets);
+    }
+    if (S == 0 || C == 0) {   // Target.cpp:923-932
+        if (lane == 0) { nsplits[t] = 0; ncalls[t] = 0; }
+        return;
+    }
+    __syncwarp();   // the warp's split and call entries are visible to all its lanes
     S = cl[C - 1] + 1;
-    cd[0] = __fsub_rn(cm[sp[0]], cm[0]);
-    for (int i = 1; i < S; i++) cd[i] = __fsub_rn(cm[sp[i]], cm[sp[i - 1]]);
-    cd[S] = __fsub_rn(cm[M - 1], cm[sp[S - 1]]);
-    nsplits[t] = S;
-    ncalls[t] = C;
+    for (int i = lane; i <= S; i += 32) {
+        const float a = i < S ? cm[sp[i]] : cm[M - 1];
+        const float p = i > 0 ? cm[sp[i - 1]] : cm[0];
+        cd[i] = __fsub_rn(a, p);
+    }
+    if (lane == 0) { nsplits[t] = S; ncalls[t] = C; }
 }
 
 cudaError_t launch_monos_calls(const uint8_t *gt, int ntgt, int M, const uint64_t *hapmajor, int wM,

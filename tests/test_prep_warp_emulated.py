@@ -1,0 +1,97 @@
+"""The phasing preparation kernels (eimp_b200/csrc/phase_prep.cu:
+hamming_kernel, besthaps_kernel, monos_calls_kernel; Target::prepPhase,
+Target.cpp:779-950) run on the CPU under the host warp emulator with the
+address and undefined-behaviour sanitizers, in the library's launch order:
+the Hamming counts of every (target, reference haplotype) pair, the K best
+haplotypes, the monomorphic sites, the split and call sites and the cM
+differences must equal the oracle restatement.  The genetic map has jumps
+larger than cMmaxsplit, so homozygous sites split by distance (several in one
+32-site chunk of the warp's scan); cases cover a partial last block of
+targets, typed sites not a multiple of 64, panels of one and two CTA columns
+and every targets-per-CTA variant (8, 4, 2, 1)."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from eimp_b200.bits import W, pack_rows
+
+CSRC = os.path.join(ROOT, "eimp_b200", "csrc")
+EMU = os.path.join(ROOT, "tests", "warp_emu")
+CMMAX = 0.125
+
+
+@pytest.fixture(scope="module")
+def emu_exe(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    d = tmp_path_factory.mktemp("prep_emu")
+    shutil.copy(os.path.join(CSRC, "common.cuh"), d / "common.cuh")
+    shutil.copy(os.path.join(CSRC, "kernels.h"), d / "kernels.h")
+    src = open(os.path.join(CSRC, "phase_prep.cu")).read()
+    a = src[src.index("__device__ __forceinline__ int block_sum_int"):src.index("cudaError_t launch_besthaps(")]
+    b = src[src.index("__global__ void __launch_bounds__(256) monos_calls_kernel("):
+            src.index("cudaError_t launch_monos_calls(")]
+    for old, new in (("extern __shared__ uint64_t shm[];", "uint64_t *shm = reinterpret_cast<uint64_t *>(emu_smem_ptr);"),
+                     ("extern __shared__ unsigned long long smo[];",
+                      "unsigned long long *smo = reinterpret_cast<unsigned long long *>(emu_smem_ptr);")):
+        assert (old in a) != (old in b)
+        a, b = a.replace(old, new), b.replace(old, new)
+    (d / "prep_emu.cpp").write_text('#include "emu.h"\n#include "common.cuh"\n#include "kernels.h"\n'
+                                    "namespace eimp {\n" + a + b + "}  // namespace eimp\n")
+    exe = d / "prep_emu"
+    cmd = ["g++", "-std=c++20", "-O1", "-g", "-fsanitize=address,undefined", "-fno-sanitize-recover=undefined",
+           "-I", EMU, "-I", str(d), os.path.join(EMU, "prep_main.cpp"), "-o", str(exe), "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-4000:]
+    return str(exe)
+
+
+@pytest.mark.parametrize("ntgt,M,nhaps,K,tb", [(11, 300, 700, 64, 8), (5, 1000, 200, 50, 4),
+                                               (3, 64, 97, 40, 2), (3, 130, 97, 33, 1)])
+def test_prep_emulated(emu_exe, tmp_path, ntgt, M, nhaps, K, tb):
+    from oracle import restate as R
+    rng = np.random.default_rng(M + 31 * nhaps + tb)
+    dense = (rng.random((nhaps, M)) < rng.uniform(0.02, 0.5, M)[None, :]).astype(np.uint8)
+    dense[:, rng.random(M) < 0.1] = 0   # some sites monomorphic in the panel
+    hm = pack_rows(dense, W(M))
+    gt = (dense[rng.integers(0, nhaps, ntgt)] + dense[rng.integers(0, nhaps, ntgt)]).astype(np.uint8)
+    flip = rng.random(gt.shape) < 0.05
+    gt[flip] = rng.integers(0, 3, int(flip.sum()))
+    gt[rng.random(gt.shape) < 0.03] = 3
+    inc = np.where(rng.random(M) < 0.04, rng.uniform(0.13, 0.4, M), rng.uniform(0.0, 0.004, M))
+    cm = np.cumsum(inc).astype(np.float32)
+    np.array([ntgt, M, nhaps, K, tb], np.int32).tofile(tmp_path / "params_i.bin")
+    np.array([CMMAX], np.float32).tofile(tmp_path / "params_f.bin")
+    gt.tofile(tmp_path / "gt.bin")
+    hm.tofile(tmp_path / "hapmajor.bin")
+    cm.tofile(tmp_path / "cm.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    rd = lambda n, dt: np.fromfile(tmp_path / n, dt)  # noqa: E731
+    nerr = rd("o_nerr.bin", np.uint32).reshape(ntgt, nhaps)
+    bh = rd("o_besthaps.bin", np.int32).reshape(ntgt, K)
+    mo = rd("o_monos.bin", np.uint64).reshape(ntgt, W(M))
+    sp = rd("o_splits.bin", np.int32).reshape(ntgt, M)
+    ca = rd("o_calls.bin", np.int32).reshape(ntgt, M)
+    cd = rd("o_cmdiffs.bin", np.float32).reshape(ntgt, M + 1)
+    ns, nc = rd("o_nsplits.bin", np.int32), rd("o_ncalls.bin", np.int32)
+    homsplits = 0
+    for t in range(ntgt):
+        obh, onerr = R.besthaps(gt[t], hm, K)
+        np.testing.assert_array_equal(nerr[t], onerr, err_msg=f"target {t}: Hamming counts")
+        np.testing.assert_array_equal(bh[t], obh, err_msg=f"target {t}: best haplotypes")
+        omo = R.monos(hm, M, obh)
+        np.testing.assert_array_equal(mo[t], omo, err_msg=f"target {t}: monomorphic sites")
+        osp, oca, ocd = R.calllocs(gt[t], omo, cm, CMMAX)
+        assert ns[t] == len(osp), f"target {t}: {ns[t]} splits, oracle {len(osp)}"
+        if len(osp):
+            np.testing.assert_array_equal(sp[t, :ns[t]], osp)
+            assert nc[t] == len(oca)
+            np.testing.assert_array_equal(ca[t, :nc[t]], oca)
+            np.testing.assert_array_equal(cd[t, :ns[t] + 1], ocd)
+            homsplits += int((gt[t, osp] != 1).sum())
+    assert homsplits > 0   # the distance rule was exercised

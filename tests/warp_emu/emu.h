@@ -196,6 +196,9 @@ inline unsigned atomicOr(unsigned *p, unsigned v) { return __atomic_fetch_or(p, 
 inline unsigned long long atomicOr(unsigned long long *p, unsigned long long v) {
     return __atomic_fetch_or(p, v, __ATOMIC_SEQ_CST);
 }
+inline unsigned long long atomicAnd(unsigned long long *p, unsigned long long v) {
+    return __atomic_fetch_and(p, v, __ATOMIC_SEQ_CST);
+}
 inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
     const uint64_t v = ((uint64_t)hi << 32) | lo;
     return (unsigned)(v >> (sh & 31));
