@@ -891,11 +891,25 @@ __global__ void __launch_bounds__(256, 4) dosage_kernel(
     const int KMASK = 0x7fffffff;
 
     // window start: the first match ending after the span's first segment
+    // (n if none).  The list is sorted by end, so a 32-way search narrows
+    // [qlo, qhi] to at most 32 candidates in a few dependent loads (a linear
+    // scan from the list's start took one per 32 matches before the span).
     const int kmin0 = sinfo[mref_begin + t0 * 64].x & KMASK;
-    int wb = n;
-    for (int b = 0; b < n; b += 32) {
-        const unsigned f = __ballot_sync(FULL, b + lane < n && mt[b + lane].y > kmin0);
-        if (f) { wb = b + __ffs(f) - 1; break; }
+    int qlo = 0, qhi = n;   // the answer lies in [qlo, qhi]
+    while (qhi - qlo > 32) {
+        const int step = (qhi - qlo + 31) >> 5;   // probes qlo, qlo + step, ..., 31 of them before qhi
+        const int p = qlo + lane * step;
+        const unsigned f = __ballot_sync(FULL, p >= qhi || mt[p].y > kmin0);
+        const int t = f ? __ffs((int)f) - 1 : 32;   // the first probe at or past the answer
+        if (t == 0) { qhi = qlo; break; }
+        const int nqlo = qlo + (t - 1) * step + 1;
+        if (t < 32) qhi = min(qhi, qlo + t * step);
+        qlo = nqlo;
+    }
+    int wb = qhi;
+    {
+        const unsigned f = __ballot_sync(FULL, qlo + lane < qhi && mt[qlo + lane].y > kmin0);
+        if (f) wb = qlo + __ffs((int)f) - 1;
     }
     int4 win = wb + lane < n ? mt[wb + lane] : NONE;
     // slots of the covering set (cwb, cncov): per window lane its height and

@@ -162,6 +162,36 @@ def test_dosages_shortcut_and_wide_tiles(emu_exe, tmp_path):
     assert taken == {False, True}
 
 
+def test_dosages_long_match_lists(emu_exe, tmp_path):
+    """Targets unrelated to a random panel: short set-maximal matches, hundreds
+    per haplotype, so every span's window start is found by the search over
+    the sorted match list (more than 32 matches before most spans); windows
+    starting at the panel's first site and deep inside it."""
+    from oracle import restate as R
+    rng = np.random.default_rng(4242)
+    Mref, nh, M = 6000, 64, 3000
+    typed = np.sort(rng.choice(Mref, M, replace=False)).astype(np.int64)
+    ref = (rng.random((nh, Mref)) < 0.5).astype(np.uint8)
+    af = ref.mean(axis=0).astype(np.float32)
+    sm_full = pack_rows(ref.T.copy(), W(nh))
+    sm_typed = np.ascontiguousarray(sm_full[typed])
+    nt = 2
+    th = (rng.random((2 * nt, M)) < 0.5).astype(np.uint8)
+    gt = (th[0::2] + th[1::2]).astype(np.uint8)
+    gt[0, rng.random(M) < 0.02] = 3
+    phased = pack_rows(th, W(M))
+    compr, c0, ap = R.pbwt(sm_typed, nh, absperm=True)
+    matches = [R.smmatches(compr, c0, M, nh, phased[h], np.where(gt[h // 2] == 3)[0].astype(np.int64))
+               for h in range(2 * nt)]
+    assert min(len(m) for m in matches) > 300
+    od, ob = oracle_full(matches, ap, sm_full, typed, af, nh, phased, gt)
+    full = unpack_rows(ob, Mref)
+    for k, (b0, n) in enumerate(((0, Mref), (3001, 2000), (Mref - 700, 700))):
+        dos, bits = run_kernel(emu_exe, tmp_path / f"l{k}", matches, ap, sm_full, typed, af, phased, gt, b0, n)
+        np.testing.assert_array_equal(dos, od[:, b0:b0 + n])
+        np.testing.assert_array_equal(unpack_rows(bits, n), full[:, b0:b0 + n])
+
+
 def test_dosage_division_helpers(tmp_path):
     """The dosage kernel's integer-only conversions (uint64 -> double below
     2^52, double -> float rounded to nearest even) give exactly the C casts
