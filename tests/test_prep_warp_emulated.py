@@ -95,3 +95,59 @@ def test_prep_emulated(emu_exe, tmp_path, ntgt, M, nhaps, K, tb):
             np.testing.assert_array_equal(cd[t, :ns[t] + 1], ocd)
             homsplits += int((gt[t, osp] != 1).sum())
     assert homsplits > 0   # the distance rule was exercised
+
+
+@pytest.mark.parametrize("K,self0,haploid,tb", [(40, 3, True, 8), (0, -1, True, 4), (0, 3, False, 8),
+                                                (33, 5, False, 2)])
+def test_prep_exclusions_emulated(emu_exe, tmp_path, K, self0, haploid, tb):
+    """Haplotypes a target may not select (Target.cpp:791-838): in phasing
+    iterations after the first, the target's own two (its sample is self0 + t
+    in the panel); with haploid reference samples, each one's placeholder
+    second column.  Their Hamming counts must read 0xffffffff, the rest the
+    oracle's; the selection is the K smallest (errors, index) among the
+    others, in index order, or all of them when K covers them (K = 0 here:
+    K is their count, as the reference clamps K to the haplotypes a target
+    may select before it selects)."""
+    from oracle import restate as R
+    rng = np.random.default_rng([K, self0 + 1, tb])
+    ntgt, M, nhaps = 9, 400, 160
+    dense = (rng.random((nhaps, M)) < rng.uniform(0.02, 0.5, M)[None, :]).astype(np.uint8)
+    hapl = (rng.random(nhaps // 2) < 0.25).astype(np.uint8) if haploid else np.zeros(nhaps // 2, np.uint8)
+    if haploid:
+        dense[1::2][hapl == 1] = dense[0::2][hapl == 1]   # a haploid sample as a homozygous pair
+    hm = pack_rows(dense, W(M))
+    gt = (dense[rng.integers(0, nhaps, ntgt)] + dense[rng.integers(0, nhaps, ntgt)]).astype(np.uint8)
+    gt[rng.random(gt.shape) < 0.03] = 3
+    cm = np.cumsum(rng.uniform(0.0, 0.01, M)).astype(np.float32)
+    if K == 0:   # every selectable haplotype (the same count for every target here)
+        K = nhaps - int(hapl.sum()) - (2 if self0 >= 0 else 0)
+    np.array([ntgt, M, nhaps, K, tb, self0, int(haploid)], np.int32).tofile(tmp_path / "params_i.bin")
+    np.array([CMMAX], np.float32).tofile(tmp_path / "params_f.bin")
+    gt.tofile(tmp_path / "gt.bin")
+    hm.tofile(tmp_path / "hapmajor.bin")
+    cm.tofile(tmp_path / "cm.bin")
+    hapl.tofile(tmp_path / "haploid.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    nerr = np.fromfile(tmp_path / "o_nerr.bin", np.uint32).reshape(ntgt, nhaps)
+    bh = np.fromfile(tmp_path / "o_besthaps.bin", np.int32).reshape(ntgt, K)
+    fl = np.fromfile(tmp_path / "o_flags.bin", np.uint64).reshape(ntgt, W(nhaps))
+    h = np.arange(nhaps)
+    for t in range(ntgt):
+        excl = ((h & 1) == 1) & (hapl[h >> 1] == 1) if haploid else np.zeros(nhaps, bool)
+        if self0 >= 0:
+            excl |= (h >> 1) == self0 + t
+        _, onerr = R.besthaps(gt[t], hm, nhaps)
+        if haploid or K < nhaps - (2 if self0 >= 0 else 0):   # the counts are computed (launch_besthaps)
+            np.testing.assert_array_equal(nerr[t, excl], np.uint32(0xffffffff))
+            np.testing.assert_array_equal(nerr[t, ~excl], onerr[~excl], err_msg=f"target {t}: Hamming counts")
+        allowed = h[~excl]
+        if K >= len(allowed):
+            want = allowed
+        else:
+            order = np.lexsort((allowed, onerr[allowed]))
+            want = np.sort(allowed[order[:K]])
+        np.testing.assert_array_equal(bh[t], want, err_msg=f"target {t}: best haplotypes")
+        sel = np.zeros(W(nhaps) * 64, np.uint8)
+        sel[want] = 1
+        np.testing.assert_array_equal(fl[t], pack_rows(sel[None, :], W(nhaps))[0], err_msg=f"target {t}: flags")

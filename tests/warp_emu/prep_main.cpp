@@ -5,10 +5,12 @@
 //
 //   prep_emu <dir>
 //
-// <dir> holds params_i.bin (ntgt, M, nhaps, K, tb), params_f.bin
+// <dir> holds params_i.bin (ntgt, M, nhaps, K, tb[, self0, use_haploid]),
+// haploid.bin (nhaps / 2 uint8, when use_haploid), params_f.bin
 // (cMmaxsplit), gt.bin (ntgt x M uint8), hapmajor.bin (nhaps x W(M) words)
 // and cm.bin (M float).  Outputs: o_nerr.bin (ntgt x nhaps uint32),
-// o_besthaps.bin (ntgt x K int32), o_monos.bin (ntgt x W(M) words),
+// o_besthaps.bin (ntgt x K int32), o_flags.bin (ntgt x W(nhaps) words),
+// o_monos.bin (ntgt x W(M) words),
 // o_splits.bin / o_calls.bin (ntgt x M int32), o_cmdiffs.bin (ntgt x (M+1)
 // float), o_nsplits.bin / o_ncalls.bin (ntgt int32).  Exit status 3: a
 // divergent warp collective.
@@ -75,6 +77,9 @@ int main(int argc, char **argv) {
     const auto hapmajor = rd<uint64_t>(d, "hapmajor.bin");
     const auto cm = rd<float>(d, "cm.bin");
     const int ntgt = pi[0], M = pi[1], nhaps = pi[2], K = pi[3], tb = pi[4];
+    const int self0 = pi.size() > 5 ? pi[5] : -1;
+    const std::vector<uint8_t> hapl = pi.size() > 6 && pi[6] ? rd<uint8_t>(d, "haploid.bin") : std::vector<uint8_t>();
+    const uint8_t *haploid = hapl.empty() ? nullptr : hapl.data();
     const float cMmaxsplit = pf[0];
     const int wM = (int)eimp_W(M), wN = (int)eimp_W(nhaps);
     std::vector<uint32_t> nerr((size_t)ntgt * nhaps, 0xdeadbeefu);
@@ -89,16 +94,16 @@ int main(int argc, char **argv) {
     for (unsigned bx = 0; bx < gx; bx++)
         for (unsigned by = 0; by < gy; by++)
             run_block(bx, by, 32 * eimp::HAM_WARPS, hsm, [&] {
-                if (tb == 8) eimp::hamming_kernel<8>(gt.data(), ntgt, M, hapmajor.data(), nhaps, wM, nerr.data(), -1, nullptr);
-                else if (tb == 4) eimp::hamming_kernel<4>(gt.data(), ntgt, M, hapmajor.data(), nhaps, wM, nerr.data(), -1, nullptr);
-                else if (tb == 2) eimp::hamming_kernel<2>(gt.data(), ntgt, M, hapmajor.data(), nhaps, wM, nerr.data(), -1, nullptr);
-                else eimp::hamming_kernel<1>(gt.data(), ntgt, M, hapmajor.data(), nhaps, wM, nerr.data(), -1, nullptr);
+                if (tb == 8) eimp::hamming_kernel<8>(gt.data(), ntgt, M, hapmajor.data(), nhaps, wM, nerr.data(), self0, haploid);
+                else if (tb == 4) eimp::hamming_kernel<4>(gt.data(), ntgt, M, hapmajor.data(), nhaps, wM, nerr.data(), self0, haploid);
+                else if (tb == 2) eimp::hamming_kernel<2>(gt.data(), ntgt, M, hapmajor.data(), nhaps, wM, nerr.data(), self0, haploid);
+                else eimp::hamming_kernel<1>(gt.data(), ntgt, M, hapmajor.data(), nhaps, wM, nerr.data(), self0, haploid);
             });
-    wr(d, "o_nerr.bin", nerr);   // before the selection reads them
+    wr(d, "o_nerr.bin", nerr);
     for (int t = 0; t < ntgt; t++)
         run_block(t, 0, 512, 0, [&] {
             eimp::besthaps_kernel(gt.data(), M, hapmajor.data(), nhaps, wM, K, nerr.data(), besthaps.data(),
-                                  flags.data(), wN, -1, nullptr);
+                                  flags.data(), wN, self0, haploid);
         });
     for (int t = 0; t < ntgt; t++)
         run_block(t, 0, 256, (size_t)2 * wM * 8, [&] {
@@ -107,6 +112,7 @@ int main(int argc, char **argv) {
                                      ncalls.data(), nullptr);
         });
     wr(d, "o_besthaps.bin", besthaps);
+    wr(d, "o_flags.bin", flags);
     wr(d, "o_monos.bin", monos);
     wr(d, "o_splits.bin", splits);
     wr(d, "o_calls.bin", calls);
