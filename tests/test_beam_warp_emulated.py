@@ -92,19 +92,23 @@ def golden_inputs(g, K):
                 pbwt=g[pre + "pbwt"], count0=g[pre + "count0"], rows=g[pre + "rows"])
 
 
-def test_beam_emulated_matches_reference_golden(emu_exe, tmp_path):
+@pytest.mark.parametrize("K", [64, 50, 200])
+def test_beam_emulated_matches_reference_golden(emu_exe, tmp_path, K):
+    """The reference's own phasing of the golden panel (beam 16): K = 50 is
+    not a multiple of 32 (padded PBWT rows), K = 200 takes every reference
+    haplotype."""
     g = np.load(golden_path("golden_tiny.npz"))
-    K = 64
+    pre = f"K{K}_"
     write_inputs(tmp_path, K=K, P=16, prephase=False, **golden_inputs(g, K))
     nt, M = g["gt"].shape
     mats, pats, dm, dp, tc, nc, st = run_emu(emu_exe, tmp_path, nt, M)
     assert not st.any()
-    np.testing.assert_array_equal(mats, g["K64_mat"])
-    np.testing.assert_array_equal(pats, g["K64_pat"])
-    np.testing.assert_array_equal(dm, g["K64_dos_mat"])
-    np.testing.assert_array_equal(dp, g["K64_dos_pat"])
-    np.testing.assert_array_equal(tc, g["K64_totalconf"])
-    np.testing.assert_array_equal(nc, g["K64_ncallsites"])
+    np.testing.assert_array_equal(mats, g[pre + "mat"])
+    np.testing.assert_array_equal(pats, g[pre + "pat"])
+    np.testing.assert_array_equal(dm, g[pre + "dos_mat"])
+    np.testing.assert_array_equal(dp, g[pre + "dos_pat"])
+    np.testing.assert_array_equal(tc, g[pre + "totalconf"])
+    np.testing.assert_array_equal(nc, g[pre + "ncallsites"])
 
 
 def test_beam_emulated_persistent_queue(emu_exe, tmp_path):
