@@ -14,7 +14,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, golden_path
 from eimp_b200.bits import W, pack_rows, transpose_bits
 
 CSRC = os.path.join(ROOT, "eimp_b200", "csrc")
@@ -94,3 +94,34 @@ def test_cref_emulated(emu_exe, tmp_path, M, nhaps, K, kinds):
     for t in range(ntgt):
         ocr, _ = R.cref(gt[t], sm, nhaps, bh[t], sp[t])
         np.testing.assert_array_equal(out[rowoff[t]:rowoff[t + 1]], ocr, err_msg=f"target {t} ({kinds[t]})")
+
+
+@pytest.mark.parametrize("K", [64, 50, 200])
+def test_cref_emulated_golden(emu_exe, tmp_path, K):
+    """The reference's own condensed references of the golden panel (made by
+    its Target::condensedReferenceT from its own best haplotypes and split
+    sites): K = 50 is not a multiple of 32, K = 200 takes every reference
+    haplotype (the identity selection)."""
+    g = np.load(golden_path("golden_tiny.npz"))
+    pre = f"K{K}_"
+    gt = np.ascontiguousarray(g["gt"], np.uint8)
+    ntgt, M = gt.shape
+    nhaps = int(g["nhaps"])
+    ns = g[pre + "nsplits"].astype(np.int32)
+    rowoff = np.concatenate([[0], np.cumsum(g[pre + "rows"])]).astype(np.int64)
+    assert np.array_equal(np.diff(rowoff), 2 * ns + 1)
+    splits = np.zeros((ntgt, M), np.int32)
+    off = np.concatenate([[0], np.cumsum(ns)])
+    for t in range(ntgt):
+        splits[t, :ns[t]] = g[pre + "splits"][off[t]:off[t + 1]]
+    np.array([ntgt, M, nhaps, K], np.int32).tofile(tmp_path / "params_i.bin")
+    gt.tofile(tmp_path / "gt.bin")
+    np.ascontiguousarray(g["hapmajor_typed"]).tofile(tmp_path / "hapmajor.bin")
+    g[pre + "besthaps"].astype(np.int32).tofile(tmp_path / "besthaps.bin")
+    splits.tofile(tmp_path / "splits.bin")
+    ns.tofile(tmp_path / "nsplits.bin")
+    rowoff.tofile(tmp_path / "rowoff.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    out = np.fromfile(tmp_path / "o_cref.bin", np.uint64).reshape(-1, W(K))
+    np.testing.assert_array_equal(out, g[pre + "cref"])

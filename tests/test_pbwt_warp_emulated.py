@@ -13,7 +13,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, golden_path
 from eimp_b200.bits import W
 
 CSRC = os.path.join(ROOT, "eimp_b200", "csrc")
@@ -87,3 +87,23 @@ def test_pbwt_emulated(emu_exe, tmp_path, K, wpt, nrows):
         np.testing.assert_array_equal(got[n:, :kw], bck)
         assert (got[:, kw:] == 0).all()   # row padding
         np.testing.assert_array_equal(c0[r0:r0 + n], fc0)
+
+
+@pytest.mark.parametrize("K", [64, 50, 200])
+def test_pbwt_emulated_golden(emu_exe, tmp_path, K):
+    """The reference's own forward and backward PBWTs (PBWT::buildComprPBWT)
+    of the golden panel's condensed references, and the forward zero counts."""
+    g = np.load(golden_path("golden_tiny.npz"))
+    pre = f"K{K}_"
+    Kc = min(K, int(g["nhaps"]))
+    rows = g[pre + "rows"].astype(np.int64)
+    rowoff = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
+    kw = 2 * ((Kc + 31) // 32)
+    np.array([len(rows), Kc, kw, 1, 1], np.int32).tofile(tmp_path / "params_i.bin")
+    rowoff.tofile(tmp_path / "rowoff.bin")
+    np.ascontiguousarray(g[pre + "cref"]).tofile(tmp_path / "cref.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    out = np.fromfile(tmp_path / "o_pbwt.bin", np.uint32).reshape(-1, kw)
+    np.testing.assert_array_equal(out, g[pre + "pbwt"])
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "o_count0.bin", np.int32), g[pre + "count0"])

@@ -16,7 +16,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, golden_path
 from eimp_b200.bits import W, pack_rows
 
 CSRC = os.path.join(ROOT, "eimp_b200", "csrc")
@@ -151,3 +151,40 @@ def test_prep_exclusions_emulated(emu_exe, tmp_path, K, self0, haploid, tb):
         sel = np.zeros(W(nhaps) * 64, np.uint8)
         sel[want] = 1
         np.testing.assert_array_equal(fl[t], pack_rows(sel[None, :], W(nhaps))[0], err_msg=f"target {t}: flags")
+
+
+@pytest.mark.parametrize("K", [64, 50, 200])
+def test_prep_emulated_golden(emu_exe, tmp_path, K):
+    """The reference's own preparation of the golden targets (Target::prepPhase:
+    best haplotypes, monomorphic sites, split and call sites, cM differences;
+    K = 200 takes every reference haplotype)."""
+    g = np.load(golden_path("golden_tiny.npz"))
+    pre = f"K{K}_"
+    gt = np.ascontiguousarray(g["gt"], np.uint8)
+    ntgt, M = gt.shape
+    nhaps = int(g["nhaps"])
+    np.array([ntgt, M, nhaps, K, 8], np.int32).tofile(tmp_path / "params_i.bin")
+    np.array([CMMAX], np.float32).tofile(tmp_path / "params_f.bin")
+    gt.tofile(tmp_path / "gt.bin")
+    np.ascontiguousarray(g["hapmajor_typed"]).tofile(tmp_path / "hapmajor.bin")
+    np.ascontiguousarray(g["cm_typed"], np.float32).tofile(tmp_path / "cm.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    rd = lambda n, dt: np.fromfile(tmp_path / n, dt)  # noqa: E731
+    Kc = min(K, nhaps)
+    np.testing.assert_array_equal(rd("o_besthaps.bin", np.int32).reshape(ntgt, K)[:, :Kc], g[pre + "besthaps"])
+    np.testing.assert_array_equal(rd("o_monos.bin", np.uint64).reshape(ntgt, W(M)), g[pre + "monos"])
+    ns, nc = rd("o_nsplits.bin", np.int32), rd("o_ncalls.bin", np.int32)
+    np.testing.assert_array_equal(ns, g[pre + "nsplits"])
+    np.testing.assert_array_equal(nc[ns > 0], g[pre + "ncalls"][ns > 0])
+    sp = rd("o_splits.bin", np.int32).reshape(ntgt, M)
+    ca = rd("o_calls.bin", np.int32).reshape(ntgt, M)
+    cd = rd("o_cmdiffs.bin", np.float32).reshape(ntgt, M + 1)
+    o_s = np.concatenate([[0], np.cumsum(g[pre + "nsplits"])])
+    o_c = np.concatenate([[0], np.cumsum(g[pre + "ncalls"])])
+    o_d = np.concatenate([[0], np.cumsum([s + 1 if s else 0 for s in g[pre + "nsplits"]])])
+    for t in range(ntgt):
+        np.testing.assert_array_equal(sp[t, :ns[t]], g[pre + "splits"][o_s[t]:o_s[t + 1]])
+        if ns[t]:
+            np.testing.assert_array_equal(ca[t, :nc[t]], g[pre + "calls"][o_c[t]:o_c[t + 1]])
+            np.testing.assert_array_equal(cd[t, :ns[t] + 1], g[pre + "cmdiffs"][o_d[t]:o_d[t + 1]])
