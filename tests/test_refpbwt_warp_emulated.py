@@ -13,7 +13,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, golden_path
 from eimp_b200.bits import W
 
 CSRC = os.path.join(ROOT, "eimp_b200", "csrc")
@@ -70,3 +70,22 @@ def test_refpbwt_emulated(emu_exe, tmp_path, M, K, in_smem, stage):
     np.testing.assert_array_equal(ap, rap)
     np.testing.assert_array_equal(compr, rc)
     np.testing.assert_array_equal(c0, rc0)
+
+
+@pytest.mark.parametrize("in_smem,stage", [(1, 1), (0, 0)])
+def test_refpbwt_emulated_golden(emu_exe, tmp_path, in_smem, stage):
+    """The reference's own imputation PBWT of the golden panel's typed sites
+    (PBWTImputer's compressed rows and prefix arrays)."""
+    g = np.load(golden_path("golden_tiny.npz"))
+    sm = np.ascontiguousarray(g["sitemajor_typed"])
+    M, wN = sm.shape
+    K = int(g["nhaps"])
+    np.array([M, K, wN, in_smem, stage], np.int32).tofile(tmp_path / "params_i.bin")
+    sm.tofile(tmp_path / "sitemajor.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    kw = 2 * ((K + 31) // 32)
+    compr = np.fromfile(tmp_path / "o_compr.bin", np.uint32).reshape(M, kw)
+    ap = np.fromfile(tmp_path / "o_absperm.bin", np.int32).reshape(M + 1, K)
+    np.testing.assert_array_equal(compr, g["imp_compr"].reshape(M, kw))
+    np.testing.assert_array_equal(ap, g["imp_absperm"].reshape(M + 1, K))
