@@ -188,3 +188,28 @@ def test_prep_emulated_golden(emu_exe, tmp_path, K):
         if ns[t]:
             np.testing.assert_array_equal(ca[t, :nc[t]], g[pre + "calls"][o_c[t]:o_c[t + 1]])
             np.testing.assert_array_equal(cd[t, :ns[t] + 1], g[pre + "cmdiffs"][o_d[t]:o_d[t + 1]])
+
+
+@pytest.mark.parametrize("K", [64, 175])
+def test_prep_emulated_golden_haploid(emu_exe, tmp_path, K):
+    """The reference's own best haplotypes of the diploid golden targets on a
+    panel with haploid samples (their placeholder second columns are never
+    chosen, Target.cpp:798-838); K = 175 is every existing haplotype (the
+    reference clamps K to them, PBWTPhaser.cpp:159, 210)."""
+    g = np.load(golden_path("golden_haploid.npz"))
+    dip = g["tgt_haploid"] == 0
+    gt = np.ascontiguousarray(g["gt"][dip], np.uint8)
+    ntgt, M = gt.shape
+    nhaps = int(g["nhaps"])
+    hapl = np.ascontiguousarray(g["ref_haploid"], np.uint8)
+    assert nhaps - int(hapl.sum()) == 175
+    np.array([ntgt, M, nhaps, K, 8, -1, 1], np.int32).tofile(tmp_path / "params_i.bin")
+    np.array([CMMAX], np.float32).tofile(tmp_path / "params_f.bin")
+    gt.tofile(tmp_path / "gt.bin")
+    np.ascontiguousarray(g["hapmajor_typed"]).tofile(tmp_path / "hapmajor.bin")
+    np.ascontiguousarray(g["cm_typed"], np.float32).tofile(tmp_path / "cm.bin")
+    hapl.tofile(tmp_path / "haploid.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    bh = np.fromfile(tmp_path / "o_besthaps.bin", np.int32).reshape(ntgt, K)
+    np.testing.assert_array_equal(bh, g[f"K{64 if K == 64 else 200}_besthaps"])
