@@ -238,3 +238,51 @@ int main() {
     assert r.returncode == 0, r.stderr[-3000:]
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and r.stdout.strip() == "0", r.stdout + r.stderr
+
+
+def test_dosages_haploid_golden(emu_exe, tmp_path):
+    """The reference's own imputation of the haploid golden case: a reduced
+    reference of the 175 existing panel haplotypes read through their panel
+    columns (haploidsRefMap, TargetImp.cpp:536) and the 13 existing target
+    haplotypes through a row map (PBWTImputer.cpp:130, 202); every site the
+    reference writes (untyped, and missing typed ones) must equal its dosage
+    and allele."""
+    g = np.load(golden_path("golden_haploid.npz"))
+    gt = np.ascontiguousarray(g["gt"], np.uint8)
+    nt, M = gt.shape
+    Mref, nh_panel, K = int(g["Mref"]), int(g["nhaps"]), int(g["imp_K"])
+    hapl = g["ref_haploid"]
+    refmap = np.array([c for s in range(nh_panel // 2) for c in ([2 * s] if hapl[s] else [2 * s, 2 * s + 1])],
+                      np.int32)
+    assert len(refmap) == K
+    hapmap = np.array([h for t in range(nt) for h in ([2 * t] if g["tgt_haploid"][t] else [2 * t, 2 * t + 1])],
+                      np.int32)
+    counts = g["imp_nmatches"]
+    assert len(counts) == len(hapmap)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    cap = max(1, int(counts.max()))
+    mt = np.zeros((2 * nt, cap, 4), np.int32)
+    nm = np.zeros(2 * nt, np.int32)
+    for j, h in enumerate(hapmap):
+        mt[h, :counts[j]] = g["imp_matches"][off[j]:off[j + 1]]
+        nm[h] = counts[j]
+    hapfull = transpose_bits(g["sitemajor_full"], Mref, nh_panel)
+    phased = g["imp_phased"]
+    params = np.array([len(hapmap), cap, K, hapfull.shape[1], M, phased.shape[1], nh_panel, 0, Mref, 0, Mref,
+                       2 * nt, 1], np.int32)
+    for name, a in [("params_i", params), ("matches", mt), ("nmatch", nm),
+                    ("absperm", g["imp_absperm"].astype(np.int32)), ("hapfull", hapfull),
+                    ("typed", np.asarray(g["typed"], np.int64)), ("af", g["af_full"].astype(np.float32)),
+                    ("phased", phased.astype(np.uint64)), ("gt", gt), ("hapmap", hapmap), ("refmap", refmap)]:
+        np.ascontiguousarray(a).tofile(tmp_path / (name + ".bin"))
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    dos = np.fromfile(tmp_path / "o_dos.bin", np.float32).reshape(2 * nt, Mref)
+    bits = np.fromfile(tmp_path / "o_bits.bin", np.uint64).reshape(2 * nt, (Mref + 63) // 64)
+    sel = np.ones((nt, Mref), bool)
+    sel[:, g["typed"]] = gt == 3
+    for h in hapmap:
+        s = sel[h // 2]
+        np.testing.assert_array_equal(dos[h][s], g["imp_dos"][h][s])
+        got, want = unpack_rows(bits[h:h + 1], Mref)[0], unpack_rows(g["imp_bits"][h:h + 1], Mref)[0]
+        np.testing.assert_array_equal(got[s], want[s])

@@ -5,13 +5,17 @@
 //
 // <dir> holds the inputs as raw little-endian arrays in the layout of the
 // device buffers: params_i.bin (nhaps, cap, K, wMref, M, wM, nrefhaps_total,
-// mref_begin, nsites, imputeCalls, Mref), matches.bin (nhaps x cap int4),
+// mref_begin, nsites, imputeCalls, Mref[, nrows, maps]), matches.bin (nhaps x cap int4),
 // nmatch.bin (nhaps i32), absperm.bin ((M+1) x K i32), hapfull.bin (K x wMref
 // u64), typed.bin (M i64), af.bin (Mref f32), phased.bin (nhaps x wM u64),
 // gt.bin (nhaps/2 x M u8).  The segment map and the per-site pairs come from
 // the segment-map kernel, run site by site.  Outputs: o_dos.bin (nhaps x
 // nsites f32), o_bits.bin (nhaps x ceil(nsites/64) u64), o_segm.bin,
-// o_sinfo.bin.  Every input is its own allocation so the address sanitizer
+// o_sinfo.bin.  With maps set, the matches, phased rows and outputs have
+// nrows rows (the target haplotypes), of which the nhaps listed in
+// hapmap.bin are imputed, and refmap.bin gives the panel column of each
+// haplotype of the reduced reference (hapfull.bin then has the panel's
+// columns).  Every input is its own allocation so the address sanitizer
 // sees reads past it.
 // Exit status 3: a divergent warp collective was seen.
 #include "dosage_emu.cpp"
@@ -52,6 +56,13 @@ int main(int argc, char **argv) {
     const auto pi = rd<int32_t>(d, "params_i.bin");
     const int nhaps = pi[0], cap = pi[1], K = pi[2], wMref = pi[3], M = pi[4], wM = pi[5], ntot = pi[6];
     const int mref_begin = pi[7], nsites = pi[8], impcalls = pi[9], Mref = pi[10];
+    // optional: nrows target haplotype rows of which the nhaps in hapmap.bin
+    // are imputed, and refmap.bin, the panel column of each of the K
+    // haplotypes of the reduced reference (haploid samples)
+    const int nrows = pi.size() > 11 ? pi[11] : nhaps;
+    const bool maps = pi.size() > 12 && pi[12];
+    const std::vector<int32_t> hapmap = maps ? rd<int32_t>(d, "hapmap.bin") : std::vector<int32_t>();
+    const std::vector<int32_t> refmap = maps ? rd<int32_t>(d, "refmap.bin") : std::vector<int32_t>();
     const auto matches = rd<int4>(d, "matches.bin");
     const auto nmatch = rd<int32_t>(d, "nmatch.bin");
     const auto absperm = rd<int32_t>(d, "absperm.bin");
@@ -71,8 +82,8 @@ int main(int argc, char **argv) {
     const auto gt = rd<uint8_t>(d, "gt.bin");
     const int ntiles = (nsites + 63) / 64, ldb = ntiles;
     const int nspans = (ntiles + eimp::DOS_SPAN - 1) / eimp::DOS_SPAN;
-    std::vector<float> dos((size_t)nhaps * nsites, -7.0f);
-    std::vector<uint64_t> bits((size_t)nhaps * ldb, 0x5A5A5A5A5A5A5A5Aull);
+    std::vector<float> dos((size_t)nrows * nsites, -7.0f);
+    std::vector<uint64_t> bits((size_t)nrows * ldb, 0x5A5A5A5A5A5A5A5Aull);
     for (long gw = 0; gw < (long)nhaps * nspans; gw++) {
         EmuWarp warp;
         std::vector<std::thread> lanes;
@@ -83,8 +94,9 @@ int main(int argc, char **argv) {
                 blockDim.x = 32;
                 emu_warp = &warp;
                 (M < 131071 ? eimp::dosage_kernel<false, eimp::DOS_SPAN> : eimp::dosage_kernel<true, eimp::DOS_SPAN>)(
-                    matches.data(), cap, nmatch.data(), absperm.data(), K, nullptr, hapfull.data(), wMref,
-                    sinfo.data(), phased.data(), wM, gt.data(), M, nhaps, nullptr, mref_begin, nsites, impcalls,
+                    matches.data(), cap, nmatch.data(), absperm.data(), K, maps ? refmap.data() : nullptr,
+                    hapfull.data(), wMref, sinfo.data(), phased.data(), wM, gt.data(), M, nhaps,
+                    maps ? hapmap.data() : nullptr, mref_begin, nsites, impcalls,
                     dos.data(), nsites, bits.data(), ldb);
             });
         for (auto &x : lanes) x.join();
