@@ -153,3 +153,35 @@ def test_errors_reported(emu_exe, tmp_path):
             for a, b in zip(g0, g1):
                 if a is not None:
                     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("which", [0, 1, 2], ids=["wide", "compact", "compact16"])
+def test_matches_haploid_golden(emu_exe, tmp_path, which):
+    """The reference's own matches of the haploid golden case: the 13 existing
+    target haplotypes (a row map, PBWTImputer.cpp:130, 202) against its
+    reduced imputation PBWT of the 175 existing panel haplotypes."""
+    g = np.load(golden_path("golden_haploid.npz"))
+    gt = np.ascontiguousarray(g["gt"], np.uint8)
+    nt, M = gt.shape
+    K = int(g["imp_K"])
+    compr = np.ascontiguousarray(g["imp_compr"], np.uint32)
+    count0 = compr[:, -1].astype(np.int32)   # the last pair's zeros (the tail is padded with ones)
+    hapmap = np.array([h for t in range(nt) for h in ([2 * t] if g["tgt_haploid"][t] else [2 * t, 2 * t + 1])],
+                      np.int32)
+    cap = M // 4 + 64
+    d = tmp_path / "k"
+    os.makedirs(d, exist_ok=True)
+    for name, a in [("params_i", np.array([len(hapmap), M, K, 0, cap, 2 * nt, 1], np.int32)), ("compr", compr),
+                    ("count0", count0), ("phased", g["imp_phased"].astype(np.uint64)), ("gt", gt),
+                    ("hapmap", hapmap)]:
+        np.ascontiguousarray(a).tofile(d / (name + ".bin"))
+    r = subprocess.run([emu_exe, str(d), str(which), "0"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    m = np.fromfile(d / "o_matches.bin", np.int32).reshape(2 * nt, cap, 4)
+    n = np.fromfile(d / "o_nmatch.bin", np.int32)
+    assert int(np.fromfile(d / "o_status.bin", np.uint32)[0]) == 0
+    counts = g["imp_nmatches"]
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for j, h in enumerate(hapmap):
+        assert n[h] == counts[j]
+        np.testing.assert_array_equal(m[h, :n[h]].astype(np.int64), g["imp_matches"][off[j]:off[j + 1]])

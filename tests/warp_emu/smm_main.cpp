@@ -9,10 +9,12 @@
 //
 // Both launches of launch_smm run: the small node pool first, then the retry
 // pass with the large pool.  <dir> holds the inputs as raw little-endian arrays in the layout of the
-// device buffers: params_i.bin (nhaps, M, K, setmaxerrors, cap), compr.bin
+// device buffers: params_i.bin (nhaps, M, K, setmaxerrors, cap[, nrows, use_hapmap]), compr.bin
 // (M x kw u32), count0.bin (M i32), phased.bin (nhaps x W(M) u64), gt.bin
 // (nhaps/2 x M u8).  Outputs: o_matches.bin (nhaps x cap int4), o_nmatch.bin,
-// o_status.bin, o_retried.bin (haplotypes redone by the retry pass).  Each haplotype gets its own shared-memory block so the
+// o_status.bin, o_retried.bin (haplotypes redone by the retry pass).  With use_hapmap,
+// the phased rows and outputs have nrows rows (the target haplotypes) and
+// hapmap.bin lists the nhaps of them that are searched.  Each haplotype gets its own shared-memory block so the
 // address sanitizer sees accesses past it.  Exit status 3: a divergent warp
 // collective was seen.
 #include "smm_emu.cpp"
@@ -54,13 +56,16 @@ int main(int argc, char **argv) {
     const int pool_slots = argc > 3 ? atoi(argv[3]) : 0;
     const auto pi = rd<int32_t>(d, "params_i.bin");
     const int nhaps = pi[0], M = pi[1], K = pi[2], sme = pi[3], cap = pi[4];
+    const int nrows = pi.size() > 5 ? pi[5] : nhaps;
+    const std::vector<int32_t> hapmap = pi.size() > 6 && pi[6] ? rd<int32_t>(d, "hapmap.bin") : std::vector<int32_t>();
+    const int32_t *hm = hapmap.empty() ? nullptr : hapmap.data();
     const auto compr = rd<uint32_t>(d, "compr.bin");
     const auto count0 = rd<int32_t>(d, "count0.bin");
     const auto phased = rd<uint64_t>(d, "phased.bin");
     const auto gt = rd<uint8_t>(d, "gt.bin");
     const int wM = (int)eimp_W(M);
-    std::vector<int4> matches((size_t)nhaps * cap, int4{-7, -7, -7, -7});
-    std::vector<int32_t> nmatch(nhaps, -7);
+    std::vector<int4> matches((size_t)nrows * cap, int4{-7, -7, -7, -7});
+    std::vector<int32_t> nmatch(nrows, -7);
     uint32_t status = 0;
     int retried = 0;
     // global tree pools of the first pass (exact size: the address sanitizer
@@ -79,7 +84,7 @@ int main(int argc, char **argv) {
                                    : (pass ? sizeof(eimp::SmmWarpSmem<SMM_NODES_RETRY>)
                                            : sizeof(eimp::SmmWarpSmem<SMM_NODES>));
         for (int h = 0; h < nhaps; h++) {
-            if (pass) retried += nmatch[h] == eimp::SMM_RETRY;
+            if (pass) retried += nmatch[hm ? hm[h] : h] == eimp::SMM_RETRY;
             // a fill pattern instead of zeros: the kernel must not read what it has not written
             uint8_t *smem = (uint8_t *)aligned_alloc(16, (smb + 15) / 16 * 16);
             memset(smem, 0x5A, smb);
@@ -96,18 +101,18 @@ int main(int argc, char **argv) {
                     if (which == 2) {
                         auto kern = pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, uint16_t>
                                          : eimp::smm_compact_kernel<SMM_NODES, 1, false, uint16_t>;
-                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
+                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, hm, sme,
                              matches.data(), cap, nmatch.data(), &status, pass ? nullptr : (Big16 *)gp,
                              pass ? 0 : pool_slots, pass ? nullptr : &gnext);
                     } else if (which == 1) {
                         auto kern = pass ? eimp::smm_compact_kernel<SMM_NODES_RETRY, 1, true, int>
                                          : eimp::smm_compact_kernel<SMM_NODES, 1, false, int>;
-                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
+                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, hm, sme,
                              matches.data(), cap, nmatch.data(), &status, pass ? nullptr : (Big32 *)gp,
                              pass ? 0 : pool_slots, pass ? nullptr : &gnext);
                     } else {
                         auto kern = pass ? eimp::smm_kernel<SMM_NODES_RETRY, 1, true> : eimp::smm_kernel<SMM_NODES, 1, false>;
-                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, nullptr, sme,
+                        kern(compr.data(), count0.data(), M, K, phased.data(), wM, gt.data(), nhaps, hm, sme,
                              matches.data(), cap, nmatch.data(), &status);
                     }
                 });
