@@ -1,9 +1,11 @@
 // Phasing preparation, condensed reference and PBWT kernels for B200 (sm_100a).
 //
-//  besthaps_kernel    -- Target::findBestHaps (Target.cpp:779-875) with the
-//                        Hamming count of GenotypeVector::compare_withPreInit
-//                        (Datatypes.cpp:107-116); exact K-smallest selection
-//                        by (errors, index) via a threshold search.
+//  hamming_kernel     -- the Hamming counts of GenotypeVector::compare_withPreInit
+//                        (Datatypes.cpp:107-116), 8 targets x 512 reference
+//                        haplotypes per CTA.
+//  besthaps_kernel    -- Target::findBestHaps (Target.cpp:779-875): exact
+//                        K-smallest selection by (errors, index) via a
+//                        threshold search.
 //  monos_calls_kernel -- Target::findMonos + findCallLocs (Target.cpp:878-950)
 //  cref_kernel        -- Target::condensedReferenceT (Target.cpp:953-1059),
 //                        one lane per selected haplotype (haplotype-major).
