@@ -3,7 +3,9 @@ host warp emulator (tests/warp_emu): every warp collective must be reached by
 all 32 lanes from the same call site, no access may leave its buffers
 (address and undefined-behaviour sanitizers), and the phased haplotypes,
 dosages and confidences must equal the golden fixtures made by the reference
-(beam 16) and the oracle restatement (beams 64 and 4 with pre-phasing)."""
+(beam 16 at K = 64, 50 and 200) and the oracle restatement (beams 128, 64 and
+4 with pre-phasing; K = 4096 and beam 128 on cfg1 targets, the bench's
+setting)."""
 import os
 import shutil
 import subprocess
@@ -180,3 +182,46 @@ def test_beam_emulated_start_phases_match_reference(emu_exe, tmp_path, prephase)
         assert tc[t] == np.float32(c) and nc[t] == n
     rc.close()
 
+
+
+def test_beam_emulated_bench_setting(emu_exe, tmp_path):
+    """K = 4096 conditioning haplotypes (PBWT rows of 128 words staged per
+    warp) and beam 128 with the reference's history sizes, as the bench runs
+    them: two cfg1 targets (5,000 reference haplotypes, 2,000 typed sites).
+    The inputs come from the oracle's preparation, condensed reference and
+    PBWTs (pinned to the reference's golden fixtures); the phased haplotypes
+    and dosages must equal the oracle's beam."""
+    from eimp_b200 import synth
+    from oracle import restate as R
+    if not R.available():
+        pytest.skip("oracle library not built")
+    panel, groups = synth.generate("cfg1")
+    tg = groups[0]
+    hm, sm, cm = synth.typed_views(panel, tg.typed)
+    K, P = 4096, 128
+    gt = np.ascontiguousarray(tg.gt[:2], np.uint8)
+    nt, M = gt.shape
+    monos, splits, calls, cmds, pb, c0s, rows = [], [], [], [], [], [], []
+    for t in range(nt):
+        bh, _ = R.besthaps(gt[t], hm, K)
+        mo = R.monos(hm, M, bh)
+        sp, ca, cd = R.calllocs(gt[t], mo, cm)
+        cr, c0 = R.cref(gt[t], sm, panel.nhaps, bh, sp)
+        pb.append(np.concatenate([R.pbwt(cr, K)[0], R.pbwt(cr, K, reverse=True)[0]]))
+        monos.append(mo)
+        splits.append(sp)
+        calls.append(ca)
+        cmds.append(cd)
+        c0s.append(c0)
+        rows.append(len(cr))
+    assert min(len(s) for s in splits) > 100
+    write_inputs(tmp_path, gt=gt, monos=np.stack(monos), splits=splits, calls=calls, cmd=cmds,
+                 pbwt=np.concatenate(pb), count0=np.concatenate(c0s), rows=np.array(rows), K=K, P=P,
+                 prephase=False)
+    mats, pats, dm, dp, tc, nc, st = run_emu(emu_exe, tmp_path, nt, M)
+    assert not st.any()
+    om, op, odm, odp = R.phase_many(gt, hm, sm, cm, R.params_c(K=K, beamwidth=P), 2)
+    np.testing.assert_array_equal(mats, om)
+    np.testing.assert_array_equal(pats, op)
+    np.testing.assert_array_equal(dm, odm)
+    np.testing.assert_array_equal(dp, odp)
