@@ -213,3 +213,44 @@ def test_prep_emulated_golden_haploid(emu_exe, tmp_path, K):
     assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
     bh = np.fromfile(tmp_path / "o_besthaps.bin", np.int32).reshape(ntgt, K)
     np.testing.assert_array_equal(bh, g[f"K{64 if K == 64 else 200}_besthaps"])
+
+
+def test_prep_emulated_bench_setting(emu_exe, tmp_path):
+    """K = 4096 of the 5,000 cfg1 reference haplotypes (the threshold search
+    picks most of the panel, with ties at the threshold taken in index order)
+    at 2,000 typed sites: best haplotypes, monomorphic sites, split and call
+    sites and cM differences against the oracle."""
+    from eimp_b200 import synth
+    from oracle import restate as R
+    panel, groups = synth.generate("cfg1")
+    tg = groups[0]
+    hm, _sm, cm = synth.typed_views(panel, tg.typed)
+    gt = np.ascontiguousarray(tg.gt[:3], np.uint8)
+    ntgt, M = gt.shape
+    K = 4096
+    np.array([ntgt, M, panel.nhaps, K, 8], np.int32).tofile(tmp_path / "params_i.bin")
+    np.array([CMMAX], np.float32).tofile(tmp_path / "params_f.bin")
+    gt.tofile(tmp_path / "gt.bin")
+    np.ascontiguousarray(hm).tofile(tmp_path / "hapmajor.bin")
+    np.ascontiguousarray(cm, np.float32).tofile(tmp_path / "cm.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    rd = lambda n, dt: np.fromfile(tmp_path / n, dt)  # noqa: E731
+    nerr = rd("o_nerr.bin", np.uint32).reshape(ntgt, panel.nhaps)
+    bh = rd("o_besthaps.bin", np.int32).reshape(ntgt, K)
+    mo = rd("o_monos.bin", np.uint64).reshape(ntgt, W(M))
+    ns, nc = rd("o_nsplits.bin", np.int32), rd("o_ncalls.bin", np.int32)
+    sp = rd("o_splits.bin", np.int32).reshape(ntgt, M)
+    ca = rd("o_calls.bin", np.int32).reshape(ntgt, M)
+    cd = rd("o_cmdiffs.bin", np.float32).reshape(ntgt, M + 1)
+    for t in range(ntgt):
+        obh, onerr = R.besthaps(gt[t], hm, K)
+        np.testing.assert_array_equal(nerr[t], onerr)
+        np.testing.assert_array_equal(bh[t], obh)
+        omo = R.monos(hm, M, obh)
+        np.testing.assert_array_equal(mo[t], omo)
+        osp, oca, ocd = R.calllocs(gt[t], omo, cm, CMMAX)
+        assert ns[t] == len(osp) > 100
+        np.testing.assert_array_equal(sp[t, :ns[t]], osp)
+        np.testing.assert_array_equal(ca[t, :nc[t]], oca)
+        np.testing.assert_array_equal(cd[t, :ns[t] + 1], ocd)
