@@ -125,3 +125,39 @@ def test_cref_emulated_golden(emu_exe, tmp_path, K):
     assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
     out = np.fromfile(tmp_path / "o_cref.bin", np.uint64).reshape(-1, W(K))
     np.testing.assert_array_equal(out, g[pre + "cref"])
+
+
+def test_cref_emulated_bench_setting(emu_exe, tmp_path):
+    """K = 4096 of the 5,000 cfg1 reference haplotypes with the oracle's own
+    best haplotypes and split sites of cfg1 targets (16 CTAs per target)."""
+    from eimp_b200 import synth
+    from oracle import restate as R
+    panel, groups = synth.generate("cfg1")
+    tg = groups[0]
+    hm, sm, cm = synth.typed_views(panel, tg.typed)
+    gt = np.ascontiguousarray(tg.gt[:2], np.uint8)
+    ntgt, M = gt.shape
+    K = 4096
+    bh, sp = [], []
+    for t in range(ntgt):
+        b, _ = R.besthaps(gt[t], hm, K)
+        bh.append(b)
+        sp.append(R.calllocs(gt[t], R.monos(hm, M, b), cm)[0])
+    nsp = np.array([len(s) for s in sp], np.int32)
+    rowoff = np.concatenate([[0], np.cumsum(2 * nsp + 1)]).astype(np.int64)
+    splits = np.zeros((ntgt, M), np.int32)
+    for t, s in enumerate(sp):
+        splits[t, :len(s)] = s
+    np.array([ntgt, M, panel.nhaps, K], np.int32).tofile(tmp_path / "params_i.bin")
+    gt.tofile(tmp_path / "gt.bin")
+    np.ascontiguousarray(hm).tofile(tmp_path / "hapmajor.bin")
+    np.stack(bh).astype(np.int32).tofile(tmp_path / "besthaps.bin")
+    splits.tofile(tmp_path / "splits.bin")
+    nsp.tofile(tmp_path / "nsplits.bin")
+    rowoff.tofile(tmp_path / "rowoff.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    out = np.fromfile(tmp_path / "o_cref.bin", np.uint64).reshape(-1, W(K))
+    for t in range(ntgt):
+        ocr, _ = R.cref(gt[t], sm, panel.nhaps, bh[t], sp[t])
+        np.testing.assert_array_equal(out[rowoff[t]:rowoff[t + 1]], ocr)

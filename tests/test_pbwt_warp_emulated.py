@@ -107,3 +107,36 @@ def test_pbwt_emulated_golden(emu_exe, tmp_path, K):
     out = np.fromfile(tmp_path / "o_pbwt.bin", np.uint32).reshape(-1, kw)
     np.testing.assert_array_equal(out, g[pre + "pbwt"])
     np.testing.assert_array_equal(np.fromfile(tmp_path / "o_count0.bin", np.int32), g[pre + "count0"])
+
+
+def test_pbwt_emulated_bench_setting(emu_exe, tmp_path):
+    """K = 4096: the oracle's condensed references of two cfg1 targets (the
+    rows the bench's PBWT sweep sees), forward and backward, against the
+    oracle's PBWTs."""
+    from eimp_b200 import synth
+    from oracle import restate as R
+    panel, groups = synth.generate("cfg1")
+    tg = groups[0]
+    hm, sm, cm = synth.typed_views(panel, tg.typed)
+    K = 4096
+    crefs = []
+    for t in range(2):
+        b, _ = R.besthaps(tg.gt[t], hm, K)
+        sp = R.calllocs(tg.gt[t], R.monos(hm, len(tg.typed), b), cm)[0]
+        crefs.append(R.cref(tg.gt[t], sm, panel.nhaps, b, sp)[0])
+    nrows = [len(c) for c in crefs]
+    rowoff = np.concatenate([[0], np.cumsum(nrows)]).astype(np.int64)
+    kw = 2 * ((K + 31) // 32)
+    np.array([len(nrows), K, kw, 1, 1], np.int32).tofile(tmp_path / "params_i.bin")
+    rowoff.tofile(tmp_path / "rowoff.bin")
+    np.ascontiguousarray(np.concatenate(crefs)).tofile(tmp_path / "cref.bin")
+    r = subprocess.run([emu_exe, str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, f"rc {r.returncode}: {r.stderr[-4000:]}"
+    out = np.fromfile(tmp_path / "o_pbwt.bin", np.uint32).reshape(-1, kw)
+    c0 = np.fromfile(tmp_path / "o_count0.bin", np.int32)
+    for t, cr in enumerate(crefs):
+        r0, n = int(rowoff[t]), nrows[t]
+        fwd, fc0 = R.pbwt(cr, K)[:2]
+        np.testing.assert_array_equal(out[2 * r0:2 * r0 + n], fwd)
+        np.testing.assert_array_equal(out[2 * r0 + n:2 * r0 + 2 * n], R.pbwt(cr, K, reverse=True)[0])
+        np.testing.assert_array_equal(c0[r0:r0 + n], fc0)
